@@ -1,0 +1,198 @@
+// C ABI entry points: validation, dispatch by precision, device queries.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "scene_internal.h"
+
+namespace ac {
+
+std::string &last_error_slot() {
+    static thread_local std::string slot;
+    return slot;
+}
+
+int device_sm_count(int device) {
+    static std::mutex mu;
+    static std::vector<int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    if (device >= static_cast<int>(cache.size())) cache.resize(device + 1, 0);
+    if (cache[device] == 0) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms < 1) sms = 1;
+        cache[device] = sms;
+    }
+    return cache[device];
+}
+
+double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p) {
+    const double R = static_cast<double>(std::max<int64_t>(1, p->num_rays));
+    const double B = static_cast<double>(std::max<int32_t>(1, p->num_bounces));
+    const double ray_scale = (4.0 * kPi) / R;
+    const double imd = std::max(p->irradiance_min_distance, 1e-3);
+    const double distance_term = 1.0 / (4.0 * kPi * imd * imd);
+    const double w = p->dipole_weight;
+    const double gain = std::pow(std::max(1.0, std::fabs(1.0 - 2.0 * w)), std::max(0.0, p->dipole_power));
+    const double s_hi = std::max({1.0, std::fabs(scene->max_scattering), std::fabs(scene->min_scattering)});
+    const double lobe = s_hi / kPi + (std::max(0.0, p->specular_exponent) + 2.0) / (8.0 * kPi) *
+                                         std::max(1.0, std::fabs(1.0 - scene->min_scattering));
+    const double growth = std::min(1e300, std::pow(std::max(1.0, scene->max_reflection), B + 1.0));
+    const double max_deposit = ray_scale * gain * distance_term * lobe * growth;
+    const double budget = 6.0 * R * B * max_deposit;
+    int exponent = static_cast<int>(std::floor(std::log2(std::ldexp(1.0, 62) / budget)));
+    exponent = std::min(100, std::max(-60, exponent));
+    return std::ldexp(1.0, exponent);
+}
+
+int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o) {
+    if (!scene || !p || !o) return fail(AC_ERR_INVALID, "ac_trace: null argument");
+    if (p->num_rays < 1 || p->num_rays > 0x7FFFFFFF) return fail(AC_ERR_INVALID, "num_rays must be in [1, 2^31)");
+    if (p->num_bounces < 0 || p->num_bounces > 0xFFFFFE) return fail(AC_ERR_INVALID, "num_bounces must be in [0, 2^24-1)");
+    if (p->num_bins < 1) return fail(AC_ERR_INVALID, "num_bins must be positive");
+    if (!(p->bin_duration > 0.0) || !(p->speed_of_sound > 0.0))
+        return fail(AC_ERR_INVALID, "bin duration and speed of sound must be positive");
+    const double values[] = {p->source[0], p->source[1], p->source[2], p->listener[0], p->listener[1], p->listener[2],
+                             p->source_forward[0], p->source_forward[1], p->source_forward[2], p->max_path_length,
+                             p->direct_delay, p->listener_radius, p->source_radius, p->irradiance_min_distance,
+                             p->specular_exponent, p->dipole_weight, p->dipole_power};
+    for (double v : values)
+        if (!std::isfinite(v)) return fail(AC_ERR_INVALID, "trace parameters must be finite");
+    if (p->precision != AC_PRECISION_FP32 && p->precision != AC_PRECISION_FP64)
+        return fail(AC_ERR_INVALID, "precision must be AC_PRECISION_FP32 or AC_PRECISION_FP64");
+    if (p->rng_mode != AC_RNG_REFERENCE && p->rng_mode != AC_RNG_PHILOX)
+        return fail(AC_ERR_INVALID, "rng_mode must be AC_RNG_REFERENCE or AC_RNG_PHILOX");
+    if (p->rng_mode == AC_RNG_REFERENCE && (!p->directions || (p->num_bounces > 0 && (!p->diffuse_random || !p->diffuse_indices))))
+        return fail(AC_ERR_INVALID, "reference-stream mode needs directions, diffuse_random and diffuse_indices");
+    if (p->num_bounces > 0 && (p->num_bank < 1 || !p->diffuse_bank))
+        return fail(AC_ERR_INVALID, "diffuse sample bank is required");
+    if (!o->echogram_fx || !o->hit_counts || !o->contrib_counts || !o->surface_energy_fx || !o->counters)
+        return fail(AC_ERR_INVALID, "echogram, per-surface and counter outputs are required");
+    if (p->render_ambisonics && !o->ambisonic_fx)
+        return fail(AC_ERR_INVALID, "render_ambisonics needs the ambisonic accumulator");
+    if (p->energy_scale < 0.0 || !std::isfinite(p->energy_scale))
+        return fail(AC_ERR_INVALID, "energy_scale must be zero (automatic) or positive");
+    return AC_OK;
+}
+
+template <typename T>
+__global__ void philox_workspace_kernel(uint64_t seed, uint64_t key, int64_t R, int32_t B, int32_t K, T *dirs, T *random,
+                                        int32_t *indices) {
+    Job<T> job{};
+    job.rng_mode = 1;
+    job.seed = seed;
+    job.stream_key = key;
+    job.num_rays = R;
+    for (int64_t ri = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; ri < R;
+         ri += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        T d[3];
+        initial_direction(job, ri, d);
+        dirs[3 * ri] = d[0];
+        dirs[3 * ri + 1] = d[1];
+        dirs[3 * ri + 2] = d[2];
+        for (int32_t b = 0; b < B; ++b) {
+            const u32x4 r = trace_draw(seed, key, static_cast<uint32_t>(ri), static_cast<uint32_t>(b) + 1u);
+            random[static_cast<size_t>(b) * R + ri] = static_cast<T>(u01_53(r.x, r.y));
+            indices[static_cast<size_t>(b) * R + ri] = static_cast<int32_t>(below(r.z, static_cast<uint32_t>(K)));
+        }
+    }
+}
+
+}  // namespace ac
+
+extern "C" {
+
+const char *ac_last_error(void) { return ac::last_error_slot().c_str(); }
+
+int ac_abi_version(void) { return AC_ABI_VERSION; }
+
+int ac_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major, int32_t *cc_minor, int32_t *sm_count) {
+    cudaDeviceProp prop;
+    AC_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (name && name_len) {
+        std::strncpy(name, prop.name, name_len - 1);
+        name[name_len - 1] = '\0';
+    }
+    if (cc_major) *cc_major = prop.major;
+    if (cc_minor) *cc_minor = prop.minor;
+    if (sm_count) *sm_count = prop.multiProcessorCount;
+    return AC_OK;
+}
+
+int ac_energy_scale(ac_scene_t scene, const ac_trace_params *params, double *scale) {
+    if (!scene || !params || !scale) return ac::fail(AC_ERR_INVALID, "ac_energy_scale: null argument");
+    *scale = params->energy_scale > 0.0 ? params->energy_scale : ac::choose_energy_scale(scene, params);
+    return AC_OK;
+}
+
+int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_outputs *outputs, void *stream) {
+    int rc = ac::validate_trace(scene, params, outputs);
+    if (rc != AC_OK) return rc;
+    const double scale = params->energy_scale > 0.0 ? params->energy_scale : ac::choose_energy_scale(scene, params);
+    if (outputs->scale_out) *outputs->scale_out = scale;
+    if (params->precision == AC_PRECISION_FP64) return ac::launch_trace_f64(scene, params, outputs, scale, stream);
+    return ac::launch_trace_f32(scene, params, outputs, scale, stream);
+}
+
+int ac_batch_workspace_size(int32_t num_jobs, const ac_batch_config *config, size_t *bytes) {
+    (void)config;
+    if (num_jobs < 0 || !bytes) return ac::fail(AC_ERR_INVALID, "ac_batch_workspace_size: bad argument");
+    // Enough for either precision; the two partitions of a mixed batch run back to back.
+    *bytes = std::max(ac::batch_workspace_bytes_f32(num_jobs), ac::batch_workspace_bytes_f64(num_jobs));
+    return AC_OK;
+}
+
+int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
+                   size_t workspace_bytes, void *host_staging, void *stream) {
+    if (num_jobs < 0 || (num_jobs > 0 && (!jobs || !workspace)))
+        return ac::fail(AC_ERR_INVALID, "ac_trace_batch: bad argument");
+    std::vector<int32_t> f32, f64;
+    for (int32_t j = 0; j < num_jobs; ++j) {
+        const int rc = ac::validate_trace(jobs[j].scene, &jobs[j].params, &jobs[j].outputs);
+        if (rc != AC_OK) return ac::fail(rc, "job %d: %s", j, ac_last_error());
+        (jobs[j].params.precision == AC_PRECISION_FP64 ? f64 : f32).push_back(j);
+    }
+    if (!f32.empty() && !f64.empty()) {
+        // Both partitions share the workspace, so the second must wait for the first.
+        int rc = ac::launch_batch_f32(jobs, f32.data(), static_cast<int32_t>(f32.size()), config, workspace,
+                                      workspace_bytes, host_staging, stream);
+        if (rc != AC_OK) return rc;
+        AC_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+        return ac::launch_batch_f64(jobs, f64.data(), static_cast<int32_t>(f64.size()), config, workspace,
+                                    workspace_bytes, host_staging, stream);
+    }
+    if (!f64.empty())
+        return ac::launch_batch_f64(jobs, f64.data(), static_cast<int32_t>(f64.size()), config, workspace,
+                                    workspace_bytes, host_staging, stream);
+    if (!f32.empty())
+        return ac::launch_batch_f32(jobs, f32.data(), static_cast<int32_t>(f32.size()), config, workspace,
+                                    workspace_bytes, host_staging, stream);
+    return AC_OK;
+}
+
+int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces, int32_t num_bank,
+                        int32_t precision, void *directions, void *random, int32_t *indices, void *stream) {
+    if (num_rays < 1 || num_rays > 0x7FFFFFFF || num_bounces < 0 || num_bank < 1 || !directions ||
+        (num_bounces > 0 && (!random || !indices)))
+        return ac::fail(AC_ERR_INVALID, "ac_philox_workspace: bad argument");
+    const int block = 256;
+    const int grid = static_cast<int>(std::min<int64_t>((num_rays + block - 1) / block, 4096));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (precision == AC_PRECISION_FP64)
+        ac::philox_workspace_kernel<double><<<grid, block, 0, s>>>(seed, stream_key, num_rays, num_bounces, num_bank,
+                                                                   static_cast<double *>(directions),
+                                                                   static_cast<double *>(random), indices);
+    else
+        ac::philox_workspace_kernel<float><<<grid, block, 0, s>>>(seed, stream_key, num_rays, num_bounces, num_bank,
+                                                                  static_cast<float *>(directions),
+                                                                  static_cast<float *>(random), indices);
+    AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}
+
+}  // extern "C"

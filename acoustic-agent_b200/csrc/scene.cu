@@ -1,0 +1,265 @@
+// Scene upload: the reference's float64 surface SoA (steam_rt.py:834-924) is
+// validated, given a BVH if it has none (bvh.py:8-77 restated in
+// bvh_build.cpp), and packed into 16-byte aligned quads, once in float32 for
+// the production kernel and once in float64 for the parity kernel.  One device
+// allocation per precision; the handle owns both.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "scene_internal.h"
+
+namespace {
+
+template <typename T>
+inline T tag_value(int tag);
+template <>
+inline float tag_value<float>(int tag) {
+    float f;
+    std::memcpy(&f, &tag, sizeof(f));
+    return f;
+}
+template <>
+inline double tag_value<double>(int tag) { return static_cast<double>(tag); }
+
+struct Offsets {
+    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, total;  // in elements
+};
+
+inline size_t round4(size_t v) { return (v + 3) & ~static_cast<size_t>(3); }
+
+Offsets layout(size_t S, size_t P, size_t N, size_t C) {
+    Offsets o{};
+    size_t off = 0;
+    o.prims_linear = off; off += round4(S * ac::kPrimStride);
+    o.prims_leaf = off;   off += round4(P * ac::kPrimStride);
+    o.nodes = off;        off += round4(N * ac::kNodeStride);
+    o.mats = off;         off += round4(S * ac::kMatStride);
+    o.corners = off;      off += round4(C * 2);
+    o.normals = off;      off += round4(S * 3);
+    o.total = off;
+    return o;
+}
+
+template <typename T>
+void pack_record(const ac_scene_desc *d, int64_t si, T *rec) {
+    std::fill(rec, rec + ac::kPrimStride, T(0));
+    const int kind = static_cast<int>(d->kinds[si]);
+    if (kind == AC_KIND_WALL) {
+        rec[0] = T(d->wall_a[2 * si]);
+        rec[1] = T(d->wall_a[2 * si + 1]);
+        rec[2] = T(d->wall_delta[2 * si]);
+        rec[3] = T(d->wall_delta[2 * si + 1]);
+        rec[4] = T(d->wall_z[2 * si]);
+        rec[5] = T(d->wall_z[2 * si + 1]);
+        rec[6] = T(d->normals[3 * si]);
+        rec[7] = T(d->normals[3 * si + 1]);
+        rec[8] = T(d->normals[3 * si + 2]);
+    } else if (kind == AC_KIND_BOX) {
+        rec[0] = T(d->box_center[2 * si]);
+        rec[1] = T(d->box_center[2 * si + 1]);
+        rec[2] = T(d->box_axis_u[2 * si]);
+        rec[3] = T(d->box_axis_u[2 * si + 1]);
+        rec[4] = T(d->box_axis_v[2 * si]);
+        rec[5] = T(d->box_axis_v[2 * si + 1]);
+        rec[6] = T(d->box_half[2 * si]);
+        rec[7] = T(d->box_half[2 * si + 1]);
+        rec[8] = T(d->box_z[2 * si]);
+        rec[9] = T(d->box_z[2 * si + 1]);
+    } else {
+        rec[0] = T(d->z_values[si]);
+        rec[1] = T(d->normals[3 * si]);
+        rec[2] = T(d->normals[3 * si + 1]);
+        rec[3] = T(d->normals[3 * si + 2]);
+    }
+    rec[11] = tag_value<T>(static_cast<int>(si) * 4 + kind);
+}
+
+template <typename T>
+int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, ac_scene_s *s, void **storage, size_t *bytes,
+                    ac::SceneDev<T> *view) {
+    const size_t S = static_cast<size_t>(d->num_surfaces);
+    const size_t N = static_cast<size_t>(bvh.node_count);
+    const size_t P = S;
+    const size_t C = static_cast<size_t>(d->num_corners);
+    const Offsets o = layout(S, P, N, C);
+    std::vector<T> host(o.total, T(0));
+    for (size_t si = 0; si < S; ++si) pack_record<T>(d, static_cast<int64_t>(si), host.data() + o.prims_linear + si * ac::kPrimStride);
+    for (size_t k = 0; k < P; ++k)
+        pack_record<T>(d, bvh.primitives[k], host.data() + o.prims_leaf + k * ac::kPrimStride);
+    for (size_t n = 0; n < N; ++n) {
+        T *np = host.data() + o.nodes + n * ac::kNodeStride;
+        for (int a = 0; a < 3; ++a) {
+            np[a] = T(bvh.bounds_min[3 * n + a]);
+            np[4 + a] = T(bvh.bounds_max[3 * n + a]);
+        }
+        np[3] = tag_value<T>(static_cast<int>(bvh.escape[n]));
+        const int64_t start = bvh.count[n] > 0 ? bvh.start[n] : 0;
+        np[7] = tag_value<T>(static_cast<int>(start | (bvh.count[n] << 24)));
+    }
+    for (size_t si = 0; si < S; ++si) {
+        T *m = host.data() + o.mats + si * ac::kMatStride;
+        for (int b = 0; b < 6; ++b) m[b] = T(d->reflection[6 * si + b]);
+        m[6] = T(d->scattering[si]);
+    }
+    for (size_t c = 0; c < 2 * C; ++c) host[o.corners + c] = T(d->corners[c]);
+    for (size_t k = 0; k < 3 * S; ++k) host[o.normals + k] = T(d->normals[k]);
+
+    *bytes = o.total * sizeof(T);
+    void *dev = nullptr;
+    cudaError_t err = cudaMalloc(&dev, *bytes);
+    if (err != cudaSuccess) return ac::fail(AC_ERR_NOMEM, "scene allocation of %zu bytes failed: %s", *bytes, cudaGetErrorString(err));
+    err = cudaMemcpy(dev, host.data(), *bytes, cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) {
+        cudaFree(dev);
+        return ac::fail(AC_ERR_CUDA, "scene upload failed: %s", cudaGetErrorString(err));
+    }
+    *storage = dev;
+    const T *base = static_cast<const T *>(dev);
+    view->prims_linear = base + o.prims_linear;
+    view->prims_leaf = base + o.prims_leaf;
+    view->nodes = base + o.nodes;
+    view->mats = base + o.mats;
+    view->corners = base + o.corners;
+    view->normals = base + o.normals;
+    view->num_surfaces = static_cast<int32_t>(S);
+    view->num_nodes = static_cast<int32_t>(N);
+    view->num_corners = static_cast<int32_t>(C);
+    view->num_leaf_prims = static_cast<int32_t>(P);
+    (void)s;
+    return AC_OK;
+}
+
+bool finite_all(const double *p, size_t n) {
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+}  // namespace
+
+extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
+    if (!d || !out) return ac::fail(AC_ERR_INVALID, "ac_scene_create: null argument");
+    *out = nullptr;
+    const int64_t S = d->num_surfaces;
+    if (S < 1) return ac::fail(AC_ERR_INVALID, "scene needs at least one surface");
+    if (S >= (1 << 22)) return ac::fail(AC_ERR_CAPACITY, "scene has %lld surfaces; the limit is 4194303", (long long)S);
+    if (!d->kinds || !d->wall_a || !d->wall_delta || !d->wall_z || !d->z_values || !d->box_center || !d->box_axis_u ||
+        !d->box_axis_v || !d->box_half || !d->box_z || !d->normals || !d->reflection || !d->scattering)
+        return ac::fail(AC_ERR_INVALID, "scene description has a null surface array");
+    bool has_horizontal = false;
+    for (int64_t i = 0; i < S; ++i) {
+        if (d->kinds[i] < 0 || d->kinds[i] > 2) return ac::fail(AC_ERR_INVALID, "surface %lld has unknown kind %lld", (long long)i, (long long)d->kinds[i]);
+        has_horizontal |= d->kinds[i] == AC_KIND_HORIZONTAL;
+    }
+    if (has_horizontal && (d->num_corners < 3 || !d->corners))
+        return ac::fail(AC_ERR_INVALID, "horizontal surfaces need a room polygon of at least 3 corners");
+    const size_t s2 = 2 * static_cast<size_t>(S);
+    if (!finite_all(d->wall_a, s2) || !finite_all(d->wall_delta, s2) || !finite_all(d->wall_z, s2) ||
+        !finite_all(d->z_values, S) || !finite_all(d->box_center, s2) || !finite_all(d->box_axis_u, s2) ||
+        !finite_all(d->box_axis_v, s2) || !finite_all(d->box_half, s2) || !finite_all(d->box_z, s2) ||
+        !finite_all(d->normals, 3 * S) || !finite_all(d->reflection, 6 * S) || !finite_all(d->scattering, S) ||
+        (d->num_corners > 0 && !finite_all(d->corners, 2 * static_cast<size_t>(d->num_corners))))
+        return ac::fail(AC_ERR_INVALID, "scene arrays must be finite");
+
+    // BVH: given, or built here from the padded surface bounds.
+    std::vector<double> bmin, bmax;
+    std::vector<int64_t> bstart, bcount, besc, bprims;
+    ac_bvh bvh{};
+    if (d->bvh_node_count > 0) {
+        if (!d->bvh_bounds_min || !d->bvh_bounds_max || !d->bvh_start || !d->bvh_count || !d->bvh_escape || !d->bvh_primitives)
+            return ac::fail(AC_ERR_INVALID, "BVH arrays missing");
+        bvh.bounds_min = const_cast<double *>(d->bvh_bounds_min);
+        bvh.bounds_max = const_cast<double *>(d->bvh_bounds_max);
+        bvh.start = const_cast<int64_t *>(d->bvh_start);
+        bvh.count = const_cast<int64_t *>(d->bvh_count);
+        bvh.escape = const_cast<int64_t *>(d->bvh_escape);
+        bvh.primitives = const_cast<int64_t *>(d->bvh_primitives);
+        bvh.node_count = d->bvh_node_count;
+        int64_t leaves = 0;
+        for (int64_t n = 0; n < d->bvh_node_count; ++n) leaves += d->bvh_count[n] > 0;
+        bvh.leaf_count = leaves;
+    } else {
+        if (!d->surface_bounds_min || !d->surface_bounds_max)
+            return ac::fail(AC_ERR_INVALID, "surface bounds required to build the BVH");
+        const size_t cap = 2 * static_cast<size_t>(S);
+        bmin.resize(3 * cap); bmax.resize(3 * cap); bstart.resize(cap); bcount.resize(cap); besc.resize(cap); bprims.resize(S);
+        bvh.bounds_min = bmin.data(); bvh.bounds_max = bmax.data(); bvh.start = bstart.data(); bvh.count = bcount.data();
+        bvh.escape = besc.data(); bvh.primitives = bprims.data();
+        const int rc = ac_bvh_build(d->surface_bounds_min, d->surface_bounds_max, S, 4, &bvh);
+        if (rc != AC_OK) return rc;
+    }
+    // Structural checks: the kernel walks escape links and reads leaf slots.
+    int32_t max_leaf = 0;
+    for (int64_t n = 0; n < bvh.node_count; ++n) {
+        if (bvh.escape[n] <= n || bvh.escape[n] > bvh.node_count)
+            return ac::fail(AC_ERR_INVALID, "BVH node %lld has an invalid escape link", (long long)n);
+        if (bvh.count[n] < 0 || bvh.count[n] > 255)
+            return ac::fail(AC_ERR_INVALID, "BVH leaf %lld holds %lld primitives (limit 255)", (long long)n, (long long)bvh.count[n]);
+        if (bvh.count[n] > 0 && (bvh.start[n] < 0 || bvh.start[n] + bvh.count[n] > S || bvh.start[n] >= (1 << 24)))
+            return ac::fail(AC_ERR_INVALID, "BVH leaf %lld addresses primitives out of range", (long long)n);
+        max_leaf = std::max<int32_t>(max_leaf, static_cast<int32_t>(bvh.count[n]));
+        if (!std::isfinite(bvh.bounds_min[3 * n]) || !std::isfinite(bvh.bounds_max[3 * n]))
+            return ac::fail(AC_ERR_INVALID, "BVH bounds must be finite");
+    }
+    for (int64_t k = 0; k < S; ++k)
+        if (bvh.primitives[k] < 0 || bvh.primitives[k] >= S)
+            return ac::fail(AC_ERR_INVALID, "BVH primitive slot %lld references surface %lld", (long long)k, (long long)bvh.primitives[k]);
+
+    int ndev = 0;
+    AC_CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (d->device < 0 || d->device >= ndev) return ac::fail(AC_ERR_UNSUPPORTED, "CUDA device %d is not available", d->device);
+    AC_CUDA_TRY(cudaSetDevice(d->device));
+
+    ac_scene_s *s = new (std::nothrow) ac_scene_s();
+    if (!s) return ac::fail(AC_ERR_NOMEM, "out of host memory");
+    s->device = d->device;
+    s->num_surfaces = S;
+    s->num_corners = d->num_corners;
+    s->node_count = bvh.node_count;
+    s->leaf_count = bvh.leaf_count;
+    s->max_leaf = max_leaf;
+    s->max_reflection = 0.0;
+    s->max_scattering = -1e300;
+    s->min_scattering = 1e300;
+    for (int64_t i = 0; i < 6 * S; ++i) s->max_reflection = std::max(s->max_reflection, std::fabs(d->reflection[i]));
+    for (int64_t i = 0; i < S; ++i) {
+        s->max_scattering = std::max(s->max_scattering, d->scattering[i]);
+        s->min_scattering = std::min(s->min_scattering, d->scattering[i]);
+    }
+    int rc = pack_and_upload<float>(d, bvh, s, &s->storage_f32, &s->bytes_f32, &s->f32);
+    if (rc == AC_OK) rc = pack_and_upload<double>(d, bvh, s, &s->storage_f64, &s->bytes_f64, &s->f64);
+    if (rc != AC_OK) {
+        if (s->storage_f32) cudaFree(s->storage_f32);
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return AC_OK;
+}
+
+extern "C" int ac_scene_destroy(ac_scene_t s) {
+    if (!s) return AC_OK;
+    cudaSetDevice(s->device);
+    if (s->storage_f32) cudaFree(s->storage_f32);
+    if (s->storage_f64) cudaFree(s->storage_f64);
+    delete s;
+    return AC_OK;
+}
+
+extern "C" int ac_scene_get_info(ac_scene_t s, ac_scene_info *info) {
+    if (!s || !info) return ac::fail(AC_ERR_INVALID, "ac_scene_get_info: null argument");
+    info->num_surfaces = s->num_surfaces;
+    info->num_corners = s->num_corners;
+    info->node_count = s->node_count;
+    info->leaf_count = s->leaf_count;
+    info->device_bytes = static_cast<int64_t>(s->bytes_f32 + s->bytes_f64);
+    info->device = s->device;
+    info->max_leaf = s->max_leaf;
+    return AC_OK;
+}

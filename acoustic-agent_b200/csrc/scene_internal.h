@@ -1,0 +1,59 @@
+// Device-resident scene: the surface SoA packed into 16-byte aligned quads,
+// one copy per precision, plus the host-side facts the launchers need.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "acoustic_rt.h"
+#include "trace_kernel.cuh"
+
+struct ac_scene_s {
+    int32_t device = 0;
+    int64_t num_surfaces = 0;
+    int64_t num_corners = 0;
+    int64_t node_count = 0;
+    int64_t leaf_count = 0;
+    int32_t max_leaf = 0;
+    void *storage_f32 = nullptr;
+    void *storage_f64 = nullptr;
+    size_t bytes_f32 = 0;
+    size_t bytes_f64 = 0;
+    ac::SceneDev<float> f32{};
+    ac::SceneDev<double> f64{};
+    double max_reflection = 0.0;   // bound used when choosing the fixed-point scale
+    double max_scattering = 0.0;
+    double min_scattering = 0.0;
+};
+
+namespace ac {
+
+template <typename T>
+inline const SceneDev<T> &scene_view(const ac_scene_s *s);
+template <>
+inline const SceneDev<float> &scene_view<float>(const ac_scene_s *s) { return s->f32; }
+template <>
+inline const SceneDev<double> &scene_view<double>(const ac_scene_s *s) { return s->f64; }
+
+// Power-of-two fixed-point scale such that no echogram bin, ambisonic bin or
+// per-surface energy accumulator can exceed 2^62 in magnitude.
+double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p);
+
+// Validates trace parameters against a scene (host-side, before any launch).
+int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o);
+
+int device_sm_count(int device);
+
+// Per-precision launchers (trace_f32.cu / trace_f64.cu).
+int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o, double scale,
+                     void *stream);
+int launch_trace_f64(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o, double scale,
+                     void *stream);
+int launch_batch_f32(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg,
+                     void *workspace, size_t bytes, void *host_staging, void *stream);
+int launch_batch_f64(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg,
+                     void *workspace, size_t bytes, void *host_staging, void *stream);
+size_t batch_workspace_bytes_f32(int32_t count);
+size_t batch_workspace_bytes_f64(int32_t count);
+
+}  // namespace ac

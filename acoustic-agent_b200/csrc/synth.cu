@@ -1,0 +1,216 @@
+// Echogram -> six band impulse responses on the GPU.
+//
+// Restates acoustic_agent/steam_rt.py:2205-2232 (reconstruct_band_irs) and
+// :3070-3083 + :4131-4212 (bandlimit_band_signals, _band_limit, the biquad
+// recursion) so that, given the same float32 echogram and noise, every output
+// sample is bit-identical to the reference.  This file is compiled with
+// -fmad=false: the reference evaluates each multiply and add separately in
+// float64, and each biquad section hands its successor a float32-rounded signal.
+//
+// The recursion is sequential in time, so parallelism comes from elsewhere:
+// one warp is a systolic array of 8 four-section low-pass chains.  Lane
+// (unit, chain, stage) runs one biquad section; each iteration it passes its
+// float32 output one lane up, so section s works on sample n-s while section
+// s+1 works on sample n-s-1.  A "unit" is one band of one RIR: bands 1-4 need
+// two chains (the low-pass at the upper and lower crossover, subtracted),
+// bands 0 and 5 one.  Four units per warp.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "philox.cuh"
+
+namespace ac {
+namespace {
+
+constexpr int kSynthBands = 6;
+constexpr double kSynthPi = 3.141592653589793;
+
+struct SynthArgs {
+    double crossover[100];
+    double air_coefficients[6];
+    double speed_of_sound;
+    int32_t num_rirs;
+    int32_t num_bins;
+    int32_t spb;
+    int32_t sample_rate;
+};
+
+inline size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
+
+struct SynthLayout {
+    size_t amps, air, wtab, white, total;
+};
+
+SynthLayout synth_layout(const ac_synth_params *p) {
+    const size_t cells = static_cast<size_t>(p->num_rirs) * kSynthBands * p->num_bins;
+    const size_t N = static_cast<size_t>(p->num_bins) * p->samples_per_bin;
+    SynthLayout l{};
+    size_t off = 0;
+    l.amps = off; off = align256(off + cells * sizeof(double));
+    l.air = off;  off = align256(off + (p->air ? 0 : cells * sizeof(double)));
+    l.wtab = off; off = align256(off + static_cast<size_t>(p->samples_per_bin) * sizeof(double));
+    l.white = off; off = align256(off + (p->rng_mode == AC_RNG_PHILOX ? N * sizeof(double) : 0));
+    l.total = off;
+    return l;
+}
+
+// Envelope amplitudes, air gains, interpolation weights and (Philox mode) noise.
+__global__ void synth_prepare_kernel(const float *echo, const double *direct_delays, const __grid_constant__ SynthArgs a,
+                                     double *amps, double *air, double *wtab, double *white, uint64_t seed) {
+    const size_t cells = static_cast<size_t>(a.num_rirs) * kSynthBands * a.num_bins;
+    const size_t N = static_cast<size_t>(a.num_bins) * a.spb;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < cells; i += stride) {
+        // numpy keeps a float32 echogram in float32: clip, divide by float32(4pi), sqrt.
+        const float e = echo[i];
+        const float cl = e > 0.0f ? e : 0.0f;
+        const float amp = sqrtf(cl / static_cast<float>(4.0 * kSynthPi));
+        amps[i] = e < static_cast<float>(1e-9) ? 0.0 : static_cast<double>(amp);
+        if (air) {
+            const int bin = static_cast<int>(i % a.num_bins);
+            const int band = static_cast<int>((i / a.num_bins) % kSynthBands);
+            const int j = static_cast<int>(i / (static_cast<size_t>(a.num_bins) * kSynthBands));
+            // steam_rt.py:2196-2198, path time at the bin centre
+            const double t = direct_delays[j] + ((static_cast<double>(bin) + 0.5) * a.spb) / a.sample_rate;
+            const double dist = (t > 0.0 ? t : 0.0) * (a.speed_of_sound > 0.0 ? a.speed_of_sound : 0.0);
+            const double coeff = a.air_coefficients[band] > 0.0 ? a.air_coefficients[band] : 0.0;
+            air[i] = exp(-coeff * dist);
+        }
+    }
+    for (size_t k = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; k < static_cast<size_t>(a.spb); k += stride)
+        wtab[k] = static_cast<double>(k) / static_cast<double>(a.spb);
+    if (white) {
+        for (size_t n = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; n < N; n += stride) {
+            const u32x4 r = noise_draw(seed, static_cast<uint32_t>(n >> 1));
+            const double u = (n & 1) ? u01_53(r.z, r.w) : u01_53(r.x, r.y);
+            white[n] = -1.0 + 2.0 * u;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128) synth_filter_kernel(const double *amps, const double *air, const double *wtab,
+                                                           const double *white, size_t white_stride,
+                                                           const __grid_constant__ SynthArgs a, float *out) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
+    const int stage = lane & 3;
+    const int chain = (lane >> 2) & 1;
+    const int unit = warp * 4 + (lane >> 3);
+    const int units = a.num_rirs * kSynthBands;
+    const bool valid_unit = unit < units;
+    const int j = valid_unit ? unit / kSynthBands : 0;
+    const int band = valid_unit ? unit % kSynthBands : 0;
+    int cutoff;
+    bool active;
+    if (band == 0) { cutoff = 0; active = chain == 0; }
+    else if (band == kSynthBands - 1) { cutoff = 4; active = chain == 0; }
+    else { cutoff = chain == 0 ? band : band - 1; active = true; }
+    active = active && valid_unit;
+    const double *co = a.crossover + cutoff * 20 + stage * 5;
+    const double b0 = co[0], b1 = co[1], b2 = co[2], a1 = co[3], a2 = co[4];
+    double x1 = 0.0, x2 = 0.0, y1 = 0.0, y2 = 0.0;
+
+    const int N = a.num_bins * a.spb;
+    const size_t row = (static_cast<size_t>(j) * kSynthBands + band) * a.num_bins;
+    const double *white_row = white + static_cast<size_t>(j) * white_stride;
+    float *out_row = out + (static_cast<size_t>(j) * kSynthBands + band) * static_cast<size_t>(N);
+
+    float carry_y = 0.0f;
+    double carry_x = 0.0;
+    int bin = 0, k = 0;  // sample `it` = bin * spb + k for the section-0 lanes
+    for (int it = 0; it < N + 3; ++it) {
+        const float from_prev = __shfl_up_sync(full, carry_y, 1);
+        const double x_prev = __shfl_up_sync(full, carry_x, 1);
+        double x_new = 0.0;
+        if (valid_unit && it < N) {
+            // steam_rt.py:2221-2230: interpolated envelope * air gain * noise
+            const double w = __ldg(wtab + k);
+            const double cur = __ldg(amps + row + bin);
+            const double prev = bin == 0 ? cur : __ldg(amps + row + bin - 1);
+            double seg = (1.0 - w) * prev + w * cur;
+            seg = seg * __ldg(air + row + bin);
+            x_new = seg * __ldg(white_row + it);
+        }
+        if (++k == a.spb) { k = 0; ++bin; }
+        const double in = stage == 0 ? x_new : static_cast<double>(from_prev);
+        const double x_orig = stage == 0 ? x_new : x_prev;
+        const int n = it - stage;
+        float y_f = 0.0f;
+        if (active && n >= 0 && n < N) {
+            const double y0 = b0 * in + b1 * x1 + b2 * x2 - a1 * y1 - a2 * y2;
+            y_f = static_cast<float>(y0);
+            x2 = x1; x1 = in;
+            y2 = y1; y1 = y0;
+        }
+        carry_y = y_f;
+        carry_x = x_orig;
+        const float lower = __shfl_down_sync(full, y_f, 4);
+        if (stage == 3 && chain == 0 && active && n >= 0 && n < N) {
+            float o;
+            if (band == 0) o = y_f;
+            else if (band == kSynthBands - 1) o = static_cast<float>(x_orig - static_cast<double>(y_f));
+            else o = y_f - lower;
+            out_row[n] = o;
+        }
+    }
+}
+
+}  // namespace
+}  // namespace ac
+
+extern "C" int ac_synth_workspace_size(const ac_synth_params *p, size_t *bytes) {
+    if (!p || !bytes) return ac::fail(AC_ERR_INVALID, "ac_synth_workspace_size: null argument");
+    if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1)
+        return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
+    *bytes = ac::synth_layout(p).total;
+    return AC_OK;
+}
+
+extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, float *band_irs, void *workspace,
+                             size_t workspace_bytes, void *stream_ptr) {
+    if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize: null argument");
+    if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
+        return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
+    const int64_t N = static_cast<int64_t>(p->num_bins) * p->samples_per_bin;
+    if (N + 3 > 0x7FFFFFFF) return ac::fail(AC_ERR_CAPACITY, "signal of %lld samples is too long", (long long)N);
+    if (p->rng_mode == AC_RNG_REFERENCE && !p->white) return ac::fail(AC_ERR_INVALID, "reference mode needs white noise");
+    if (!p->air && !p->direct_delays) return ac::fail(AC_ERR_INVALID, "need an air table or the direct delays");
+    if (p->num_rirs == 0) return AC_OK;
+    const ac::SynthLayout l = ac::synth_layout(p);
+    if (!workspace || workspace_bytes < l.total)
+        return ac::fail(AC_ERR_CAPACITY, "synthesis workspace too small: %zu < %zu", workspace_bytes, l.total);
+    ac::SynthArgs a;
+    std::memcpy(a.crossover, p->crossover, sizeof(a.crossover));
+    std::memcpy(a.air_coefficients, p->air_coefficients, sizeof(a.air_coefficients));
+    a.speed_of_sound = p->speed_of_sound;
+    a.num_rirs = p->num_rirs;
+    a.num_bins = p->num_bins;
+    a.spb = p->samples_per_bin;
+    a.sample_rate = p->sample_rate;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    double *amps = reinterpret_cast<double *>(ws + l.amps);
+    double *air = p->air ? nullptr : reinterpret_cast<double *>(ws + l.air);
+    double *wtab = reinterpret_cast<double *>(ws + l.wtab);
+    double *white = p->rng_mode == AC_RNG_PHILOX ? reinterpret_cast<double *>(ws + l.white) : nullptr;
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t cells = static_cast<size_t>(p->num_rirs) * 6 * p->num_bins;
+    const size_t work = std::max<size_t>(cells, static_cast<size_t>(white ? N : p->samples_per_bin));
+    const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, 8192));
+    ac::synth_prepare_kernel<<<grid, 256, 0, stream>>>(echograms, p->direct_delays, a, amps, air, wtab, white, p->seed);
+    AC_CUDA_TRY(cudaGetLastError());
+    const double *air_table = p->air ? p->air : air;
+    const double *noise = white ? white : p->white;
+    const size_t stride = (white || p->white_shared) ? 0 : static_cast<size_t>(N);
+    const int units = p->num_rirs * 6;
+    const int warps = (units + 3) / 4;
+    const int threads = 128;
+    const int blocks = (warps * 32 + threads - 1) / threads;
+    ac::synth_filter_kernel<<<blocks, threads, 0, stream>>>(amps, air_table, wtab, noise, stride, a, band_irs);
+    AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}

@@ -1,0 +1,63 @@
+"""Room-acoustic decay metrics on six-band echograms.
+
+Used to judge a trace against the float64 oracle when ray-by-ray identity is
+not expected (float32 arithmetic, or a different random stream):
+
+* EDC: Schroeder backward integral of bin energies, in dB re the total
+  (the reference's decay fits start from the same integral,
+  steam_rt.py:2727-2792 ``_schroeder_fit_rt60``);
+* T30: decay time from a least-squares line over -5 .. -35 dB, times 2;
+* EDT: same over 0 .. -10 dB, times 6;
+* C50: early-to-late energy ratio at 50 ms after the first arrival bin.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def edc_db(echogram: np.ndarray) -> np.ndarray:
+    """[bands, bins] energy decay curve in dB (0 dB at t=0; -inf after the last energy)."""
+    e = np.clip(np.asarray(echogram, dtype=np.float64), 0.0, None)
+    tail = np.cumsum(e[:, ::-1], axis=1)[:, ::-1]
+    total = tail[:, :1]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return 10.0 * np.log10(np.where(total > 0, tail / np.where(total > 0, total, 1.0), 0.0))
+
+
+def edc_error_db(a: np.ndarray, b: np.ndarray, range_db: float = 30.0) -> np.ndarray:
+    """Per-band max |EDC_a - EDC_b| over the bins where EDC_b >= -range_db."""
+    ea, eb = edc_db(a), edc_db(b)
+    out = np.zeros(ea.shape[0])
+    for band in range(ea.shape[0]):
+        mask = eb[band] >= -range_db
+        if np.any(mask):
+            out[band] = float(np.max(np.abs(ea[band, mask] - eb[band, mask])))
+    return out
+
+
+def _decay_time(edc: np.ndarray, bin_dur: float, hi_db: float, lo_db: float, factor: float) -> float:
+    t = (np.arange(edc.shape[0]) + 0.5) * bin_dur
+    mask = (edc <= hi_db) & (edc >= lo_db) & np.isfinite(edc)
+    if np.count_nonzero(mask) < 2:
+        return 0.0
+    slope = np.polyfit(t[mask], edc[mask], 1)[0]
+    return float(factor * (-10.0 / slope)) if slope < 0 else 0.0
+
+
+def t30(echogram: np.ndarray, bin_dur: float) -> np.ndarray:
+    e = edc_db(echogram)
+    return np.asarray([_decay_time(e[b], bin_dur, -5.0, -35.0, 6.0) for b in range(e.shape[0])])
+
+
+def edt(echogram: np.ndarray, bin_dur: float) -> np.ndarray:
+    e = edc_db(echogram)
+    return np.asarray([_decay_time(e[b], bin_dur, 0.0, -10.0, 6.0) for b in range(e.shape[0])])
+
+
+def c50(echogram: np.ndarray, bin_dur: float) -> np.ndarray:
+    e = np.clip(np.asarray(echogram, dtype=np.float64), 0.0, None)
+    k = max(1, int(round(0.05 / bin_dur)))
+    early = np.sum(e[:, :k], axis=1)
+    late = np.sum(e[:, k:], axis=1)
+    with np.errstate(divide="ignore"):
+        return 10.0 * np.log10(np.where(late > 0, early / np.where(late > 0, late, 1.0), np.inf))

@@ -1,0 +1,447 @@
+"""Device runtime: resident scenes, trace launches, band synthesis.
+
+PyTorch supplies device memory and streams; every computation runs in
+libacoustic_rt.so.  Nothing here falls back to the CPU: without a CUDA device
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from collections import OrderedDict
+from dataclasses import dataclass, field
+from threading import Lock
+from typing import Any, Mapping, Sequence
+
+import numpy as np
+import torch
+
+from acoustic_agent_b200 import _lib, bands, rng
+from acoustic_agent_b200.scene import SceneArrays
+
+NUM_BANDS = 6
+NUM_BANK = 128
+
+
+def require_cuda(device: int = 0) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 reflection backend needs a CUDA device; it has no CPU fallback")
+    if not 0 <= int(device) < torch.cuda.device_count():
+        raise RuntimeError(f"CUDA device {device} is not available")
+    return torch.device("cuda", int(device))
+
+
+def _f64(a: Any) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i64(a: Any) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(_lib.c_double_p)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(_lib.c_int64_p)
+
+
+def _stream_ptr(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+class DeviceScene:
+    """A scene uploaded with ac_scene_create; owns its device memory."""
+
+    def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0) -> None:
+        require_cuda(device)
+        a = arrays.arrays if isinstance(arrays, SceneArrays) else dict(arrays)
+        self.names: tuple[str, ...] = tuple(a["names"])
+        keep = {
+            "kinds": _i64(a["kinds"]), "wall_a": _f64(a["wall_a"]), "wall_delta": _f64(a["wall_delta"]),
+            "wall_z": _f64(a["wall_z"]), "z_values": _f64(a["z_values"]), "box_center": _f64(a["box_center"]),
+            "box_axis_u": _f64(a["box_axis_u"]), "box_axis_v": _f64(a["box_axis_v"]),
+            "box_half": _f64(a["box_half"]), "box_z": _f64(a["box_z"]), "normals": _f64(a["normals"]),
+            "reflection": _f64(a["reflection"]), "scattering": _f64(a["scattering"]),
+            "corners": _f64(np.asarray(a["corners"])[:, :2]), "bvh_bounds_min": _f64(a["bvh_bounds_min"]),
+            "bvh_bounds_max": _f64(a["bvh_bounds_max"]), "bvh_start": _i64(a["bvh_start"]),
+            "bvh_count": _i64(a["bvh_count"]), "bvh_escape": _i64(a["bvh_escape"]),
+            "bvh_primitives": _i64(a["bvh_primitives"]),
+        }
+        S = keep["kinds"].shape[0]
+        desc = _lib.ACSceneDesc()
+        desc.num_surfaces = S
+        desc.kinds = _ip(keep["kinds"])
+        for name in ("wall_a", "wall_delta", "wall_z", "z_values", "box_center", "box_axis_u", "box_axis_v",
+                     "box_half", "box_z", "normals", "reflection", "scattering", "corners"):
+            setattr(desc, name, _dp(keep[name]))
+        desc.num_corners = keep["corners"].shape[0]
+        desc.bvh_node_count = keep["bvh_start"].shape[0]
+        desc.bvh_bounds_min = _dp(keep["bvh_bounds_min"])
+        desc.bvh_bounds_max = _dp(keep["bvh_bounds_max"])
+        desc.bvh_start = _ip(keep["bvh_start"])
+        desc.bvh_count = _ip(keep["bvh_count"])
+        desc.bvh_escape = _ip(keep["bvh_escape"])
+        desc.bvh_primitives = _ip(keep["bvh_primitives"])
+        desc.device = int(device)
+        handle = ctypes.c_void_p()
+        _lib.check(_lib.load().ac_scene_create(ctypes.byref(desc), ctypes.byref(handle)), "ac_scene_create")
+        self.handle = handle
+        self.device = int(device)
+        self.num_surfaces = S
+        info = _lib.ACSceneInfo()
+        _lib.check(_lib.load().ac_scene_get_info(handle, ctypes.byref(info)), "ac_scene_get_info")
+        self.device_bytes = int(info.device_bytes)
+        self.node_count = int(info.node_count)
+        self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.load().ac_scene_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter teardown order varies
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class TraceSpec:
+    """Host-side description of one trace (the fields of ac_trace_params)."""
+
+    source: Sequence[float]
+    listener: Sequence[float]
+    num_rays: int
+    num_bounces: int
+    num_bins: int
+    bin_duration: float
+    speed_of_sound: float
+    max_path_length: float
+    direct_delay: float
+    source_forward: Sequence[float] = (1.0, 0.0, 0.0)
+    listener_radius: float = 0.1
+    source_radius: float = 0.1
+    irradiance_min_distance: float = 1.0
+    specular_exponent: float = 100.0
+    dipole_weight: float = 0.0
+    dipole_power: float = 1.0
+    use_bvh: bool = False
+    render_ambisonics: bool = False
+    precision: str = "float32"
+    rng: str = "philox"
+    seed: int = 1729
+    stream_key: int = 0
+    energy_scale: float = 0.0
+    block_size: int = 0
+    grid_blocks: int = 0
+
+    @property
+    def dtype(self) -> torch.dtype:
+        return torch.float64 if self.precision == "float64" else torch.float32
+
+
+class _StreamCache:
+    """Device copies of reference-stream workspaces (cf. steam_rt_cuda.py:229-261), LRU by bytes."""
+
+    def __init__(self, limit_bytes: int = 512 * 1024 * 1024) -> None:
+        self.limit = limit_bytes
+        self.entries: OrderedDict[tuple, tuple[torch.Tensor, ...]] = OrderedDict()
+        self.bytes = 0
+        self.hits = 0
+        self.misses = 0
+        self.lock = Lock()
+
+    def get(self, key: tuple, build) -> tuple[torch.Tensor, ...]:
+        with self.lock:
+            hit = self.entries.get(key)
+            if hit is not None:
+                self.entries.move_to_end(key)
+                self.hits += 1
+                return hit
+        value = build()
+        size = sum(t.numel() * t.element_size() for t in value)
+        with self.lock:
+            self.misses += 1
+            while self.entries and self.bytes + size > self.limit:
+                _, old = self.entries.popitem(last=False)
+                self.bytes -= sum(t.numel() * t.element_size() for t in old)
+            if size <= self.limit:
+                self.entries[key] = value
+                self.bytes += size
+        return value
+
+
+STREAMS = _StreamCache()
+
+
+def diffuse_bank(dtype: torch.dtype, device: torch.device) -> torch.Tensor:
+    key = ("bank", NUM_BANK, dtype, device.index)
+    return STREAMS.get(key, lambda: (torch.as_tensor(rng.diffuse_sample_bank(NUM_BANK), dtype=dtype, device=device),))[0]
+
+
+def reference_stream(spec: TraceSpec, device: torch.device) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+    key = ("stream", int(spec.num_rays), int(spec.num_bounces), NUM_BANK, int(spec.seed), spec.dtype, device.index)
+
+    def build():
+        directions = rng.sphere_samples(spec.num_rays, spec.seed)
+        random_values, indices = rng.diffuse_random_sequence(spec.num_rays, spec.num_bounces, NUM_BANK, spec.seed)
+        return (torch.as_tensor(directions, dtype=spec.dtype, device=device),
+                torch.as_tensor(random_values, dtype=spec.dtype, device=device),
+                torch.as_tensor(np.ascontiguousarray(indices), dtype=torch.int32, device=device))
+
+    return STREAMS.get(key, build)
+
+
+@dataclass
+class TraceBuffers:
+    """Device outputs of one trace."""
+
+    echogram_fx: torch.Tensor
+    hit_counts: torch.Tensor
+    contrib_counts: torch.Tensor
+    surface_energy_fx: torch.Tensor
+    counters: torch.Tensor
+    echogram: torch.Tensor
+    surface_energy: torch.Tensor
+    ambisonic_fx: torch.Tensor | None = None
+    ambisonic: torch.Tensor | None = None
+    ray_surfaces: torch.Tensor | None = None
+    scale: ctypes.c_double = field(default_factory=lambda: ctypes.c_double(0.0))
+
+    @classmethod
+    def allocate(cls, num_surfaces: int, num_bins: int, device: torch.device, *, ambisonics: bool = False,
+                 record_rays: tuple[int, int] | None = None) -> "TraceBuffers":
+        z64 = lambda *shape: torch.zeros(*shape, dtype=torch.int64, device=device)
+        return cls(
+            echogram_fx=z64(NUM_BANDS, num_bins), hit_counts=z64(num_surfaces), contrib_counts=z64(num_surfaces),
+            surface_energy_fx=z64(num_surfaces), counters=z64(8),
+            echogram=torch.zeros(NUM_BANDS, num_bins, dtype=torch.float32, device=device),
+            surface_energy=torch.zeros(num_surfaces, dtype=torch.float32, device=device),
+            ambisonic_fx=z64(NUM_BANDS, 4, num_bins) if ambisonics else None,
+            ambisonic=torch.zeros(NUM_BANDS, 4, num_bins, dtype=torch.float32, device=device) if ambisonics else None,
+            ray_surfaces=(torch.empty(record_rays[0], record_rays[1], dtype=torch.int32, device=device)
+                          if record_rays else None),
+        )
+
+    def outputs_struct(self) -> _lib.ACTraceOutputs:
+        o = _lib.ACTraceOutputs()
+        o.echogram_fx = self.echogram_fx.data_ptr()
+        o.ambisonic_fx = self.ambisonic_fx.data_ptr() if self.ambisonic_fx is not None else None
+        o.hit_counts = self.hit_counts.data_ptr()
+        o.contrib_counts = self.contrib_counts.data_ptr()
+        o.surface_energy_fx = self.surface_energy_fx.data_ptr()
+        o.counters = self.counters.data_ptr()
+        o.echogram = self.echogram.data_ptr()
+        o.ambisonic = self.ambisonic.data_ptr() if self.ambisonic is not None else None
+        o.surface_energy = self.surface_energy.data_ptr()
+        o.ray_surfaces = self.ray_surfaces.data_ptr() if self.ray_surfaces is not None else None
+        o.scale_out = ctypes.pointer(self.scale)
+        return o
+
+
+def params_struct(spec: TraceSpec, device: torch.device,
+                  keepalive: list[Any] | None = None) -> _lib.ACTraceParams:
+    p = _lib.ACTraceParams()
+    p.source[:] = [float(v) for v in spec.source]
+    p.listener[:] = [float(v) for v in spec.listener]
+    p.source_forward[:] = [float(v) for v in spec.source_forward]
+    p.num_rays = int(spec.num_rays)
+    p.num_bounces = int(spec.num_bounces)
+    p.num_bins = int(spec.num_bins)
+    p.bin_duration = float(spec.bin_duration)
+    p.speed_of_sound = float(spec.speed_of_sound)
+    p.max_path_length = float(spec.max_path_length)
+    p.direct_delay = float(spec.direct_delay)
+    p.listener_radius = float(spec.listener_radius)
+    p.source_radius = float(spec.source_radius)
+    p.irradiance_min_distance = float(spec.irradiance_min_distance)
+    p.specular_exponent = float(spec.specular_exponent)
+    p.dipole_weight = float(spec.dipole_weight)
+    p.dipole_power = float(spec.dipole_power)
+    p.use_bvh = 1 if spec.use_bvh else 0
+    p.render_ambisonics = 1 if spec.render_ambisonics else 0
+    if spec.precision not in ("float32", "float64"):
+        raise ValueError("rt_precision must be float32 or float64")
+    p.precision = _lib.AC_PRECISION_FP64 if spec.precision == "float64" else _lib.AC_PRECISION_FP32
+    if spec.rng not in ("reference", "philox"):
+        raise ValueError("rng must be 'reference' or 'philox'")
+    p.rng_mode = _lib.AC_RNG_REFERENCE if spec.rng == "reference" else _lib.AC_RNG_PHILOX
+    p.seed = int(spec.seed) & 0xFFFFFFFFFFFFFFFF
+    p.stream_key = int(spec.stream_key) & 0xFFFFFFFFFFFFFFFF
+    bank = diffuse_bank(spec.dtype, device)
+    p.diffuse_bank = bank.data_ptr()
+    p.num_bank = NUM_BANK
+    if spec.rng == "reference":
+        directions, random_values, indices = reference_stream(spec, device)
+        p.directions = directions.data_ptr()
+        p.diffuse_random = random_values.data_ptr()
+        p.diffuse_indices = indices.data_ptr()
+        if keepalive is not None:
+            keepalive.extend([directions, random_values, indices])
+    if keepalive is not None:
+        keepalive.append(bank)
+    p.energy_scale = float(spec.energy_scale)
+    p.block_size = int(spec.block_size)
+    p.grid_blocks = int(spec.grid_blocks)
+    return p
+
+
+def trace(scene: DeviceScene, spec: TraceSpec, buffers: TraceBuffers | None = None, *,
+          stream: torch.cuda.Stream | None = None, record_rays: bool = False) -> TraceBuffers:
+    """Launch one trace asynchronously on `stream` and return its device buffers."""
+    device = require_cuda(scene.device)
+    if buffers is None:
+        buffers = TraceBuffers.allocate(scene.num_surfaces, int(spec.num_bins), device,
+                                        ambisonics=spec.render_ambisonics,
+                                        record_rays=(int(spec.num_rays), int(spec.num_bounces)) if record_rays else None)
+    keep: list[Any] = []
+    params = params_struct(spec, device, keep)
+    outputs = buffers.outputs_struct()
+    _lib.check(_lib.load().ac_trace(scene.handle, ctypes.byref(params), ctypes.byref(outputs), _stream_ptr(stream)),
+               "ac_trace")
+    buffers._keepalive = keep  # type: ignore[attr-defined]
+    return buffers
+
+
+class BatchWorkspace:
+    """Reusable device workspace + pinned staging for ac_trace_batch."""
+
+    def __init__(self, device: torch.device) -> None:
+        self.device = device
+        self.capacity_jobs = 0
+        self.device_buffer: torch.Tensor | None = None
+        self.host_buffer: torch.Tensor | None = None
+
+    def ensure(self, num_jobs: int) -> tuple[int, int, int]:
+        if num_jobs > self.capacity_jobs or self.device_buffer is None:
+            size = ctypes.c_size_t()
+            cap = max(num_jobs, 2 * self.capacity_jobs, 16)
+            _lib.check(_lib.load().ac_batch_workspace_size(cap, None, ctypes.byref(size)), "ac_batch_workspace_size")
+            self.device_buffer = torch.empty(int(size.value), dtype=torch.uint8, device=self.device)
+            self.host_buffer = torch.empty(int(size.value), dtype=torch.uint8, pin_memory=True)
+            self.capacity_jobs = cap
+        assert self.device_buffer is not None and self.host_buffer is not None
+        return self.device_buffer.data_ptr(), self.device_buffer.numel(), self.host_buffer.data_ptr()
+
+
+def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
+                block_size: int = 0, grid_blocks: int = 0, stream: torch.cuda.Stream | None = None) -> None:
+    """All jobs in one persistent launch (ac_trace_batch)."""
+    if not jobs:
+        return
+    device = require_cuda(jobs[0][0].device)
+    arr = (_lib.ACJob * len(jobs))()
+    keep: list[Any] = []
+    for k, (scene, spec, buffers) in enumerate(jobs):
+        arr[k].scene = scene.handle.value
+        arr[k].params = params_struct(spec, device, keep)
+        arr[k].outputs = buffers.outputs_struct()
+    cfg = _lib.ACBatchConfig(int(block_size), 0, int(grid_blocks), 0)
+    ws, ws_bytes, host = workspace.ensure(len(jobs))
+    _lib.check(_lib.load().ac_trace_batch(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
+                                          ctypes.c_void_p(host), _stream_ptr(stream)), "ac_trace_batch")
+    workspace._keepalive = keep  # type: ignore[attr-defined]
+
+
+def host_field(buffers: TraceBuffers, names: Sequence[str], spec: TraceSpec) -> dict[str, Any]:
+    """Copy one trace's outputs to the host in the reference's result layout (steam_rt.py:1892-1923)."""
+    echogram = buffers.echogram.cpu().numpy()
+    hits = buffers.hit_counts.cpu().numpy()
+    contrib = buffers.contrib_counts.cpu().numpy()
+    energy = buffers.surface_energy.cpu().numpy()
+    counters = buffers.counters.cpu().numpy()
+    total_energy = np.sum(echogram, axis=0)
+    nonzero = np.flatnonzero(total_energy > 0.0)
+    out = {
+        "echogram": echogram,
+        "ambisonic_echogram": buffers.ambisonic.cpu().numpy() if buffers.ambisonic is not None else None,
+        "num_bins": int(spec.num_bins),
+        "bin_duration_s": float(spec.bin_duration),
+        "direct_delay_s": float(spec.direct_delay),
+        "actual_bounces": int(counters[0]),
+        "active_ray_count": int(counters[1]),
+        "last_energy_time_s": float(nonzero[-1] * spec.bin_duration) if nonzero.size else 0.0,
+        "surface_hit_count": {names[i]: int(hits[i]) for i in range(len(names)) if int(hits[i]) > 0},
+        "surface_contribution_count": {names[i]: int(contrib[i]) for i in range(len(names)) if int(contrib[i]) > 0},
+        "surface_energy": {names[i]: float(energy[i]) for i in range(len(names)) if float(energy[i]) > 0.0},
+        "ray_bounces": int(counters[2]),
+        "shadow_rays": int(counters[3]),
+        "energy_scale": float(buffers.scale.value),
+    }
+    if buffers.ray_surfaces is not None:
+        out["ray_surfaces"] = buffers.ray_surfaces.cpu().numpy()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Band synthesis
+
+
+class SynthWorkspace:
+    def __init__(self, device: torch.device) -> None:
+        self.device = device
+        self.buffer: torch.Tensor | None = None
+
+    def ensure(self, nbytes: int) -> torch.Tensor:
+        if self.buffer is None or self.buffer.numel() < nbytes:
+            self.buffer = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=self.device)
+        return self.buffer
+
+
+def synth_params(num_rirs: int, num_bins: int, bin_duration: float, fs: int, speed_of_sound: float, *,
+                 rng_mode: str, seed: int, white: torch.Tensor | None = None, white_shared: bool = True,
+                 direct_delays: torch.Tensor | None = None, air: torch.Tensor | None = None) -> _lib.ACSynthParams:
+    p = _lib.ACSynthParams()
+    p.num_rirs = int(num_rirs)
+    p.num_bins = int(num_bins)
+    p.samples_per_bin = bands.samples_per_bin(bin_duration, fs)
+    p.sample_rate = int(fs)
+    p.rng_mode = _lib.AC_RNG_PHILOX if rng_mode == "philox" else _lib.AC_RNG_REFERENCE
+    p.white_shared = 1 if white_shared else 0
+    p.white = white.data_ptr() if white is not None else None
+    p.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    p.air = air.data_ptr() if air is not None else None
+    p.direct_delays = direct_delays.data_ptr() if direct_delays is not None else None
+    p.air_coefficients[:] = list(bands.AIR_ABSORPTION_NP_PER_M)
+    p.speed_of_sound = float(speed_of_sound)
+    p.crossover[:] = [float(v) for v in bands.crossover_table(fs).reshape(-1)]
+    return p
+
+
+def synthesize(echograms: torch.Tensor, params: _lib.ACSynthParams, workspace: SynthWorkspace,
+               out: torch.Tensor | None = None, *, stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """[J,6,bins] float32 echograms -> [J,6,N] float32 band IRs (ac_synthesize)."""
+    if echograms.dtype != torch.float32 or not echograms.is_cuda or not echograms.is_contiguous():
+        raise ValueError("echograms must be a contiguous float32 CUDA tensor")
+    J = int(params.num_rirs)
+    N = int(params.num_bins) * int(params.samples_per_bin)
+    if out is None:
+        out = torch.empty(J, NUM_BANDS, N, dtype=torch.float32, device=echograms.device)
+    size = ctypes.c_size_t()
+    _lib.check(_lib.load().ac_synth_workspace_size(ctypes.byref(params), ctypes.byref(size)), "ac_synth_workspace_size")
+    ws = workspace.ensure(int(size.value))
+    _lib.check(_lib.load().ac_synthesize(ctypes.c_void_p(echograms.data_ptr()), ctypes.byref(params),
+                                         ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
+                                         ws.numel(), _stream_ptr(stream)), "ac_synthesize")
+    return out
+
+
+def device_info(device: int = 0) -> dict[str, Any]:
+    name = ctypes.create_string_buffer(256)
+    major, minor, sms = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    _lib.check(_lib.load().ac_device_info(int(device), name, 256, ctypes.byref(major), ctypes.byref(minor),
+                                          ctypes.byref(sms)), "ac_device_info")
+    return {"id": int(device), "name": name.value.decode(), "compute_capability": f"{major.value}.{minor.value}",
+            "sm_count": int(sms.value)}
+
+
+def ray_bounce_count(buffers: TraceBuffers) -> int:
+    return int(buffers.counters[2].item())
+
+
+def num_bins_for(duration_s: float, rt_duration_s: float, bin_duration_s: float) -> int:
+    return max(1, int(math.ceil(max(float(rt_duration_s), float(duration_s)) / float(bin_duration_s))))

@@ -1,0 +1,347 @@
+"""Benchmark: RIRs/s (and ray-bounces/s) of the B200 reflection backend.
+
+Default workload (one step = one pass over one batch): the furnished U-shaped
+room of the second benchmark configuration -- 6 x 10 x 2.8 m, 20 seeded boxes
+(30 surfaces), cardioid source, 8-channel circular array, 200,000 rays x 100
+bounces per channel, fs 48 kHz, 2 s, 1 ms bins -- traced in float32 with the
+on-device Philox stream and turned into six band IRs per channel: 8 RIRs per
+step, all in one persistent trace launch plus one synthesis launch, replayed
+as a CUDA graph.  Inputs (the scene) are resident in HBM; L2 is flushed
+between timed steps.
+
+``--impl reference`` times the reference algorithm on the host cores instead
+(the float64 CPU restatement, all threads) on the same workload, one RIR per
+step.  Under torchrun each rank runs an independent replica (replicas only:
+jobs are independent, no collective on the data path); rank 0 prints one JSON
+line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from datetime import timedelta
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+METRIC = "RIRs/s"
+L2_FLUSH_BYTES = 256 * 1024 * 1024
+LAUNCHES_PER_STEP = 5  # zero-outputs, trace, finalize, synth-prepare, synth-filter
+
+
+def _peaks() -> dict:
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def _workload(name: str):
+    from acoustic_agent_b200 import workloads
+    if name == "u_room_20_boxes":
+        return [workloads.u_furnished(1729)]
+    if name == "shoebox":
+        return [workloads.shoebox(1729)]
+    if name == "apartment":
+        return [workloads.apartment(1729)]
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """NVML clock / throttle-reason sampling during the timed region (read-only)."""
+
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+        0x100: "display_clock_setting",
+    }
+
+    def __init__(self, index: int) -> None:
+        self.samples: list[int] = []
+        self.reasons: set[str] = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = int(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nvml = None
+
+    def _run(self) -> None:
+        while not self._stop.is_set():
+            try:
+                self.samples.append(int(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM)))
+                mask = int(self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle))
+                self.reasons |= {name for bit, name in self.REASONS.items() if mask & bit and name != "gpu_idle"}
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        if self.nvml is not None:
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread is not None:
+            self._thread.join()
+
+    def summary(self) -> dict:
+        return {"sm_mhz": int(statistics.median(self.samples)) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def _dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference(workload, steps: int, warmup: int, *, channel: int = 0, rays: int | None = None) -> dict:
+    """The reference algorithm on the host: float64 trace + band synthesis of one RIR per step (all cores)."""
+    from oracle import oracle
+    from acoustic_agent_b200 import scene as scene_mod, rng as rng_mod
+    from acoustic_agent_b200.directivity import source_directivity, source_forward
+    cfg = workload.config
+    arrays = scene_mod.compile_scene(workload.spec)
+    R = int(rays or cfg.rt_num_rays)
+    B = cfg.rt_num_bounces
+    key = rng_mod.stream_key(workload.name, 0)
+    directions, rnd, idx = oracle.philox_workspace(R, B, cfg.seed, key)
+    _, bank, _, _ = oracle.workspace(1, 0, 0)
+    emitter = source_directivity(workload.source_model)
+    src = np.asarray(workload.sources[0], dtype=float)
+    lst = np.asarray(workload.listeners[channel], dtype=float)
+    delay = float(np.linalg.norm(src - lst)) / cfg.c
+    spb = max(1, int(math.ceil(cfg.rt_bin_duration_s * cfg.fs)))
+    white = np.random.default_rng(cfg.seed + 7).uniform(-1.0, 1.0, size=cfg.num_bins * spb)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    times = []
+    stats = None
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        res = oracle.trace(arrays, source=src, listener=lst, directions=directions, diffuse_bank=bank,
+                           diffuse_random=rnd, diffuse_indices=idx, num_bins=cfg.num_bins,
+                           bin_dur=cfg.rt_bin_duration_s, c=cfg.c, max_path_len=cfg.max_path_length,
+                           direct_delay=delay, source_forward=source_forward(emitter),
+                           dipole_weight=float(emitter["dipole_weight"]), dipole_power=float(emitter["dipole_power"]),
+                           use_bvh=cfg.intersection_backend == "bvh", threads=cores)
+        oracle.synthesize(res["echogram"].astype(np.float32), fs=cfg.fs, bin_dur=cfg.rt_bin_duration_s,
+                          direct_delay=delay, c=cfg.c, white=white)
+        if k >= warmup:
+            times.append(time.perf_counter() - t0)
+        stats = res
+    per_rir = float(np.mean(times))
+    # Algorithmic bytes per ray-bounce in the reference's traversal order (survey 8(d) definition):
+    # nodes 32 B, walls 32 B, polygons 16 B + 8 B per edge, boxes 48 B, one 32 B material row per bounce.
+    q = stats["closest_queries"]
+    walls, polys, boxes = stats["prims_tested"]
+    bytes_total = (stats["nodes_visited"] * 32 + walls * 32 + polys * 16 + stats["polygon_edges"] * 8 + boxes * 48
+                   + q * 32)
+    return {
+        "value": 1.0 / per_rir, "seconds_per_rir": per_rir, "cores": cores, "ray_bounces": q,
+        "ray_bounces_per_s": q / per_rir, "bytes_per_ray_bounce": bytes_total / max(q, 1),
+        "sample": (f"channel {channel} of {len(workload.listeners)}: {R} rays x {B} bounces, float64 trace + "
+                   f"band synthesis, {cores} threads, mean of {steps} after {warmup} warm-up"),
+    }
+
+
+def run_reference_arm(args, workload_name: str) -> None:
+    world, rank, _ = _dist_setup()
+    if rank != 0:
+        return
+    workload = _workload(workload_name)[0]
+    ref = cpu_reference(workload, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": ref["value"], "unit": "RIRs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds_per_rir"] * 1000.0,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload.name, "rays": workload.config.rt_num_rays,
+                   "bounces": workload.config.rt_num_bounces, "channels_per_step": 1,
+                   "note": "the reference is Python/Numba; this arm times its float64 algorithm restated in C"},
+        "ray_bounces_per_s": ref["ray_bounces_per_s"],
+        "cpu_baseline": {"value": ref["value"], "unit": "RIRs/s", "cores": ref["cores"], "kind": "port",
+                         "sample": ref["sample"]},
+        "e2e": {"value": ref["value"], "unit": "RIRs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> int:
+    parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--workload", default="u_room_20_boxes", choices=("u_room_20_boxes", "shoebox", "apartment"))
+    parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
+    parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--block", type=int, default=0)
+    args = parser.parse_args()
+    if args.warmup < 3:
+        parser.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        run_reference_arm(args, args.workload)
+        return 0
+
+    import torch
+    from acoustic_agent_b200 import batching, runtime, scene as scene_mod
+
+    world, rank, local = _dist_setup()
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
+
+    workloads_ = _workload(args.workload)
+    specs, jobs = batching.workload_jobs(workloads_, precision="float32", rng_mode="philox")
+    renderer = batching.RIRRenderer(local, block_size=args.block)
+    arrays = [scene_mod.compile_scene(s) for s in specs]
+    plan = renderer.plan(arrays, jobs)
+    if not args.no_graph:
+        renderer.capture(plan)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+
+    for _ in range(args.warmup):
+        renderer.launch(plan)
+    torch.cuda.synchronize(device)
+    ray_bounces_per_step = renderer.ray_bounces(plan)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(device)
+    with sampler:
+        for k in range(args.steps):
+            flush.fill_(float(k))  # evict L2 (256 MiB > 126 MB) outside the timed event pair
+            starts[k].record(stream)
+            renderer.launch(plan)
+            stops[k].record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    ms_per_step = float(np.mean(step_ms))
+    if dist is not None:
+        t = torch.tensor([ms_per_step], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+    rirs_per_step = plan.num_rirs
+    value = world * rirs_per_step / (ms_per_step / 1000.0)
+
+    # Tracer kernel alone (for the roofline): eager trace_batch launches timed with events.
+    trace_ms = []
+    job_list = [(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)]
+    for k in range(max(3, args.steps // 2)):
+        flush.fill_(float(k))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        runtime.trace_batch(job_list, plan.workspace, block_size=args.block, stream=stream)
+        e.record(stream)
+        e.synchronize()
+        trace_ms.append(s.elapsed_time(e))
+    trace_launch_ms = float(np.median(trace_ms))
+
+    # End to end through the public API: host scene arrays in, host band IRs out, every step.
+    e2e_times = []
+    h2d = d2h = 0
+    pinned_out = {key: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for key, t in plan.band_irs.items()}
+    for k in range(args.warmup + max(3, args.steps // 2)):
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        scenes_k = [runtime.DeviceScene(a, device=local) for a in arrays]
+        plan_k = renderer.plan(scenes_k, jobs)
+        renderer.launch(plan_k)
+        for key, t in plan_k.band_irs.items():
+            pinned_out[key].copy_(t, non_blocking=True)
+        torch.cuda.synchronize(device)
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+        h2d = sum(s.device_bytes for s in scenes_k) + plan_k.workspace.device_buffer.numel()
+        d2h = sum(t.numel() * t.element_size() for t in plan_k.band_irs.values())
+        for s in scenes_k:
+            s.close()
+    e2e_value = world * rirs_per_step / float(np.mean(e2e_times))
+
+    peaks = _peaks()
+    result = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_reference(workloads_[0], steps=1, warmup=0)
+        bytes_per_rb = cpu["bytes_per_ray_bounce"] if cpu else None
+        achieved = (bytes_per_rb * ray_bounces_per_step / (trace_launch_ms / 1000.0) / 1e9) if bytes_per_rb else None
+        traffic = _profiled_traffic(args.workload)
+        result = {
+            "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": f"{workloads_[0].name}: U room 6x10x2.8 m, 20 boxes, 8-mic circular array"
+                       if args.workload == "u_room_20_boxes" else workloads_[0].name,
+                       "rirs_per_step": rirs_per_step, "rays_per_rir": workloads_[0].config.rt_num_rays,
+                       "max_bounces": workloads_[0].config.rt_num_bounces, "fs": workloads_[0].config.fs,
+                       "bins": workloads_[0].config.num_bins, "rng": "philox", "graph": not args.no_graph,
+                       "parallelism": f"replicas x{world}", "l2": "flushed between timed steps (256 MiB write)"},
+            "ray_bounces_per_step": ray_bounces_per_step,
+            "ray_bounces_per_s": world * ray_bounces_per_step / (ms_per_step / 1000.0),
+            "trace_launch_ms": trace_launch_ms,
+            "e2e": {"value": e2e_value, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": LAUNCHES_PER_STEP * args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
+                         "peak_source": peaks["source"],
+                         "kernel": "trace_kernel (ac_trace_batch)",
+                         "bytes_per_ray_bounce": bytes_per_rb},
+            "cpu_baseline": ({"value": cpu["value"], "unit": "RIRs/s", "cores": cpu["cores"], "kind": "port",
+                              "sample": cpu["sample"]} if cpu else None),
+            "clocks": sampler.summary(),
+        }
+        print(json.dumps(result), flush=True)
+    if dist is not None:
+        dist.barrier(device_ids=[local])
+        dist.destroy_process_group()
+    return 0
+
+
+def _profiled_traffic(workload: str):
+    """DRAM bytes per trace launch from the committed ncu summary, if one exists for this workload."""
+    path = REPO / "profiles" / f"trace_kernel_{workload}.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        if line.lower().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,249 @@
+/*
+ * acoustic_rt.h -- C ABI of the B200 reflection-tracing backend for
+ * Acoustic Agent.
+ *
+ * One shared library (libacoustic_rt.so) holds the sm_100a kernels and this
+ * ABI.  Every entry point returns an int status (AC_OK or a negative AC_ERR_*
+ * code); nothing throws across the ABI and nothing calls exit/abort.  A
+ * human-readable message for the last failure on the calling thread is
+ * available from ac_last_error().
+ *
+ * Threading: scene handles are immutable after ac_scene_create and may be
+ * shared between threads; each caller thread should use its own CUDA stream.
+ * All device work is asynchronous on the stream passed in (a cudaStream_t,
+ * passed as void*; NULL = the legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the Acoustic Agent project):
+ *   ac_bvh_build        acoustic_agent/bvh.py:8-77                   build_bvh
+ *   ac_scene_create     acoustic_agent/steam_rt.py:834-924           _scene_kernel_arrays
+ *                       + acoustic_agent/steam_rt_cuda.py:76-115     device upload / cache
+ *   ac_trace            acoustic_agent/steam_rt.py:1757-1804         trace_energy_field
+ *                       (kernels: steam_rt.py:4708-4850, steam_rt_cuda.py:491-710)
+ *   ac_trace_batch      acoustic_agent/api.py:477-639, batch.py:139-185, engine.py:64-73
+ *                       (the per-job loops, run as one persistent launch)
+ *   ac_synthesize       acoustic_agent/steam_rt.py:2205-2232         reconstruct_band_irs
+ *                       + steam_rt.py:3070-3083                      bandlimit_band_signals
+ */
+#ifndef ACOUSTIC_RT_H
+#define ACOUSTIC_RT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AC_ABI_VERSION 1
+
+#define AC_OK 0
+#define AC_ERR_INVALID (-1)     /* bad argument, shape or value (reference: ValueError) */
+#define AC_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define AC_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define AC_ERR_UNSUPPORTED (-4) /* no usable sm_100 device, or option not built */
+#define AC_ERR_CAPACITY (-5)    /* a size exceeds a fixed capacity */
+
+enum { AC_KIND_WALL = 0, AC_KIND_HORIZONTAL = 1, AC_KIND_BOX = 2 };
+enum { AC_PRECISION_FP32 = 0, AC_PRECISION_FP64 = 1 };
+enum { AC_RNG_REFERENCE = 0, AC_RNG_PHILOX = 1 };
+
+typedef struct ac_scene_s *ac_scene_t;
+
+/* Output of ac_bvh_build.  The caller allocates every array with room for
+ * 2*num_surfaces-1 nodes and num_surfaces primitives. */
+typedef struct ac_bvh {
+    double *bounds_min;   /* [nodes,3] */
+    double *bounds_max;   /* [nodes,3] */
+    int64_t *start;       /* [nodes] first primitive slot of a leaf, -1 for inner nodes */
+    int64_t *count;       /* [nodes] primitives in a leaf, 0 for inner nodes */
+    int64_t *escape;      /* [nodes] preorder index of the node after this subtree */
+    int64_t *primitives;  /* [num_surfaces] surface index per primitive slot */
+    int64_t node_count;
+    int64_t leaf_count;
+    int64_t max_depth;
+} ac_bvh;
+
+/* Scene surfaces in the reference's SoA layout (all float64, row-major).
+ * If bvh_node_count == 0 the library builds the BVH itself from the padded
+ * per-surface AABBs in surface_bounds_min/max (ac_bvh_build, leaf size 4). */
+typedef struct ac_scene_desc {
+    int64_t num_surfaces;
+    const int64_t *kinds;        /* [S] AC_KIND_* */
+    const double *wall_a;        /* [S,2] */
+    const double *wall_delta;    /* [S,2] */
+    const double *wall_z;        /* [S,2] */
+    const double *z_values;      /* [S] */
+    const double *box_center;    /* [S,2] */
+    const double *box_axis_u;    /* [S,2] */
+    const double *box_axis_v;    /* [S,2] */
+    const double *box_half;      /* [S,2] */
+    const double *box_z;         /* [S,2] */
+    const double *normals;       /* [S,3] */
+    const double *reflection;    /* [S,6] energy reflection = 1 - absorption */
+    const double *scattering;    /* [S] band-mean scattering */
+    int64_t num_corners;
+    const double *corners;       /* [C,2] room polygon for horizontal surfaces */
+    const double *surface_bounds_min; /* [S,3] padded AABBs (used when the BVH is built here) */
+    const double *surface_bounds_max; /* [S,3] */
+    int64_t bvh_node_count;      /* 0: build here with leaf size 4 */
+    const double *bvh_bounds_min;
+    const double *bvh_bounds_max;
+    const int64_t *bvh_start;
+    const int64_t *bvh_count;
+    const int64_t *bvh_escape;
+    const int64_t *bvh_primitives;
+    int32_t device;              /* CUDA device ordinal that will own the scene */
+    int32_t reserved;
+} ac_scene_desc;
+
+typedef struct ac_scene_info {
+    int64_t num_surfaces;
+    int64_t num_corners;
+    int64_t node_count;
+    int64_t leaf_count;
+    int64_t device_bytes;        /* device memory held by the scene */
+    int32_t device;
+    int32_t max_leaf;
+} ac_scene_info;
+
+/* One trace: rays from the listener, next-event estimation to the source.
+ * Field meanings follow steam_rt.py:1822-1890 (the kernel arguments). */
+typedef struct ac_trace_params {
+    double source[3];
+    double listener[3];
+    double source_forward[3];
+    int64_t num_rays;
+    int32_t num_bounces;
+    int32_t num_bins;
+    double bin_duration;
+    double speed_of_sound;
+    double max_path_length;      /* duration * c */
+    double direct_delay;         /* |source - listener| / c */
+    double listener_radius;
+    double source_radius;
+    double irradiance_min_distance;
+    double specular_exponent;
+    double dipole_weight;
+    double dipole_power;
+    int32_t use_bvh;             /* 0: linear scan over all surfaces, 1: BVH */
+    int32_t render_ambisonics;   /* 1: also fill the first-order ambisonic echogram */
+    int32_t precision;           /* AC_PRECISION_FP32 (production) or AC_PRECISION_FP64 (parity) */
+    int32_t rng_mode;            /* AC_RNG_REFERENCE: arrays below; AC_RNG_PHILOX: on-device stream */
+    uint64_t seed;               /* Philox key part 1 */
+    uint64_t stream_key;         /* Philox key part 2 (scene identity) */
+    /* reference-stream arrays, DEVICE pointers, element type double for FP64
+     * and float for FP32 (diffuse_indices is int32 in both):
+     * directions [R,3], diffuse_random [B,R], diffuse_indices [B,R]. */
+    const void *directions;
+    const void *diffuse_random;
+    const int32_t *diffuse_indices;
+    const void *diffuse_bank;    /* [K,3] device, element type as above; both RNG modes */
+    int32_t num_bank;
+    int32_t block_size;          /* 0: library default */
+    double energy_scale;         /* fixed-point scale (a power of two); 0: library picks */
+    int32_t grid_blocks;         /* 0: library default (persistent, SM-count based) */
+    int32_t reserved;
+} ac_trace_params;
+
+/* Outputs.  All pointers are DEVICE memory owned by the caller.  The int64
+ * fixed-point accumulators are zeroed by the call itself; NULL optional
+ * outputs are skipped. */
+typedef struct ac_trace_outputs {
+    int64_t *echogram_fx;        /* [6,bins] required: echogram * energy_scale, rounded per deposit */
+    int64_t *ambisonic_fx;       /* [6,4,bins] when render_ambisonics */
+    int64_t *hit_counts;         /* [S] required */
+    int64_t *contrib_counts;     /* [S] required */
+    int64_t *surface_energy_fx;  /* [S] required */
+    int64_t *counters;           /* [8] required: actual_bounces, active_rays, ray_bounces, shadow_rays,
+                                    work counter (scratch), 3 reserved */
+    float *echogram;             /* [6,bins] optional dequantized copy */
+    float *ambisonic;            /* [6,4,bins] optional */
+    float *surface_energy;       /* [S] optional */
+    int32_t *ray_surfaces;       /* [R,B] optional per-ray hit surface per bounce, -1 after termination */
+    double *scale_out;           /* optional host pointer: receives the fixed-point scale used */
+} ac_trace_outputs;
+
+/* One job of a batched launch: a scene, its trace parameters and outputs. */
+typedef struct ac_job {
+    ac_scene_t scene;
+    ac_trace_params params;
+    ac_trace_outputs outputs;
+} ac_job;
+
+typedef struct ac_batch_config {
+    int32_t block_size;          /* threads per block; 0: autotuned default */
+    int32_t chunk_rays;          /* rays per work item; 0: default */
+    int32_t grid_blocks;         /* persistent blocks; 0: SM count * occupancy */
+    int32_t reserved;
+} ac_batch_config;
+
+/* Band synthesis of J echograms (steam_rt.py:2205-2232, 3070-3083): per
+ * band, the amplitude envelope sqrt(E/4pi) interpolated linearly from the
+ * previous bin, times the per-bin air-absorption gain, times white noise,
+ * then the six-band crossover (eight-pole low-pass differences). */
+typedef struct ac_synth_params {
+    int32_t num_rirs;
+    int32_t num_bins;
+    int32_t samples_per_bin;     /* ceil(bin_duration * fs) */
+    int32_t sample_rate;
+    int32_t rng_mode;            /* AC_RNG_REFERENCE: noise from `white`; AC_RNG_PHILOX: generated from seed */
+    int32_t white_shared;        /* 1: one noise row [N] for all RIRs, 0: [J,N] */
+    const double *white;         /* device uniform(-1,1) noise (reference mode) */
+    uint64_t seed;               /* noise key in Philox mode */
+    const double *air;           /* optional [J,6,bins] device air gains; NULL: computed from the fields below */
+    const double *direct_delays; /* [J] device seconds (used when air is NULL) */
+    double air_coefficients[6];  /* Np/m per band (acoustics.py:12-22) */
+    double speed_of_sound;
+    double crossover[100];       /* [5 cutoffs][4 sections][b0,b1,b2,a1,a2] low-pass coefficients */
+} ac_synth_params;
+
+const char *ac_last_error(void);
+int ac_abi_version(void);
+
+/* Host-only: build the preorder escape-link BVH of bvh.py:8-77. */
+int ac_bvh_build(const double *bounds_min, const double *bounds_max, int64_t num_surfaces, int32_t leaf_size,
+                 ac_bvh *out);
+
+/* Device info for the reference's `cuda` result field. */
+int ac_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major, int32_t *cc_minor,
+                   int32_t *sm_count);
+
+int ac_scene_create(const ac_scene_desc *desc, ac_scene_t *out);
+int ac_scene_destroy(ac_scene_t scene);
+int ac_scene_get_info(ac_scene_t scene, ac_scene_info *info);
+
+/* Fixed-point scale the library would pick for these parameters (a power of
+ * two chosen so no accumulator can overflow int64). */
+int ac_energy_scale(ac_scene_t scene, const ac_trace_params *params, double *scale);
+
+int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_outputs *outputs, void *stream);
+
+/* Device workspace needed by ac_trace_batch for num_jobs jobs. */
+int ac_batch_workspace_size(int32_t num_jobs, const ac_batch_config *config, size_t *bytes);
+
+/* Many jobs (any mix of scenes, ray budgets, bins) in one persistent launch.
+ * `workspace` is caller-owned device memory of ac_batch_workspace_size bytes.
+ * Host-side it writes the job table into `host_staging` (pinned memory of the
+ * same size, or NULL to use a pageable copy). */
+int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
+                   size_t workspace_bytes, void *host_staging, void *stream);
+
+/* Device workspace needed by ac_synthesize. */
+int ac_synth_workspace_size(const ac_synth_params *params, size_t *bytes);
+
+/* echograms: [J,6,bins] float32 device.  band_irs: [J,6,bins*spb] float32 device.
+ * `workspace` is caller-owned device memory of ac_synth_workspace_size bytes. */
+int ac_synthesize(const float *echograms, const ac_synth_params *params, float *band_irs, void *workspace,
+                  size_t workspace_bytes, void *stream);
+
+/* Debug/test: fill the Philox reference-equivalent workspace the kernels
+ * generate internally (directions [R,3], random [B,R], indices [B,R]). */
+int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces,
+                        int32_t num_bank, int32_t precision, void *directions, void *random,
+                        int32_t *indices, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ACOUSTIC_RT_H */

@@ -1,0 +1,376 @@
+"""CPU oracle for the reflection hot path.  TEST INFRASTRUCTURE ONLY.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module, always as the checker or the CPU baseline,
+never as part of the product path.
+
+* ``trace``        float64 tracer restated in C (trace_oracle.c), following
+                   acoustic_agent/steam_rt.py:4258-4850 operation by operation
+* ``synthesize``   echogram -> band signals (steam_rt.py:2205-2232, 3070-3083, 4131-4212)
+* ``build_bvh``    numpy restatement of acoustic_agent/bvh.py:8-77
+* ``workspace``    the reference's random workspace (steam_rt.py:3959-4044)
+* ``philox_workspace`` numpy Philox4x32-10 (Salmon et al., SC'11) producing the
+                   directions / uniforms / bank indices the GPU's counter-based
+                   mode draws, so that mode can be checked ray by ray
+
+Parity is pinned against golden vectors produced by running the reference
+itself (tests/golden/make_golden.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+from pathlib import Path
+from typing import Any, Mapping
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+SOURCE = ORACLE_DIR / "trace_oracle.c"
+LIBRARY = ORACLE_DIR / "liboracle.so"
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_i32 = ctypes.POINTER(ctypes.c_int32)
+_f32 = ctypes.POINTER(ctypes.c_float)
+
+
+class _Scene(ctypes.Structure):
+    _fields_ = [("num_surfaces", ctypes.c_int64), ("kinds", _i64), ("wall_a", _d), ("wall_delta", _d),
+                ("wall_z", _d), ("z_values", _d), ("box_center", _d), ("box_axis_u", _d), ("box_axis_v", _d),
+                ("box_half", _d), ("box_z", _d), ("normals", _d), ("reflection", _d), ("scattering", _d),
+                ("num_corners", ctypes.c_int64), ("corners", _d), ("num_nodes", ctypes.c_int64), ("bvh_min", _d),
+                ("bvh_max", _d), ("bvh_start", _i64), ("bvh_count", _i64), ("bvh_escape", _i64), ("bvh_prims", _i64),
+                ("use_bvh", ctypes.c_int64)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("source", ctypes.c_double * 3), ("listener", ctypes.c_double * 3),
+                ("source_forward", ctypes.c_double * 3), ("num_rays", ctypes.c_int64),
+                ("num_bounces", ctypes.c_int64), ("num_bins", ctypes.c_int64), ("num_bank", ctypes.c_int64),
+                ("bin_dur", ctypes.c_double), ("c", ctypes.c_double), ("max_path_len", ctypes.c_double),
+                ("direct_delay", ctypes.c_double), ("listener_radius", ctypes.c_double),
+                ("source_radius", ctypes.c_double), ("irradiance_min_distance", ctypes.c_double),
+                ("specular_exponent", ctypes.c_double), ("dipole_weight", ctypes.c_double),
+                ("dipole_power", ctypes.c_double), ("render_ambisonics", ctypes.c_int64),
+                ("num_threads", ctypes.c_int64), ("directions", _d), ("diffuse_bank", _d), ("diffuse_random", _d),
+                ("diffuse_indices", _i32)]
+
+
+class _Outputs(ctypes.Structure):
+    _fields_ = [("echogram", _d), ("ambisonic", _d), ("hit_counts", _i64), ("contrib_counts", _i64),
+                ("surface_energy", _d), ("actual_bounces", ctypes.c_int64), ("active_count", ctypes.c_int64),
+                ("ray_surfaces", _i32), ("ray_bounces", _i32), ("closest_queries", ctypes.c_int64),
+                ("shadow_queries", ctypes.c_int64), ("nodes_visited", ctypes.c_int64),
+                ("prims_tested", ctypes.c_int64 * 3), ("polygon_edges", ctypes.c_int64)]
+
+
+def build(force: bool = False) -> Path:
+    """Compile the C restatement (gcc, OpenMP, no FP contraction)."""
+    if not force and LIBRARY.exists() and LIBRARY.stat().st_mtime >= SOURCE.stat().st_mtime:
+        return LIBRARY
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    cmd = ["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math", "-std=c11",
+           str(SOURCE), "-o", str(tmp), "-lm"]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+_LIB: ctypes.CDLL | None = None
+
+
+def _lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        if not LIBRARY.exists():
+            build()
+        lib = ctypes.CDLL(str(LIBRARY))
+        lib.oracle_trace.restype = ctypes.c_int
+        lib.oracle_trace.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Params), ctypes.POINTER(_Outputs)]
+        lib.oracle_closest_hit.restype = ctypes.c_int
+        lib.oracle_closest_hit.argtypes = [ctypes.POINTER(_Scene), _d, _d, _d, _d]
+        lib.oracle_synthesize.restype = ctypes.c_int
+        lib.oracle_synthesize.argtypes = [_d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _d, _d, _d, _f32]
+        _LIB = lib
+    return _LIB
+
+
+def _p(a: np.ndarray, t):
+    return a.ctypes.data_as(t)
+
+
+class Scene:
+    """Holds contiguous copies of a scene's arrays for the C oracle."""
+
+    def __init__(self, arrays: Mapping[str, Any], use_bvh: bool) -> None:
+        f = lambda k: np.ascontiguousarray(arrays[k], dtype=np.float64)
+        i = lambda k: np.ascontiguousarray(arrays[k], dtype=np.int64)
+        self.keep = {k: f(k) for k in ("wall_a", "wall_delta", "wall_z", "z_values", "box_center", "box_axis_u",
+                                       "box_axis_v", "box_half", "box_z", "normals", "reflection", "scattering",
+                                       "bvh_bounds_min", "bvh_bounds_max")}
+        self.keep["corners"] = np.ascontiguousarray(np.asarray(arrays["corners"], dtype=np.float64)[:, :2])
+        self.keep.update({k: i(k) for k in ("kinds", "bvh_start", "bvh_count", "bvh_escape", "bvh_primitives")})
+        k = self.keep
+        self.struct = _Scene(
+            k["kinds"].shape[0], _p(k["kinds"], _i64), _p(k["wall_a"], _d), _p(k["wall_delta"], _d),
+            _p(k["wall_z"], _d), _p(k["z_values"], _d), _p(k["box_center"], _d), _p(k["box_axis_u"], _d),
+            _p(k["box_axis_v"], _d), _p(k["box_half"], _d), _p(k["box_z"], _d), _p(k["normals"], _d),
+            _p(k["reflection"], _d), _p(k["scattering"], _d), k["corners"].shape[0], _p(k["corners"], _d),
+            k["bvh_start"].shape[0], _p(k["bvh_bounds_min"], _d), _p(k["bvh_bounds_max"], _d),
+            _p(k["bvh_start"], _i64), _p(k["bvh_count"], _i64), _p(k["bvh_escape"], _i64),
+            _p(k["bvh_primitives"], _i64), 1 if use_bvh else 0)
+
+    def closest_hit(self, origin, direction) -> tuple[int, float, np.ndarray]:
+        o = np.ascontiguousarray(origin, dtype=np.float64)
+        d = np.ascontiguousarray(direction, dtype=np.float64)
+        t = np.zeros(1)
+        n = np.zeros(3)
+        s = _lib().oracle_closest_hit(ctypes.byref(self.struct), _p(o, _d), _p(d, _d), _p(t, _d), _p(n, _d))
+        return int(s), float(t[0]), n
+
+
+def trace(arrays: Mapping[str, Any], *, source, listener, directions, diffuse_bank, diffuse_random, diffuse_indices,
+          num_bins: int, bin_dur: float, c: float, max_path_len: float, direct_delay: float,
+          listener_radius: float = 0.1, source_radius: float = 0.1, irradiance_min_distance: float = 1.0,
+          specular_exponent: float = 100.0, source_forward=(1.0, 0.0, 0.0), dipole_weight: float = 0.0,
+          dipole_power: float = 1.0, use_bvh: bool = False, render_ambisonics: bool = False, threads: int = 0,
+          record_rays: bool = False) -> dict[str, Any]:
+    """float64 trace of steam_rt.py:4708-4850 (plus per-ray hit sequences and traversal counts)."""
+    scene = Scene(arrays, use_bvh)
+    dirs = np.ascontiguousarray(directions, dtype=np.float64)
+    bank = np.ascontiguousarray(diffuse_bank, dtype=np.float64)
+    rnd = np.ascontiguousarray(diffuse_random, dtype=np.float64)
+    idx = np.ascontiguousarray(diffuse_indices, dtype=np.int32)
+    R = dirs.shape[0]
+    B = rnd.shape[0]
+    S = scene.keep["kinds"].shape[0]
+    params = _Params()
+    params.source[:] = [float(v) for v in source]
+    params.listener[:] = [float(v) for v in listener]
+    params.source_forward[:] = [float(v) for v in source_forward]
+    params.num_rays, params.num_bounces, params.num_bins, params.num_bank = R, B, int(num_bins), bank.shape[0]
+    params.bin_dur, params.c, params.max_path_len, params.direct_delay = float(bin_dur), float(c), float(max_path_len), float(direct_delay)
+    params.listener_radius, params.source_radius = float(listener_radius), float(source_radius)
+    params.irradiance_min_distance, params.specular_exponent = float(irradiance_min_distance), float(specular_exponent)
+    params.dipole_weight, params.dipole_power = float(dipole_weight), float(dipole_power)
+    params.render_ambisonics = 1 if render_ambisonics else 0
+    params.num_threads = int(threads)
+    params.directions, params.diffuse_bank = _p(dirs, _d), _p(bank, _d)
+    params.diffuse_random, params.diffuse_indices = _p(rnd, _d), _p(idx, _i32)
+    echogram = np.zeros((6, int(num_bins)))
+    ambisonic = np.zeros((6, 4, int(num_bins))) if render_ambisonics else None
+    hits = np.zeros(S, np.int64)
+    contrib = np.zeros(S, np.int64)
+    energy = np.zeros(S)
+    ray_surfaces = np.zeros((R, B), np.int32) if record_rays else None
+    ray_bounces = np.zeros(R, np.int32) if record_rays else None
+    out = _Outputs()
+    out.echogram = _p(echogram, _d)
+    out.ambisonic = _p(ambisonic, _d) if ambisonic is not None else None
+    out.hit_counts, out.contrib_counts, out.surface_energy = _p(hits, _i64), _p(contrib, _i64), _p(energy, _d)
+    out.ray_surfaces = _p(ray_surfaces, _i32) if record_rays else None
+    out.ray_bounces = _p(ray_bounces, _i32) if record_rays else None
+    rc = _lib().oracle_trace(ctypes.byref(scene.struct), ctypes.byref(params), ctypes.byref(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle_trace failed ({rc})")
+    result = {
+        "echogram": echogram, "ambisonic_echogram": ambisonic, "hit_counts": hits, "contrib_counts": contrib,
+        "surface_energy": energy, "actual_bounces": int(out.actual_bounces), "active_ray_count": int(out.active_count),
+        "closest_queries": int(out.closest_queries), "shadow_queries": int(out.shadow_queries),
+        "nodes_visited": int(out.nodes_visited), "prims_tested": [int(v) for v in out.prims_tested],
+        "polygon_edges": int(out.polygon_edges),
+    }
+    if record_rays:
+        result["ray_surfaces"] = ray_surfaces
+        result["ray_bounces"] = ray_bounces
+    return result
+
+
+def synthesize(echogram: np.ndarray, *, fs: int, bin_dur: float, direct_delay: float, c: float,
+               white: np.ndarray) -> np.ndarray:
+    """reconstruct_band_irs (steam_rt.py:2205-2232) for one echogram; float32 [6, N]."""
+    e = np.asarray(echogram)
+    is_f32 = e.dtype == np.float32
+    e64 = np.ascontiguousarray(e, dtype=np.float64)
+    num_bins = e64.shape[1]
+    spb = max(1, int(math.ceil(float(bin_dur) * int(fs))))
+    N = num_bins * spb
+    air = air_gains(num_bins, spb, fs, direct_delay, c)
+    xo = crossover_table(fs)
+    w = np.ascontiguousarray(white, dtype=np.float64)
+    if w.shape[0] < N:
+        raise ValueError("white noise shorter than the signal")
+    out = np.zeros((6, N), dtype=np.float32)
+    rc = _lib().oracle_synthesize(_p(e64, _d), 1 if is_f32 else 0, num_bins, spb, _p(air, _d), _p(w, _d),
+                                  _p(xo, _d), _p(out, _f32))
+    if rc != 0:
+        raise RuntimeError(f"oracle_synthesize failed ({rc})")
+    return out
+
+
+_AIR = (0.0, 0.00011513, 0.00034539, 0.00057565, 0.0011513, 0.0034539)  # acoustics.py:12-22
+
+
+def air_gains(num_bins: int, spb: int, fs: int, direct_delay: float, c: float) -> np.ndarray:
+    """steam_rt.py:2190-2193 / 2226-2227 per-bin air amplitude at the bin centre."""
+    out = np.empty((6, num_bins))
+    dd = max(0.0, float(direct_delay))
+    for band, coeff in enumerate(_AIR):
+        for b in range(num_bins):
+            t = dd + (b + 0.5) * spb / int(fs)
+            out[band, b] = math.exp(-max(0.0, coeff) * (max(0.0, t) * max(0.0, float(c))))
+    return np.ascontiguousarray(out)
+
+
+def crossover_table(fs: int) -> np.ndarray:
+    """[5, 4, 5] low-pass sections at the inner crossovers (steam_rt.py:4123-4170)."""
+    nyquist = fs * 0.5
+    rows = []
+    for cutoff_hz in (176.78, 353.55, 707.11, 1414.2, 2828.4):
+        cutoff = float(np.clip(cutoff_hz, 1e-3, nyquist * 0.999))
+        sections = []
+        for s in range(4):
+            q = 1.0 / (2.0 * math.cos((2.0 * s + 1.0) * math.pi / 16.0))
+            w0 = 2.0 * math.pi * cutoff / fs
+            cw0, sw0 = math.cos(w0), math.sin(w0)
+            alpha = sw0 / (2.0 * q)
+            a0 = 1.0 + alpha
+            b0 = ((1.0 - cw0) / 2.0) / a0
+            sections.append((b0, (1.0 - cw0) / a0, b0, (-2.0 * cw0) / a0, (1.0 - alpha) / a0))
+        rows.append(sections)
+    return np.ascontiguousarray(rows, dtype=np.float64)
+
+
+def build_bvh(bounds_min: np.ndarray, bounds_max: np.ndarray, leaf_size: int = 4) -> dict[str, Any]:
+    """acoustic_agent/bvh.py:8-77."""
+    lower = np.asarray(bounds_min, dtype=np.float64)
+    upper = np.asarray(bounds_max, dtype=np.float64)
+    centroids = 0.5 * (lower + upper)
+    mn, mx, st, ct, esc, prims = [], [], [], [], [], []
+    depth_max = [0]
+    leaves = [0]
+
+    def node(ix: np.ndarray, depth: int) -> None:
+        k = len(mn)
+        mn.append(np.min(lower[ix], axis=0))
+        mx.append(np.max(upper[ix], axis=0))
+        st.append(-1)
+        ct.append(0)
+        esc.append(-1)
+        depth_max[0] = max(depth_max[0], depth)
+        if ix.size <= leaf_size:
+            ordered = np.sort(ix, kind="stable")
+            st[k] = len(prims)
+            ct[k] = int(ordered.size)
+            prims.extend(int(v) for v in ordered)
+            leaves[0] += 1
+        else:
+            axis = int(np.argmax(np.ptp(centroids[ix], axis=0)))
+            srt = ix[np.argsort(centroids[ix, axis], kind="stable")]
+            half = srt.size // 2
+            node(srt[:half], depth + 1)
+            node(srt[half:], depth + 1)
+        esc[k] = len(mn)
+
+    node(np.arange(lower.shape[0], dtype=np.int64), 1)
+    return {"bounds_min": np.asarray(mn), "bounds_max": np.asarray(mx), "start": np.asarray(st, np.int64),
+            "count": np.asarray(ct, np.int64), "escape": np.asarray(esc, np.int64),
+            "primitives": np.asarray(prims, np.int64), "node_count": len(mn), "leaf_count": leaves[0],
+            "max_depth": depth_max[0]}
+
+
+def workspace(num_rays: int, num_bounces: int, seed: int, bank_size: int = 128):
+    """The reference's host random workspace (steam_rt.py:3959-4044)."""
+    n = max(1, int(num_rays))
+    rng = np.random.default_rng(seed)
+    i = np.arange(n) + 0.5
+    z = 1.0 - 2.0 * i / n
+    r = np.sqrt(np.clip(1.0 - z * z, 0.0, 1.0))
+    theta = i * (math.pi * (3.0 - math.sqrt(5.0))) + rng.uniform(-0.02, 0.02, n)
+    directions = np.stack([np.cos(theta) * r, np.sin(theta) * r, z], axis=1)
+    k = np.arange(bank_size, dtype=np.uint64)
+    bits = k.copy()
+    inverse = np.zeros(bank_size)
+    factor = 0.5
+    while np.any(bits):
+        inverse += factor * (bits & 1)
+        bits >>= 1
+        factor *= 0.5
+    u = (np.arange(bank_size, dtype=np.float64) + 0.5) / bank_size
+    bank = np.stack([np.sqrt(u) * np.cos(2.0 * math.pi * inverse), np.sqrt(u) * np.sin(2.0 * math.pi * inverse),
+                     np.sqrt(np.clip(1.0 - u, 0.0, 1.0))], axis=1)
+    rng2 = np.random.default_rng(int(seed) + 1)
+    rnd = np.empty((num_bounces, n))
+    idx = np.empty((num_bounces, n), np.int32)
+    for b in range(num_bounces):
+        rnd[b] = rng2.random(n)
+        idx[b] = rng2.integers(0, bank_size, size=n, dtype=np.int32)
+    return directions, bank, rnd, idx
+
+
+# ---------------------------------------------------------------------------
+# Philox4x32-10 (vectorised numpy, uint64 arithmetic on 32-bit lanes)
+
+_M0, _M1 = np.uint64(0xD2511F53), np.uint64(0xCD9E8D57)
+_W0, _W1 = np.uint64(0x9E3779B9), np.uint64(0xBB67AE85)
+_MASK = np.uint64(0xFFFFFFFF)
+
+
+def philox4x32_10(c0, c1, c2, c3, k0, k1):
+    c0, c1, c2, c3 = (np.asarray(v, dtype=np.uint64) & _MASK for v in (c0, c1, c2, c3))
+    k0 = np.uint64(int(k0) & 0xFFFFFFFF)
+    k1 = np.uint64(int(k1) & 0xFFFFFFFF)
+    for _ in range(10):
+        p0 = _M0 * c0
+        p1 = _M1 * c2
+        hi0, lo0 = p0 >> np.uint64(32), p0 & _MASK
+        hi1, lo1 = p1 >> np.uint64(32), p1 & _MASK
+        c0, c1, c2, c3 = (hi1 ^ c1 ^ k0) & _MASK, lo1, (hi0 ^ c3 ^ k1) & _MASK, lo0
+        k0 = (k0 + _W0) & _MASK
+        k1 = (k1 + _W1) & _MASK
+    return c0, c1, c2, c3
+
+
+def _u01_53(hi, lo):
+    bits = ((hi >> np.uint64(5)) << np.uint64(26)) | (lo >> np.uint64(6))
+    return bits.astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def philox_workspace(num_rays: int, num_bounces: int, seed: int, stream_key: int, bank_size: int = 128):
+    """Directions, diffuse uniforms and bank indices of the GPU's counter-based mode, in float64."""
+    R = int(num_rays)
+    ray = np.arange(R, dtype=np.uint64)
+    key_lo, key_hi = int(stream_key) & 0xFFFFFFFF, (int(stream_key) >> 32) & 0xFFFFFFFF
+    s0, s1 = int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF
+    x, y, _, _ = philox4x32_10(ray, np.zeros(R, np.uint64), np.full(R, key_lo, np.uint64),
+                               np.full(R, key_hi, np.uint64), s0, s1)
+    jitter = -0.02 + 0.04 * _u01_53(x, y)
+    i = np.arange(R, dtype=np.float64) + 0.5
+    z = 1.0 - 2.0 * i / R
+    r = np.sqrt(np.clip(1.0 - z * z, 0.0, 1.0))
+    theta = i * 2.399963229728653 + jitter
+    directions = np.stack([np.cos(theta) * r, np.sin(theta) * r, z], axis=1)
+    rnd = np.empty((num_bounces, R))
+    idx = np.empty((num_bounces, R), np.int32)
+    for b in range(num_bounces):
+        x, y, zz, _ = philox4x32_10(ray, np.full(R, b + 1, np.uint64), np.full(R, key_lo, np.uint64),
+                                    np.full(R, key_hi, np.uint64), s0, s1)
+        rnd[b] = _u01_53(x, y)
+        idx[b] = ((zz * np.uint64(bank_size)) >> np.uint64(32)).astype(np.int32)
+    return directions, rnd, idx
+
+
+def philox_noise(num_samples: int, seed: int) -> np.ndarray:
+    """Synthesis noise of the counter-based mode: uniform(-1, 1), two samples per Philox block."""
+    pairs = (int(num_samples) + 1) // 2
+    p = np.arange(pairs, dtype=np.uint64)
+    s0, s1 = int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF
+    x, y, z, w = philox4x32_10(p, np.full(pairs, 1 << 24, np.uint64), np.zeros(pairs, np.uint64),
+                               np.zeros(pairs, np.uint64), s0, s1)
+    out = np.empty(2 * pairs)
+    out[0::2] = -1.0 + 2.0 * _u01_53(x, y)
+    out[1::2] = -1.0 + 2.0 * _u01_53(z, w)
+    return out[:num_samples]

@@ -1,0 +1,103 @@
+"""The drop-in ``trace_energy_field`` on the GPU: result contract and error behaviour."""
+from __future__ import annotations
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import load_case
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+# Keys of the reference CUDA backend's result (steam_rt.py:1892-1923).
+REFERENCE_KEYS = {
+    "echogram", "ambisonic_echogram", "num_bins", "bin_duration_s", "direct_delay_s", "actual_bounces",
+    "active_ray_count", "last_energy_time_s", "surface_hit_count", "surface_contribution_count", "surface_energy",
+    "visual_candidates", "accelerator", "precision", "cuda", "device_input_cache", "kernel_time_s",
+    "transfer_time_s", "intersection_backend", "source_directivity",
+}
+
+
+@pytest.fixture(scope="module")
+def backend():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from acoustic_agent_b200 import backend as b
+    return b
+
+
+def small_config(**over):
+    from acoustic_agent_b200.workloads import TraceConfig
+    cfg = TraceConfig(duration_s=0.3, rt_duration_s=0.3, rt_num_rays=256, rt_num_bounces=6, rt_precision="float32",
+                      intersection_backend="auto")
+    return replace(cfg, **over)
+
+
+def test_result_dictionary_matches_reference_contract(backend):
+    from acoustic_agent_b200 import scene, workloads
+    w = workloads.shoebox(3)
+    arrays = scene.compile_scene(w.spec)
+    field = backend.trace_energy_field(arrays, np.asarray(w.sources[0]), np.asarray(w.listeners[0]), small_config(),
+                                       render_ambisonics=True)
+    assert set(field) == REFERENCE_KEYS
+    assert field["echogram"].dtype == np.float32 and field["echogram"].shape == (6, field["num_bins"])
+    assert field["ambisonic_echogram"].shape == (6, 4, field["num_bins"])
+    assert field["accelerator"] == "b200" and field["precision"] == "float32"
+    assert field["intersection_backend"] == "linear"
+    assert field["cuda"]["compute_capability"].startswith("10.")
+    assert field["actual_bounces"] == 6
+    assert sum(field["surface_hit_count"].values()) > 0
+    assert field["kernel_time_s"] > 0.0
+
+
+def test_drop_in_float64_equals_golden(backend):
+    case = load_case("u_room_kat")
+    tr = case["trace"]
+    cfg = small_config(duration_s=tr["duration"], rt_duration_s=tr["duration"], rt_num_rays=tr["rays"],
+                       rt_num_bounces=tr["bounces"], seed=tr["seed"], rt_precision="fp64")
+    field = backend.trace_energy_field(case["arrays"], np.asarray(tr["source"]), np.asarray(tr["listener"]), cfg,
+                                       render_ambisonics=True)
+    names = case["arrays"]["names"]
+    expected = {names[i]: int(v) for i, v in enumerate(case["hit_counts"]) if v > 0}
+    assert field["surface_hit_count"] == expected
+    np.testing.assert_allclose(field["echogram"], case["echogram"].astype(np.float32), rtol=2e-6, atol=1e-12)
+    assert field["active_ray_count"] == int(case["active_ray_count"])
+
+
+def test_invalid_configuration_is_rejected(backend):
+    from acoustic_agent_b200 import scene, workloads
+    w = workloads.shoebox(3)
+    arrays = scene.compile_scene(w.spec)
+    with pytest.raises(ValueError):
+        backend.trace_energy_field(arrays, np.asarray(w.sources[0]), np.asarray(w.listeners[0]),
+                                   small_config(rt_precision="float16"))
+    with pytest.raises(ValueError):
+        backend.trace_energy_field(arrays, np.asarray(w.sources[0]), np.asarray(w.listeners[0]),
+                                   small_config(intersection_backend="octree"))
+    with pytest.raises(ValueError):
+        backend.trace_energy_field(arrays, np.asarray(w.sources[0]), np.asarray(w.listeners[0]), small_config(),
+                                   source_model="laser")
+
+
+def test_install_routes_only_the_b200_accelerator(backend):
+    import types
+    calls = []
+    fake = types.SimpleNamespace(
+        trace_energy_field=lambda *a, **k: calls.append("reference") or {"accelerator": "numba"},
+        _normalize_rt_accelerator=lambda v: v if v in {"auto", "numba", "cuda"} else (_ for _ in ()).throw(
+            ValueError("rt_accelerator must be auto, numba, or cuda")))
+    handle = backend.install(fake)
+    from acoustic_agent_b200 import scene, workloads
+    w = workloads.shoebox(3)
+    arrays = scene.compile_scene(w.spec)
+    field = fake.trace_energy_field(arrays, np.asarray(w.sources[0]), np.asarray(w.listeners[0]), small_config())
+    assert field["accelerator"] == "b200"
+    assert fake.trace_energy_field(arrays, None, None, small_config(rt_accelerator="numba"))["accelerator"] == "numba"
+    assert fake._normalize_rt_accelerator("b200") == "b200"
+    with pytest.raises(ValueError):
+        fake._normalize_rt_accelerator("metal")
+    handle.uninstall()
+    with pytest.raises(ValueError):
+        fake._normalize_rt_accelerator("b200")

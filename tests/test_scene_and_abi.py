@@ -1,0 +1,121 @@
+"""Host-side pieces that need no GPU: scene compiler, native BVH builder, ABI surface, validation."""
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO, load_case
+
+from acoustic_agent_b200 import _lib, scene, workloads
+from acoustic_agent_b200.directivity import source_directivity, source_forward
+from acoustic_agent_b200.backend import normalize_precision, resolve_intersection_backend
+
+ARRAY_KEYS = ("kinds", "wall_a", "wall_delta", "wall_z", "z_values", "box_center", "box_axis_u", "box_axis_v",
+              "box_half", "box_z", "normals", "reflection", "scattering", "corners", "surface_bounds_min",
+              "surface_bounds_max", "bvh_bounds_min", "bvh_bounds_max", "bvh_start", "bvh_count", "bvh_escape",
+              "bvh_primitives")
+
+
+def test_scene_compiler_matches_reference_arrays(golden_case):
+    _, case = golden_case
+    compiled = scene.compile_scene(case["spec"])
+    for key in ARRAY_KEYS:
+        np.testing.assert_array_equal(np.asarray(compiled[key]), case["arrays"][key], err_msg=key)
+    assert tuple(compiled["names"]) == case["arrays"]["names"]
+
+
+def test_native_bvh_builder_matches_reference(golden_case):
+    _, case = golden_case
+    a = case["arrays"]
+    bvh = _lib.build_bvh(a["surface_bounds_min"], a["surface_bounds_max"])
+    for key in ("bounds_min", "bounds_max", "start", "count", "escape", "primitives"):
+        np.testing.assert_array_equal(bvh[key], a[f"bvh_{key}"], err_msg=key)
+
+
+def test_native_bvh_large_random_scene_matches_oracle():
+    from oracle import oracle
+    rng = np.random.default_rng(3)
+    lo = rng.uniform(0, 50, (3000, 3))
+    hi = lo + rng.uniform(0, 2, (3000, 3))
+    hi[::7] = lo[::7]  # degenerate boxes and centroid ties
+    ours = _lib.build_bvh(lo, hi)
+    ref = oracle.build_bvh(lo, hi)
+    for key in ("bounds_min", "bounds_max", "start", "count", "escape", "primitives"):
+        np.testing.assert_array_equal(ours[key], ref[key])
+    assert ours["max_depth"] == ref["max_depth"] and ours["leaf_count"] == ref["leaf_count"]
+
+
+@pytest.mark.parametrize("lo,hi,message", [
+    (np.zeros((0, 3)), np.zeros((0, 3)), "at least one surface"),
+    (np.asarray([[0.0, 0.0, np.nan]]), np.ones((1, 3)), "finite"),
+    (np.ones((1, 3)), np.zeros((1, 3)), "below minimum"),
+])
+def test_bvh_builder_rejects_what_the_reference_rejects(lo, hi, message):
+    with pytest.raises(ValueError, match=message):
+        _lib.build_bvh(lo, hi)
+
+
+def test_library_exports_every_declared_symbol():
+    header = (REPO / "include" / "acoustic_rt.h").read_text()
+    declared = set(re.findall(r"^(?:const char \*|int )\s*\*?(ac_\w+)\(", header, flags=re.M))
+    assert declared, "no declarations parsed"
+    lib = ctypes.CDLL(str(_lib.LIBRARY_PATH))
+    missing = [name for name in sorted(declared) if not hasattr(lib, name)]
+    assert not missing
+    assert declared == set(_lib.SIGNATURES), "ctypes binding and header disagree"
+    assert _lib.load().ac_abi_version() == 1
+
+
+def test_scene_create_rejects_bad_descriptions_without_touching_the_gpu():
+    lib = _lib.load()
+    handle = ctypes.c_void_p()
+    assert lib.ac_scene_create(None, ctypes.byref(handle)) == _lib.AC_ERR_INVALID
+    desc = _lib.ACSceneDesc()
+    desc.num_surfaces = 0
+    assert lib.ac_scene_create(ctypes.byref(desc), ctypes.byref(handle)) == _lib.AC_ERR_INVALID
+    assert b"at least one surface" in lib.ac_last_error()
+
+
+def test_trace_validation_happens_before_launch():
+    lib = _lib.load()
+    params = _lib.ACTraceParams()
+    outputs = _lib.ACTraceOutputs()
+    assert lib.ac_trace(None, ctypes.byref(params), ctypes.byref(outputs), None) == _lib.AC_ERR_INVALID
+
+
+def test_directivity_and_config_normalisation_match_reference_rules():
+    assert source_directivity("cardioid")["dipole_weight"] == 0.5
+    assert source_directivity({"type": "weighted_dipole", "pattern": "focused"})["dipole_power"] == 4.0
+    np.testing.assert_allclose(source_forward(source_directivity({"type": "omni", "orientation_deg": 90})),
+                               [0.0, 1.0, 0.0], atol=1e-15)
+    with pytest.raises(ValueError):
+        source_directivity("laser")
+    with pytest.raises(ValueError):
+        source_directivity({"type": "weighted_dipole", "dipole_weight": 1.5})
+    assert normalize_precision("fp64") == "float64"
+    with pytest.raises(ValueError):
+        normalize_precision("float16")
+    assert resolve_intersection_backend("auto", 16, 16) == "bvh"
+    assert resolve_intersection_backend("auto", 15, 16) == "linear"
+    with pytest.raises(ValueError):
+        resolve_intersection_backend("octree", 10, 16)
+
+
+def test_workloads_are_seeded_and_shaped_like_the_configs():
+    a = workloads.shoebox(1729)
+    assert scene.count_surfaces(a.spec) == 6 and a.config.num_bins == 100
+    u = workloads.u_furnished(1729)
+    assert u.num_traces == 8 and u.config.num_bins == 2000 and u.config.rt_num_rays == 200_000
+    s = scene.compile_scene(u.spec)
+    assert s.num_surfaces == 30
+    apt = workloads.apartment(1729)
+    sa = scene.compile_scene(apt.spec)
+    assert 6 <= apt.meta["rooms"] <= 8 and 4 <= apt.meta["doors"] <= 8
+    assert sa.num_surfaces > 200
+    again = workloads.apartment(1729)
+    assert again.spec == apt.spec
+    mix = workloads.mixed_batch(5, 8)
+    assert len(mix) == 8 and all(1 <= len(w.sources) <= 4 and 1 <= len(w.listeners) <= 8 for w in mix)
