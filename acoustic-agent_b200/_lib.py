@@ -51,7 +51,7 @@ class ACSceneDesc(ctypes.Structure):
         ("corners", c_double_p), ("surface_bounds_min", c_double_p), ("surface_bounds_max", c_double_p),
         ("bvh_node_count", ctypes.c_int64), ("bvh_bounds_min", c_double_p), ("bvh_bounds_max", c_double_p),
         ("bvh_start", c_int64_p), ("bvh_count", c_int64_p), ("bvh_escape", c_int64_p),
-        ("bvh_primitives", c_int64_p), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("bvh_primitives", c_int64_p), ("device", ctypes.c_int32), ("cluster_size", ctypes.c_int32),
     ]
 
 
@@ -59,7 +59,7 @@ class ACSceneInfo(ctypes.Structure):
     _fields_ = [
         ("num_surfaces", ctypes.c_int64), ("num_corners", ctypes.c_int64), ("node_count", ctypes.c_int64),
         ("leaf_count", ctypes.c_int64), ("device_bytes", ctypes.c_int64), ("device", ctypes.c_int32),
-        ("max_leaf", ctypes.c_int32),
+        ("max_leaf", ctypes.c_int32), ("num_clusters", ctypes.c_int64),
     ]
 
 
@@ -121,7 +121,7 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_energy_scale": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACTraceParams), c_double_p]),
     "ac_trace": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACTraceParams), ctypes.POINTER(ACTraceOutputs),
                                 ctypes.c_void_p]),
-    "ac_batch_workspace_size": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ACBatchConfig),
+    "ac_batch_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACJob), ctypes.c_int32, ctypes.POINTER(ACBatchConfig),
                                                ctypes.POINTER(ctypes.c_size_t)]),
     "ac_trace_batch": (ctypes.c_int, [ctypes.POINTER(ACJob), ctypes.c_int32, ctypes.POINTER(ACBatchConfig),
                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),

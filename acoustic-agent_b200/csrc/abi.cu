@@ -44,9 +44,11 @@ double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p) {
                                          std::max(1.0, std::fabs(1.0 - scene->min_scattering));
     const double growth = std::min(1e300, std::pow(std::max(1.0, scene->max_reflection), B + 1.0));
     const double max_deposit = ray_scale * gain * distance_term * lobe * growth;
-    const double budget = 6.0 * R * B * max_deposit;
+    // Accumulators are 128-bit, so only one deposit must fit an int64 quantum:
+    // the six-band sum of the largest possible deposit stays below 2^62.
+    const double budget = 6.0 * max_deposit;
     int exponent = static_cast<int>(std::floor(std::log2(std::ldexp(1.0, 62) / budget)));
-    exponent = std::min(100, std::max(-60, exponent));
+    exponent = std::min(200, std::max(-60, exponent));
     return std::ldexp(1.0, exponent);
 }
 
@@ -139,11 +141,14 @@ int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_out
     return ac::launch_trace_f32(scene, params, outputs, scale, stream);
 }
 
-int ac_batch_workspace_size(int32_t num_jobs, const ac_batch_config *config, size_t *bytes) {
-    (void)config;
-    if (num_jobs < 0 || !bytes) return ac::fail(AC_ERR_INVALID, "ac_batch_workspace_size: bad argument");
+int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, size_t *bytes) {
+    if (num_jobs < 0 || !bytes || (num_jobs > 0 && !jobs))
+        return ac::fail(AC_ERR_INVALID, "ac_batch_workspace_size: bad argument");
+    for (int32_t j = 0; j < num_jobs; ++j)
+        if (!jobs[j].scene) return ac::fail(AC_ERR_INVALID, "job %d has no scene", j);
     // Enough for either precision; the two partitions of a mixed batch run back to back.
-    *bytes = std::max(ac::batch_workspace_bytes_f32(num_jobs), ac::batch_workspace_bytes_f64(num_jobs));
+    *bytes = std::max(ac::batch_workspace_bytes_f32(jobs, num_jobs, config),
+                      ac::batch_workspace_bytes_f64(jobs, num_jobs, config));
     return AC_OK;
 }
 

@@ -28,22 +28,63 @@ template <>
 inline double tag_value<double>(int tag) { return static_cast<double>(tag); }
 
 struct Offsets {
-    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, total;  // in elements
+    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, clusters, cluster_prims, edges, total;  // elements
 };
 
 inline size_t round4(size_t v) { return (v + 3) & ~static_cast<size_t>(3); }
 
-Offsets layout(size_t S, size_t P, size_t N, size_t C) {
+Offsets layout(size_t S, size_t P, size_t N, size_t C, size_t NC) {
     Offsets o{};
     size_t off = 0;
-    o.prims_linear = off; off += round4(S * ac::kPrimStride);
-    o.prims_leaf = off;   off += round4(P * ac::kPrimStride);
-    o.nodes = off;        off += round4(N * ac::kNodeStride);
-    o.mats = off;         off += round4(S * ac::kMatStride);
-    o.corners = off;      off += round4(C * 2);
-    o.normals = off;      off += round4(S * 3);
+    o.prims_linear = off;  off += round4(S * ac::kPrimStride);
+    o.prims_leaf = off;    off += round4(P * ac::kPrimStride);
+    o.nodes = off;         off += round4(N * ac::kNodeStride);
+    o.mats = off;          off += round4(S * ac::kMatStride);
+    o.corners = off;       off += round4(C * 2);
+    o.normals = off;       off += round4(S * 3);
+    o.clusters = off;      off += round4(NC * ac::kClusterStride);
+    o.cluster_prims = off; off += round4(NC ? S * ac::kPrimStride : 0);
+    o.edges = off;         off += round4(NC ? C * 4 : 0);
     o.total = off;
     return o;
+}
+
+// Padded per-surface AABBs (steam_rt.py:234-262), used when the caller passes none.
+void surface_bounds(const ac_scene_desc *d, std::vector<double> &lo, std::vector<double> &hi) {
+    const int64_t S = d->num_surfaces;
+    lo.assign(3 * S, 0.0);
+    hi.assign(3 * S, 0.0);
+    double cx0 = 0, cx1 = 0, cy0 = 0, cy1 = 0;
+    for (int64_t c = 0; c < d->num_corners; ++c) {
+        const double x = d->corners[2 * c], y = d->corners[2 * c + 1];
+        if (c == 0 || x < cx0) cx0 = x;
+        if (c == 0 || x > cx1) cx1 = x;
+        if (c == 0 || y < cy0) cy0 = y;
+        if (c == 0 || y > cy1) cy1 = y;
+    }
+    for (int64_t i = 0; i < S; ++i) {
+        double l[3], h[3];
+        if (d->kinds[i] == AC_KIND_WALL) {
+            const double ax = d->wall_a[2 * i], ay = d->wall_a[2 * i + 1];
+            const double bx = ax + d->wall_delta[2 * i], by = ay + d->wall_delta[2 * i + 1];
+            l[0] = std::min(ax, bx); l[1] = std::min(ay, by); l[2] = d->wall_z[2 * i];
+            h[0] = std::max(ax, bx); h[1] = std::max(ay, by); h[2] = d->wall_z[2 * i + 1];
+        } else if (d->kinds[i] == AC_KIND_BOX) {
+            const double ex = std::fabs(d->box_axis_u[2 * i]) * d->box_half[2 * i] +
+                              std::fabs(d->box_axis_v[2 * i]) * d->box_half[2 * i + 1];
+            const double ey = std::fabs(d->box_axis_u[2 * i + 1]) * d->box_half[2 * i] +
+                              std::fabs(d->box_axis_v[2 * i + 1]) * d->box_half[2 * i + 1];
+            l[0] = d->box_center[2 * i] - ex; l[1] = d->box_center[2 * i + 1] - ey; l[2] = d->box_z[2 * i];
+            h[0] = d->box_center[2 * i] + ex; h[1] = d->box_center[2 * i + 1] + ey; h[2] = d->box_z[2 * i + 1];
+        } else {
+            l[0] = cx0; l[1] = cy0; l[2] = d->z_values[i];
+            h[0] = cx1; h[1] = cy1; h[2] = d->z_values[i];
+        }
+        for (int a = 0; a < 3; ++a) {
+            lo[3 * i + a] = l[a] - 2.0e-6;
+            hi[3 * i + a] = h[a] + 2.0e-6;
+        }
+    }
 }
 
 template <typename T>
@@ -81,14 +122,45 @@ void pack_record(const ac_scene_desc *d, int64_t si, T *rec) {
 }
 
 template <typename T>
-int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, ac_scene_s *s, void **storage, size_t *bytes,
-                    ac::SceneDev<T> *view) {
+int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clusters, ac_scene_s *s,
+                    void **storage, size_t *bytes, ac::SceneDev<T> *view) {
     const size_t S = static_cast<size_t>(d->num_surfaces);
     const size_t N = static_cast<size_t>(bvh.node_count);
     const size_t P = S;
     const size_t C = static_cast<size_t>(d->num_corners);
-    const Offsets o = layout(S, P, N, C);
+    const size_t NC = clusters ? static_cast<size_t>(clusters->leaf_count) : 0;
+    const Offsets o = layout(S, P, N, C, NC);
     std::vector<T> host(o.total, T(0));
+    if (clusters) {
+        // Float32 scan: clusters = leaves of the cluster BVH in preorder.
+        size_t c = 0;
+        for (int64_t n = 0; n < clusters->node_count; ++n) {
+            if (clusters->count[n] <= 0) continue;
+            T *cp = host.data() + o.clusters + c * ac::kClusterStride;
+            for (int a = 0; a < 3; ++a) {
+                cp[a] = T(clusters->bounds_min[3 * n + a]);
+                cp[4 + a] = T(clusters->bounds_max[3 * n + a]);
+            }
+            cp[3] = tag_value<T>(static_cast<int>(clusters->start[n]));
+            cp[7] = tag_value<T>(static_cast<int>(clusters->count[n]));
+            ++c;
+        }
+        for (size_t k = 0; k < S; ++k)
+            pack_record<T>(d, clusters->primitives[k], host.data() + o.cluster_prims + k * ac::kPrimStride);
+        // Polygon edges for the even-odd test: {x_i, y_i, y_j, (x_j - x_i) / (y_j - y_i)} with j the
+        // previous corner (steam_rt.py:4259-4274); an edge the reference skips gets y_j = y_i.
+        for (size_t i = 0; i < C; ++i) {
+            const size_t j = (i + C - 1) % C;
+            const double xi = d->corners[2 * i], yi = d->corners[2 * i + 1];
+            const double xj = d->corners[2 * j], yj = d->corners[2 * j + 1];
+            T *e = host.data() + o.edges + 4 * i;
+            const bool skip = std::fabs(yj - yi) <= 1e-12;
+            e[0] = T(xi);
+            e[1] = T(yi);
+            e[2] = skip ? T(yi) : T(yj);
+            e[3] = skip ? T(0) : T((xj - xi) / (yj - yi));
+        }
+    }
     for (size_t si = 0; si < S; ++si) pack_record<T>(d, static_cast<int64_t>(si), host.data() + o.prims_linear + si * ac::kPrimStride);
     for (size_t k = 0; k < P; ++k)
         pack_record<T>(d, bvh.primitives[k], host.data() + o.prims_leaf + k * ac::kPrimStride);
@@ -131,7 +203,15 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, ac_scene_s *s, vo
     view->num_nodes = static_cast<int32_t>(N);
     view->num_corners = static_cast<int32_t>(C);
     view->num_leaf_prims = static_cast<int32_t>(P);
-    (void)s;
+    if (clusters) {
+        const float *fbase = reinterpret_cast<const float *>(dev);
+        s->fast.clusters = fbase + o.clusters;
+        s->fast.prims = fbase + o.cluster_prims;
+        s->fast.edges = fbase + o.edges;
+        s->fast.num_clusters = static_cast<int32_t>(NC);
+        s->fast.num_edges = static_cast<int32_t>(C);
+        s->num_clusters = static_cast<int64_t>(NC);
+    }
     return AC_OK;
 }
 
@@ -232,8 +312,26 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
         s->max_scattering = std::max(s->max_scattering, d->scattering[i]);
         s->min_scattering = std::min(s->min_scattering, d->scattering[i]);
     }
-    int rc = pack_and_upload<float>(d, bvh, s, &s->storage_f32, &s->bytes_f32, &s->f32);
-    if (rc == AC_OK) rc = pack_and_upload<double>(d, bvh, s, &s->storage_f64, &s->bytes_f64, &s->f64);
+    // Cluster BVH for the float32 scan: leaves of `cluster_size` surfaces.
+    std::vector<double> slo, shi;
+    const double *blo = d->surface_bounds_min, *bhi = d->surface_bounds_max;
+    if (!blo || !bhi) {
+        surface_bounds(d, slo, shi);
+        blo = slo.data();
+        bhi = shi.data();
+    }
+    s->cluster_size = d->cluster_size > 0 ? std::min(d->cluster_size, 64) : 8;
+    const size_t cap = 2 * static_cast<size_t>(S);
+    std::vector<double> cmin(3 * cap), cmax(3 * cap);
+    std::vector<int64_t> cstart(cap), ccount(cap), cesc(cap), cprims(S);
+    ac_bvh cbvh{cmin.data(), cmax.data(), cstart.data(), ccount.data(), cesc.data(), cprims.data(), 0, 0, 0};
+    int rc = ac_bvh_build(blo, bhi, S, s->cluster_size, &cbvh);
+    if (rc != AC_OK) {
+        delete s;
+        return rc;
+    }
+    rc = pack_and_upload<float>(d, bvh, &cbvh, s, &s->storage_f32, &s->bytes_f32, &s->f32);
+    if (rc == AC_OK) rc = pack_and_upload<double>(d, bvh, nullptr, s, &s->storage_f64, &s->bytes_f64, &s->f64);
     if (rc != AC_OK) {
         if (s->storage_f32) cudaFree(s->storage_f32);
         delete s;
@@ -261,5 +359,6 @@ extern "C" int ac_scene_get_info(ac_scene_t s, ac_scene_info *info) {
     info->device_bytes = static_cast<int64_t>(s->bytes_f32 + s->bytes_f64);
     info->device = s->device;
     info->max_leaf = s->max_leaf;
+    info->num_clusters = s->num_clusters;
     return AC_OK;
 }

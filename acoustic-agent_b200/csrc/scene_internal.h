@@ -6,7 +6,7 @@
 #include <cstdint>
 
 #include "acoustic_rt.h"
-#include "trace_kernel.cuh"
+#include "trace_fast.cuh"
 
 struct ac_scene_s {
     int32_t device = 0;
@@ -21,6 +21,9 @@ struct ac_scene_s {
     size_t bytes_f64 = 0;
     ac::SceneDev<float> f32{};
     ac::SceneDev<double> f64{};
+    ac::FastScene fast{};          // float32 cluster scan data (inside storage_f32)
+    int32_t cluster_size = 8;
+    int64_t num_clusters = 0;
     double max_reflection = 0.0;   // bound used when choosing the fixed-point scale
     double max_scattering = 0.0;
     double min_scattering = 0.0;
@@ -35,8 +38,8 @@ inline const SceneDev<float> &scene_view<float>(const ac_scene_s *s) { return s-
 template <>
 inline const SceneDev<double> &scene_view<double>(const ac_scene_s *s) { return s->f64; }
 
-// Power-of-two fixed-point scale such that no echogram bin, ambisonic bin or
-// per-surface energy accumulator can exceed 2^62 in magnitude.
+// Power-of-two fixed-point scale: the largest deposit the scene and parameters
+// allow, summed over the six bands, maps to at most 2^62.
 double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p);
 
 // Validates trace parameters against a scene (host-side, before any launch).
@@ -53,7 +56,7 @@ int launch_batch_f32(const ac_job *jobs, const int32_t *indices, int32_t count, 
                      void *workspace, size_t bytes, void *host_staging, void *stream);
 int launch_batch_f64(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg,
                      void *workspace, size_t bytes, void *host_staging, void *stream);
-size_t batch_workspace_bytes_f32(int32_t count);
-size_t batch_workspace_bytes_f64(int32_t count);
+size_t batch_workspace_bytes_f32(const ac_job *jobs, int32_t count, const ac_batch_config *cfg);
+size_t batch_workspace_bytes_f64(const ac_job *jobs, int32_t count, const ac_batch_config *cfg);
 
 }  // namespace ac

@@ -7,7 +7,8 @@
 // -fmad=false: the reference evaluates each multiply and add separately in
 // float64, and each biquad section hands its successor a float32-rounded signal.
 //
-// The recursion is sequential in time, so parallelism comes from elsewhere:
+// The raw band signals are materialised first by a fully parallel kernel.  The
+// recursion itself is sequential in time, so parallelism comes from elsewhere:
 // one warp is a systolic array of 8 four-section low-pass chains.  Lane
 // (unit, chain, stage) runs one biquad section; each iteration it passes its
 // float32 output one lane up, so section s works on sample n-s while section
@@ -42,7 +43,7 @@ struct SynthArgs {
 inline size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
 struct SynthLayout {
-    size_t amps, air, wtab, white, total;
+    size_t amps, air, wtab, white, raw, total;
 };
 
 SynthLayout synth_layout(const ac_synth_params *p) {
@@ -54,6 +55,7 @@ SynthLayout synth_layout(const ac_synth_params *p) {
     l.air = off;  off = align256(off + (p->air ? 0 : cells * sizeof(double)));
     l.wtab = off; off = align256(off + static_cast<size_t>(p->samples_per_bin) * sizeof(double));
     l.white = off; off = align256(off + (p->rng_mode == AC_RNG_PHILOX ? N * sizeof(double) : 0));
+    l.raw = off;  off = align256(off + static_cast<size_t>(p->num_rirs) * kSynthBands * N * sizeof(double));
     l.total = off;
     return l;
 }
@@ -92,9 +94,46 @@ __global__ void synth_prepare_kernel(const float *echo, const double *direct_del
     }
 }
 
-__global__ void __launch_bounds__(128) synth_filter_kernel(const double *amps, const double *air, const double *wtab,
-                                                           const double *white, size_t white_stride,
-                                                           const __grid_constant__ SynthArgs a, float *out) {
+// Raw band signals (steam_rt.py:2221-2230): the envelope interpolated from the
+// previous bin, times the bin's air gain, times the noise -- every sample
+// independent, so one thread per sample.
+__global__ void synth_raw_kernel(const double *amps, const double *air, const double *wtab, const double *white,
+                                 size_t white_stride, const __grid_constant__ SynthArgs a, double *raw) {
+    const size_t N = static_cast<size_t>(a.num_bins) * a.spb;
+    const size_t total = static_cast<size_t>(a.num_rirs) * kSynthBands * N;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const size_t unit = i / N;            // j * 6 + band
+        const size_t n = i - unit * N;
+        const size_t j = unit / kSynthBands;
+        const int bin = static_cast<int>(n / a.spb);
+        const int k = static_cast<int>(n - static_cast<size_t>(bin) * a.spb);
+        const size_t row = unit * a.num_bins;
+        const double w = wtab[k];
+        const double cur = amps[row + bin];
+        const double prev = bin == 0 ? cur : amps[row + bin - 1];
+        double seg = (1.0 - w) * prev + w * cur;
+        seg = seg * air[row + bin];
+        raw[i] = seg * white[j * white_stride + n];
+    }
+}
+
+// One section of an eight-pole low-pass (steam_rt.py:4131-4146).
+struct Section {
+    double b0, b1, b2, a1, a2, x1, x2, y1, y2;
+
+    __device__ __forceinline__ float step(double in) {
+        const double y0 = b0 * in + b1 * x1 + b2 * x2 - a1 * y1 - a2 * y2;
+        x2 = x1; x1 = in;
+        y2 = y1; y1 = y0;
+        return static_cast<float>(y0);
+    }
+};
+
+constexpr int kPrefetch = 4;
+
+__global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, const __grid_constant__ SynthArgs a,
+                                                           float *out) {
     const unsigned full = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int warp = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
@@ -103,7 +142,6 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *amps, c
     const int unit = warp * 4 + (lane >> 3);
     const int units = a.num_rirs * kSynthBands;
     const bool valid_unit = unit < units;
-    const int j = valid_unit ? unit / kSynthBands : 0;
     const int band = valid_unit ? unit % kSynthBands : 0;
     int cutoff;
     bool active;
@@ -112,51 +150,45 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *amps, c
     else { cutoff = chain == 0 ? band : band - 1; active = true; }
     active = active && valid_unit;
     const double *co = a.crossover + cutoff * 20 + stage * 5;
-    const double b0 = co[0], b1 = co[1], b2 = co[2], a1 = co[3], a2 = co[4];
-    double x1 = 0.0, x2 = 0.0, y1 = 0.0, y2 = 0.0;
+    Section sec{co[0], co[1], co[2], co[3], co[4], 0.0, 0.0, 0.0, 0.0};
 
     const int N = a.num_bins * a.spb;
-    const size_t row = (static_cast<size_t>(j) * kSynthBands + band) * a.num_bins;
-    const double *white_row = white + static_cast<size_t>(j) * white_stride;
-    float *out_row = out + (static_cast<size_t>(j) * kSynthBands + band) * static_cast<size_t>(N);
+    const double *x = raw + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
+    float *out_row = out + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
 
-    float carry_y = 0.0f;
-    double carry_x = 0.0;
-    int bin = 0, k = 0;  // sample `it` = bin * spb + k for the section-0 lanes
-    for (int it = 0; it < N + 3; ++it) {
-        const float from_prev = __shfl_up_sync(full, carry_y, 1);
-        const double x_prev = __shfl_up_sync(full, carry_x, 1);
-        double x_new = 0.0;
-        if (valid_unit && it < N) {
-            // steam_rt.py:2221-2230: interpolated envelope * air gain * noise
-            const double w = __ldg(wtab + k);
-            const double cur = __ldg(amps + row + bin);
-            const double prev = bin == 0 ? cur : __ldg(amps + row + bin - 1);
-            double seg = (1.0 - w) * prev + w * cur;
-            seg = seg * __ldg(air + row + bin);
-            x_new = seg * __ldg(white_row + it);
+    // Section 0 reads sample `it`; section s works on sample it - s with the
+    // float32 output section s-1 produced one iteration earlier.
+    double ahead[kPrefetch];
+#pragma unroll
+    for (int u = 0; u < kPrefetch; ++u) ahead[u] = (valid_unit && u < N) ? __ldg(x + u) : 0.0;
+    float carry = 0.0f;
+    for (int base = 0; base < N + 3; base += kPrefetch) {
+        double next[kPrefetch];
+#pragma unroll
+        for (int u = 0; u < kPrefetch; ++u) {
+            const int m = base + kPrefetch + u;
+            next[u] = (valid_unit && m < N) ? __ldg(x + m) : 0.0;
         }
-        if (++k == a.spb) { k = 0; ++bin; }
-        const double in = stage == 0 ? x_new : static_cast<double>(from_prev);
-        const double x_orig = stage == 0 ? x_new : x_prev;
-        const int n = it - stage;
-        float y_f = 0.0f;
-        if (active && n >= 0 && n < N) {
-            const double y0 = b0 * in + b1 * x1 + b2 * x2 - a1 * y1 - a2 * y2;
-            y_f = static_cast<float>(y0);
-            x2 = x1; x1 = in;
-            y2 = y1; y1 = y0;
+#pragma unroll
+        for (int u = 0; u < kPrefetch; ++u) {
+            const int it = base + u;
+            const float from_prev = __shfl_up_sync(full, carry, 1);
+            const double in = stage == 0 ? ahead[u] : static_cast<double>(from_prev);
+            const int n = it - stage;
+            float y = 0.0f;
+            if (active && n >= 0 && n < N) y = sec.step(in);
+            carry = y;
+            const float lower = __shfl_down_sync(full, y, 4);
+            if (stage == 3 && chain == 0 && active && n >= 0 && n < N) {
+                float o;
+                if (band == 0) o = y;
+                else if (band == kSynthBands - 1) o = static_cast<float>(__ldg(x + n) - static_cast<double>(y));
+                else o = y - lower;
+                out_row[n] = o;
+            }
         }
-        carry_y = y_f;
-        carry_x = x_orig;
-        const float lower = __shfl_down_sync(full, y_f, 4);
-        if (stage == 3 && chain == 0 && active && n >= 0 && n < N) {
-            float o;
-            if (band == 0) o = y_f;
-            else if (band == kSynthBands - 1) o = static_cast<float>(x_orig - static_cast<double>(y_f));
-            else o = y_f - lower;
-            out_row[n] = o;
-        }
+#pragma unroll
+        for (int u = 0; u < kPrefetch; ++u) ahead[u] = next[u];
     }
 }
 
@@ -206,11 +238,15 @@ extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, f
     const double *air_table = p->air ? p->air : air;
     const double *noise = white ? white : p->white;
     const size_t stride = (white || p->white_shared) ? 0 : static_cast<size_t>(N);
+    double *raw = reinterpret_cast<double *>(ws + l.raw);
+    const size_t samples = static_cast<size_t>(p->num_rirs) * 6 * static_cast<size_t>(N);
+    const int raw_grid = static_cast<int>(std::min<size_t>((samples + 255) / 256, 65536));
+    ac::synth_raw_kernel<<<raw_grid, 256, 0, stream>>>(amps, air_table, wtab, noise, stride, a, raw);
+    AC_CUDA_TRY(cudaGetLastError());
     const int units = p->num_rirs * 6;
     const int warps = (units + 3) / 4;
-    const int threads = 128;
-    const int blocks = (warps * 32 + threads - 1) / threads;
-    ac::synth_filter_kernel<<<blocks, threads, 0, stream>>>(amps, air_table, wtab, noise, stride, a, band_irs);
+    const int threads = 32;  // one warp per block: spread the sequential chains over all SMs
+    ac::synth_filter_kernel<<<warps, threads, 0, stream>>>(raw, a, band_irs);
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
 }

@@ -13,8 +13,9 @@
 //     the warp's other rays finish;
 //   * many jobs (scene, source, listener, outputs) may share one launch; a
 //     lane maps its global ray index to (job, ray) through a prefix table;
-//   * the echogram is accumulated as int64 fixed point (energy * 2^s rounded
-//     per deposit), so the result is bit-identical for any schedule;
+//   * the echogram is accumulated as 128-bit fixed point (energy * 2^s rounded
+//     per deposit to int64, summed exactly), so the result is bit-identical
+//     for any schedule;
 //   * per-surface hit counters are aggregated per warp (match_any) before
 //     the atomic, removing the same-address contention of one atomic per
 //     bounce per ray;
@@ -132,11 +133,11 @@ struct Job {
     const T *diffuse_random;       // [B,R]
     const int32_t *diffuse_indices;// [B,R]
     const T *diffuse_bank;         // [K,3]
-    unsigned long long *echogram_fx;   // [6,bins]
-    unsigned long long *ambisonic_fx;  // [6,4,bins] or null
+    unsigned long long *echogram_fx;   // [6,bins,2] 128-bit fixed point (low, high)
+    unsigned long long *ambisonic_fx;  // [6,4,bins,2] or null
     unsigned long long *hit_counts;    // [S]
     unsigned long long *contrib_counts;// [S]
-    unsigned long long *surface_energy_fx; // [S]
+    unsigned long long *surface_energy_fx; // [S,2]
     unsigned long long *counters;      // [8]
     int32_t *ray_surfaces;             // [R,B] or null
 };
@@ -408,6 +409,19 @@ __device__ __forceinline__ double t_pow<double>(double x, double y) { return pow
 __device__ __forceinline__ long long quantize(float e, double scale) { return __double2ll_rn(static_cast<double>(e) * scale); }
 __device__ __forceinline__ long long quantize(double e, double scale) { return __double2ll_rn(e * scale); }
 
+// Exact 128-bit two's-complement accumulation of a signed 64-bit quantum into
+// acc[0] (low word) / acc[1] (high word).  The low-word atomic returns the
+// value it replaced, so the carry is known exactly; both word updates are
+// commutative, so the final 128-bit value does not depend on the order.
+__device__ __forceinline__ void add128(unsigned long long *acc, long long q) {
+    if (q == 0) return;
+    const unsigned long long uq = static_cast<unsigned long long>(q);
+    const unsigned long long old = atomicAdd(acc, uq);
+    const unsigned long long carry = (old + uq < old) ? 1ull : 0ull;
+    const unsigned long long hi = carry + (q < 0 ? ~0ull : 0ull);
+    if (hi) atomicAdd(acc + 1, hi);
+}
+
 // Initial direction of ray `ri` of a job.
 template <typename T>
 __device__ __forceinline__ void initial_direction(const Job<T> &job, int64_t ri, T *d) {
@@ -419,17 +433,19 @@ __device__ __forceinline__ void initial_direction(const Job<T> &job, int64_t ri,
     }
     // Jittered Fibonacci sphere (steam_rt.py:3959-3968) with the jitter drawn
     // from the counter-based stream instead of a sequential generator.
+    // Explicitly rounded operations: the result must not depend on whether the
+    // translation unit allows FMA contraction.
     const u32x4 r = trace_draw(job.seed, job.stream_key, static_cast<uint32_t>(ri), 0u);
-    const double jitter = -0.02 + 0.04 * u01_53(r.x, r.y);
+    const double jitter = __dadd_rn(-0.02, __dmul_rn(0.04, u01_53(r.x, r.y)));
     const double i = static_cast<double>(ri) + 0.5;
-    const double z = 1.0 - 2.0 * i / static_cast<double>(job.num_rays);
-    double rr = 1.0 - z * z;
-    rr = sqrt(rr < 0.0 ? 0.0 : (rr > 1.0 ? 1.0 : rr));
-    const double theta = i * kGoldenAngle + jitter;
+    const double z = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(2.0, i), static_cast<double>(job.num_rays)));
+    double rr = __dsub_rn(1.0, __dmul_rn(z, z));
+    rr = __dsqrt_rn(rr < 0.0 ? 0.0 : (rr > 1.0 ? 1.0 : rr));
+    const double theta = __dadd_rn(__dmul_rn(i, kGoldenAngle), jitter);
     double s, c;
     sincos(theta, &s, &c);
-    d[0] = static_cast<T>(c * rr);
-    d[1] = static_cast<T>(s * rr);
+    d[0] = static_cast<T>(__dmul_rn(c, rr));
+    d[1] = static_cast<T>(__dmul_rn(s, rr));
     d[2] = static_cast<T>(z);
 }
 
@@ -603,23 +619,20 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                                 for (int b = 0; b < kBands; ++b) {
                                     const T e = common * refl[b] * s.acc[b];
                                     const long long qe = quantize(e, job.energy_scale);
-                                    atomicAdd(job.echogram_fx + static_cast<size_t>(b) * job.num_bins + bin,
-                                              static_cast<unsigned long long>(qe));
+                                    add128(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
                                     if (job.ambisonic_fx) {
                                         unsigned long long *a =
-                                            job.ambisonic_fx + static_cast<size_t>(b) * 4 * job.num_bins + bin;
-                                        atomicAdd(a, static_cast<unsigned long long>(qe));
-                                        atomicAdd(a + job.num_bins,
-                                                  static_cast<unsigned long long>(quantize(e * s.d0[0], job.energy_scale)));
-                                        atomicAdd(a + 2 * job.num_bins,
-                                                  static_cast<unsigned long long>(quantize(e * s.d0[1], job.energy_scale)));
-                                        atomicAdd(a + 3 * job.num_bins,
-                                                  static_cast<unsigned long long>(quantize(e * s.d0[2], job.energy_scale)));
+                                            job.ambisonic_fx + 2 * (static_cast<size_t>(b) * 4 * job.num_bins + bin);
+                                        const size_t stride = 2 * static_cast<size_t>(job.num_bins);
+                                        add128(a, qe);
+                                        add128(a + stride, quantize(e * s.d0[0], job.energy_scale));
+                                        add128(a + 2 * stride, quantize(e * s.d0[1], job.energy_scale));
+                                        add128(a + 3 * stride, quantize(e * s.d0[2], job.energy_scale));
                                     }
                                     esum += qe;
                                 }
                                 atomicAdd(job.contrib_counts + surf, 1ull);
-                                atomicAdd(job.surface_energy_fx + surf, static_cast<unsigned long long>(esum));
+                                add128(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
                             }
                         }
                     }

@@ -22,17 +22,18 @@ __global__ void zero_outputs_kernel(const Job<T> *jobs, int num_jobs, unsigned l
     if (blockIdx.x == 0 && threadIdx.x == 0 && work_counter) *work_counter = 0ull;
     for (int j = blockIdx.y; j < num_jobs; j += gridDim.y) {
         const Job<T> &job = jobs[j];
-        const size_t nb = static_cast<size_t>(kBands) * job.num_bins;
+        // word counts: 128-bit accumulators take two words each
+        const size_t nb = 2 * static_cast<size_t>(kBands) * job.num_bins;
         const size_t na = job.ambisonic_fx ? 4 * nb : 0;
         const size_t ns = static_cast<size_t>(job.scene.num_surfaces);
-        const size_t total = nb + na + 3 * ns + 8;
+        const size_t total = nb + na + 4 * ns + 8;
         for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
             if (i < nb) job.echogram_fx[i] = 0ull;
             else if (i < nb + na) job.ambisonic_fx[i - nb] = 0ull;
             else if (i < nb + na + ns) job.hit_counts[i - nb - na] = 0ull;
             else if (i < nb + na + 2 * ns) job.contrib_counts[i - nb - na - ns] = 0ull;
-            else if (i < nb + na + 3 * ns) job.surface_energy_fx[i - nb - na - 2 * ns] = 0ull;
-            else job.counters[i - nb - na - 3 * ns] = 0ull;
+            else if (i < nb + na + 4 * ns) job.surface_energy_fx[i - nb - na - 2 * ns] = 0ull;
+            else job.counters[i - nb - na - 4 * ns] = 0ull;
         }
     }
 }
@@ -42,6 +43,12 @@ struct FinalizeTargets {
     float *ambisonic;
     float *surface_energy;
 };
+
+// 128-bit fixed point (low, high) -> double.
+__device__ __forceinline__ double fixed_to_double(const unsigned long long *w, double inv_scale) {
+    const double v = ldexp(static_cast<double>(static_cast<long long>(w[1])), 64) + static_cast<double>(w[0]);
+    return v * inv_scale;
+}
 
 // Fixed point -> float32 copies (the reference CUDA backend returns float32).
 template <typename T>
@@ -57,14 +64,13 @@ __global__ void finalize_kernel(const Job<T> *jobs, const FinalizeTargets *targe
         const size_t total = ne + na + ns;
         for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
             if (i < ne) {
-                tg.echogram[i] = static_cast<float>(static_cast<double>(static_cast<long long>(job.echogram_fx[i])) * inv);
+                tg.echogram[i] = static_cast<float>(fixed_to_double(job.echogram_fx + 2 * i, inv));
             } else if (i < ne + na) {
                 const size_t k = i - ne;
-                tg.ambisonic[k] = static_cast<float>(static_cast<double>(static_cast<long long>(job.ambisonic_fx[k])) * inv);
+                tg.ambisonic[k] = static_cast<float>(fixed_to_double(job.ambisonic_fx + 2 * k, inv));
             } else {
                 const size_t k = i - ne - na;
-                tg.surface_energy[k] =
-                    static_cast<float>(static_cast<double>(static_cast<long long>(job.surface_energy_fx[k])) * inv);
+                tg.surface_energy[k] = static_cast<float>(fixed_to_double(job.surface_energy_fx + 2 * k, inv));
             }
         }
     }
@@ -139,13 +145,13 @@ inline int launch_single(const ac_scene_s *scene, const ac_trace_params *p, cons
     Job<T> job;
     fill_job<T>(scene, p, o, scale, job);
     AC_CUDA_TRY(cudaSetDevice(scene->device));
-    const size_t nb = static_cast<size_t>(kBands) * p->num_bins;
+    const size_t nb = 2 * static_cast<size_t>(kBands) * p->num_bins;  // 128-bit accumulators: two words
     AC_CUDA_TRY(cudaMemsetAsync(o->echogram_fx, 0, nb * sizeof(int64_t), stream));
     if (job.ambisonic_fx) AC_CUDA_TRY(cudaMemsetAsync(o->ambisonic_fx, 0, 4 * nb * sizeof(int64_t), stream));
     const size_t ns = static_cast<size_t>(scene->num_surfaces) * sizeof(int64_t);
     AC_CUDA_TRY(cudaMemsetAsync(o->hit_counts, 0, ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->contrib_counts, 0, ns, stream));
-    AC_CUDA_TRY(cudaMemsetAsync(o->surface_energy_fx, 0, ns, stream));
+    AC_CUDA_TRY(cudaMemsetAsync(o->surface_energy_fx, 0, 2 * ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->counters, 0, 8 * sizeof(int64_t), stream));
     const int block = p->block_size > 0 ? p->block_size : kDefaultBlock;
     if (block % 32 != 0 || block > 256) return fail(AC_ERR_INVALID, "block_size must be a multiple of 32 up to 256");
@@ -168,14 +174,13 @@ __global__ void finalize_single_kernel(const __grid_constant__ Job<T> job, Final
     const size_t total = ne + na + ns;
     for (size_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         if (i < ne) {
-            tg.echogram[i] = static_cast<float>(static_cast<double>(static_cast<long long>(job.echogram_fx[i])) * inv);
+            tg.echogram[i] = static_cast<float>(fixed_to_double(job.echogram_fx + 2 * i, inv));
         } else if (i < ne + na) {
             const size_t k = i - ne;
-            tg.ambisonic[k] = static_cast<float>(static_cast<double>(static_cast<long long>(job.ambisonic_fx[k])) * inv);
+            tg.ambisonic[k] = static_cast<float>(fixed_to_double(job.ambisonic_fx + 2 * k, inv));
         } else {
             const size_t k = i - ne - na;
-            tg.surface_energy[k] =
-                static_cast<float>(static_cast<double>(static_cast<long long>(job.surface_energy_fx[k])) * inv);
+            tg.surface_energy[k] = static_cast<float>(fixed_to_double(job.surface_energy_fx + 2 * k, inv));
         }
     }
 }

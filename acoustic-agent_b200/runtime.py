@@ -55,7 +55,7 @@ def _stream_ptr(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
 class DeviceScene:
     """A scene uploaded with ac_scene_create; owns its device memory."""
 
-    def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0) -> None:
+    def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0) -> None:
         require_cuda(device)
         a = arrays.arrays if isinstance(arrays, SceneArrays) else dict(arrays)
         self.names: tuple[str, ...] = tuple(a["names"])
@@ -86,6 +86,12 @@ class DeviceScene:
         desc.bvh_escape = _ip(keep["bvh_escape"])
         desc.bvh_primitives = _ip(keep["bvh_primitives"])
         desc.device = int(device)
+        desc.cluster_size = int(cluster_size)
+        if "surface_bounds_min" in a and "surface_bounds_max" in a:
+            keep["surface_bounds_min"] = _f64(a["surface_bounds_min"])
+            keep["surface_bounds_max"] = _f64(a["surface_bounds_max"])
+            desc.surface_bounds_min = _dp(keep["surface_bounds_min"])
+            desc.surface_bounds_max = _dp(keep["surface_bounds_max"])
         handle = ctypes.c_void_p()
         _lib.check(_lib.load().ac_scene_create(ctypes.byref(desc), ctypes.byref(handle)), "ac_scene_create")
         self.handle = handle
@@ -95,6 +101,7 @@ class DeviceScene:
         _lib.check(_lib.load().ac_scene_get_info(handle, ctypes.byref(info)), "ac_scene_get_info")
         self.device_bytes = int(info.device_bytes)
         self.node_count = int(info.node_count)
+        self.num_clusters = int(info.num_clusters)
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
 
     def close(self) -> None:
@@ -217,11 +224,11 @@ class TraceBuffers:
                  record_rays: tuple[int, int] | None = None) -> "TraceBuffers":
         z64 = lambda *shape: torch.zeros(*shape, dtype=torch.int64, device=device)
         return cls(
-            echogram_fx=z64(NUM_BANDS, num_bins), hit_counts=z64(num_surfaces), contrib_counts=z64(num_surfaces),
-            surface_energy_fx=z64(num_surfaces), counters=z64(8),
+            echogram_fx=z64(NUM_BANDS, num_bins, 2), hit_counts=z64(num_surfaces), contrib_counts=z64(num_surfaces),
+            surface_energy_fx=z64(num_surfaces, 2), counters=z64(8),
             echogram=torch.zeros(NUM_BANDS, num_bins, dtype=torch.float32, device=device),
             surface_energy=torch.zeros(num_surfaces, dtype=torch.float32, device=device),
-            ambisonic_fx=z64(NUM_BANDS, 4, num_bins) if ambisonics else None,
+            ambisonic_fx=z64(NUM_BANDS, 4, num_bins, 2) if ambisonics else None,
             ambisonic=torch.zeros(NUM_BANDS, 4, num_bins, dtype=torch.float32, device=device) if ambisonics else None,
             ray_surfaces=(torch.empty(record_rays[0], record_rays[1], dtype=torch.int32, device=device)
                           if record_rays else None),
@@ -316,20 +323,22 @@ class BatchWorkspace:
         self.device_buffer: torch.Tensor | None = None
         self.host_buffer: torch.Tensor | None = None
 
-    def ensure(self, num_jobs: int) -> tuple[int, int, int]:
-        if num_jobs > self.capacity_jobs or self.device_buffer is None:
-            size = ctypes.c_size_t()
-            cap = max(num_jobs, 2 * self.capacity_jobs, 16)
-            _lib.check(_lib.load().ac_batch_workspace_size(cap, None, ctypes.byref(size)), "ac_batch_workspace_size")
-            self.device_buffer = torch.empty(int(size.value), dtype=torch.uint8, device=self.device)
-            self.host_buffer = torch.empty(int(size.value), dtype=torch.uint8, pin_memory=True)
-            self.capacity_jobs = cap
+    def ensure(self, jobs, num_jobs: int, cfg) -> tuple[int, int, int]:
+        size = ctypes.c_size_t()
+        _lib.check(_lib.load().ac_batch_workspace_size(jobs, num_jobs, ctypes.byref(cfg), ctypes.byref(size)),
+                   "ac_batch_workspace_size")
+        need = int(size.value)
+        if self.device_buffer is None or self.device_buffer.numel() < need:
+            cap = max(need, 2 * (self.device_buffer.numel() if self.device_buffer is not None else 0), 1 << 16)
+            self.device_buffer = torch.empty(cap, dtype=torch.uint8, device=self.device)
+            self.host_buffer = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
         assert self.device_buffer is not None and self.host_buffer is not None
         return self.device_buffer.data_ptr(), self.device_buffer.numel(), self.host_buffer.data_ptr()
 
 
 def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
-                block_size: int = 0, grid_blocks: int = 0, stream: torch.cuda.Stream | None = None) -> None:
+                block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0,
+                stream: torch.cuda.Stream | None = None) -> None:
     """All jobs in one persistent launch (ac_trace_batch)."""
     if not jobs:
         return
@@ -340,11 +349,19 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
         arr[k].scene = scene.handle.value
         arr[k].params = params_struct(spec, device, keep)
         arr[k].outputs = buffers.outputs_struct()
-    cfg = _lib.ACBatchConfig(int(block_size), 0, int(grid_blocks), 0)
-    ws, ws_bytes, host = workspace.ensure(len(jobs))
+    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), 0)
+    ws, ws_bytes, host = workspace.ensure(arr, len(jobs), cfg)
     _lib.check(_lib.load().ac_trace_batch(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
                                           ctypes.c_void_p(host), _stream_ptr(stream)), "ac_trace_batch")
     workspace._keepalive = keep  # type: ignore[attr-defined]
+
+
+def fixed_to_float64(fixed: torch.Tensor, scale: float) -> np.ndarray:
+    """128-bit (low, high) fixed-point words [..., 2] -> float64 values (value = (high*2^64 + low) / scale)."""
+    words = fixed.cpu().numpy()
+    low = words[..., 0].view(np.uint64).astype(np.float64)
+    high = words[..., 1].astype(np.float64)
+    return (high * 18446744073709551616.0 + low) / float(scale)
 
 
 def host_field(buffers: TraceBuffers, names: Sequence[str], spec: TraceSpec) -> dict[str, Any]:

@@ -93,7 +93,7 @@ typedef struct ac_scene_desc {
     const int64_t *bvh_escape;
     const int64_t *bvh_primitives;
     int32_t device;              /* CUDA device ordinal that will own the scene */
-    int32_t reserved;
+    int32_t cluster_size;        /* surfaces per cluster of the float32 scan (0: 8) */
 } ac_scene_desc;
 
 typedef struct ac_scene_info {
@@ -104,6 +104,7 @@ typedef struct ac_scene_info {
     int64_t device_bytes;        /* device memory held by the scene */
     int32_t device;
     int32_t max_leaf;
+    int64_t num_clusters;        /* clusters of the float32 scan */
 } ac_scene_info;
 
 /* One trace: rays from the listener, next-event estimation to the source.
@@ -140,20 +141,23 @@ typedef struct ac_trace_params {
     const void *diffuse_bank;    /* [K,3] device, element type as above; both RNG modes */
     int32_t num_bank;
     int32_t block_size;          /* 0: library default */
-    double energy_scale;         /* fixed-point scale (a power of two); 0: library picks */
+    double energy_scale;         /* fixed-point scale (a power of two); 0: library picks (ac_energy_scale) */
     int32_t grid_blocks;         /* 0: library default (persistent, SM-count based) */
     int32_t reserved;
 } ac_trace_params;
 
-/* Outputs.  All pointers are DEVICE memory owned by the caller.  The int64
- * fixed-point accumulators are zeroed by the call itself; NULL optional
+/* Outputs.  All pointers are DEVICE memory owned by the caller.  Energies
+ * are accumulated as 128-bit two's-complement fixed point, stored as
+ * (low word, high word) int64 pairs: value = (high * 2^64 + low) / scale,
+ * where each deposit is rounded to an integer multiple of 1/scale before the
+ * exact sum.  The accumulators are zeroed by the call itself; NULL optional
  * outputs are skipped. */
 typedef struct ac_trace_outputs {
-    int64_t *echogram_fx;        /* [6,bins] required: echogram * energy_scale, rounded per deposit */
-    int64_t *ambisonic_fx;       /* [6,4,bins] when render_ambisonics */
+    int64_t *echogram_fx;        /* [6,bins,2] required */
+    int64_t *ambisonic_fx;       /* [6,4,bins,2] when render_ambisonics */
     int64_t *hit_counts;         /* [S] required */
     int64_t *contrib_counts;     /* [S] required */
-    int64_t *surface_energy_fx;  /* [S] required */
+    int64_t *surface_energy_fx;  /* [S,2] required */
     int64_t *counters;           /* [8] required: actual_bounces, active_rays, ray_bounces, shadow_rays,
                                     work counter (scratch), 3 reserved */
     float *echogram;             /* [6,bins] optional dequantized copy */
@@ -171,8 +175,8 @@ typedef struct ac_job {
 } ac_job;
 
 typedef struct ac_batch_config {
-    int32_t block_size;          /* threads per block; 0: autotuned default */
-    int32_t chunk_rays;          /* rays per work item; 0: default */
+    int32_t block_size;          /* threads per block; 0: library default */
+    int32_t chunk_rays;          /* rays per work item a warp takes from the queue; 0: default */
     int32_t grid_blocks;         /* persistent blocks; 0: SM count * occupancy */
     int32_t reserved;
 } ac_batch_config;
@@ -212,14 +216,14 @@ int ac_scene_create(const ac_scene_desc *desc, ac_scene_t *out);
 int ac_scene_destroy(ac_scene_t scene);
 int ac_scene_get_info(ac_scene_t scene, ac_scene_info *info);
 
-/* Fixed-point scale the library would pick for these parameters (a power of
- * two chosen so no accumulator can overflow int64). */
+/* Fixed-point scale the library would pick for these parameters: a power of
+ * two that maps the largest possible six-band deposit to at most 2^62. */
 int ac_energy_scale(ac_scene_t scene, const ac_trace_params *params, double *scale);
 
 int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_outputs *outputs, void *stream);
 
-/* Device workspace needed by ac_trace_batch for num_jobs jobs. */
-int ac_batch_workspace_size(int32_t num_jobs, const ac_batch_config *config, size_t *bytes);
+/* Device (and pinned staging) bytes ac_trace_batch needs for these jobs. */
+int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, size_t *bytes);
 
 /* Many jobs (any mix of scenes, ray budgets, bins) in one persistent launch.
  * `workspace` is caller-owned device memory of ac_batch_workspace_size bytes.

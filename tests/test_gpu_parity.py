@@ -53,9 +53,9 @@ def run(rt, case, spec, record_rays=True):
     out["contrib"] = buffers.contrib_counts.cpu().numpy()
     out["echogram_fx"] = buffers.echogram_fx.cpu().numpy()
     out["ambisonic"] = buffers.ambisonic.cpu().numpy() if buffers.ambisonic is not None else None
-    out["fx_echogram64"] = buffers.echogram_fx.cpu().numpy().astype(np.float64) / buffers.scale.value
+    out["fx_echogram64"] = rt.fixed_to_float64(buffers.echogram_fx, buffers.scale.value)
     if buffers.ambisonic_fx is not None:
-        out["fx_ambisonic64"] = buffers.ambisonic_fx.cpu().numpy().astype(np.float64) / buffers.scale.value
+        out["fx_ambisonic64"] = rt.fixed_to_float64(buffers.ambisonic_fx, buffers.scale.value)
     scene.close()
     return out
 
@@ -119,6 +119,7 @@ def test_philox_stream_matches_oracle_restatement(rt):
     od, orand, oidx = oracle.philox_workspace(R, B, seed, key)
     np.testing.assert_array_equal(r.cpu().numpy(), orand)
     np.testing.assert_array_equal(i.cpu().numpy(), oidx)
+    # cos/sin of the device math library vs numpy's: last-place differences only
     np.testing.assert_allclose(d.cpu().numpy(), od, rtol=0, atol=4e-16)
 
 
@@ -152,14 +153,28 @@ def test_philox_fp64_trace_matches_oracle_ray_by_ray(rt):
 
 
 def test_philox_fp32_statistics_match_reference_stream(rt):
-    """A different random stream is a different Monte-Carlo sample: compare decay curves, not bins."""
+    """A different random stream is a different Monte-Carlo sample: compare decay curves, not bins.
+
+    At 10,000 rays the reference's own seed-to-seed EDC spread on this room is
+    0.4-1.8 dB, so the comparison uses 200,000 rays on both sides: the float32
+    Philox GPU trace against the float64 oracle on the reference's stream.
+    """
     from acoustic_agent_b200 import metrics
+    from oracle import oracle
     case = load_case("shoebox_linear")
-    res = run(rt, case, spec_for(rt, case, "float32", rng="philox", stream_key=5), record_rays=False)
-    ref = case["echogram"]
+    tr = case["trace"]
+    R = 200_000
+    res = run(rt, case, spec_for(rt, case, "float32", rng="philox", stream_key=5, num_rays=R), record_rays=False)
+    dirs, bank, rnd, idx = oracle.workspace(R, tr["bounces"], tr["seed"])
+    ref = oracle.trace(case["arrays"], source=tr["source"], listener=tr["listener"], directions=dirs,
+                       diffuse_bank=bank, diffuse_random=rnd, diffuse_indices=idx, num_bins=int(case["num_bins"]),
+                       bin_dur=tr["bin_dur"], c=343.0, max_path_len=tr["duration"] * 343.0,
+                       direct_delay=float(case["direct_delay"]))["echogram"]
     assert np.max(metrics.edc_error_db(res["echogram"], ref)) <= 0.5
-    np.testing.assert_allclose(res["echogram"].sum(axis=1), ref.sum(axis=1), rtol=0.05)
-    np.testing.assert_allclose(metrics.t30(res["echogram"], 0.01), metrics.t30(ref, 0.01), rtol=0.05)
+    np.testing.assert_allclose(res["echogram"].sum(axis=1), ref.sum(axis=1), rtol=0.02)
+    np.testing.assert_allclose(metrics.t30(res["echogram"], 0.01), metrics.t30(ref, 0.01), rtol=0.02)
+    np.testing.assert_allclose(metrics.edt(res["echogram"], 0.01), metrics.edt(ref, 0.01), rtol=0.03)
+    np.testing.assert_allclose(metrics.c50(res["echogram"], 0.01), metrics.c50(ref, 0.01), atol=0.2)
 
 
 @pytest.mark.parametrize("precision", ["float32", "float64"])
@@ -222,21 +237,27 @@ def test_gpu_synthesis_is_bit_exact(rt, label):
 
 
 def test_gpu_synthesis_device_air_and_batching(rt):
+    """Three echograms in one launch, air gains computed on the device: each row equals the oracle."""
     from acoustic_agent_b200 import bands
+    from oracle import oracle
     s = np.load(GOLDEN / "synthesis.npz")
     fs, bin_dur, delay, seed = s["furnished_f32_meta"]
     fs = int(fs)
     e = s["furnished_f32_input"]
     nb = e.shape[1]
     spb = bands.samples_per_bin(bin_dur, fs)
-    white = torch.as_tensor(np.random.default_rng(int(seed) + 7).uniform(-1, 1, size=nb * spb), device="cuda")
-    batch = np.stack([e, e * 0.5, e * 2.0]).astype(np.float32)
-    delays = torch.full((3,), float(delay), dtype=torch.float64, device="cuda")
+    white_np = np.random.default_rng(int(seed) + 7).uniform(-1, 1, size=nb * spb)
+    white = torch.as_tensor(white_np, device="cuda")
+    batch = np.stack([e, e * 0.5, e * 3.0]).astype(np.float32)
+    delays_np = [float(delay), float(delay) + 0.01, 0.0]
+    delays = torch.as_tensor(delays_np, dtype=torch.float64, device="cuda")
     params = rt.synth_params(3, nb, float(bin_dur), fs, 343.0, rng_mode="reference", seed=int(seed), white=white,
                              direct_delays=delays)
     out = rt.synthesize(torch.as_tensor(batch, device="cuda"), params, rt.SynthWorkspace(torch.device("cuda")))
     torch.cuda.synchronize()
-    ref = s["furnished_f32_output"]
-    scale = float(np.max(np.abs(ref)))
-    np.testing.assert_allclose(out[0].cpu().numpy(), ref, rtol=1e-5, atol=1e-6 * scale)
-    np.testing.assert_allclose(out[1].cpu().numpy(), ref * np.sqrt(0.5), rtol=1e-4, atol=1e-5 * scale)
+    for row in range(3):
+        ref = oracle.synthesize(batch[row], fs=fs, bin_dur=float(bin_dur), direct_delay=delays_np[row], c=343.0,
+                                white=white_np)
+        scale = float(np.max(np.abs(ref)))
+        # device exp() vs libm exp() in the air gains: last-place differences
+        np.testing.assert_allclose(out[row].cpu().numpy(), ref, rtol=1e-6, atol=1e-7 * scale)
