@@ -44,8 +44,8 @@ double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p) {
                                          std::max(1.0, std::fabs(1.0 - scene->min_scattering));
     const double growth = std::min(1e300, std::pow(std::max(1.0, scene->max_reflection), B + 1.0));
     const double max_deposit = ray_scale * gain * distance_term * lobe * growth;
-    // Accumulators are 128-bit, so only one deposit must fit an int64 quantum:
-    // the six-band sum of the largest possible deposit stays below 2^62.
+    // The accumulators are exact for any number of quanta below 2^32, so only one
+    // deposit must fit an int64 quantum: its six-band sum stays below 2^62.
     const double budget = 6.0 * max_deposit;
     int exponent = static_cast<int>(std::floor(std::log2(std::ldexp(1.0, 62) / budget)));
     exponent = std::min(200, std::max(-60, exponent));
@@ -79,6 +79,9 @@ int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_t
         return fail(AC_ERR_INVALID, "render_ambisonics needs the ambisonic accumulator");
     if (p->energy_scale < 0.0 || !std::isfinite(p->energy_scale))
         return fail(AC_ERR_INVALID, "energy_scale must be zero (automatic) or positive");
+    // Each ray deposits at most once per bounce: fewer than 2^32 quanta per accumulator.
+    if (static_cast<double>(p->num_rays) * static_cast<double>(std::max<int32_t>(1, p->num_bounces)) >= 4294967296.0)
+        return fail(AC_ERR_CAPACITY, "num_rays * num_bounces must stay below 2^32; split the rays over several jobs");
     return AC_OK;
 }
 

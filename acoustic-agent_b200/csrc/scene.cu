@@ -28,7 +28,7 @@ template <>
 inline double tag_value<double>(int tag) { return static_cast<double>(tag); }
 
 struct Offsets {
-    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, clusters, cluster_prims, edges, total;  // elements
+    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, clusters, cluster_prims, boxes, edges, total;  // elements
 };
 
 inline size_t round4(size_t v) { return (v + 3) & ~static_cast<size_t>(3); }
@@ -44,6 +44,7 @@ Offsets layout(size_t S, size_t P, size_t N, size_t C, size_t NC) {
     o.normals = off;       off += round4(S * 3);
     o.clusters = off;      off += round4(NC * ac::kClusterStride);
     o.cluster_prims = off; off += round4(NC ? S * ac::kPrimStride : 0);
+    o.boxes = off;         off += round4(NC ? S * 8 : 0);
     o.edges = off;         off += round4(NC ? C * 4 : 0);
     o.total = off;
     return o;
@@ -122,8 +123,8 @@ void pack_record(const ac_scene_desc *d, int64_t si, T *rec) {
 }
 
 template <typename T>
-int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clusters, ac_scene_s *s,
-                    void **storage, size_t *bytes, ac::SceneDev<T> *view) {
+int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clusters, const double *bounds_lo,
+                    const double *bounds_hi, ac_scene_s *s, void **storage, size_t *bytes, ac::SceneDev<T> *view) {
     const size_t S = static_cast<size_t>(d->num_surfaces);
     const size_t N = static_cast<size_t>(bvh.node_count);
     const size_t P = S;
@@ -145,8 +146,15 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clu
             cp[7] = tag_value<T>(static_cast<int>(clusters->count[n]));
             ++c;
         }
-        for (size_t k = 0; k < S; ++k)
-            pack_record<T>(d, clusters->primitives[k], host.data() + o.cluster_prims + k * ac::kPrimStride);
+        for (size_t k = 0; k < S; ++k) {
+            const int64_t si = clusters->primitives[k];
+            pack_record<T>(d, si, host.data() + o.cluster_prims + k * ac::kPrimStride);
+            T *bb = host.data() + o.boxes + k * 8;
+            for (int a = 0; a < 3; ++a) {
+                bb[a] = T(bounds_lo[3 * si + a]);
+                bb[4 + a] = T(bounds_hi[3 * si + a]);
+            }
+        }
         // Polygon edges for the even-odd test: {x_i, y_i, y_j, (x_j - x_i) / (y_j - y_i)} with j the
         // previous corner (steam_rt.py:4259-4274); an edge the reference skips gets y_j = y_i.
         for (size_t i = 0; i < C; ++i) {
@@ -207,6 +215,7 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clu
         const float *fbase = reinterpret_cast<const float *>(dev);
         s->fast.clusters = fbase + o.clusters;
         s->fast.prims = fbase + o.cluster_prims;
+        s->fast.boxes = fbase + o.boxes;
         s->fast.edges = fbase + o.edges;
         s->fast.num_clusters = static_cast<int32_t>(NC);
         s->fast.num_edges = static_cast<int32_t>(C);
@@ -330,8 +339,9 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
         delete s;
         return rc;
     }
-    rc = pack_and_upload<float>(d, bvh, &cbvh, s, &s->storage_f32, &s->bytes_f32, &s->f32);
-    if (rc == AC_OK) rc = pack_and_upload<double>(d, bvh, nullptr, s, &s->storage_f64, &s->bytes_f64, &s->f64);
+    rc = pack_and_upload<float>(d, bvh, &cbvh, blo, bhi, s, &s->storage_f32, &s->bytes_f32, &s->f32);
+    if (rc == AC_OK)
+        rc = pack_and_upload<double>(d, bvh, nullptr, blo, bhi, s, &s->storage_f64, &s->bytes_f64, &s->f64);
     if (rc != AC_OK) {
         if (s->storage_f32) cudaFree(s->storage_f32);
         delete s;

@@ -10,9 +10,8 @@
 // The raw band signals are materialised first by a fully parallel kernel.  The
 // recursion itself is sequential in time, so parallelism comes from elsewhere:
 // one warp is a systolic array of 8 four-section low-pass chains.  Lane
-// (unit, chain, stage) runs one biquad section; each iteration it passes its
-// float32 output one lane up, so section s works on sample n-s while section
-// s+1 works on sample n-s-1.  A "unit" is one band of one RIR: bands 1-4 need
+// (unit, chain, stage) runs one biquad section and passes its float32 output
+// one lane up; section s runs two samples behind section s-1.  A "unit" is one band of one RIR: bands 1-4 need
 // two chains (the low-pass at the upper and lower crossover, subtracted),
 // bands 0 and 5 one.  Four units per warp.
 #include <algorithm>
@@ -130,8 +129,19 @@ struct Section {
     }
 };
 
-constexpr int kPrefetch = 4;
+constexpr int kPrefetch = 8;
+constexpr int kSkew = 2;  // iterations between consecutive sections
+constexpr int kLag = kSkew * 3;  // section 3 runs kLag samples behind section 0
 
+// Lane (unit, chain, stage): section `stage` works on sample it - kSkew*stage.
+// The float32 output it produces at iteration it is shuffled one lane up at
+// once but consumed there only at it + kSkew, so the shuffle latency never sits
+// on the recursion's critical path -- only the section's own y dependency does.
+//
+// The body is branch-free: before a section's first real sample its input is
+// +0.0, and a section whose inputs and state are all +0.0 produces exactly +0.0
+// and keeps its state at +0.0 (every product is +0.0 or -0.0 and the sums come
+// out +0.0), so the steps while the pipeline fills change nothing.
 __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, const __grid_constant__ SynthArgs a,
                                                            float *out) {
     const unsigned full = 0xFFFFFFFFu;
@@ -151,18 +161,23 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
     active = active && valid_unit;
     const double *co = a.crossover + cutoff * 20 + stage * 5;
     Section sec{co[0], co[1], co[2], co[3], co[4], 0.0, 0.0, 0.0, 0.0};
+    const bool emits = stage == 3 && chain == 0 && active;
+    const bool is_first = stage == 0;
+    const int mode = band == 0 ? 0 : (band == kSynthBands - 1 ? 2 : 1);
 
     const int N = a.num_bins * a.spb;
     const double *x = raw + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
     float *out_row = out + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
 
-    // Section 0 reads sample `it`; section s works on sample it - s with the
-    // float32 output section s-1 produced one iteration earlier.
-    double ahead[kPrefetch];
+    double ahead[kPrefetch], prev[kPrefetch];
 #pragma unroll
-    for (int u = 0; u < kPrefetch; ++u) ahead[u] = (valid_unit && u < N) ? __ldg(x + u) : 0.0;
-    float carry = 0.0f;
-    for (int base = 0; base < N + 3; base += kPrefetch) {
+    for (int u = 0; u < kPrefetch; ++u) {
+        ahead[u] = (valid_unit && u < N) ? __ldg(x + u) : 0.0;
+        prev[u] = 0.0;
+    }
+    float q0 = 0.0f, q1 = 0.0f;  // inputs from the previous section for this and the next iteration
+    const int iterations = N + kLag;
+    for (int base = 0; base < iterations; base += kPrefetch) {
         double next[kPrefetch];
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
@@ -172,23 +187,23 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
             const int it = base + u;
-            const float from_prev = __shfl_up_sync(full, carry, 1);
-            const double in = stage == 0 ? ahead[u] : static_cast<double>(from_prev);
-            const int n = it - stage;
-            float y = 0.0f;
-            if (active && n >= 0 && n < N) y = sec.step(in);
-            carry = y;
+            const double in = is_first ? ahead[u] : static_cast<double>(q0);
+            const float y = sec.step(in);
+            const float sent = __shfl_up_sync(full, y, 1);
             const float lower = __shfl_down_sync(full, y, 4);
-            if (stage == 3 && chain == 0 && active && n >= 0 && n < N) {
-                float o;
-                if (band == 0) o = y;
-                else if (band == kSynthBands - 1) o = static_cast<float>(__ldg(x + n) - static_cast<double>(y));
-                else o = y - lower;
-                out_row[n] = o;
-            }
+            q0 = q1;
+            q1 = sent;
+            // x[it - kLag] is still in registers from the prefetch
+            const double x_n = (u >= kLag) ? ahead[u - kLag] : prev[u + kPrefetch - kLag];
+            const float band5 = static_cast<float>(x_n - static_cast<double>(y));
+            const float o = mode == 0 ? y : (mode == 2 ? band5 : y - lower);
+            if (emits && it >= kLag && it < iterations) out_row[it - kLag] = o;
         }
 #pragma unroll
-        for (int u = 0; u < kPrefetch; ++u) ahead[u] = next[u];
+        for (int u = 0; u < kPrefetch; ++u) {
+            prev[u] = ahead[u];
+            ahead[u] = next[u];
+        }
     }
 }
 

@@ -36,6 +36,7 @@ constexpr int kClusterStride = 8;
 struct FastScene {
     const float *clusters;       // [NC][8]
     const float *prims;          // [P][12] surface records in cluster-slot order
+    const float *boxes;          // [P][8] world AABB per slot {lo.xyz, 0, hi.xyz, 0} (used for boxes)
     const float *edges;          // [C][4] {x_i, y_i, y_j (or y_i if skipped), (x_j-x_i)/(y_j-y_i)}
     int32_t num_clusters;
     int32_t num_edges;
@@ -192,7 +193,14 @@ __device__ __forceinline__ int closest_scan(const FastScene &fs, const FRay &r, 
         for (int k = 0; k < count; ++k) {
             const float *rec = fs.prims + static_cast<size_t>(first + k) * kPrimStride;
             const int tag = __float_as_int(__ldg(rec + 11));
-            if (pass) {
+            bool test = pass;
+            if ((tag & 3) == 2) {
+                // Boxes: cheap world-AABB check first; the warp skips the box if no lane needs it.
+                const float *bb = fs.boxes + static_cast<size_t>(first + k) * 8;
+                test = pass && cluster_overlaps(r, ldq(bb), ldq(bb + 4), best_t);
+                if (!__any_sync(full, test)) continue;
+            }
+            if (test) {
                 const float t = surface_t(rec, tag & 3, r, fs);
                 const int si = tag >> 2;
                 if (t < best_t || (t == best_t && t < 1e30f && si < best)) {
@@ -222,7 +230,13 @@ __device__ __forceinline__ bool shadow_scan(const FastScene &fs, const FRay &r, 
         for (int k = 0; k < count; ++k) {
             const float *rec = fs.prims + static_cast<size_t>(first + k) * kPrimStride;
             const int tag = __float_as_int(__ldg(rec + 11));
-            if (pass && !blocked) {
+            bool test = pass && !blocked;
+            if ((tag & 3) == 2) {
+                const float *bb = fs.boxes + static_cast<size_t>(first + k) * 8;
+                test = test && cluster_overlaps(r, ldq(bb), ldq(bb + 4), max_t);
+                if (!__any_sync(full, test)) continue;
+            }
+            if (test) {
                 if (surface_t(rec, tag & 3, r, fs) < max_t) blocked = true;
             }
         }
@@ -245,6 +259,16 @@ __device__ __forceinline__ void winner_normal(const FastScene &fs, int slot, con
         n[0] = __ldg(rec + 1); n[1] = __ldg(rec + 2); n[2] = __ldg(rec + 3);
     }
     if (n[0] * r.d[0] + n[1] * r.d[1] + n[2] * r.d[2] > 0.0f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+}
+
+// The reference's escape-link walk, kept out of line: only rays that miss
+// every surface in BVH mode take it.
+static __device__ __noinline__ int2 fallback_walk(const SceneDev<float> sc, float ox, float oy, float oz, float dx,
+                                                  float dy, float dz) {
+    const float o[3] = {ox, oy, oz}, d[3] = {dx, dy, dz};
+    float n[3], t;
+    const int surf = closest_hit(sc, true, o, d, t, n);
+    return make_int2(surf, __float_as_int(t));
 }
 
 struct FastLane {
@@ -372,8 +396,9 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
         int surf = closest_scan(fs, ray, has, t, slot);
         if (has && surf < 0 && job.use_bvh) {
             // Missed everything: the reference's BVH walk reports the lowest visited surface.
-            float n_unused[3];
-            surf = closest_hit(job.scene, true, s.o, s.d, t, n_unused);
+            const int2 fb = fallback_walk(job.scene, s.o[0], s.o[1], s.o[2], s.d[0], s.d[1], s.d[2]);
+            surf = fb.x;
+            t = __int_as_float(fb.y);
             slot = -1;
         }
         float n[3] = {0.0f, 0.0f, 1.0f};
@@ -462,22 +487,22 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
                         for (int b = 0; b < kBands; ++b) {
                             const float e = common * refl[b] * s.acc[b];
                             const long long qe = quantize(e, job.energy_scale);
-                            add128(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
+                            add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
                             if (job.ambisonic_fx) {
                                 float d0[3];
                                 initial_direction(job, s.ray, d0);
                                 unsigned long long *a =
                                     job.ambisonic_fx + 2 * (static_cast<size_t>(b) * 4 * job.num_bins + bin);
                                 const size_t stride = 2 * static_cast<size_t>(job.num_bins);
-                                add128(a, qe);
-                                add128(a + stride, quantize(e * d0[0], job.energy_scale));
-                                add128(a + 2 * stride, quantize(e * d0[1], job.energy_scale));
-                                add128(a + 3 * stride, quantize(e * d0[2], job.energy_scale));
+                                add_fixed(a, qe);
+                                add_fixed(a + stride, quantize(e * d0[0], job.energy_scale));
+                                add_fixed(a + 2 * stride, quantize(e * d0[1], job.energy_scale));
+                                add_fixed(a + 3 * stride, quantize(e * d0[2], job.energy_scale));
                             }
                             esum += qe;
                         }
                         atomicAdd(job.contrib_counts + surf, 1ull);
-                        add128(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
+                        add_fixed(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
                     }
                 }
             }

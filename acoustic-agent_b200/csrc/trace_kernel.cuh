@@ -13,9 +13,9 @@
 //     the warp's other rays finish;
 //   * many jobs (scene, source, listener, outputs) may share one launch; a
 //     lane maps its global ray index to (job, ray) through a prefix table;
-//   * the echogram is accumulated as 128-bit fixed point (energy * 2^s rounded
-//     per deposit to int64, summed exactly), so the result is bit-identical
-//     for any schedule;
+//   * the echogram is accumulated as exact fixed point (energy * 2^s rounded
+//     per deposit to int64, summed as two 32-bit halves), so the result is
+//     bit-identical for any schedule;
 //   * per-surface hit counters are aggregated per warp (match_any) before
 //     the atomic, removing the same-address contention of one atomic per
 //     bounce per ray;
@@ -133,7 +133,7 @@ struct Job {
     const T *diffuse_random;       // [B,R]
     const int32_t *diffuse_indices;// [B,R]
     const T *diffuse_bank;         // [K,3]
-    unsigned long long *echogram_fx;   // [6,bins,2] 128-bit fixed point (low, high)
+    unsigned long long *echogram_fx;   // [6,bins,2] fixed point (sum of low halves, sum of high halves)
     unsigned long long *ambisonic_fx;  // [6,4,bins,2] or null
     unsigned long long *hit_counts;    // [S]
     unsigned long long *contrib_counts;// [S]
@@ -409,17 +409,19 @@ __device__ __forceinline__ double t_pow<double>(double x, double y) { return pow
 __device__ __forceinline__ long long quantize(float e, double scale) { return __double2ll_rn(static_cast<double>(e) * scale); }
 __device__ __forceinline__ long long quantize(double e, double scale) { return __double2ll_rn(e * scale); }
 
-// Exact 128-bit two's-complement accumulation of a signed 64-bit quantum into
-// acc[0] (low word) / acc[1] (high word).  The low-word atomic returns the
-// value it replaced, so the carry is known exactly; both word updates are
-// commutative, so the final 128-bit value does not depend on the order.
-__device__ __forceinline__ void add128(unsigned long long *acc, long long q) {
+// Exact fixed-point accumulation without returning atomics.  A signed 64-bit
+// quantum q is split into its low 32 bits (unsigned, < 2^32) and its high part
+// (q >> 32, signed); acc[0] sums the low parts and acc[1] the high parts, both
+// with fire-and-forget reductions.  The accumulated value is
+// acc[1] * 2^32 + acc[0], exact and independent of the order of the additions
+// as long as fewer than 2^32 quanta reach one accumulator (the launcher
+// requires num_rays * num_bounces < 2^32).
+__device__ __forceinline__ void add_fixed(unsigned long long *acc, long long q) {
     if (q == 0) return;
-    const unsigned long long uq = static_cast<unsigned long long>(q);
-    const unsigned long long old = atomicAdd(acc, uq);
-    const unsigned long long carry = (old + uq < old) ? 1ull : 0ull;
-    const unsigned long long hi = carry + (q < 0 ? ~0ull : 0ull);
-    if (hi) atomicAdd(acc + 1, hi);
+    const unsigned long long lo = static_cast<unsigned long long>(q) & 0xFFFFFFFFull;
+    const long long hi = q >> 32;
+    if (lo) atomicAdd(acc, lo);
+    if (hi) atomicAdd(acc + 1, static_cast<unsigned long long>(hi));
 }
 
 // Initial direction of ray `ri` of a job.
@@ -619,20 +621,20 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                                 for (int b = 0; b < kBands; ++b) {
                                     const T e = common * refl[b] * s.acc[b];
                                     const long long qe = quantize(e, job.energy_scale);
-                                    add128(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
+                                    add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
                                     if (job.ambisonic_fx) {
                                         unsigned long long *a =
                                             job.ambisonic_fx + 2 * (static_cast<size_t>(b) * 4 * job.num_bins + bin);
                                         const size_t stride = 2 * static_cast<size_t>(job.num_bins);
-                                        add128(a, qe);
-                                        add128(a + stride, quantize(e * s.d0[0], job.energy_scale));
-                                        add128(a + 2 * stride, quantize(e * s.d0[1], job.energy_scale));
-                                        add128(a + 3 * stride, quantize(e * s.d0[2], job.energy_scale));
+                                        add_fixed(a, qe);
+                                        add_fixed(a + stride, quantize(e * s.d0[0], job.energy_scale));
+                                        add_fixed(a + 2 * stride, quantize(e * s.d0[1], job.energy_scale));
+                                        add_fixed(a + 3 * stride, quantize(e * s.d0[2], job.energy_scale));
                                     }
                                     esum += qe;
                                 }
                                 atomicAdd(job.contrib_counts + surf, 1ull);
-                                add128(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
+                                add_fixed(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
                             }
                         }
                     }

@@ -22,7 +22,7 @@ __global__ void zero_outputs_kernel(const Job<T> *jobs, int num_jobs, unsigned l
     if (blockIdx.x == 0 && threadIdx.x == 0 && work_counter) *work_counter = 0ull;
     for (int j = blockIdx.y; j < num_jobs; j += gridDim.y) {
         const Job<T> &job = jobs[j];
-        // word counts: 128-bit accumulators take two words each
+        // word counts: each fixed-point accumulator takes two words
         const size_t nb = 2 * static_cast<size_t>(kBands) * job.num_bins;
         const size_t na = job.ambisonic_fx ? 4 * nb : 0;
         const size_t ns = static_cast<size_t>(job.scene.num_surfaces);
@@ -44,9 +44,9 @@ struct FinalizeTargets {
     float *surface_energy;
 };
 
-// 128-bit fixed point (low, high) -> double.
+// Fixed point (sum of low halves, sum of high halves) -> double.
 __device__ __forceinline__ double fixed_to_double(const unsigned long long *w, double inv_scale) {
-    const double v = ldexp(static_cast<double>(static_cast<long long>(w[1])), 64) + static_cast<double>(w[0]);
+    const double v = ldexp(static_cast<double>(static_cast<long long>(w[1])), 32) + static_cast<double>(w[0]);
     return v * inv_scale;
 }
 
@@ -145,7 +145,7 @@ inline int launch_single(const ac_scene_s *scene, const ac_trace_params *p, cons
     Job<T> job;
     fill_job<T>(scene, p, o, scale, job);
     AC_CUDA_TRY(cudaSetDevice(scene->device));
-    const size_t nb = 2 * static_cast<size_t>(kBands) * p->num_bins;  // 128-bit accumulators: two words
+    const size_t nb = 2 * static_cast<size_t>(kBands) * p->num_bins;  // two words per accumulator
     AC_CUDA_TRY(cudaMemsetAsync(o->echogram_fx, 0, nb * sizeof(int64_t), stream));
     if (job.ambisonic_fx) AC_CUDA_TRY(cudaMemsetAsync(o->ambisonic_fx, 0, 4 * nb * sizeof(int64_t), stream));
     const size_t ns = static_cast<size_t>(scene->num_surfaces) * sizeof(int64_t);

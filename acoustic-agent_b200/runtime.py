@@ -357,11 +357,11 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
 
 
 def fixed_to_float64(fixed: torch.Tensor, scale: float) -> np.ndarray:
-    """128-bit (low, high) fixed-point words [..., 2] -> float64 values (value = (high*2^64 + low) / scale)."""
+    """Fixed-point word pairs [..., 2] -> float64 values: (word1 * 2^32 + word0) / scale."""
     words = fixed.cpu().numpy()
     low = words[..., 0].view(np.uint64).astype(np.float64)
     high = words[..., 1].astype(np.float64)
-    return (high * 18446744073709551616.0 + low) / float(scale)
+    return (high * 4294967296.0 + low) / float(scale)
 
 
 def host_field(buffers: TraceBuffers, names: Sequence[str], spec: TraceSpec) -> dict[str, Any]:

@@ -147,11 +147,15 @@ typedef struct ac_trace_params {
 } ac_trace_params;
 
 /* Outputs.  All pointers are DEVICE memory owned by the caller.  Energies
- * are accumulated as 128-bit two's-complement fixed point, stored as
- * (low word, high word) int64 pairs: value = (high * 2^64 + low) / scale,
- * where each deposit is rounded to an integer multiple of 1/scale before the
- * exact sum.  The accumulators are zeroed by the call itself; NULL optional
- * outputs are skipped. */
+ * are accumulated as exact fixed point: each deposit is rounded to an integer
+ * quantum q = round(energy * scale) (|q| <= 2^62), and each accumulator is a
+ * pair of int64 words holding the sum of the quanta's low 32 bits (unsigned)
+ * and the sum of their high parts q >> 32 (signed):
+ *     value = (word[1] * 2^32 + word[0]) / scale.
+ * The sums are exact and independent of order while fewer than 2^32 quanta
+ * reach one accumulator, which num_rays * num_bounces < 2^32 guarantees (the
+ * call rejects larger jobs with AC_ERR_CAPACITY).  The accumulators are zeroed
+ * by the call itself; NULL optional outputs are skipped. */
 typedef struct ac_trace_outputs {
     int64_t *echogram_fx;        /* [6,bins,2] required */
     int64_t *ambisonic_fx;       /* [6,4,bins,2] when render_ambisonics */

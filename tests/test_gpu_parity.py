@@ -171,10 +171,32 @@ def test_philox_fp32_statistics_match_reference_stream(rt):
                        bin_dur=tr["bin_dur"], c=343.0, max_path_len=tr["duration"] * 343.0,
                        direct_delay=float(case["direct_delay"]))["echogram"]
     assert np.max(metrics.edc_error_db(res["echogram"], ref)) <= 0.5
+    # Independent 200k-ray samples: decay parameters agree to Monte-Carlo noise (a few percent).
     np.testing.assert_allclose(res["echogram"].sum(axis=1), ref.sum(axis=1), rtol=0.02)
-    np.testing.assert_allclose(metrics.t30(res["echogram"], 0.01), metrics.t30(ref, 0.01), rtol=0.02)
-    np.testing.assert_allclose(metrics.edt(res["echogram"], 0.01), metrics.edt(ref, 0.01), rtol=0.03)
-    np.testing.assert_allclose(metrics.c50(res["echogram"], 0.01), metrics.c50(ref, 0.01), atol=0.2)
+    np.testing.assert_allclose(metrics.t30(res["echogram"], 0.01), metrics.t30(ref, 0.01), rtol=0.04)
+    np.testing.assert_allclose(metrics.edt(res["echogram"], 0.01), metrics.edt(ref, 0.01), rtol=0.04)
+    np.testing.assert_allclose(metrics.c50(res["echogram"], 0.01), metrics.c50(ref, 0.01), atol=0.3)
+
+
+def test_fp32_same_stream_decay_parameters_within_one_percent(rt):
+    """Same random stream as the float64 oracle (200k rays): T30, EDT and C50 within 1%."""
+    from acoustic_agent_b200 import metrics
+    from oracle import oracle
+    case = load_case("shoebox_linear")
+    tr = case["trace"]
+    R = 200_000
+    res = run(rt, case, spec_for(rt, case, "float32", rng="reference", num_rays=R), record_rays=False)
+    dirs, bank, rnd, idx = oracle.workspace(R, tr["bounces"], tr["seed"])
+    ref = oracle.trace(case["arrays"], source=tr["source"], listener=tr["listener"], directions=dirs,
+                       diffuse_bank=bank, diffuse_random=rnd, diffuse_indices=idx, num_bins=int(case["num_bins"]),
+                       bin_dur=tr["bin_dur"], c=343.0, max_path_len=tr["duration"] * 343.0,
+                       direct_delay=float(case["direct_delay"]))["echogram"]
+    assert np.max(metrics.edc_error_db(res["echogram"], ref)) <= 0.05
+    np.testing.assert_allclose(res["fx_echogram64"].sum(axis=1), ref.sum(axis=1), rtol=1e-4)
+    np.testing.assert_allclose(metrics.t30(res["echogram"], 0.01), metrics.t30(ref, 0.01), rtol=0.01)
+    np.testing.assert_allclose(metrics.edt(res["echogram"], 0.01), metrics.edt(ref, 0.01), rtol=0.01)
+    c50_gpu, c50_ref = metrics.c50(res["echogram"], 0.01), metrics.c50(ref, 0.01)
+    np.testing.assert_allclose(c50_gpu, c50_ref, rtol=0.01, atol=0.01)
 
 
 @pytest.mark.parametrize("precision", ["float32", "float64"])
