@@ -108,6 +108,31 @@ __global__ void philox_workspace_kernel(uint64_t seed, uint64_t key, int64_t R, 
     }
 }
 
+std::vector<Partition> partition_jobs(const ac_job *jobs, int32_t count) {
+    std::vector<Partition> parts;
+    for (int32_t j = 0; j < count; ++j) {
+        const bool fp64 = jobs[j].params.precision == AC_PRECISION_FP64;
+        const int key = fp64 ? 4 : ((jobs[j].params.rng_mode == AC_RNG_PHILOX ? 2 : 0) |
+                                    (jobs[j].params.render_ambisonics ? 1 : 0));
+        Partition *found = nullptr;
+        for (Partition &p : parts)
+            if (p.key == key) found = &p;
+        if (!found) {
+            parts.push_back(Partition{key, fp64, {}});
+            found = &parts.back();
+        }
+        found->indices.push_back(j);
+    }
+    return parts;
+}
+
+size_t partition_bytes(const ac_job *jobs, const Partition &part, const ac_batch_config *cfg) {
+    const int32_t n = static_cast<int32_t>(part.indices.size());
+    const size_t b = part.fp64 ? batch_workspace_bytes_f64(jobs, part.indices.data(), n, cfg)
+                               : batch_workspace_bytes_f32(jobs, part.indices.data(), n, cfg);
+    return (b + 255) & ~static_cast<size_t>(255);
+}
+
 }  // namespace ac
 
 extern "C" {
@@ -149,37 +174,36 @@ int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch
         return ac::fail(AC_ERR_INVALID, "ac_batch_workspace_size: bad argument");
     for (int32_t j = 0; j < num_jobs; ++j)
         if (!jobs[j].scene) return ac::fail(AC_ERR_INVALID, "job %d has no scene", j);
-    // Enough for either precision; the two partitions of a mixed batch run back to back.
-    *bytes = std::max(ac::batch_workspace_bytes_f32(jobs, num_jobs, config),
-                      ac::batch_workspace_bytes_f64(jobs, num_jobs, config));
+    size_t total = 0;
+    for (const ac::Partition &part : ac::partition_jobs(jobs, num_jobs)) total += ac::partition_bytes(jobs, part, config);
+    *bytes = total;
     return AC_OK;
 }
 
+// Jobs run in one launch per (precision, random stream, ambisonics) partition;
+// each partition has its own region of the workspace, so the launches are
+// simply enqueued one after another on the stream.
 int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
                    size_t workspace_bytes, void *host_staging, void *stream) {
     if (num_jobs < 0 || (num_jobs > 0 && (!jobs || !workspace)))
         return ac::fail(AC_ERR_INVALID, "ac_trace_batch: bad argument");
-    std::vector<int32_t> f32, f64;
     for (int32_t j = 0; j < num_jobs; ++j) {
         const int rc = ac::validate_trace(jobs[j].scene, &jobs[j].params, &jobs[j].outputs);
         if (rc != AC_OK) return ac::fail(rc, "job %d: %s", j, ac_last_error());
-        (jobs[j].params.precision == AC_PRECISION_FP64 ? f64 : f32).push_back(j);
     }
-    if (!f32.empty() && !f64.empty()) {
-        // Both partitions share the workspace, so the second must wait for the first.
-        int rc = ac::launch_batch_f32(jobs, f32.data(), static_cast<int32_t>(f32.size()), config, workspace,
-                                      workspace_bytes, host_staging, stream);
+    size_t offset = 0;
+    for (const ac::Partition &part : ac::partition_jobs(jobs, num_jobs)) {
+        const size_t bytes = ac::partition_bytes(jobs, part, config);
+        if (offset + bytes > workspace_bytes)
+            return ac::fail(AC_ERR_CAPACITY, "batch workspace too small: %zu < %zu", workspace_bytes, offset + bytes);
+        unsigned char *ws = static_cast<unsigned char *>(workspace) + offset;
+        unsigned char *host = host_staging ? static_cast<unsigned char *>(host_staging) + offset : nullptr;
+        const int32_t n = static_cast<int32_t>(part.indices.size());
+        const int rc = part.fp64 ? ac::launch_batch_f64(jobs, part.indices.data(), n, config, ws, bytes, host, stream)
+                                 : ac::launch_batch_f32(jobs, part.indices.data(), n, config, ws, bytes, host, stream);
         if (rc != AC_OK) return rc;
-        AC_CUDA_TRY(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
-        return ac::launch_batch_f64(jobs, f64.data(), static_cast<int32_t>(f64.size()), config, workspace,
-                                    workspace_bytes, host_staging, stream);
+        offset += bytes;
     }
-    if (!f64.empty())
-        return ac::launch_batch_f64(jobs, f64.data(), static_cast<int32_t>(f64.size()), config, workspace,
-                                    workspace_bytes, host_staging, stream);
-    if (!f32.empty())
-        return ac::launch_batch_f32(jobs, f32.data(), static_cast<int32_t>(f32.size()), config, workspace,
-                                    workspace_bytes, host_staging, stream);
     return AC_OK;
 }
 

@@ -69,7 +69,10 @@ AC_HD u32x4 noise_draw(uint64_t seed, uint32_t pair_index) {
                          static_cast<uint32_t>(seed >> 32));
 }
 
-// pi * (3 - sqrt(5)) as Python evaluates it (steam_rt.py:3965 golden-angle step).
+// pi * (3 - sqrt(5)) as Python evaluates it (steam_rt.py:3965 golden-angle step),
+// and the same step in turns, (3 - sqrt(5)) / 2.
 constexpr double kGoldenAngle = 2.399963229728653;
+constexpr double kGoldenTurns = 0.3819660112501051;
+constexpr double kInvTwoPi = 0.15915494309189535;
 
 }  // namespace ac

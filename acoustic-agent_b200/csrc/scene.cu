@@ -4,6 +4,7 @@
 // the production kernel and once in float64 for the parity kernel.  One device
 // allocation per precision; the handle owns both.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -28,12 +29,50 @@ template <>
 inline double tag_value<double>(int tag) { return static_cast<double>(tag); }
 
 struct Offsets {
-    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, clusters, cluster_prims, boxes, edges, total;  // elements
+    size_t prims_linear, prims_leaf, nodes, mats, corners, normals, wall_clusters, walls, polys, box_clusters,
+        box_bounds, boxes, edges, total;  // elements
 };
 
 inline size_t round4(size_t v) { return (v + 3) & ~static_cast<size_t>(3); }
 
-Offsets layout(size_t S, size_t P, size_t N, size_t C, size_t NC) {
+// Float32 scan lists: walls and boxes in clusters of up to 32 (leaves of a BVH
+// over each kind's bounds, preorder), horizontal polygons as a flat list.
+struct FastLists {
+    std::vector<int64_t> wall_slots, box_slots, polys;                    // surface index per slot
+    std::vector<std::array<int64_t, 2>> wall_clusters, box_clusters;      // {first slot, count}
+    std::vector<std::array<double, 6>> wall_cluster_bounds, box_cluster_bounds;
+};
+
+int cluster_kind(const ac_scene_desc *d, const double *blo, const double *bhi, int64_t kind, int leaf,
+                 std::vector<int64_t> &slots, std::vector<std::array<int64_t, 2>> &clusters,
+                 std::vector<std::array<double, 6>> &bounds) {
+    std::vector<int64_t> members;
+    for (int64_t i = 0; i < d->num_surfaces; ++i)
+        if (d->kinds[i] == kind) members.push_back(i);
+    if (members.empty()) return AC_OK;
+    const int64_t M = static_cast<int64_t>(members.size());
+    std::vector<double> lo(3 * M), hi(3 * M);
+    for (int64_t k = 0; k < M; ++k)
+        for (int a = 0; a < 3; ++a) {
+            lo[3 * k + a] = blo[3 * members[k] + a];
+            hi[3 * k + a] = bhi[3 * members[k] + a];
+        }
+    const size_t cap = 2 * static_cast<size_t>(M);
+    std::vector<double> nmin(3 * cap), nmax(3 * cap);
+    std::vector<int64_t> nstart(cap), ncount(cap), nesc(cap), nprims(M);
+    ac_bvh b{nmin.data(), nmax.data(), nstart.data(), ncount.data(), nesc.data(), nprims.data(), 0, 0, 0};
+    const int rc = ac_bvh_build(lo.data(), hi.data(), M, leaf, &b);
+    if (rc != AC_OK) return rc;
+    for (int64_t k = 0; k < M; ++k) slots.push_back(members[nprims[k]]);
+    for (int64_t n = 0; n < b.node_count; ++n) {
+        if (ncount[n] <= 0) continue;
+        clusters.push_back({nstart[n], ncount[n]});
+        bounds.push_back({nmin[3 * n], nmin[3 * n + 1], nmin[3 * n + 2], nmax[3 * n], nmax[3 * n + 1], nmax[3 * n + 2]});
+    }
+    return AC_OK;
+}
+
+Offsets layout(size_t S, size_t P, size_t N, size_t C, const FastLists *f) {
     Offsets o{};
     size_t off = 0;
     o.prims_linear = off;  off += round4(S * ac::kPrimStride);
@@ -42,10 +81,13 @@ Offsets layout(size_t S, size_t P, size_t N, size_t C, size_t NC) {
     o.mats = off;          off += round4(S * ac::kMatStride);
     o.corners = off;       off += round4(C * 2);
     o.normals = off;       off += round4(S * 3);
-    o.clusters = off;      off += round4(NC * ac::kClusterStride);
-    o.cluster_prims = off; off += round4(NC ? S * ac::kPrimStride : 0);
-    o.boxes = off;         off += round4(NC ? S * 8 : 0);
-    o.edges = off;         off += round4(NC ? C * 4 : 0);
+    o.wall_clusters = off; off += round4(f ? f->wall_clusters.size() * ac::kClusterStride : 0);
+    o.walls = off;         off += round4(f ? f->wall_slots.size() * 8 : 0);
+    o.polys = off;         off += round4(f ? f->polys.size() * 4 : 0);
+    o.box_clusters = off;  off += round4(f ? f->box_clusters.size() * ac::kClusterStride : 0);
+    o.box_bounds = off;    off += round4(f ? f->box_slots.size() * 8 : 0);
+    o.boxes = off;         off += round4(f ? f->box_slots.size() * ac::kPrimStride : 0);
+    o.edges = off;         off += round4(f ? C * 4 : 0);
     o.total = off;
     return o;
 }
@@ -123,37 +165,55 @@ void pack_record(const ac_scene_desc *d, int64_t si, T *rec) {
 }
 
 template <typename T>
-int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clusters, const double *bounds_lo,
+int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const FastLists *f, const double *bounds_lo,
                     const double *bounds_hi, ac_scene_s *s, void **storage, size_t *bytes, ac::SceneDev<T> *view) {
     const size_t S = static_cast<size_t>(d->num_surfaces);
     const size_t N = static_cast<size_t>(bvh.node_count);
     const size_t P = S;
     const size_t C = static_cast<size_t>(d->num_corners);
-    const size_t NC = clusters ? static_cast<size_t>(clusters->leaf_count) : 0;
-    const Offsets o = layout(S, P, N, C, NC);
+    const Offsets o = layout(S, P, N, C, f);
     std::vector<T> host(o.total, T(0));
-    if (clusters) {
-        // Float32 scan: clusters = leaves of the cluster BVH in preorder.
-        size_t c = 0;
-        for (int64_t n = 0; n < clusters->node_count; ++n) {
-            if (clusters->count[n] <= 0) continue;
-            T *cp = host.data() + o.clusters + c * ac::kClusterStride;
-            for (int a = 0; a < 3; ++a) {
-                cp[a] = T(clusters->bounds_min[3 * n + a]);
-                cp[4 + a] = T(clusters->bounds_max[3 * n + a]);
+    if (f) {
+        auto put_clusters = [&](size_t base, const std::vector<std::array<int64_t, 2>> &cl,
+                                const std::vector<std::array<double, 6>> &cb) {
+            for (size_t c = 0; c < cl.size(); ++c) {
+                T *cp = host.data() + base + c * ac::kClusterStride;
+                for (int a = 0; a < 3; ++a) {
+                    cp[a] = T(cb[c][a]);
+                    cp[4 + a] = T(cb[c][3 + a]);
+                }
+                cp[3] = tag_value<T>(static_cast<int>(cl[c][0]));
+                cp[7] = tag_value<T>(static_cast<int>(cl[c][1]));
             }
-            cp[3] = tag_value<T>(static_cast<int>(clusters->start[n]));
-            cp[7] = tag_value<T>(static_cast<int>(clusters->count[n]));
-            ++c;
+        };
+        put_clusters(o.wall_clusters, f->wall_clusters, f->wall_cluster_bounds);
+        put_clusters(o.box_clusters, f->box_clusters, f->box_cluster_bounds);
+        for (size_t k = 0; k < f->wall_slots.size(); ++k) {
+            const int64_t si = f->wall_slots[k];
+            T *w = host.data() + o.walls + 8 * k;
+            w[0] = T(d->wall_a[2 * si]);
+            w[1] = T(d->wall_a[2 * si + 1]);
+            w[2] = T(d->wall_delta[2 * si]);
+            w[3] = T(d->wall_delta[2 * si + 1]);
+            w[4] = T(d->wall_z[2 * si]);
+            w[5] = T(d->wall_z[2 * si + 1]);
+            w[6] = tag_value<T>(static_cast<int>(si) * 4 + AC_KIND_WALL);
         }
-        for (size_t k = 0; k < S; ++k) {
-            const int64_t si = clusters->primitives[k];
-            pack_record<T>(d, si, host.data() + o.cluster_prims + k * ac::kPrimStride);
-            T *bb = host.data() + o.boxes + k * 8;
+        for (size_t k = 0; k < f->polys.size(); ++k) {
+            const int64_t si = f->polys[k];
+            T *pp = host.data() + o.polys + 4 * k;
+            pp[0] = T(d->z_values[si]);
+            pp[1] = tag_value<T>(static_cast<int>(si) * 4 + AC_KIND_HORIZONTAL);
+        }
+        for (size_t k = 0; k < f->box_slots.size(); ++k) {
+            const int64_t si = f->box_slots[k];
+            pack_record<T>(d, si, host.data() + o.boxes + k * ac::kPrimStride);
+            T *bb = host.data() + o.box_bounds + 8 * k;
             for (int a = 0; a < 3; ++a) {
                 bb[a] = T(bounds_lo[3 * si + a]);
                 bb[4 + a] = T(bounds_hi[3 * si + a]);
             }
+            bb[3] = tag_value<T>(static_cast<int>(si) * 4 + AC_KIND_BOX);
         }
         // Polygon edges for the even-odd test: {x_i, y_i, y_j, (x_j - x_i) / (y_j - y_i)} with j the
         // previous corner (steam_rt.py:4259-4274); an edge the reference skips gets y_j = y_i.
@@ -211,15 +271,20 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const ac_bvh *clu
     view->num_nodes = static_cast<int32_t>(N);
     view->num_corners = static_cast<int32_t>(C);
     view->num_leaf_prims = static_cast<int32_t>(P);
-    if (clusters) {
+    if (f) {
         const float *fbase = reinterpret_cast<const float *>(dev);
-        s->fast.clusters = fbase + o.clusters;
-        s->fast.prims = fbase + o.cluster_prims;
+        s->fast.wall_clusters = fbase + o.wall_clusters;
+        s->fast.walls = fbase + o.walls;
+        s->fast.polys = fbase + o.polys;
+        s->fast.box_clusters = fbase + o.box_clusters;
+        s->fast.box_bounds = fbase + o.box_bounds;
         s->fast.boxes = fbase + o.boxes;
         s->fast.edges = fbase + o.edges;
-        s->fast.num_clusters = static_cast<int32_t>(NC);
+        s->fast.num_wall_clusters = static_cast<int32_t>(f->wall_clusters.size());
+        s->fast.num_polys = static_cast<int32_t>(f->polys.size());
+        s->fast.num_box_clusters = static_cast<int32_t>(f->box_clusters.size());
         s->fast.num_edges = static_cast<int32_t>(C);
-        s->num_clusters = static_cast<int64_t>(NC);
+        s->num_clusters = static_cast<int64_t>(f->wall_clusters.size() + f->box_clusters.size());
     }
     return AC_OK;
 }
@@ -329,17 +394,20 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
         blo = slo.data();
         bhi = shi.data();
     }
-    s->cluster_size = d->cluster_size > 0 ? std::min(d->cluster_size, 64) : 8;
-    const size_t cap = 2 * static_cast<size_t>(S);
-    std::vector<double> cmin(3 * cap), cmax(3 * cap);
-    std::vector<int64_t> cstart(cap), ccount(cap), cesc(cap), cprims(S);
-    ac_bvh cbvh{cmin.data(), cmax.data(), cstart.data(), ccount.data(), cesc.data(), cprims.data(), 0, 0, 0};
-    int rc = ac_bvh_build(blo, bhi, S, s->cluster_size, &cbvh);
+    s->cluster_size = d->cluster_size > 0 ? std::min(d->cluster_size, ac::kMaxCluster) : ac::kMaxCluster;
+    FastLists lists;
+    for (int64_t i = 0; i < S; ++i)
+        if (d->kinds[i] == AC_KIND_HORIZONTAL) lists.polys.push_back(i);
+    int rc = cluster_kind(d, blo, bhi, AC_KIND_WALL, s->cluster_size, lists.wall_slots, lists.wall_clusters,
+                          lists.wall_cluster_bounds);
+    if (rc == AC_OK)
+        rc = cluster_kind(d, blo, bhi, AC_KIND_BOX, s->cluster_size, lists.box_slots, lists.box_clusters,
+                          lists.box_cluster_bounds);
     if (rc != AC_OK) {
         delete s;
         return rc;
     }
-    rc = pack_and_upload<float>(d, bvh, &cbvh, blo, bhi, s, &s->storage_f32, &s->bytes_f32, &s->f32);
+    rc = pack_and_upload<float>(d, bvh, &lists, blo, bhi, s, &s->storage_f32, &s->bytes_f32, &s->f32);
     if (rc == AC_OK)
         rc = pack_and_upload<double>(d, bvh, nullptr, blo, bhi, s, &s->storage_f64, &s->bytes_f64, &s->f64);
     if (rc != AC_OK) {

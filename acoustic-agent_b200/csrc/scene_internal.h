@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "acoustic_rt.h"
 #include "trace_fast.cuh"
@@ -56,7 +57,16 @@ int launch_batch_f32(const ac_job *jobs, const int32_t *indices, int32_t count, 
                      void *workspace, size_t bytes, void *host_staging, void *stream);
 int launch_batch_f64(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg,
                      void *workspace, size_t bytes, void *host_staging, void *stream);
-size_t batch_workspace_bytes_f32(const ac_job *jobs, int32_t count, const ac_batch_config *cfg);
-size_t batch_workspace_bytes_f64(const ac_job *jobs, int32_t count, const ac_batch_config *cfg);
+size_t batch_workspace_bytes_f32(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg);
+size_t batch_workspace_bytes_f64(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg);
+
+// Jobs of one batch launch: same precision, random-stream mode and ambisonics setting.
+struct Partition {
+    int key;
+    bool fp64;
+    std::vector<int32_t> indices;
+};
+std::vector<Partition> partition_jobs(const ac_job *jobs, int32_t count);
+size_t partition_bytes(const ac_job *jobs, const Partition &part, const ac_batch_config *cfg);
 
 }  // namespace ac

@@ -9,13 +9,19 @@ namespace ac {
 
 namespace {
 
-constexpr int kDefaultChunkRays = 256;
+constexpr int kDefaultChunkRays = 32;
+
+using FastKernel = void (*)(const Job<float>, const FastScene, const FastTable);
 
 template <bool kSingle>
-int fast_grid(int device, int block, int64_t total_rays, int requested) {
+FastKernel pick_kernel(bool philox, bool amb) {
+    if (philox) return amb ? trace_fast_kernel<kSingle, true, true> : trace_fast_kernel<kSingle, true, false>;
+    return amb ? trace_fast_kernel<kSingle, false, true> : trace_fast_kernel<kSingle, false, false>;
+}
+
+int fast_grid(FastKernel kernel, int device, int block, int64_t total_rays, int requested) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_fast_kernel<kSingle>, block, 0) != cudaSuccess ||
-        per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     int grid = requested > 0 ? requested : per_sm * device_sm_count(device);
     const int64_t needed = (total_rays + block - 1) / block;
@@ -85,19 +91,17 @@ int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac
     FastTable table{};
     table.chunk_rays = kDefaultChunkRays;
     table.chunk_counter = reinterpret_cast<unsigned long long *>(o->counters) + 4;
-    const int grid = fast_grid<true>(scene->device, block, p->num_rays, p->grid_blocks);
-    trace_fast_kernel<true><<<grid, block, 0, stream>>>(job, scene->fast, table);
+    const FastKernel kernel = pick_kernel<true>(p->rng_mode == AC_RNG_PHILOX, p->render_ambisonics != 0);
+    const int grid = fast_grid(kernel, scene->device, block, p->num_rays, p->grid_blocks);
+    kernel<<<grid, block, 0, stream>>>(job, scene->fast, table);
     AC_CUDA_TRY(cudaGetLastError());
     return launch_finalize_single<float>(scene, p, o, scale, stream_ptr);
 }
 
-size_t batch_workspace_bytes_f32(const ac_job *jobs, int32_t count, const ac_batch_config *cfg) {
-    std::vector<int32_t> all(count);
-    std::iota(all.begin(), all.end(), 0);
+size_t batch_workspace_bytes_f32(const ac_job *jobs, const int32_t *indices, int32_t count, const ac_batch_config *cfg) {
     const int64_t chunk_rays = (cfg && cfg->chunk_rays > 0) ? cfg->chunk_rays : kDefaultChunkRays;
     int64_t groups = 0, chunks = 0;
-    if (jobs) count_groups_chunks(jobs, scene_order(jobs, all.data(), count), chunk_rays, &groups, &chunks);
-    else { groups = count; chunks = count; }
+    count_groups_chunks(jobs, scene_order(jobs, indices, count), chunk_rays, &groups, &chunks);
     return f32_layout(count, groups, chunks).total;
 }
 
@@ -145,6 +149,8 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         double scale = in.params.energy_scale;
         if (!(scale > 0.0)) scale = choose_energy_scale(in.scene, &in.params);
         fill_job<float>(in.scene, &in.params, &in.outputs, scale, jobs[k]);
+        if (k > 0 && (jobs[k].rng_mode != jobs[0].rng_mode || jobs[k].render_ambisonics != jobs[0].render_ambisonics))
+            return fail(AC_ERR_INVALID, "one float32 launch needs one random-stream mode and ambisonics setting");
         if (in.outputs.scale_out) *in.outputs.scale_out = scale;
         prefix[k] = total;
         jobs[k].ray_begin = total;
@@ -180,8 +186,10 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         Job<float> unused;
         std::memset(&unused, 0, sizeof(unused));
         FastScene none{};
-        const int grid = fast_grid<false>(device, block, total, cfg ? cfg->grid_blocks : 0);
-        trace_fast_kernel<false><<<grid, block, 0, stream>>>(unused, none, table);
+        // ac_trace_batch partitions jobs so that one launch has one kernel variant.
+        const FastKernel kernel = pick_kernel<false>(jobs[0].rng_mode == AC_RNG_PHILOX, jobs[0].render_ambisonics != 0);
+        const int grid = fast_grid(kernel, device, block, total, cfg ? cfg->grid_blocks : 0);
+        kernel<<<grid, block, 0, stream>>>(unused, none, table);
         AC_CUDA_TRY(cudaGetLastError());
     }
     {

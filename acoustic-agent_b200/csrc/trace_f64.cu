@@ -16,6 +16,8 @@ int launch_batch_f64(const ac_job *jobs, const int32_t *indices, int32_t count, 
     return launch_batch<double>(jobs, indices, count, cfg, workspace, bytes, host_staging, stream);
 }
 
-size_t batch_workspace_bytes_f64(const ac_job *, int32_t count, const ac_batch_config *) { return batch_bytes<double>(count); }
+size_t batch_workspace_bytes_f64(const ac_job *, const int32_t *, int32_t count, const ac_batch_config *) {
+    return batch_bytes<double>(count);
+}
 
 }  // namespace ac

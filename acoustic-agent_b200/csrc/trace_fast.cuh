@@ -2,19 +2,22 @@
 //
 // Same per-ray algorithm as trace_kernel.cuh (steam_rt.py:4708-4850), but the
 // intersection queries are organised for SIMT instead of restating the
-// reference's per-thread escape-link walk:
+// reference's per-thread escape-link walk.  A warp always works on ONE scene;
+// its surfaces are kept in three kind-separated lists:
 //
-//   * a warp always works on ONE scene.  All 32 lanes step through the
-//     scene's surface clusters (leaves of a BVH built with 8 surfaces per leaf,
-//     in preorder) together; each lane tests its own ray against the cluster's
-//     AABB with its current best t, and the warp skips the cluster when no lane
-//     needs it (__any_sync).  Inside a cluster every lane tests the same surface
-//     at the same time, so the surface-kind branch is uniform and each record is
-//     one broadcast load;
+//   * walls (2-D segments with a z range) and horizontal polygons are tested by
+//     every lane in lockstep: all lanes read the same record (one broadcast
+//     load) and the code path is uniform.  Walls are grouped in clusters of up
+//     to 32 with an AABB the warp skips when no lane's ray can reach it;
+//   * boxes (oriented furniture proxies) are grouped in clusters of up to 32.
+//     Each lane first builds a 32-bit candidate mask from cheap world-AABB
+//     tests done in lockstep, then all lanes pop their OWN next candidate
+//     together -- same instructions, different box -- so the warp runs as many
+//     exact box tests as the busiest lane needs, not the union over lanes;
 //   * primitive tests compute only t, with reciprocal multiplies; the normal is
 //     evaluated once, for the winning surface (boxes re-run the slab test);
-//   * the shadow query runs the same scan with an early exit once every lane
-//     that needs it has found a blocker;
+//   * the shadow query tests boxes first (the likely blockers) and stops once
+//     every lane that needs it has found a blocker;
 //   * lanes refill the moment their ray ends from the warp's current range of
 //     (job, ray) work items; all jobs that share a scene form one range, so the
 //     eight channels of an array trace as one stream.  A warp moves to another
@@ -30,15 +33,26 @@
 
 namespace ac {
 
-// Cluster record: {lo.x, lo.y, lo.z, first slot} {hi.x, hi.y, hi.z, count}
+// Resident 256-thread blocks per SM the register allocation targets.
+#ifndef AC_FAST_MIN_BLOCKS
+#define AC_FAST_MIN_BLOCKS 3
+#endif
+
+// Cluster record: {lo.x, lo.y, lo.z, first} {hi.x, hi.y, hi.z, count}, count <= 32
 constexpr int kClusterStride = 8;
+constexpr int kMaxCluster = 32;
 
 struct FastScene {
-    const float *clusters;       // [NC][8]
-    const float *prims;          // [P][12] surface records in cluster-slot order
-    const float *boxes;          // [P][8] world AABB per slot {lo.xyz, 0, hi.xyz, 0} (used for boxes)
-    const float *edges;          // [C][4] {x_i, y_i, y_j (or y_i if skipped), (x_j-x_i)/(y_j-y_i)}
-    int32_t num_clusters;
+    const float *wall_clusters;  // [NWC][8]
+    const float *walls;          // [NW][8]  {ax, ay, sx, sy} {z0, z1, tag, 0}
+    const float *polys;          // [NP][4]  {z, tag, 0, 0}
+    const float *box_clusters;   // [NBC][8]
+    const float *box_bounds;     // [NB][8]  world AABB {lo.xyz, tag} {hi.xyz, 0}
+    const float *boxes;          // [NB][12] box records (trace_kernel.cuh layout)
+    const float *edges;          // [C][4]   {x_i, y_i, y_j (or y_i if skipped), (x_j-x_i)/(y_j-y_i)}
+    int32_t num_wall_clusters;
+    int32_t num_polys;
+    int32_t num_box_clusters;
     int32_t num_edges;
 };
 
@@ -105,6 +119,7 @@ __device__ __forceinline__ bool cluster_overlaps(const FRay &r, const Quad<float
 
 __device__ __forceinline__ bool point_in_polygon_fast(float x, float y, const float *edges, int n) {
     bool inside = false;
+#pragma unroll 1
     for (int i = 0; i < n; ++i) {
         const Quad<float> e = ldq(edges + 4 * i);  // uniform across the warp
         if ((e.y > y) != (e.z > y)) {
@@ -114,147 +129,156 @@ __device__ __forceinline__ bool point_in_polygon_fast(float x, float y, const fl
     return inside;
 }
 
-// t of one surface for one ray (1e30 = miss); steam_rt.py:4361-4392 restated with reciprocals.
-__device__ __forceinline__ float surface_t(const float *rec, int kind, const FRay &r, const FastScene &fs) {
-    if (kind == 0) {
-        const Quad<float> A = ldq(rec), B = ldq(rec + 4);
-        const float det = A.z * r.d[1] - A.w * r.d[0];
-        if (fabsf(det) > 1e-12f) {
-            const float inv = __frcp_rn(det);
-            const float relx = r.o[0] - A.x, rely = r.o[1] - A.y;
-            const float t = (relx * A.w - rely * A.z) * inv;
-            const float u = (relx * r.d[1] - rely * r.d[0]) * inv;
-            const float z = r.o[2] + t * r.d[2];
-            if (t > 1e-6f && u >= -1e-6f && u <= 1.000001f && z >= B.x - 1e-6f && z <= B.y + 1e-6f) return t;
-        }
-        return 1e30f;
-    }
-    if (kind == 2) {
-        const Quad<float> A = ldq(rec), B = ldq(rec + 4), C = ldq(rec + 8);
+// Wall t (steam_rt.py:4366-4377 with a reciprocal); 1e30 = miss.
+__device__ __forceinline__ float wall_t(const Quad<float> &A, const Quad<float> &B, const FRay &r) {
+    const float det = A.z * r.d[1] - A.w * r.d[0];
+    if (fabsf(det) > 1e-12f) {
+        const float inv = __frcp_rn(det);
         const float relx = r.o[0] - A.x, rely = r.o[1] - A.y;
-        const float ox = relx * A.z + rely * A.w;
-        const float oy = relx * B.x + rely * B.y;
-        const float dx = r.d[0] * A.z + r.d[1] * A.w;
-        const float dy = r.d[0] * B.x + r.d[1] * B.y;
-        float t_min = -1e30f, t_max = 1e30f;
-        if (fabsf(dx) <= 1e-12f) {
-            if (ox < -B.z || ox > B.z) return 1e30f;
-        } else {
-            const float ix = __frcp_rn(dx);
-            const float a = (-B.z - ox) * ix, b = (B.z - ox) * ix;
-            t_min = fminf(a, b);
-            t_max = fmaxf(a, b);
-        }
-        if (fabsf(dy) <= 1e-12f) {
-            if (oy < -B.w || oy > B.w) return 1e30f;
-        } else {
-            const float iy = __frcp_rn(dy);
-            const float a = (-B.w - oy) * iy, b = (B.w - oy) * iy;
-            t_min = fmaxf(t_min, fminf(a, b));
-            t_max = fminf(t_max, fmaxf(a, b));
-        }
-        if (fabsf(r.d[2]) <= 1e-12f) {
-            if (r.o[2] < C.x || r.o[2] > C.y) return 1e30f;
-        } else {
-            const float a = (C.x - r.o[2]) * r.inv[2], b = (C.y - r.o[2]) * r.inv[2];
-            t_min = fmaxf(t_min, fminf(a, b));
-            t_max = fminf(t_max, fmaxf(a, b));
-        }
-        if (t_min > t_max || t_max <= 1e-6f) return 1e30f;
-        const float t = t_min > 1e-6f ? t_min : t_max;
-        return t < 1e29f ? t : 1e30f;
-    }
-    const Quad<float> A = ldq(rec);
-    if (fabsf(r.d[2]) > 1e-12f) {
-        const float t = (A.x - r.o[2]) * r.inv[2];
-        if (t > 1e-6f) {
-            const float px = r.o[0] + t * r.d[0];
-            const float py = r.o[1] + t * r.d[1];
-            if (point_in_polygon_fast(px, py, fs.edges, fs.num_edges)) return t;
-        }
+        const float t = (relx * A.w - rely * A.z) * inv;
+        const float u = (relx * r.d[1] - rely * r.d[0]) * inv;
+        const float z = r.o[2] + t * r.d[2];
+        if (t > 1e-6f && u >= -1e-6f && u <= 1.000001f && z >= B.x - 1e-6f && z <= B.y + 1e-6f) return t;
     }
     return 1e30f;
 }
 
-// Warp-uniform closest hit.  Every lane of the warp must call it; `active`
-// lanes carry a ray.  Returns the winning surface index (-1: none) and its slot.
-__device__ __forceinline__ int closest_scan(const FastScene &fs, const FRay &r, bool active, float &best_t,
-                                            int &best_slot) {
-    const unsigned full = 0xFFFFFFFFu;
-    best_t = 1e30f;
-    int best = -1;
-    best_slot = -1;
-    for (int c = 0; c < fs.num_clusters; ++c) {
-        const float *cp = fs.clusters + kClusterStride * c;
-        const Quad<float> lo = ldq(cp), hi = ldq(cp + 4);
-        const bool pass = active && cluster_overlaps(r, lo, hi, best_t);
-        if (!__any_sync(full, pass)) continue;
-        const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
-        for (int k = 0; k < count; ++k) {
-            const float *rec = fs.prims + static_cast<size_t>(first + k) * kPrimStride;
-            const int tag = __float_as_int(__ldg(rec + 11));
-            bool test = pass;
-            if ((tag & 3) == 2) {
-                // Boxes: cheap world-AABB check first; the warp skips the box if no lane needs it.
-                const float *bb = fs.boxes + static_cast<size_t>(first + k) * 8;
-                test = pass && cluster_overlaps(r, ldq(bb), ldq(bb + 4), best_t);
-                if (!__any_sync(full, test)) continue;
-            }
-            if (test) {
-                const float t = surface_t(rec, tag & 3, r, fs);
-                const int si = tag >> 2;
-                if (t < best_t || (t == best_t && t < 1e30f && si < best)) {
-                    best_t = t;
-                    best = si;
-                    best_slot = first + k;
-                }
-            }
-        }
+// Oriented box t (steam_rt.py:4277-4358, slabs with reciprocals); 1e30 = miss.
+__device__ __forceinline__ float box_t(const float *rec, const FRay &r) {
+    const Quad<float> A = ldq(rec), B = ldq(rec + 4), C = ldq(rec + 8);
+    const float relx = r.o[0] - A.x, rely = r.o[1] - A.y;
+    const float ox = relx * A.z + rely * A.w;
+    const float oy = relx * B.x + rely * B.y;
+    const float dx = r.d[0] * A.z + r.d[1] * A.w;
+    const float dy = r.d[0] * B.x + r.d[1] * B.y;
+    float t_min = -1e30f, t_max = 1e30f;
+    if (fabsf(dx) <= 1e-12f) {
+        if (ox < -B.z || ox > B.z) return 1e30f;
+    } else {
+        const float ix = __frcp_rn(dx);
+        const float a = (-B.z - ox) * ix, b = (B.z - ox) * ix;
+        t_min = fminf(a, b);
+        t_max = fmaxf(a, b);
     }
-    return best;
+    if (fabsf(dy) <= 1e-12f) {
+        if (oy < -B.w || oy > B.w) return 1e30f;
+    } else {
+        const float iy = __frcp_rn(dy);
+        const float a = (-B.w - oy) * iy, b = (B.w - oy) * iy;
+        t_min = fmaxf(t_min, fminf(a, b));
+        t_max = fminf(t_max, fmaxf(a, b));
+    }
+    if (fabsf(r.d[2]) <= 1e-12f) {
+        if (r.o[2] < C.x || r.o[2] > C.y) return 1e30f;
+    } else {
+        const float a = (C.x - r.o[2]) * r.inv[2], b = (C.y - r.o[2]) * r.inv[2];
+        t_min = fmaxf(t_min, fminf(a, b));
+        t_max = fminf(t_max, fmaxf(a, b));
+    }
+    if (t_min > t_max || t_max <= 1e-6f) return 1e30f;
+    const float t = t_min > 1e-6f ? t_min : t_max;
+    return t < 1e29f ? t : 1e30f;
 }
 
-// Warp-uniform shadow query: is a surface hit before max_t?  Lanes with
-// `active` false (or that already found a blocker) ride along.
-__device__ __forceinline__ bool shadow_scan(const FastScene &fs, const FRay &r, bool active, float max_t) {
+__device__ __forceinline__ void take(float t, int si, float &best_t, int &best) {
+    if (t < best_t || (t == best_t && t < 1e30f && si < best)) {
+        best_t = t;
+        best = si;
+    }
+}
+
+// Warp-uniform scene query; every lane of the warp must call it.
+//
+// Closest-hit mode (best_t starts at 1e30): the minimum t over all surfaces,
+// ties to the lower surface index.  Any-hit mode (best_t starts at the shadow
+// ray's length): a lane stops as soon as it finds any surface closer than
+// that.  Both modes use the same update rule, so the code exists once:
+// `best` is the surface found (-1: none) and best_t its t.
+__device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, bool active, bool any_hit,
+                                           float &best_t, int &best) {
     const unsigned full = 0xFFFFFFFFu;
-    bool blocked = false;
-    for (int c = 0; c < fs.num_clusters; ++c) {
-        const bool searching = active && !blocked;
-        if (!__any_sync(full, searching)) break;
-        const float *cp = fs.clusters + kClusterStride * c;
+    best = -1;
+    // Walls, in lockstep.
+#pragma unroll 1
+    for (int c = 0; c < fs.num_wall_clusters; ++c) {
+        const bool searching = active && !(any_hit && best >= 0);
+        if (any_hit && !__any_sync(full, searching)) return;
+        const float *cp = fs.wall_clusters + kClusterStride * c;
         const Quad<float> lo = ldq(cp), hi = ldq(cp + 4);
-        const bool pass = searching && cluster_overlaps(r, lo, hi, max_t);
+        const bool pass = searching && cluster_overlaps(r, lo, hi, best_t);
         if (!__any_sync(full, pass)) continue;
         const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
+#pragma unroll 1
         for (int k = 0; k < count; ++k) {
-            const float *rec = fs.prims + static_cast<size_t>(first + k) * kPrimStride;
-            const int tag = __float_as_int(__ldg(rec + 11));
-            bool test = pass && !blocked;
-            if ((tag & 3) == 2) {
-                const float *bb = fs.boxes + static_cast<size_t>(first + k) * 8;
-                test = test && cluster_overlaps(r, ldq(bb), ldq(bb + 4), max_t);
-                if (!__any_sync(full, test)) continue;
-            }
-            if (test) {
-                if (surface_t(rec, tag & 3, r, fs) < max_t) blocked = true;
+            const float *w = fs.walls + static_cast<size_t>(first + k) * 8;
+            const Quad<float> A = ldq(w), B = ldq(w + 4);
+            if (pass) take(wall_t(A, B, r), __float_as_int(B.z) >> 2, best_t, best);
+        }
+    }
+    // Horizontal polygons (floor, ceiling), in lockstep.
+#pragma unroll 1
+    for (int k = 0; k < fs.num_polys; ++k) {
+        const Quad<float> P = ldq(fs.polys + 4 * k);
+        const float t = (P.x - r.o[2]) * r.inv[2];
+        const int si = __float_as_int(P.y) >> 2;
+        const bool cand = active && !(any_hit && best >= 0) && fabsf(r.d[2]) > 1e-12f && t > 1e-6f &&
+                          (t < best_t || (t == best_t && si < best));
+        if (__any_sync(full, cand)) {
+            const float px = r.o[0] + t * r.d[0], py = r.o[1] + t * r.d[1];
+            if (cand && point_in_polygon_fast(px, py, fs.edges, fs.num_edges)) take(t, si, best_t, best);
+        }
+    }
+    // Boxes: per-lane candidate masks from world AABBs, then per-lane candidates in lockstep.
+#pragma unroll 1
+    for (int c = 0; c < fs.num_box_clusters; ++c) {
+        const bool searching = active && !(any_hit && best >= 0);
+        if (any_hit && !__any_sync(full, searching)) return;
+        const float *cp = fs.box_clusters + kClusterStride * c;
+        const Quad<float> lo = ldq(cp), hi = ldq(cp + 4);
+        const bool pass = searching && cluster_overlaps(r, lo, hi, best_t);
+        if (!__any_sync(full, pass)) continue;
+        const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
+        unsigned mask = 0u;
+#pragma unroll 1
+        for (int k = 0; k < count; ++k) {
+            const float *bb = fs.box_bounds + static_cast<size_t>(first + k) * 8;
+            if (pass && cluster_overlaps(r, ldq(bb), ldq(bb + 4), best_t)) mask |= 1u << k;
+        }
+        while (__any_sync(full, mask != 0u)) {
+            if (mask) {
+                const int k = __ffs(mask) - 1;
+                mask &= mask - 1u;
+                const float *rec = fs.boxes + static_cast<size_t>(first + k) * kPrimStride;
+                take(box_t(rec, r), __float_as_int(__ldg(rec + 11)) >> 2, best_t, best);
+                if (any_hit && best >= 0) mask = 0u;
             }
         }
     }
-    return blocked;
 }
 
 // Normal of the winning surface, oriented against the ray.
-__device__ __forceinline__ void winner_normal(const FastScene &fs, int slot, const FRay &r, float *n) {
-    const float *rec = fs.prims + static_cast<size_t>(slot) * kPrimStride;
+__device__ __forceinline__ void winner_normal(const SceneDev<float> &sc, int si, const FRay &r, float t, float *n) {
+    const float *rec = sc.prims_linear + static_cast<size_t>(si) * kPrimStride;
     const int kind = __float_as_int(__ldg(rec + 11)) & 3;
     if (kind == 0) {
         n[0] = __ldg(rec + 6); n[1] = __ldg(rec + 7); n[2] = __ldg(rec + 8);
     } else if (kind == 2) {
+        // Face of the box the hit point lies on: the box-frame axis where the
+        // point is closest to the face, relative to the half extent.
         const Quad<float> A = ldq(rec), B = ldq(rec + 4), C = ldq(rec + 8);
-        float bn[3] = {0.0f, 0.0f, 1.0f};
-        box_hit(A, B, C, r.o, r.d, bn);
-        n[0] = bn[0]; n[1] = bn[1]; n[2] = bn[2];
+        const float px = r.o[0] + t * r.d[0] - A.x, py = r.o[1] + t * r.d[1] - A.y, pz = r.o[2] + t * r.d[2];
+        const float lx = px * A.z + py * A.w, ly = px * B.x + py * B.y;
+        const float hz = 0.5f * (C.y - C.x), lz = pz - 0.5f * (C.x + C.y);
+        const float ex = fabsf(fabsf(lx) - B.z), ey = fabsf(fabsf(ly) - B.w), ez = fabsf(fabsf(lz) - hz);
+        if (ex <= ey && ex <= ez) {
+            const float sg = lx >= 0.0f ? 1.0f : -1.0f;
+            n[0] = sg * A.z; n[1] = sg * A.w; n[2] = 0.0f;
+        } else if (ey <= ez) {
+            const float sg = ly >= 0.0f ? 1.0f : -1.0f;
+            n[0] = sg * B.x; n[1] = sg * B.y; n[2] = 0.0f;
+        } else {
+            n[0] = 0.0f; n[1] = 0.0f; n[2] = lz >= 0.0f ? 1.0f : -1.0f;
+        }
     } else {
         n[0] = __ldg(rec + 1); n[1] = __ldg(rec + 2); n[2] = __ldg(rec + 3);
     }
@@ -271,9 +295,31 @@ static __device__ __noinline__ int2 fallback_walk(const SceneDev<float> sc, floa
     return make_int2(surf, __float_as_int(t));
 }
 
+// Float32 unit vector with the reference's zero-length rule (|v| <= 1e-12 -> 0), via rsqrt.
+__device__ __forceinline__ void normalize3f(float x, float y, float z, float *out) {
+    const float n2 = x * x + y * y + z * z;
+    if (n2 <= 1e-24f) { out[0] = 0.0f; out[1] = 0.0f; out[2] = 0.0f; return; }
+    const float inv = rsqrtf(n2);
+    out[0] = x * inv; out[1] = y * inv; out[2] = z * inv;
+}
+
+// steam_rt.py:4564-4582 in float32 with rsqrt normalisation.
+__device__ __forceinline__ void diffuse_direction_f(float s0, float s1, float s2, float nx, float ny, float nz,
+                                                    float *out) {
+    float hx = 1.0f, hy = 0.0f;
+    if (fabsf(nx) >= 0.9f) { hx = 0.0f; hy = 1.0f; }
+    float t[3];
+    normalize3f(hy * nz, -hx * nz, hx * ny - hy * nx, t);
+    const float bx = ny * t[2] - nz * t[1];
+    const float by = nz * t[0] - nx * t[2];
+    const float bz = nx * t[1] - ny * t[0];
+    normalize3f(s0 * t[0] + s1 * bx + s2 * nx, s0 * t[1] + s1 * by + s2 * ny, s0 * t[2] + s1 * bz + s2 * nz, out);
+}
+
 struct FastLane {
     float o[3];
     float d[3];
+    float d0[3];  // initial direction (ambisonic coefficients)
     float acc[kBands];
     double path;
     int64_t ray;
@@ -291,8 +337,8 @@ __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int
     return lo;
 }
 
-template <bool kSingle>
-__global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__ Job<float> single,
+template <bool kSingle, bool kPhilox, bool kAmb>
+__global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(const __grid_constant__ Job<float> single,
                                                          const __grid_constant__ FastScene single_fast,
                                                          const __grid_constant__ FastTable table) {
     const unsigned full = 0xFFFFFFFFu;
@@ -360,7 +406,14 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
                 s.shadows = 0;
                 s.path = 0.0;
                 s.o[0] = job.lst[0]; s.o[1] = job.lst[1]; s.o[2] = job.lst[2];
-                initial_direction(job, ri, s.d);
+                if (kPhilox) {
+                    const double3 v = philox_direction(job.seed, job.stream_key, job.num_rays, ri);
+                    s.d[0] = static_cast<float>(v.x); s.d[1] = static_cast<float>(v.y); s.d[2] = static_cast<float>(v.z);
+                } else {
+                    s.d[0] = job.directions[3 * ri]; s.d[1] = job.directions[3 * ri + 1];
+                    s.d[2] = job.directions[3 * ri + 2];
+                }
+                if (kAmb) { s.d0[0] = s.d[0]; s.d0[1] = s.d[1]; s.d0[2] = s.d[2]; }
 #pragma unroll
                 for (int b = 0; b < kBands; ++b) s.acc[b] = 1.0f;
                 has = true;
@@ -388,72 +441,87 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
         const FastScene &fs = kSingle ? single_fast : table.groups[group].fast;
         const Job<float> &job = kSingle ? single : table.jobs[s.job];
 
-        // ---- closest hit (all lanes)
+        // ---- two queries per bounce through one copy of the scan: phase 0 finds the
+        // closest hit, phase 1 casts the shadow ray toward the source.
         FRay ray;
         make_ray(ray, s.o, s.d);
-        float t;
-        int slot;
-        int surf = closest_scan(fs, ray, has, t, slot);
-        if (has && surf < 0 && job.use_bvh) {
-            // Missed everything: the reference's BVH walk reports the lowest visited surface.
-            const int2 fb = fallback_walk(job.scene, s.o[0], s.o[1], s.o[2], s.d[0], s.d[1], s.d[2]);
-            surf = fb.x;
-            t = __int_as_float(fb.y);
-            slot = -1;
-        }
+        float t = 1e30f;
+        int surf = -1;
         float n[3] = {0.0f, 0.0f, 1.0f};
         bool finished = false, alive_at_end = false, count_hit = false;
-        bool need_shadow = false;
-        float hx = 0.0f, hy = 0.0f, hz = 0.0f, dist = 0.0f, facing = 0.0f;
+        bool need_shadow = false, occluded = false;
+        float hx = 0.0f, hy = 0.0f, hz = 0.0f, dist = 0.0f, facing = 0.0f, inv_dist = 0.0f;
         float sd[3] = {0.0f, 0.0f, 0.0f};
-        if (has) {
-            s.queries += 1;
-            bool dead = surf < 0 || t <= job.listener_radius || s.path > job.max_path_length;
-            if (!dead && s.bounce > 0) {
-                if (sphere_before(s.o, s.d, job.lst, job.listener_radius, t)) dead = true;
-                else if (job.source_distance > job.source_radius &&
-                         sphere_before(s.o, s.d, job.src, job.source_radius, t))
-                    dead = true;
+        FRay query = ray;
+        bool query_active = has;
+        float limit = 1e30f;
+#pragma unroll 1
+        for (int phase = 0; phase < 2; ++phase) {
+            float found_t = limit;
+            int found = -1;
+            scene_scan(fs, query, query_active, phase == 1, found_t, found);
+            if (phase == 1) {
+                occluded = found >= 0;
+                break;
             }
-            if (dead) {
-                finished = true;
-            } else {
-                count_hit = true;
-                if (slot >= 0) {
-                    winner_normal(fs, slot, ray, n);
+            t = found_t;
+            surf = found;
+            bool from_walk = false;
+            if (has && surf < 0 && job.use_bvh) {
+                // Missed everything: the reference's BVH walk reports the lowest visited surface.
+                const int2 fb = fallback_walk(job.scene, s.o[0], s.o[1], s.o[2], s.d[0], s.d[1], s.d[2]);
+                surf = fb.x;
+                t = __int_as_float(fb.y);
+                from_walk = true;
+            }
+            if (has) {
+                s.queries += 1;
+                bool dead = surf < 0 || t <= job.listener_radius || s.path > job.max_path_length;
+                if (!dead && s.bounce > 0) {
+                    if (sphere_before(s.o, s.d, job.lst, job.listener_radius, t)) dead = true;
+                    else if (job.source_distance > job.source_radius &&
+                             sphere_before(s.o, s.d, job.src, job.source_radius, t))
+                        dead = true;
+                }
+                if (dead) {
+                    finished = true;
                 } else {
-                    n[0] = __ldg(job.scene.normals + 3 * surf);
-                    n[1] = __ldg(job.scene.normals + 3 * surf + 1);
-                    n[2] = __ldg(job.scene.normals + 3 * surf + 2);
-                    if (n[0] * s.d[0] + n[1] * s.d[1] + n[2] * s.d[2] > 0.0f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
-                }
-                if (job.ray_surfaces) job.ray_surfaces[s.ray * job.num_bounces + s.bounce] = surf;
-                hx = s.o[0] + t * s.d[0] + 1e-2f * n[0];
-                hy = s.o[1] + t * s.d[1] + 1e-2f * n[1];
-                hz = s.o[2] + t * s.d[2] + 1e-2f * n[2];
-                const float tsx = job.src[0] - hx, tsy = job.src[1] - hy, tsz = job.src[2] - hz;
-                dist = sqrtf(tsx * tsx + tsy * tsy + tsz * tsz);
-                if (dist > job.irradiance_min_distance) {
-                    const float inv = 1.0f / dist;
-                    sd[0] = tsx * inv; sd[1] = tsy * inv; sd[2] = tsz * inv;
-                    facing = n[0] * sd[0] + n[1] * sd[1] + n[2] * sd[2];
-                    need_shadow = facing > 0.0f;
+                    count_hit = true;
+                    if (!from_walk) {
+                        winner_normal(job.scene, surf, ray, t, n);
+                    } else {
+                        n[0] = __ldg(job.scene.normals + 3 * surf);
+                        n[1] = __ldg(job.scene.normals + 3 * surf + 1);
+                        n[2] = __ldg(job.scene.normals + 3 * surf + 2);
+                        if (n[0] * s.d[0] + n[1] * s.d[1] + n[2] * s.d[2] > 0.0f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+                    }
+                    if (job.ray_surfaces) job.ray_surfaces[s.ray * job.num_bounces + s.bounce] = surf;
+                    hx = s.o[0] + t * s.d[0] + 1e-2f * n[0];
+                    hy = s.o[1] + t * s.d[1] + 1e-2f * n[1];
+                    hz = s.o[2] + t * s.d[2] + 1e-2f * n[2];
+                    const float tsx = job.src[0] - hx, tsy = job.src[1] - hy, tsz = job.src[2] - hz;
+                    const float d2 = tsx * tsx + tsy * tsy + tsz * tsz;
+                    const float inv = rsqrtf(fmaxf(d2, 1e-30f));
+                    dist = d2 * inv;
+                    if (dist > job.irradiance_min_distance) {
+                        inv_dist = inv;
+                        sd[0] = tsx * inv; sd[1] = tsy * inv; sd[2] = tsz * inv;
+                        facing = n[0] * sd[0] + n[1] * sd[1] + n[2] * sd[2];
+                        need_shadow = facing > 0.0f;
+                    }
                 }
             }
+            // per-surface hit counters: one atomic per distinct (job, surface) in the warp
+            const unsigned counting = __ballot_sync(full, count_hit);
+            if (count_hit) {
+                warp_count(counting, (static_cast<unsigned long long>(s.job) << 32) | static_cast<unsigned>(surf), 1u,
+                           job.hit_counts + surf);
+            }
+            const float h[3] = {hx, hy, hz};
+            make_ray(query, h, sd);
+            query_active = need_shadow;
+            limit = dist - 1e-6f;
         }
-
-        // ---- per-surface hit counters: one atomic per distinct (job, surface) in the warp
-        const unsigned counting = __ballot_sync(full, count_hit);
-        if (count_hit) {
-            warp_count(counting, (static_cast<unsigned long long>(s.job) << 32) | static_cast<unsigned>(surf), 1u,
-                       job.hit_counts + surf);
-        }
-
-        // ---- shadow ray toward the source (all lanes; those not needing it ride along)
-        FRay shadow;
-        const float h[3] = {hx, hy, hz};
-        make_ray(shadow, h, sd);
-        const bool occluded = shadow_scan(fs, shadow, need_shadow, dist - 1e-6f);
 
         if (has && !finished) {
             const Quad<float> m0 = ldq(job.scene.mats + static_cast<size_t>(surf) * kMatStride);
@@ -465,20 +533,21 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
                 if (!occluded) {
                     const float diffuse = static_cast<float>(1.0 / kPi) * scat * facing;
                     float half[3];
-                    normalize3(sd[0] - s.d[0], sd[1] - s.d[1], sd[2] - s.d[2], half);
+                    normalize3f(sd[0] - s.d[0], sd[1] - s.d[1], sd[2] - s.d[2], half);
                     float cos_half = half[0] * n[0] + half[1] * n[1] + half[2] * n[2];
                     cos_half = cos_half > 0.0f ? cos_half : 0.0f;
                     const float specular = ((job.specular_exponent + 2.0f) * static_cast<float>(1.0 / (8.0 * kPi))) *
                                            (1.0f - scat) * __powf(cos_half, job.specular_exponent);
-                    const float dmax = fmaxf(dist, job.irradiance_min_distance);
-                    const float distance_term = static_cast<float>(1.0 / (4.0 * kPi)) / (dmax * dmax);
+                    // dist > irradiance_min_distance here, so max(dist, min) = dist
+                    const float distance_term = static_cast<float>(1.0 / (4.0 * kPi)) * (inv_dist * inv_dist);
                     const float source_cosine = -(job.fwd[0] * sd[0] + job.fwd[1] * sd[1] + job.fwd[2] * sd[2]);
                     const float gain_base = fabsf((1.0f - job.dipole_weight) + job.dipole_weight * source_cosine);
                     const float source_gain = job.dipole_power == 1.0f ? gain_base : __powf(gain_base, job.dipole_power);
+                    // reciprocal multiplies (the float32 path needs no correctly rounded division here)
                     const double rel_delay =
-                        (s.path + static_cast<double>(t) + static_cast<double>(dist)) / job.speed_of_sound -
+                        (s.path + static_cast<double>(t) + static_cast<double>(dist)) * job.inv_speed_of_sound -
                         job.direct_delay;
-                    const double q = floor(rel_delay / job.bin_duration);
+                    const double q = floor(rel_delay * job.inv_bin_duration);
                     if (q >= 0.0 && q < static_cast<double>(job.num_bins)) {
                         const int bin = static_cast<int>(q);
                         const float common = job.ray_scale * source_gain * distance_term * (diffuse + specular);
@@ -488,9 +557,8 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
                             const float e = common * refl[b] * s.acc[b];
                             const long long qe = quantize(e, job.energy_scale);
                             add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
-                            if (job.ambisonic_fx) {
-                                float d0[3];
-                                initial_direction(job, s.ray, d0);
+                            if (kAmb) {
+                                const float *d0 = s.d0;
                                 unsigned long long *a =
                                     job.ambisonic_fx + 2 * (static_cast<size_t>(b) * 4 * job.num_bins + bin);
                                 const size_t stride = 2 * static_cast<size_t>(job.num_bins);
@@ -512,7 +580,7 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
             s.o[0] = hx; s.o[1] = hy; s.o[2] = hz;
             bool use_diffuse;
             int sample;
-            if (job.rng_mode == 0) {
+            if (!kPhilox) {
                 const size_t k = static_cast<size_t>(s.bounce) * job.num_rays + s.ray;
                 use_diffuse = job.diffuse_random[k] < scat;
                 sample = use_diffuse ? job.diffuse_indices[k] : 0;
@@ -524,10 +592,10 @@ __global__ void __launch_bounds__(256) trace_fast_kernel(const __grid_constant__
             }
             if (use_diffuse) {
                 const float *bs = job.diffuse_bank + 3 * sample;
-                diffuse_direction(__ldg(bs), __ldg(bs + 1), __ldg(bs + 2), n[0], n[1], n[2], s.d);
+                diffuse_direction_f(__ldg(bs), __ldg(bs + 1), __ldg(bs + 2), n[0], n[1], n[2], s.d);
             } else {
                 const float dot = s.d[0] * n[0] + s.d[1] * n[1] + s.d[2] * n[2];
-                normalize3(s.d[0] - 2.0f * dot * n[0], s.d[1] - 2.0f * dot * n[1], s.d[2] - 2.0f * dot * n[2], s.d);
+                normalize3f(s.d[0] - 2.0f * dot * n[0], s.d[1] - 2.0f * dot * n[1], s.d[2] - 2.0f * dot * n[2], s.d);
             }
             s.bounce += 1;
             if (s.path > job.max_path_length) {

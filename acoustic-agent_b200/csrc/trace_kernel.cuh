@@ -119,6 +119,8 @@ struct Job {
     double bin_duration;
     double max_path_length;
     double energy_scale;
+    double inv_speed_of_sound;
+    double inv_bin_duration;
     int64_t num_rays;
     int64_t ray_begin;  // first global work index of this job
     int32_t num_bounces;
@@ -424,6 +426,25 @@ __device__ __forceinline__ void add_fixed(unsigned long long *acc, long long q) 
     if (hi) atomicAdd(acc + 1, static_cast<unsigned long long>(hi));
 }
 
+// Jittered Fibonacci-sphere direction of ray `ri` drawn from the counter-based
+// stream (steam_rt.py:3959-3968 layout, jitter from Philox).  The angle is kept
+// in turns and reduced before sincospi, so no large-argument trigonometry runs;
+// explicitly rounded operations keep the result independent of FMA contraction.
+static __device__ __noinline__ double3 philox_direction(uint64_t seed, uint64_t key, int64_t num_rays, int64_t ri) {
+    const u32x4 r = trace_draw(seed, key, static_cast<uint32_t>(ri), 0u);
+    // jitter U(-0.02, 0.02) rad, expressed in turns
+    const double jitter = __dmul_rn(__dadd_rn(-0.02, __dmul_rn(0.04, u01_53(r.x, r.y))), kInvTwoPi);
+    const double i = static_cast<double>(ri) + 0.5;
+    const double z = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(2.0, i), static_cast<double>(num_rays)));
+    double rr = __dsub_rn(1.0, __dmul_rn(z, z));
+    rr = __dsqrt_rn(rr < 0.0 ? 0.0 : (rr > 1.0 ? 1.0 : rr));
+    const double turns = __dadd_rn(__dmul_rn(i, kGoldenTurns), jitter);
+    const double frac = __dsub_rn(turns, floor(turns));
+    double s, c;
+    sincospi(__dmul_rn(2.0, frac), &s, &c);
+    return make_double3(__dmul_rn(c, rr), __dmul_rn(s, rr), z);
+}
+
 // Initial direction of ray `ri` of a job.
 template <typename T>
 __device__ __forceinline__ void initial_direction(const Job<T> &job, int64_t ri, T *d) {
@@ -433,22 +454,10 @@ __device__ __forceinline__ void initial_direction(const Job<T> &job, int64_t ri,
         d[2] = job.directions[3 * ri + 2];
         return;
     }
-    // Jittered Fibonacci sphere (steam_rt.py:3959-3968) with the jitter drawn
-    // from the counter-based stream instead of a sequential generator.
-    // Explicitly rounded operations: the result must not depend on whether the
-    // translation unit allows FMA contraction.
-    const u32x4 r = trace_draw(job.seed, job.stream_key, static_cast<uint32_t>(ri), 0u);
-    const double jitter = __dadd_rn(-0.02, __dmul_rn(0.04, u01_53(r.x, r.y)));
-    const double i = static_cast<double>(ri) + 0.5;
-    const double z = __dsub_rn(1.0, __ddiv_rn(__dmul_rn(2.0, i), static_cast<double>(job.num_rays)));
-    double rr = __dsub_rn(1.0, __dmul_rn(z, z));
-    rr = __dsqrt_rn(rr < 0.0 ? 0.0 : (rr > 1.0 ? 1.0 : rr));
-    const double theta = __dadd_rn(__dmul_rn(i, kGoldenAngle), jitter);
-    double s, c;
-    sincos(theta, &s, &c);
-    d[0] = static_cast<T>(__dmul_rn(c, rr));
-    d[1] = static_cast<T>(__dmul_rn(s, rr));
-    d[2] = static_cast<T>(z);
+    const double3 v = philox_direction(job.seed, job.stream_key, job.num_rays, ri);
+    d[0] = static_cast<T>(v.x);
+    d[1] = static_cast<T>(v.y);
+    d[2] = static_cast<T>(v.z);
 }
 
 // ---------------------------------------------------------------------------

@@ -100,6 +100,8 @@ inline void fill_job(const ac_scene_s *scene, const ac_trace_params *p, const ac
     job.speed_of_sound = p->speed_of_sound;
     job.direct_delay = p->direct_delay;
     job.bin_duration = p->bin_duration;
+    job.inv_speed_of_sound = 1.0 / p->speed_of_sound;
+    job.inv_bin_duration = 1.0 / p->bin_duration;
     job.max_path_length = p->max_path_length;
     job.energy_scale = scale;
     job.num_rays = p->num_rays;

@@ -347,12 +347,14 @@ def philox_workspace(num_rays: int, num_bounces: int, seed: int, stream_key: int
     s0, s1 = int(seed) & 0xFFFFFFFF, (int(seed) >> 32) & 0xFFFFFFFF
     x, y, _, _ = philox4x32_10(ray, np.zeros(R, np.uint64), np.full(R, key_lo, np.uint64),
                                np.full(R, key_hi, np.uint64), s0, s1)
-    jitter = -0.02 + 0.04 * _u01_53(x, y)
+    # jitter U(-0.02, 0.02) rad in turns; angle = 2*pi*frac(i * (3 - sqrt 5)/2 + jitter)
+    jitter = (-0.02 + 0.04 * _u01_53(x, y)) * 0.15915494309189535
     i = np.arange(R, dtype=np.float64) + 0.5
     z = 1.0 - 2.0 * i / R
     r = np.sqrt(np.clip(1.0 - z * z, 0.0, 1.0))
-    theta = i * 2.399963229728653 + jitter
-    directions = np.stack([np.cos(theta) * r, np.sin(theta) * r, z], axis=1)
+    turns = i * 0.3819660112501051 + jitter
+    angle = np.pi * (2.0 * (turns - np.floor(turns)))
+    directions = np.stack([np.cos(angle) * r, np.sin(angle) * r, z], axis=1)
     rnd = np.empty((num_bounces, R))
     idx = np.empty((num_bounces, R), np.int32)
     for b in range(num_bounces):
