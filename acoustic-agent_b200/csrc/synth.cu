@@ -117,14 +117,25 @@ __global__ void synth_raw_kernel(const double *amps, const double *air, const do
     }
 }
 
-// One section of an eight-pole low-pass (steam_rt.py:4131-4146).
+// One section of an eight-pole low-pass (steam_rt.py:4131-4146):
+//     y0 = b0*x0 + b1*x1 + b2*x2 - a1*y1 - a2*y2, evaluated left to right.
+// The input part ((b0*x0 + b1*x1) + b2*x2) does not depend on y, so it is
+// computed one sample ahead (`feed`); the per-sample recursion (`step`) is then
+// only (S - a1*y1) - a2*y2.  Same operations in the same order as the reference.
 struct Section {
     double b0, b1, b2, a1, a2, x1, x2, y1, y2;
 
-    __device__ __forceinline__ float step(double in) {
-        const double y0 = b0 * in + b1 * x1 + b2 * x2 - a1 * y1 - a2 * y2;
-        x2 = x1; x1 = in;
-        y2 = y1; y1 = y0;
+    __device__ __forceinline__ double feed(double in) {
+        const double v = b0 * in + b1 * x1 + b2 * x2;
+        x2 = x1;
+        x1 = in;
+        return v;
+    }
+
+    __device__ __forceinline__ float step(double v) {
+        const double y0 = v - a1 * y1 - a2 * y2;
+        y2 = y1;
+        y1 = y0;
         return static_cast<float>(y0);
     }
 };
@@ -175,7 +186,9 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
         ahead[u] = (valid_unit && u < N) ? __ldg(x + u) : 0.0;
         prev[u] = 0.0;
     }
-    float q0 = 0.0f, q1 = 0.0f;  // inputs from the previous section for this and the next iteration
+    float q1 = 0.0f;  // value the previous section sent last iteration (this section's input next iteration)
+    // input part of the first sample (its input is ahead[0] for section 0 and +0.0 otherwise)
+    double v = sec.feed(is_first ? ahead[0] : 0.0);
     const int iterations = N + kLag;
     for (int base = 0; base < iterations; base += kPrefetch) {
         double next[kPrefetch];
@@ -187,11 +200,13 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
             const int it = base + u;
-            const double in = is_first ? ahead[u] : static_cast<double>(q0);
-            const float y = sec.step(in);
+            const float y = sec.step(v);
+            // input of the next iteration: section 0 reads the prefetched signal,
+            // later sections the value their predecessor sent two iterations ago
+            const double in_next = is_first ? (u + 1 < kPrefetch ? ahead[u + 1] : next[0]) : static_cast<double>(q1);
+            v = sec.feed(in_next);
             const float sent = __shfl_up_sync(full, y, 1);
             const float lower = __shfl_down_sync(full, y, 4);
-            q0 = q1;
             q1 = sent;
             // x[it - kLag] is still in registers from the prefetch
             const double x_n = (u >= kLag) ? ahead[u - kLag] : prev[u + kPrefetch - kLag];
