@@ -27,6 +27,7 @@ AC_PRECISION_FP32 = 0
 AC_PRECISION_FP64 = 1
 AC_RNG_REFERENCE = 0
 AC_RNG_PHILOX = 1
+AC_SYNTH_STATIC_BYTES = 16 << 20
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
 c_int64_p = ctypes.POINTER(ctypes.c_int64)
@@ -128,6 +129,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_synth_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACSynthParams), ctypes.POINTER(ctypes.c_size_t)]),
     "ac_synthesize": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "ac_synthesize_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
+                                            ctypes.c_void_p]),
     "ac_philox_workspace": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p]),

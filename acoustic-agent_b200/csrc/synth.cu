@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 
 #include <cuda_runtime.h>
 
@@ -277,6 +278,96 @@ extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, f
     const int warps = (units + 3) / 4;
     const int threads = 32;  // one warp per block: spread the sequential chains over all SMs
     ac::synth_filter_kernel<<<warps, threads, 0, stream>>>(raw, a, band_irs);
+    AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Band synthesis without any device allocation (ac_synthesize_static).
+//
+// For callers that must not allocate device memory themselves or through us:
+// a real-time audio thread, where cudaMalloc can block on the driver for
+// milliseconds, or a host engine that owns the whole device-memory budget and
+// forbids third-party allocations.  The workspace lives in this file-scope
+// array instead; every GPU that loads the library holds it until the process
+// exits.  Every call shares it, and it keeps the last call's contents: all
+// regions a call reads are written earlier in the same call, so nothing needs
+// clearing, but calls that overlap on the GPU (different streams, or threads)
+// race on it and must be serialised by the caller.
+
+namespace {
+
+static __device__ __align__(256) unsigned char g_synth_scratch[AC_SYNTH_STATIC_BYTES];
+
+std::mutex g_scratch_mutex;
+void *g_scratch_ptr[64] = {nullptr};
+
+// Device address of the static scratch for the current device, looked up once
+// per device (the host-side symbol is only a stand-in, never a device address).
+int static_scratch(void **out) {
+    int device = 0;
+    AC_CUDA_TRY(cudaGetDevice(&device));
+    if (device < 0 || device >= 64) return ac::fail(AC_ERR_UNSUPPORTED, "device ordinal %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_ptr[device]) {
+        void *ptr = nullptr;
+        AC_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_synth_scratch));
+        g_scratch_ptr[device] = ptr;
+    }
+    *out = g_scratch_ptr[device];
+    return AC_OK;
+}
+
+}  // namespace
+
+extern "C" int ac_synthesize_static(const float *echograms, const ac_synth_params *p, float *band_irs,
+                                    void *stream_ptr) {
+    if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize_static: null argument");
+    if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
+        return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
+    const int64_t N = static_cast<int64_t>(p->num_bins) * p->samples_per_bin;
+    if (N + 3 > 0x7FFFFFFF) return ac::fail(AC_ERR_CAPACITY, "signal of %lld samples is too long", (long long)N);
+    if (p->rng_mode == AC_RNG_REFERENCE && !p->white) return ac::fail(AC_ERR_INVALID, "reference mode needs white noise");
+    if (!p->air && !p->direct_delays) return ac::fail(AC_ERR_INVALID, "need an air table or the direct delays");
+    const ac::SynthLayout l = ac::synth_layout(p);
+    if (l.total > static_cast<size_t>(AC_SYNTH_STATIC_BYTES))
+        return ac::fail(AC_ERR_CAPACITY,
+                        "synthesis of %d RIRs x %lld samples needs %zu bytes of scratch; the static scratch holds %zu: "
+                        "split the RIRs over several calls",
+                        p->num_rirs, (long long)N, l.total, static_cast<size_t>(AC_SYNTH_STATIC_BYTES));
+    if (p->num_rirs == 0) return AC_OK;
+    void *scratch = nullptr;
+    const int rc = static_scratch(&scratch);
+    if (rc != AC_OK) return rc;
+    ac::SynthArgs a;
+    std::memcpy(a.crossover, p->crossover, sizeof(a.crossover));
+    std::memcpy(a.air_coefficients, p->air_coefficients, sizeof(a.air_coefficients));
+    a.speed_of_sound = p->speed_of_sound;
+    a.num_rirs = p->num_rirs;
+    a.num_bins = p->num_bins;
+    a.spb = p->samples_per_bin;
+    a.sample_rate = p->sample_rate;
+    unsigned char *ws = static_cast<unsigned char *>(scratch);
+    double *amps = reinterpret_cast<double *>(ws + l.amps);
+    double *air = p->air ? nullptr : reinterpret_cast<double *>(ws + l.air);
+    double *wtab = reinterpret_cast<double *>(ws + l.wtab);
+    double *white = p->rng_mode == AC_RNG_PHILOX ? reinterpret_cast<double *>(ws + l.white) : nullptr;
+    double *raw = reinterpret_cast<double *>(ws + l.raw);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    const size_t cells = static_cast<size_t>(p->num_rirs) * 6 * p->num_bins;
+    const size_t work = std::max<size_t>(cells, static_cast<size_t>(white ? N : p->samples_per_bin));
+    const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, 8192));
+    ac::synth_prepare_kernel<<<grid, 256, 0, stream>>>(echograms, p->direct_delays, a, amps, air, wtab, white, p->seed);
+    AC_CUDA_TRY(cudaGetLastError());
+    const double *air_table = p->air ? p->air : air;
+    const double *noise = white ? white : p->white;
+    const size_t stride = (white || p->white_shared) ? 0 : static_cast<size_t>(N);
+    const size_t samples = static_cast<size_t>(p->num_rirs) * 6 * static_cast<size_t>(N);
+    const int raw_grid = static_cast<int>(std::min<size_t>((samples + 255) / 256, 65536));
+    ac::synth_raw_kernel<<<raw_grid, 256, 0, stream>>>(amps, air_table, wtab, noise, stride, a, raw);
+    AC_CUDA_TRY(cudaGetLastError());
+    const int warps = (p->num_rirs * 6 + 3) / 4;
+    ac::synth_filter_kernel<<<warps, 32, 0, stream>>>(raw, a, band_irs);
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
 }

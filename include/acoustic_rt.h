@@ -244,6 +244,21 @@ int ac_synth_workspace_size(const ac_synth_params *params, size_t *bytes);
 int ac_synthesize(const float *echograms, const ac_synth_params *params, float *band_irs, void *workspace,
                   size_t workspace_bytes, void *stream);
 
+/* ac_synthesize without any device allocation.  No counterpart in the
+ * reference (its synthesis runs on the CPU).  For callers that must not
+ * allocate device memory: a real-time audio thread, where cudaMalloc can
+ * block on the driver for milliseconds, or a host engine that owns the whole
+ * device-memory budget and forbids third-party allocations.  The caller passes
+ * inputs and outputs as for ac_synthesize; the workspace comes from a static
+ * device array of AC_SYNTH_STATIC_BYTES that every GPU loading the library
+ * holds until exit.  Calls whose workspace (ac_synth_workspace_size) exceeds
+ * it fail with AC_ERR_CAPACITY; split the RIRs over several calls.  The first
+ * call on a device looks up the array's device address, so make that first
+ * call before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+#define AC_SYNTH_STATIC_BYTES (16u << 20)
+int ac_synthesize_static(const float *echograms, const ac_synth_params *params, float *band_irs, void *stream);
+
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */
 int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces,
