@@ -9,11 +9,15 @@ step, all in one persistent trace launch plus one synthesis launch, replayed
 as a CUDA graph.  Inputs (the scene) are resident in HBM; L2 is flushed
 between timed steps.
 
-``--impl reference`` times the reference algorithm on the host cores instead
-(the float64 CPU restatement, all threads) on the same workload, one RIR per
-step.  Under torchrun each rank runs an independent replica (replicas only:
-jobs are independent, no collective on the data path); rank 0 prints one JSON
-line.
+``--impl reference`` times the reference's own CPU implementation of the path
+instead: the unmodified reference package installed under baseline/_ref,
+``steam_rt.trace_energy_field`` on its float64 Numba path over all host
+threads plus ``reconstruct_band_irs``, one RIR of the same workload per step
+(the float64 C restatement when the package is absent).  The default arm also
+reports the reference's Numba-CUDA float32 backend on the same GPU
+(``reference_cuda``).  Under torchrun each rank runs an independent replica
+(replicas only: jobs are independent, no collective on the data path); rank 0
+prints one JSON line.
 """
 from __future__ import annotations
 
@@ -25,6 +29,7 @@ import statistics
 import sys
 import threading
 import time
+import types
 from datetime import timedelta
 from pathlib import Path
 
@@ -115,6 +120,129 @@ def _dist_setup():
     return world, rank, local
 
 
+REFERENCE_TARGET = REPO / "baseline" / "_ref"
+
+
+class _Stub(types.ModuleType):
+    """Stand-in for a module the reference imports at top level but the tracer never calls."""
+
+    def __getattr__(self, item):
+        if item.startswith("__"):
+            raise AttributeError(item)
+        return type(item, (), {})
+
+
+def import_reference_package():
+    """The unmodified reference installed with pip --target under baseline/_ref: (steam_rt, models) or a reason.
+
+    shapely and h5py are imported at module level by the reference but unused
+    on the reflection path, and are absent here; empty stand-ins take their place.
+    """
+    if not (REFERENCE_TARGET / "acoustic_agent" / "steam_rt.py").exists():
+        return None, "reference package not installed under baseline/_ref"
+    for name in ("shapely", "shapely.geometry", "shapely.geometry.base", "shapely.ops", "h5py"):
+        try:
+            __import__(name)
+        except Exception:
+            sys.modules[name] = _Stub(name)
+    if isinstance(sys.modules.get("shapely"), _Stub):
+        sys.modules["shapely"].affinity = _Stub("shapely.affinity")
+    try:
+        import networkx  # noqa: F401
+    except Exception:
+        sys.modules.setdefault("networkx", _Stub("networkx"))
+    if str(REFERENCE_TARGET) not in sys.path:
+        sys.path.insert(0, str(REFERENCE_TARGET))
+    try:
+        from acoustic_agent import models, steam_rt
+    except Exception as exc:  # pragma: no cover - depends on the box
+        return None, f"reference import failed: {type(exc).__name__}: {exc}"
+    return (steam_rt, models), None
+
+
+def reference_scene(steam_rt, models, spec: dict):
+    """The reference's own RoomRayScene for a workload spec (models.Room + per-surface materials)."""
+    band_names = models.FREQUENCY_BANDS
+
+    def material(kind, data):
+        absorption = data.get("absorption", [0.1] * 6)
+        scattering = data.get("scattering", [0.1] * 6)
+        return models.Material(id=f"bench_{kind}", name=kind, semantic=kind,
+                               absorption={b: float(v) for b, v in zip(band_names, absorption)},
+                               scattering={b: float(v) for b, v in zip(band_names, scattering)})
+
+    metadata = {}
+    if spec.get("surface_segments") is not None:
+        metadata["surface_segments"] = [dict(s) for s in spec["surface_segments"]]
+    if spec.get("objects") is not None:
+        metadata["objects"] = [dict(o) for o in spec["objects"]]
+    room = models.Room(id="bench", name="bench", corners=tuple((float(x), float(y)) for x, y in spec["corners"]),
+                       height_m=float(spec["height"]),
+                       materials={k: material(k, v) for k, v in spec.get("materials", {}).items()},
+                       metadata=metadata)
+    steam_rt._clear_static_caches()
+    scene = steam_rt.RoomRayScene(room)
+    if spec.get("surface_absorption") is not None:
+        for surface, row in zip(scene.surfaces, spec["surface_absorption"]):
+            surface.absorption = np.asarray(row, dtype=float)
+    if spec.get("surface_scattering") is not None:
+        for surface, value in zip(scene.surfaces, spec["surface_scattering"]):
+            surface.scattering = np.full(6, float(value))
+    return scene
+
+
+def reference_rirs(workload, steps: int, warmup: int, *, accelerator: str, precision: str,
+                   channel: int = 0, rays: int | None = None) -> dict:
+    """One RIR per step through the reference's public reflection call on one channel of the workload.
+
+    ``steam_rt.trace_energy_field`` (steam_rt.py:1757-1804; "numba" = the
+    float64 Numba CPU path over all host threads, "cuda" = its Numba-CUDA
+    float32 kernel) followed by ``reconstruct_band_irs`` (steam_rt.py:2205-2232).
+    """
+    ref, reason = import_reference_package()
+    if ref is None:
+        return {"unavailable": reason}
+    steam_rt, models = ref
+    cfg = workload.config
+    if accelerator == "cuda":
+        from acoustic_agent.steam_rt_cuda import cuda_available
+        if not cuda_available(0):
+            return {"unavailable": "the reference's Numba-CUDA backend reports no usable CUDA device"}
+    scene = reference_scene(steam_rt, models, workload.spec)
+    R = int(rays or cfg.rt_num_rays)
+    sim = models.SimConfig(fs=cfg.fs, c=cfg.c, duration_s=cfg.duration_s, rt_duration_s=cfg.rt_duration_s,
+                           rt_num_rays=R, rt_num_bounces=cfg.rt_num_bounces,
+                           rt_bin_duration_s=cfg.rt_bin_duration_s, rt_specular_exponent=cfg.rt_specular_exponent,
+                           rt_irradiance_min_distance=cfg.rt_irradiance_min_distance,
+                           rt_source_radius=cfg.rt_source_radius, rt_listener_radius=cfg.rt_listener_radius,
+                           intersection_backend=cfg.intersection_backend, seed=cfg.seed,
+                           rt_accelerator=accelerator, rt_precision=precision, collect_visual_paths=False,
+                           render_ambisonics=False)
+    src = np.asarray(workload.sources[0], dtype=float)
+    lst = np.asarray(workload.listeners[channel], dtype=float)
+    times, trace_times = [], []
+    field = None
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        field = steam_rt.trace_energy_field(scene, src, lst, sim, workload.source_model, render_ambisonics=False)
+        t1 = time.perf_counter()
+        steam_rt.reconstruct_band_irs(field, sim)
+        if k >= warmup:
+            times.append(time.perf_counter() - t0)
+            trace_times.append(t1 - t0)
+    per_rir = float(np.mean(times))
+    threads = None
+    if accelerator == "numba":
+        import numba
+        threads = int(numba.get_num_threads())
+    return {"value": 1.0 / per_rir, "seconds_per_rir": per_rir, "trace_seconds": float(np.mean(trace_times)),
+            "threads": threads, "rays": R,
+            "accelerator": field.get("accelerator") if isinstance(field, dict) else accelerator,
+            "sample": (f"channel {channel} of {len(workload.listeners)}: {R} rays x {cfg.rt_num_bounces} bounces, "
+                       f"trace_energy_field(rt_accelerator={accelerator!r}, rt_precision={precision!r}) + "
+                       f"reconstruct_band_irs, mean of {steps} after {warmup} warm-up")}
+
+
 def cpu_reference(workload, steps: int, warmup: int, *, channel: int = 0, rays: int | None = None) -> dict:
     """The reference algorithm on the host: float64 trace + band synthesis of one RIR per step (all cores)."""
     from oracle import oracle
@@ -165,20 +293,31 @@ def cpu_reference(workload, steps: int, warmup: int, *, channel: int = 0, rays: 
 
 
 def run_reference_arm(args, workload_name: str) -> None:
+    """The reference's own CPU implementation of the path, one RIR per step, all host threads.
+
+    The unmodified reference package under baseline/_ref runs its float64
+    Numba path (``rt_accelerator="numba"``); when that package cannot be
+    imported, the float64 C restatement of the same algorithm runs instead.
+    """
     world, rank, _ = _dist_setup()
     if rank != 0:
         return
     workload = _workload(workload_name)[0]
-    ref = cpu_reference(workload, args.steps, args.warmup)
+    ref = reference_rirs(workload, args.steps, args.warmup, accelerator="numba", precision="float64")
+    if "unavailable" not in ref:
+        kind, cores, note = "reference", ref["threads"], ("the reference package (baseline/_ref), "
+                                                           "steam_rt.trace_energy_field float64 Numba path")
+    else:
+        reason = ref["unavailable"]
+        ref = cpu_reference(workload, args.steps, args.warmup)
+        kind, cores, note = "port", ref["cores"], f"{reason}; float64 C restatement of the reference algorithm"
     line = {
         "impl": "reference", "metric": METRIC, "value": ref["value"], "unit": "RIRs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ref["seconds_per_rir"] * 1000.0,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": workload.name, "rays": workload.config.rt_num_rays,
-                   "bounces": workload.config.rt_num_bounces, "channels_per_step": 1,
-                   "note": "the reference is Python/Numba; this arm times its float64 algorithm restated in C"},
-        "ray_bounces_per_s": ref["ray_bounces_per_s"],
-        "cpu_baseline": {"value": ref["value"], "unit": "RIRs/s", "cores": ref["cores"], "kind": "port",
+                   "bounces": workload.config.rt_num_bounces, "channels_per_step": 1, "note": note},
+        "cpu_baseline": {"value": ref["value"], "unit": "RIRs/s", "cores": cores, "kind": kind,
                          "sample": ref["sample"]},
         "e2e": {"value": ref["value"], "unit": "RIRs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -291,9 +430,12 @@ def main() -> int:
     peaks = _peaks()
     result = None
     if rank == 0:
-        cpu = None
+        cpu = ref_cpu = ref_cuda = None
         if world == 1 and not args.no_cpu_baseline:
+            # traversal statistics of the reference algorithm (C restatement) give the algorithmic bytes
             cpu = cpu_reference(workloads_[0], steps=1, warmup=0)
+            ref_cpu = reference_rirs(workloads_[0], 1, 1, accelerator="numba", precision="float64")
+            ref_cuda = reference_rirs(workloads_[0], 3, 1, accelerator="cuda", precision="float32")
         bytes_per_rb = cpu["bytes_per_ray_bounce"] if cpu else None
         achieved = (bytes_per_rb * ray_bounces_per_step / (trace_launch_ms / 1000.0) / 1e9) if bytes_per_rb else None
         traffic = _profiled_traffic(args.workload)
@@ -318,8 +460,8 @@ def main() -> int:
                          "peak_source": peaks["source"],
                          "kernel": "trace_kernel (ac_trace_batch)",
                          "bytes_per_ray_bounce": bytes_per_rb},
-            "cpu_baseline": ({"value": cpu["value"], "unit": "RIRs/s", "cores": cpu["cores"], "kind": "port",
-                              "sample": cpu["sample"]} if cpu else None),
+            "cpu_baseline": _cpu_baseline(cpu, ref_cpu),
+            "reference_cuda": _reference_cuda_line(ref_cuda),
             "clocks": sampler.summary(),
         }
         print(json.dumps(result), flush=True)
@@ -327,6 +469,28 @@ def main() -> int:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
     return 0
+
+
+def _cpu_baseline(port, ref_cpu):
+    """The reference's float64 Numba path on the host cores; the C restatement when the package is absent."""
+    if ref_cpu and "unavailable" not in ref_cpu:
+        return {"value": ref_cpu["value"], "unit": "RIRs/s", "cores": ref_cpu["threads"], "kind": "reference",
+                "sample": ref_cpu["sample"],
+                "port": ({"value": port["value"], "cores": port["cores"], "sample": port["sample"]} if port else None)}
+    if port:
+        return {"value": port["value"], "unit": "RIRs/s", "cores": port["cores"], "kind": "port",
+                "sample": port["sample"]}
+    return None
+
+
+def _reference_cuda_line(ref_cuda):
+    """The reference's own Numba-CUDA float32 backend on this GPU (trace on the GPU, synthesis on the host)."""
+    if not ref_cuda:
+        return None
+    if "unavailable" in ref_cuda:
+        return {"unavailable": ref_cuda["unavailable"]}
+    return {"value": ref_cuda["value"], "unit": "RIRs/s", "seconds_per_rir": ref_cuda["seconds_per_rir"],
+            "trace_seconds_per_rir": ref_cuda["trace_seconds"], "sample": ref_cuda["sample"]}
 
 
 def _profiled_traffic(workload: str):
