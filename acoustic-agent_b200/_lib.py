@@ -109,6 +109,25 @@ class ACSynthParams(ctypes.Structure):
     ]
 
 
+AC_SYNTH_MAX_RATES = 4
+
+
+class ACSynthJob(ctypes.Structure):
+    _fields_ = [
+        ("echogram", ctypes.c_void_p), ("band_irs", ctypes.c_void_p), ("white", ctypes.c_void_p),
+        ("air", ctypes.c_void_p), ("seed", ctypes.c_uint64), ("direct_delay", ctypes.c_double),
+        ("speed_of_sound", ctypes.c_double), ("num_bins", ctypes.c_int32), ("samples_per_bin", ctypes.c_int32),
+        ("rate_index", ctypes.c_int32), ("rng_mode", ctypes.c_int32),
+    ]
+
+
+class ACSynthBatchConfig(ctypes.Structure):
+    _fields_ = [
+        ("num_rates", ctypes.c_int32), ("sample_rates", ctypes.c_int32 * AC_SYNTH_MAX_RATES),
+        ("crossover", (ctypes.c_double * 100) * AC_SYNTH_MAX_RATES), ("air_coefficients", ctypes.c_double * 6),
+    ]
+
+
 # Every symbol include/acoustic_rt.h declares, with (restype, argtypes).
 SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_last_error": (ctypes.c_char_p, []),
@@ -129,6 +148,12 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_synth_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACSynthParams), ctypes.POINTER(ctypes.c_size_t)]),
     "ac_synthesize": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),
+    "ac_synth_batch_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
+                                                     ctypes.POINTER(ACSynthBatchConfig),
+                                                     ctypes.POINTER(ctypes.c_size_t)]),
+    "ac_synthesize_batch": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
+                                           ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
     "ac_synthesize_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
                                             ctypes.c_void_p]),
     "ac_philox_workspace": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,

@@ -7,7 +7,8 @@ simulate_batch), which run one full trace per job, by:
 1. one persistent tracer launch over every job (``ac_trace_batch``): lanes
    pull (job, ray) work items from a shared counter, so jobs of any size
    share the GPU without per-job launch or tail costs;
-2. one synthesis launch per (bins, samples-per-bin) group (``ac_synthesize``);
+2. one ragged synthesis over every job (``ac_synthesize_batch``: three
+   launches whatever the mix of lengths and sample rates);
 3. optionally, both captured once as a CUDA graph and replayed.
 
 Per-job results are identical to running each job alone (integer echogram
@@ -47,13 +48,13 @@ class Plan:
     jobs: list[Job]
     scenes: list[runtime.DeviceScene]
     buffers: list[runtime.TraceBuffers]
-    echograms: dict[tuple[int, int, int], torch.Tensor]   # (bins, spb, fs) -> [J_g, 6, bins] view order
-    group_members: dict[tuple[int, int, int], list[int]]
-    band_irs: dict[tuple[int, int, int], torch.Tensor]
-    synth: dict[tuple[int, int, int], Any]
-    delays: dict[tuple[int, int, int], torch.Tensor]
+    echo_store: torch.Tensor            # every job's float32 [6, bins] echogram, back to back
+    ir_store: torch.Tensor              # every job's float32 [6, N] band IRs, back to back
+    irs: list[torch.Tensor]             # per job: its [6, N] view of ir_store
+    synth_jobs: Any                     # ac_synth_job array over all jobs
+    synth_config: Any                   # ac_synth_batch_config (sample rates + crossover tables)
     workspace: runtime.BatchWorkspace
-    synth_workspaces: dict[tuple[int, int, int], runtime.SynthWorkspace]
+    synth_workspace: runtime.SynthBatchWorkspace
     graph: torch.cuda.CUDAGraph | None = None
     keepalive: list[Any] = field(default_factory=list)
 
@@ -95,42 +96,41 @@ def workload_jobs(workloads: Sequence[Workload], *, precision: str = "float32", 
 class RIRRenderer:
     """Batched tracer + synthesis on one GPU."""
 
-    def __init__(self, device: int = 0, *, block_size: int = 0, grid_blocks: int = 0) -> None:
+    def __init__(self, device: int = 0, *, block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0) -> None:
         self.device = runtime.require_cuda(device)
         self.block_size = block_size
         self.grid_blocks = grid_blocks
+        self.chunk_rays = chunk_rays
+        # eager plans share one pair of staged workspaces; a captured plan gets its own
+        self._trace_ws = runtime.BatchWorkspace(self.device)
+        self._synth_ws = runtime.SynthBatchWorkspace(self.device)
 
-    def plan(self, scenes: Sequence[SceneArrays | dict[str, Any]], jobs: Sequence[Job]) -> Plan:
+    def plan(self, scenes: Sequence[SceneArrays | dict[str, Any] | runtime.DeviceScene], jobs: Sequence[Job]) -> Plan:
         device_scenes = [s if isinstance(s, runtime.DeviceScene) else
                          runtime.DeviceScene(s if isinstance(s, SceneArrays) else compile_scene(s),
                                              device=self.device.index)
                          for s in scenes]
         buffers = [runtime.TraceBuffers.allocate(device_scenes[j.scene_index].num_surfaces, j.spec.num_bins,
-                                                 self.device) for j in jobs]
-        groups: dict[tuple[int, int, int], list[int]] = {}
+                                                 self.device, echogram=False) for j in jobs]
+        bins = [int(j.spec.num_bins) for j in jobs]
+        lengths = [b * bands.samples_per_bin(j.spec.bin_duration, j.fs) for b, j in zip(bins, jobs)]
+        echo_store = torch.zeros(NUM_BANDS * sum(bins), dtype=torch.float32, device=self.device)
+        ir_store = torch.empty(NUM_BANDS * sum(lengths), dtype=torch.float32, device=self.device)
+        irs, synth = [], []
+        e_off = i_off = 0
         for k, j in enumerate(jobs):
-            key = (int(j.spec.num_bins), bands.samples_per_bin(j.spec.bin_duration, j.fs), int(j.fs))
-            groups.setdefault(key, []).append(k)
-        echograms, band_irs, synth, delays, sws = {}, {}, {}, {}, {}
-        for key, members in groups.items():
-            bins, spb, fs = key
-            # Each job's float32 echogram is written straight into its group's stacked tensor.
-            stacked = torch.zeros(len(members), NUM_BANDS, bins, dtype=torch.float32, device=self.device)
-            for row, k in enumerate(members):
-                buffers[k].echogram = stacked[row]
-            echograms[key] = stacked
-            band_irs[key] = torch.empty(len(members), NUM_BANDS, bins * spb, dtype=torch.float32, device=self.device)
-            delays[key] = torch.as_tensor([max(0.0, float(jobs[k].spec.direct_delay)) for k in members],
-                                          dtype=torch.float64, device=self.device)
-            first = jobs[members[0]]
-            seeds = {int(jobs[k].spec.seed) for k in members}
-            synth[key] = runtime.synth_params(len(members), bins, first.spec.bin_duration, fs,
-                                              first.spec.speed_of_sound, rng_mode="philox",
-                                              seed=(min(seeds) + 7), direct_delays=delays[key])
-            sws[key] = runtime.SynthWorkspace(self.device)
-        plan = Plan(list(jobs), device_scenes, buffers, echograms, groups, band_irs, synth, delays,
-                    runtime.BatchWorkspace(self.device), sws)
-        return plan
+            # each job's float32 echogram is written by the tracer straight into the synthesis input
+            buffers[k].echogram = echo_store[e_off:e_off + NUM_BANDS * bins[k]].view(NUM_BANDS, bins[k])
+            irs.append(ir_store[i_off:i_off + NUM_BANDS * lengths[k]].view(NUM_BANDS, lengths[k]))
+            e_off += NUM_BANDS * bins[k]
+            i_off += NUM_BANDS * lengths[k]
+            synth.append(runtime.SynthJob(buffers[k].echogram, irs[k], j.fs, j.spec.bin_duration,
+                                          seed=int(j.spec.seed) + 7, direct_delay=max(0.0, float(j.spec.direct_delay)),
+                                          speed_of_sound=j.spec.speed_of_sound))
+        config = runtime.synth_batch_config([j.fs for j in jobs] or [16000])
+        synth_jobs = runtime.synth_job_array(synth, config)
+        return Plan(list(jobs), device_scenes, buffers, echo_store, ir_store, irs, synth_jobs, config,
+                    self._trace_ws, self._synth_ws)
 
     def launch(self, plan: Plan, stream: torch.cuda.Stream | None = None) -> None:
         """Enqueue trace + synthesis of every job (asynchronous)."""
@@ -141,13 +141,15 @@ class RIRRenderer:
 
     def _enqueue(self, plan: Plan, stream: torch.cuda.Stream | None) -> None:
         runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
-                            plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks, stream=stream)
-        for key, params in plan.synth.items():
-            runtime.synthesize(plan.echograms[key], params, plan.synth_workspaces[key], plan.band_irs[key],
-                               stream=stream)
+                            plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
+                            chunk_rays=self.chunk_rays, stream=stream)
+        runtime.synthesize_batch((plan.synth_jobs, len(plan.jobs), plan.synth_config), plan.synth_workspace,
+                                 stream=stream)
 
     def capture(self, plan: Plan) -> None:
         """Record the launch sequence once as a CUDA graph (the job table is staged in pinned memory)."""
+        plan.workspace = runtime.BatchWorkspace(self.device)
+        plan.synth_workspace = runtime.SynthBatchWorkspace(self.device)
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
@@ -163,13 +165,13 @@ class RIRRenderer:
         return int(sum(int(b.counters[2].item()) for b in plan.buffers))
 
     def results(self, plan: Plan) -> list[np.ndarray]:
-        """Band IRs per job, [6, N] float32 host arrays, in job order."""
-        out: list[np.ndarray | None] = [None] * len(plan.jobs)
-        for key, members in plan.group_members.items():
-            host = plan.band_irs[key].cpu().numpy()
-            for row, k in enumerate(members):
-                out[k] = host[row]
-        return out  # type: ignore[return-value]
+        """Band IRs per job, [6, N] float32 host arrays, in job order (one device-to-host copy)."""
+        host = plan.ir_store.cpu().numpy()
+        out, off = [], 0
+        for t in plan.irs:
+            out.append(host[off:off + t.numel()].reshape(t.shape))
+            off += t.numel()
+        return out
 
 
 def render(workloads: Sequence[Workload], *, device: int = 0, precision: str = "float32",

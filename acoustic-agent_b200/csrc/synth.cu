@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -154,49 +155,44 @@ constexpr int kLag = kSkew * 3;  // section 3 runs kLag samples behind section 0
 // +0.0, and a section whose inputs and state are all +0.0 produces exactly +0.0
 // and keeps its state at +0.0 (every product is +0.0 or -0.0 and the sums come
 // out +0.0), so the steps while the pipeline fills change nothing.
-__global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, const __grid_constant__ SynthArgs a,
-                                                           float *out) {
+// The per-lane recursion of one warp.  `x` / `out_row` / `n_len` belong to the
+// lane's unit (band of one RIR); `co` points at the lane's section
+// coefficients.  `iterations` (the longest unit of the warp + kLag) is
+// warp-uniform: every lane runs every iteration, so the shuffles stay full-warp.
+__device__ __forceinline__ void filter_units(const double *x, float *out_row, int n_len, bool valid_unit, int band,
+                                             const double *co, int iterations) {
     const unsigned full = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
-    const int warp = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
     const int stage = lane & 3;
     const int chain = (lane >> 2) & 1;
-    const int unit = warp * 4 + (lane >> 3);
-    const int units = a.num_rirs * kSynthBands;
-    const bool valid_unit = unit < units;
-    const int band = valid_unit ? unit % kSynthBands : 0;
     int cutoff;
     bool active;
     if (band == 0) { cutoff = 0; active = chain == 0; }
     else if (band == kSynthBands - 1) { cutoff = 4; active = chain == 0; }
     else { cutoff = chain == 0 ? band : band - 1; active = true; }
     active = active && valid_unit;
-    const double *co = a.crossover + cutoff * 20 + stage * 5;
+    co += cutoff * 20 + stage * 5;
     Section sec{co[0], co[1], co[2], co[3], co[4], 0.0, 0.0, 0.0, 0.0};
     const bool emits = stage == 3 && chain == 0 && active;
     const bool is_first = stage == 0;
     const int mode = band == 0 ? 0 : (band == kSynthBands - 1 ? 2 : 1);
 
-    const int N = a.num_bins * a.spb;
-    const double *x = raw + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
-    float *out_row = out + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
-
     double ahead[kPrefetch], prev[kPrefetch];
 #pragma unroll
     for (int u = 0; u < kPrefetch; ++u) {
-        ahead[u] = (valid_unit && u < N) ? __ldg(x + u) : 0.0;
+        ahead[u] = (valid_unit && u < n_len) ? __ldg(x + u) : 0.0;
         prev[u] = 0.0;
     }
     float q1 = 0.0f;  // value the previous section sent last iteration (this section's input next iteration)
     // input part of the first sample (its input is ahead[0] for section 0 and +0.0 otherwise)
     double v = sec.feed(is_first ? ahead[0] : 0.0);
-    const int iterations = N + kLag;
+    const int last = n_len + kLag;  // this lane's own end
     for (int base = 0; base < iterations; base += kPrefetch) {
         double next[kPrefetch];
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
             const int m = base + kPrefetch + u;
-            next[u] = (valid_unit && m < N) ? __ldg(x + m) : 0.0;
+            next[u] = (valid_unit && m < n_len) ? __ldg(x + m) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
@@ -213,7 +209,7 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
             const double x_n = (u >= kLag) ? ahead[u - kLag] : prev[u + kPrefetch - kLag];
             const float band5 = static_cast<float>(x_n - static_cast<double>(y));
             const float o = mode == 0 ? y : (mode == 2 ? band5 : y - lower);
-            if (emits && it >= kLag && it < iterations) out_row[it - kLag] = o;
+            if (emits && it >= kLag && it < last) out_row[it - kLag] = o;
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
@@ -221,6 +217,135 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
             ahead[u] = next[u];
         }
     }
+}
+
+__global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, const __grid_constant__ SynthArgs a,
+                                                           float *out) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
+    const int unit = warp * 4 + (lane >> 3);
+    const int units = a.num_rirs * kSynthBands;
+    const bool valid_unit = unit < units;
+    const int band = valid_unit ? unit % kSynthBands : 0;
+    const int N = a.num_bins * a.spb;
+    const double *x = raw + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
+    float *out_row = out + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
+    filter_units(x, out_row, N, valid_unit, band, a.crossover, N + kLag);
+}
+
+// ---- ragged batches (ac_synthesize_batch) ----------------------------------
+
+// Device copy of one batch job plus its offsets into the shared arrays.
+struct SynthJobDev {
+    const float *echogram;
+    float *band_irs;
+    const double *white;
+    const double *air;
+    uint64_t seed;
+    double direct_delay;
+    double speed_of_sound;
+    int32_t num_bins;
+    int32_t spb;
+    int32_t rate_index;
+    int32_t rng_mode;
+    int64_t cells;    // offset of this job's [6, bins] rows in the amps / air arrays
+    int64_t samples;  // offset of this job's [6, N] raw rows, in units of 6 samples
+};
+
+// Largest j with prefix[j] <= i (prefix[0] = 0, strictly increasing).
+__device__ __forceinline__ int owner(const int64_t *prefix, int num_jobs, int64_t i) {
+    int lo = 0, hi = num_jobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= i) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void synth_batch_prepare_kernel(const SynthJobDev *jobs, const int64_t *cell_prefix, int num_jobs,
+                                           const __grid_constant__ ac_synth_batch_config cfg, double *amps,
+                                           double *air) {
+    const int64_t cells = cell_prefix[num_jobs];
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < cells; i += stride) {
+        const int j = owner(cell_prefix, num_jobs, i);
+        const SynthJobDev &job = jobs[j];
+        const int64_t local = i - job.cells;
+        const int band = static_cast<int>(local / job.num_bins);
+        const int bin = static_cast<int>(local - static_cast<int64_t>(band) * job.num_bins);
+        // numpy keeps a float32 echogram in float32: clip, divide by float32(4pi), sqrt.
+        const float e = job.echogram[local];
+        const float cl = e > 0.0f ? e : 0.0f;
+        const float amp = sqrtf(cl / static_cast<float>(4.0 * kSynthPi));
+        amps[i] = e < static_cast<float>(1e-9) ? 0.0 : static_cast<double>(amp);
+        if (job.air) {
+            air[i] = job.air[local];
+        } else {
+            // steam_rt.py:2196-2198 and :2214-2227: clamped direct delay, path time at the bin centre
+            const double delay = job.direct_delay > 0.0 ? job.direct_delay : 0.0;
+            const int rate = cfg.sample_rates[job.rate_index];
+            const double t = delay + ((static_cast<double>(bin) + 0.5) * job.spb) / rate;
+            const double dist = (t > 0.0 ? t : 0.0) * (job.speed_of_sound > 0.0 ? job.speed_of_sound : 0.0);
+            const double coeff = cfg.air_coefficients[band] > 0.0 ? cfg.air_coefficients[band] : 0.0;
+            air[i] = exp(-coeff * dist);
+        }
+    }
+}
+
+// One thread per (job, sample): the noise value is drawn once and used by all six bands.
+__global__ void synth_batch_raw_kernel(const SynthJobDev *jobs, const int64_t *sample_prefix, int num_jobs,
+                                       const double *amps, const double *air, double *raw) {
+    const int64_t total = sample_prefix[num_jobs];
+    const int64_t stride = static_cast<int64_t>(gridDim.x) * blockDim.x;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total; i += stride) {
+        const int j = owner(sample_prefix, num_jobs, i);
+        const SynthJobDev &job = jobs[j];
+        const int64_t n = i - sample_prefix[j];
+        const int64_t N = static_cast<int64_t>(job.num_bins) * job.spb;
+        const int bin = static_cast<int>(n / job.spb);
+        const int k = static_cast<int>(n - static_cast<int64_t>(bin) * job.spb);
+        const double w = static_cast<double>(k) / static_cast<double>(job.spb);
+        double noise;
+        if (job.rng_mode == AC_RNG_PHILOX) {
+            const u32x4 r = noise_draw(job.seed, static_cast<uint32_t>(n >> 1));
+            const double u = (n & 1) ? u01_53(r.z, r.w) : u01_53(r.x, r.y);
+            noise = -1.0 + 2.0 * u;
+        } else {
+            noise = job.white[n];
+        }
+        double *row = raw + 6 * job.samples + n;
+#pragma unroll
+        for (int band = 0; band < kSynthBands; ++band) {
+            const int64_t c = job.cells + static_cast<int64_t>(band) * job.num_bins + bin;
+            const double cur = amps[c];
+            const double prev = bin == 0 ? cur : amps[c - 1];
+            double seg = (1.0 - w) * prev + w * cur;
+            seg = seg * air[c];
+            row[band * N] = seg * noise;
+        }
+    }
+}
+
+// Warp w runs units[4w .. 4w+3] (job << 3 | band, or -1); units are ordered
+// longest job first, so the four units of a warp have similar lengths.
+__global__ void __launch_bounds__(32) synth_batch_filter_kernel(const SynthJobDev *jobs, const int32_t *units,
+                                                                int num_units,
+                                                                const __grid_constant__ ac_synth_batch_config cfg,
+                                                                const double *raw) {
+    const int lane = threadIdx.x & 31;
+    const int warp = static_cast<int>((blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x) >> 5);
+    const int slot = warp * 4 + (lane >> 3);
+    const int code = slot < num_units ? __ldg(units + slot) : -1;
+    const bool valid_unit = code >= 0;
+    const int j = valid_unit ? code >> 3 : 0;
+    const int band = valid_unit ? code & 7 : 0;
+    const SynthJobDev &job = jobs[j];
+    const int n_len = valid_unit ? job.num_bins * job.spb : 0;
+    const int longest = __reduce_max_sync(0xFFFFFFFFu, static_cast<unsigned>(n_len));
+    const double *x = raw + 6 * job.samples + static_cast<int64_t>(band) * n_len;
+    float *out_row = job.band_irs + static_cast<int64_t>(band) * n_len;
+    filter_units(x, out_row, n_len, valid_unit, band, cfg.crossover[valid_unit ? job.rate_index : 0],
+                 longest + kLag);
 }
 
 }  // namespace
@@ -278,6 +403,153 @@ extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, f
     const int warps = (units + 3) / 4;
     const int threads = 32;  // one warp per block: spread the sequential chains over all SMs
     ac::synth_filter_kernel<<<warps, threads, 0, stream>>>(raw, a, band_irs);
+    AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Ragged batches: any mix of lengths and sample rates in three launches.
+
+namespace ac {
+namespace {
+
+struct SynthBatchLayout {
+    size_t jobs, cell_prefix, sample_prefix, units, table_end, amps, air, raw, total;
+    int64_t cells, samples;
+    int32_t num_units;
+};
+
+int check_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *cfg, bool need_buffers,
+                SynthBatchLayout *out) {
+    if (num_jobs < 0 || (num_jobs > 0 && !jobs) || !cfg)
+        return ac::fail(AC_ERR_INVALID, "synthesis batch: null argument");
+    if (cfg->num_rates < 1 || cfg->num_rates > AC_SYNTH_MAX_RATES)
+        return ac::fail(AC_ERR_INVALID, "synthesis batch: num_rates must be 1..%d", AC_SYNTH_MAX_RATES);
+    for (int r = 0; r < cfg->num_rates; ++r)
+        if (cfg->sample_rates[r] < 1) return ac::fail(AC_ERR_INVALID, "synthesis batch: sample rate %d < 1", r);
+    if (static_cast<int64_t>(num_jobs) > (int64_t{1} << 28))
+        return ac::fail(AC_ERR_CAPACITY, "synthesis batch of %d jobs is too large", num_jobs);
+    SynthBatchLayout l{};
+    for (int32_t j = 0; j < num_jobs; ++j) {
+        const ac_synth_job &job = jobs[j];
+        if (job.num_bins < 1 || job.samples_per_bin < 1)
+            return ac::fail(AC_ERR_INVALID, "synthesis job %d: sizes must be positive", j);
+        const int64_t N = static_cast<int64_t>(job.num_bins) * job.samples_per_bin;
+        if (N + 3 > 0x7FFFFFFF) return ac::fail(AC_ERR_CAPACITY, "synthesis job %d: %lld samples is too long", j,
+                                                (long long)N);
+        if (job.rate_index < 0 || job.rate_index >= cfg->num_rates)
+            return ac::fail(AC_ERR_INVALID, "synthesis job %d: rate_index %d out of range", j, job.rate_index);
+        if (job.rng_mode != AC_RNG_REFERENCE && job.rng_mode != AC_RNG_PHILOX)
+            return ac::fail(AC_ERR_INVALID, "synthesis job %d: unknown rng_mode %d", j, job.rng_mode);
+        if (need_buffers) {
+            if (!job.echogram || !job.band_irs) return ac::fail(AC_ERR_INVALID, "synthesis job %d: null buffer", j);
+            if (job.rng_mode == AC_RNG_REFERENCE && !job.white)
+                return ac::fail(AC_ERR_INVALID, "synthesis job %d: reference mode needs white noise", j);
+        }
+        l.cells += 6 * static_cast<int64_t>(job.num_bins);
+        l.samples += N;
+    }
+    l.num_units = static_cast<int32_t>((6 * static_cast<int64_t>(num_jobs) + 3) / 4 * 4);
+    size_t off = 0;
+    l.jobs = off;          off = align256(off + static_cast<size_t>(num_jobs) * sizeof(SynthJobDev));
+    l.cell_prefix = off;   off = align256(off + (static_cast<size_t>(num_jobs) + 1) * sizeof(int64_t));
+    l.sample_prefix = off; off = align256(off + (static_cast<size_t>(num_jobs) + 1) * sizeof(int64_t));
+    l.units = off;         off = align256(off + static_cast<size_t>(l.num_units) * sizeof(int32_t));
+    l.table_end = off;
+    l.amps = off;          off = align256(off + static_cast<size_t>(l.cells) * sizeof(double));
+    l.air = off;           off = align256(off + static_cast<size_t>(l.cells) * sizeof(double));
+    l.raw = off;           off = align256(off + 6 * static_cast<size_t>(l.samples) * sizeof(double));
+    l.total = off;
+    *out = l;
+    return AC_OK;
+}
+
+}  // namespace
+}  // namespace ac
+
+extern "C" int ac_synth_batch_workspace_size(const ac_synth_job *jobs, int32_t num_jobs,
+                                             const ac_synth_batch_config *config, size_t *bytes) {
+    if (!bytes) return ac::fail(AC_ERR_INVALID, "ac_synth_batch_workspace_size: null argument");
+    ac::SynthBatchLayout l;
+    const int rc = ac::check_batch(jobs, num_jobs, config, false, &l);
+    if (rc != AC_OK) return rc;
+    *bytes = l.total;
+    return AC_OK;
+}
+
+extern "C" int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                                   void *workspace, size_t workspace_bytes, void *host_staging, void *stream_ptr) {
+    ac::SynthBatchLayout l;
+    const int rc = ac::check_batch(jobs, num_jobs, config, true, &l);
+    if (rc != AC_OK) return rc;
+    if (num_jobs == 0) return AC_OK;
+    if (!workspace || workspace_bytes < l.total)
+        return ac::fail(AC_ERR_CAPACITY, "synthesis batch workspace too small: %zu < %zu", workspace_bytes, l.total);
+    std::vector<unsigned char> local;
+    unsigned char *host = static_cast<unsigned char *>(host_staging);
+    if (!host) {
+        local.assign(l.table_end, 0);
+        host = local.data();
+    }
+    ac::SynthJobDev *dev_jobs = reinterpret_cast<ac::SynthJobDev *>(host + l.jobs);
+    int64_t *cell_prefix = reinterpret_cast<int64_t *>(host + l.cell_prefix);
+    int64_t *sample_prefix = reinterpret_cast<int64_t *>(host + l.sample_prefix);
+    int32_t *units = reinterpret_cast<int32_t *>(host + l.units);
+    int64_t cells = 0, samples = 0;
+    for (int32_t j = 0; j < num_jobs; ++j) {
+        const ac_synth_job &in = jobs[j];
+        ac::SynthJobDev d{};
+        d.echogram = in.echogram;
+        d.band_irs = in.band_irs;
+        d.white = in.white;
+        d.air = in.air;
+        d.seed = in.seed;
+        d.direct_delay = in.direct_delay;
+        d.speed_of_sound = in.speed_of_sound;
+        d.num_bins = in.num_bins;
+        d.spb = in.samples_per_bin;
+        d.rate_index = in.rate_index;
+        d.rng_mode = in.rng_mode;
+        d.cells = cells;
+        d.samples = samples;
+        std::memcpy(dev_jobs + j, &d, sizeof(d));
+        cell_prefix[j] = cells;
+        sample_prefix[j] = samples;
+        cells += 6 * static_cast<int64_t>(in.num_bins);
+        samples += static_cast<int64_t>(in.num_bins) * in.samples_per_bin;
+    }
+    cell_prefix[num_jobs] = cells;
+    sample_prefix[num_jobs] = samples;
+    // Filter units, longest job first (stable), six per job, padded to whole warps.
+    std::vector<int32_t> order(static_cast<size_t>(num_jobs));
+    for (int32_t j = 0; j < num_jobs; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return static_cast<int64_t>(jobs[a].num_bins) * jobs[a].samples_per_bin >
+               static_cast<int64_t>(jobs[b].num_bins) * jobs[b].samples_per_bin;
+    });
+    int32_t u = 0;
+    for (const int32_t j : order)
+        for (int band = 0; band < 6; ++band) units[u++] = (j << 3) | band;
+    for (; u < l.num_units; ++u) units[u] = -1;
+
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    AC_CUDA_TRY(cudaMemcpyAsync(ws, host, l.table_end, cudaMemcpyHostToDevice, stream));
+    if (!host_staging) AC_CUDA_TRY(cudaStreamSynchronize(stream));  // pageable source must stay alive
+    const ac::SynthJobDev *d_jobs = reinterpret_cast<const ac::SynthJobDev *>(ws + l.jobs);
+    const int64_t *d_cells = reinterpret_cast<const int64_t *>(ws + l.cell_prefix);
+    const int64_t *d_samples = reinterpret_cast<const int64_t *>(ws + l.sample_prefix);
+    const int32_t *d_units = reinterpret_cast<const int32_t *>(ws + l.units);
+    double *amps = reinterpret_cast<double *>(ws + l.amps);
+    double *air = reinterpret_cast<double *>(ws + l.air);
+    double *raw = reinterpret_cast<double *>(ws + l.raw);
+    const int prep_grid = static_cast<int>(std::min<int64_t>((cells + 255) / 256, 8192));
+    ac::synth_batch_prepare_kernel<<<prep_grid, 256, 0, stream>>>(d_jobs, d_cells, num_jobs, *config, amps, air);
+    AC_CUDA_TRY(cudaGetLastError());
+    const int raw_grid = static_cast<int>(std::min<int64_t>((samples + 255) / 256, 65536));
+    ac::synth_batch_raw_kernel<<<raw_grid, 256, 0, stream>>>(d_jobs, d_samples, num_jobs, amps, air, raw);
+    AC_CUDA_TRY(cudaGetLastError());
+    ac::synth_batch_filter_kernel<<<l.num_units / 4, 32, 0, stream>>>(d_jobs, d_units, l.num_units, *config, raw);
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
 }

@@ -221,12 +221,14 @@ class TraceBuffers:
 
     @classmethod
     def allocate(cls, num_surfaces: int, num_bins: int, device: torch.device, *, ambisonics: bool = False,
-                 record_rays: tuple[int, int] | None = None) -> "TraceBuffers":
+                 record_rays: tuple[int, int] | None = None, echogram: bool = True) -> "TraceBuffers":
+        """Zeroed device outputs; echogram=False leaves `echogram` for the caller to point at its own storage."""
         z64 = lambda *shape: torch.zeros(*shape, dtype=torch.int64, device=device)
         return cls(
             echogram_fx=z64(NUM_BANDS, num_bins, 2), hit_counts=z64(num_surfaces), contrib_counts=z64(num_surfaces),
             surface_energy_fx=z64(num_surfaces, 2), counters=z64(8),
-            echogram=torch.zeros(NUM_BANDS, num_bins, dtype=torch.float32, device=device),
+            echogram=(torch.zeros(NUM_BANDS, num_bins, dtype=torch.float32, device=device) if echogram
+                      else torch.empty(0, dtype=torch.float32, device=device)),
             surface_energy=torch.zeros(num_surfaces, dtype=torch.float32, device=device),
             ambisonic_fx=z64(NUM_BANDS, 4, num_bins, 2) if ambisonics else None,
             ambisonic=torch.zeros(NUM_BANDS, 4, num_bins, dtype=torch.float32, device=device) if ambisonics else None,
@@ -314,26 +316,51 @@ def trace(scene: DeviceScene, spec: TraceSpec, buffers: TraceBuffers | None = No
     return buffers
 
 
-class BatchWorkspace:
-    """Reusable device workspace + pinned staging for ac_trace_batch."""
+class _StagedWorkspace:
+    """Device workspace + pinned staging of a batched entry point.
+
+    The entry point writes its job table into the pinned staging on the host
+    and copies it to the device asynchronously, so the staging may be
+    rewritten only after that copy has run: `ensure` waits for the event
+    recorded after the previous launch.  (Inside a stream capture no event is
+    needed: the graph owns the staging until it is released.)
+    """
+
+    SIZE_FN = ""
 
     def __init__(self, device: torch.device) -> None:
         self.device = device
-        self.capacity_jobs = 0
         self.device_buffer: torch.Tensor | None = None
         self.host_buffer: torch.Tensor | None = None
+        self._copied: torch.cuda.Event | None = None
 
     def ensure(self, jobs, num_jobs: int, cfg) -> tuple[int, int, int]:
         size = ctypes.c_size_t()
-        _lib.check(_lib.load().ac_batch_workspace_size(jobs, num_jobs, ctypes.byref(cfg), ctypes.byref(size)),
-                   "ac_batch_workspace_size")
-        need = int(size.value)
+        _lib.check(getattr(_lib.load(), self.SIZE_FN)(jobs, num_jobs, ctypes.byref(cfg), ctypes.byref(size)),
+                   self.SIZE_FN)
+        need = max(int(size.value), 256)
+        if self._copied is not None and not torch.cuda.is_current_stream_capturing():
+            self._copied.synchronize()   # host waits are not allowed inside a capture (nor needed there)
+            self._copied = None
         if self.device_buffer is None or self.device_buffer.numel() < need:
             cap = max(need, 2 * (self.device_buffer.numel() if self.device_buffer is not None else 0), 1 << 16)
             self.device_buffer = torch.empty(cap, dtype=torch.uint8, device=self.device)
             self.host_buffer = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
         assert self.device_buffer is not None and self.host_buffer is not None
         return self.device_buffer.data_ptr(), self.device_buffer.numel(), self.host_buffer.data_ptr()
+
+    def launched(self, stream: torch.cuda.Stream | None) -> None:
+        if torch.cuda.is_current_stream_capturing():
+            return
+        ev = torch.cuda.Event()
+        ev.record(stream if stream is not None else torch.cuda.current_stream(self.device))
+        self._copied = ev
+
+
+class BatchWorkspace(_StagedWorkspace):
+    """Reusable device workspace + pinned staging for ac_trace_batch."""
+
+    SIZE_FN = "ac_batch_workspace_size"
 
 
 def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
@@ -353,6 +380,7 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
     ws, ws_bytes, host = workspace.ensure(arr, len(jobs), cfg)
     _lib.check(_lib.load().ac_trace_batch(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
                                           ctypes.c_void_p(host), _stream_ptr(stream)), "ac_trace_batch")
+    workspace.launched(stream)
     workspace._keepalive = keep  # type: ignore[attr-defined]
 
 
@@ -445,6 +473,86 @@ def synthesize(echograms: torch.Tensor, params: _lib.ACSynthParams, workspace: S
                                          ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(ws.data_ptr()),
                                          ws.numel(), _stream_ptr(stream)), "ac_synthesize")
     return out
+
+
+@dataclass
+class SynthJob:
+    """One RIR of a ragged synthesis batch (the fields of ac_synth_job)."""
+
+    echogram: torch.Tensor            # [6, bins] float32 CUDA
+    out: torch.Tensor                 # [6, bins * spb] float32 CUDA
+    fs: int
+    bin_duration: float
+    seed: int                         # Philox noise key (reconstruct_band_irs draws with config.seed + 7)
+    direct_delay: float
+    speed_of_sound: float = 343.0
+    rng: str = "philox"
+    white: torch.Tensor | None = None  # reference mode: [bins * spb] float64 CUDA noise
+    air: torch.Tensor | None = None    # optional [6, bins] float64 CUDA air gains
+
+
+def synth_batch_config(rates: Sequence[int]) -> _lib.ACSynthBatchConfig:
+    rates = list(dict.fromkeys(int(r) for r in rates))
+    if not 1 <= len(rates) <= _lib.AC_SYNTH_MAX_RATES:
+        raise ValueError(f"a synthesis batch takes 1..{_lib.AC_SYNTH_MAX_RATES} sample rates, got {len(rates)}")
+    cfg = _lib.ACSynthBatchConfig()
+    cfg.num_rates = len(rates)
+    for k, fs in enumerate(rates):
+        cfg.sample_rates[k] = fs
+        cfg.crossover[k][:] = [float(v) for v in bands.crossover_table(fs).reshape(-1)]
+    cfg.air_coefficients[:] = list(bands.AIR_ABSORPTION_NP_PER_M)
+    return cfg
+
+
+def synth_job_array(jobs: Sequence[SynthJob], config: _lib.ACSynthBatchConfig) -> ctypes.Array:
+    rate_index = {int(config.sample_rates[k]): k for k in range(config.num_rates)}
+    arr = (_lib.ACSynthJob * max(1, len(jobs)))()
+    for k, j in enumerate(jobs):
+        spb = bands.samples_per_bin(j.bin_duration, j.fs)
+        bins = int(j.echogram.shape[-1])
+        if j.echogram.dtype != torch.float32 or not j.echogram.is_contiguous() or tuple(j.echogram.shape) != (NUM_BANDS, bins):
+            raise ValueError("echogram must be a contiguous [6, bins] float32 tensor")
+        if j.out.dtype != torch.float32 or not j.out.is_contiguous() or tuple(j.out.shape) != (NUM_BANDS, bins * spb):
+            raise ValueError(f"band IR output must be a contiguous [6, {bins * spb}] float32 tensor")
+        if j.rng not in ("philox", "reference"):
+            raise ValueError("rng must be 'reference' or 'philox'")
+        a = arr[k]
+        a.echogram = j.echogram.data_ptr()
+        a.band_irs = j.out.data_ptr()
+        a.white = j.white.data_ptr() if j.white is not None else None
+        a.air = j.air.data_ptr() if j.air is not None else None
+        a.seed = int(j.seed) & 0xFFFFFFFFFFFFFFFF
+        a.direct_delay = float(j.direct_delay)
+        a.speed_of_sound = float(j.speed_of_sound)
+        a.num_bins = bins
+        a.samples_per_bin = spb
+        a.rate_index = rate_index[int(j.fs)]
+        a.rng_mode = _lib.AC_RNG_PHILOX if j.rng == "philox" else _lib.AC_RNG_REFERENCE
+    return arr
+
+
+class SynthBatchWorkspace(_StagedWorkspace):
+    """Reusable device workspace + pinned staging for ac_synthesize_batch."""
+
+    SIZE_FN = "ac_synth_batch_workspace_size"
+
+
+def synthesize_batch(jobs: Sequence[SynthJob] | tuple[ctypes.Array, int, _lib.ACSynthBatchConfig],
+                     workspace: SynthBatchWorkspace, *, stream: torch.cuda.Stream | None = None) -> None:
+    """Band IRs of every job in three launches (ac_synthesize_batch); outputs land in each job's `out`."""
+    if isinstance(jobs, tuple):
+        arr, n, cfg = jobs
+    else:
+        if not jobs:
+            return
+        cfg = synth_batch_config([j.fs for j in jobs])
+        arr, n = synth_job_array(jobs, cfg), len(jobs)
+    if n == 0:
+        return
+    ws, ws_bytes, host = workspace.ensure(arr, n, cfg)
+    _lib.check(_lib.load().ac_synthesize_batch(arr, n, ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
+                                               ctypes.c_void_p(host), _stream_ptr(stream)), "ac_synthesize_batch")
+    workspace.launched(stream)
 
 
 def device_info(device: int = 0) -> dict[str, Any]:

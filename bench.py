@@ -409,20 +409,19 @@ def main() -> int:
     # End to end through the public API: host scene arrays in, host band IRs out, every step.
     e2e_times = []
     h2d = d2h = 0
-    pinned_out = {key: torch.empty(t.shape, dtype=t.dtype, pin_memory=True) for key, t in plan.band_irs.items()}
+    pinned_out = torch.empty(plan.ir_store.shape, dtype=plan.ir_store.dtype, pin_memory=True)
     for k in range(args.warmup + max(3, args.steps // 2)):
         torch.cuda.synchronize(device)
         t0 = time.perf_counter()
         scenes_k = [runtime.DeviceScene(a, device=local) for a in arrays]
         plan_k = renderer.plan(scenes_k, jobs)
         renderer.launch(plan_k)
-        for key, t in plan_k.band_irs.items():
-            pinned_out[key].copy_(t, non_blocking=True)
+        pinned_out.copy_(plan_k.ir_store, non_blocking=True)
         torch.cuda.synchronize(device)
         if k >= args.warmup:
             e2e_times.append(time.perf_counter() - t0)
         h2d = sum(s.device_bytes for s in scenes_k) + plan_k.workspace.device_buffer.numel()
-        d2h = sum(t.numel() * t.element_size() for t in plan_k.band_irs.values())
+        d2h = plan_k.ir_store.numel() * plan_k.ir_store.element_size()
         for s in scenes_k:
             s.close()
     e2e_value = world * rirs_per_step / float(np.mean(e2e_times))

@@ -23,6 +23,8 @@
  *                       (the per-job loops, run as one persistent launch)
  *   ac_synthesize       acoustic_agent/steam_rt.py:2205-2232         reconstruct_band_irs
  *                       + steam_rt.py:3070-3083                      bandlimit_band_signals
+ *   ac_synthesize_batch the same per RIR, over the per-job loops of engine.py:64-73 and
+ *                       batch.py:139-185 (one ragged batch instead of one call per RIR)
  */
 #ifndef ACOUSTIC_RT_H
 #define ACOUSTIC_RT_H
@@ -34,7 +36,7 @@
 extern "C" {
 #endif
 
-#define AC_ABI_VERSION 1
+#define AC_ABI_VERSION 2
 
 #define AC_OK 0
 #define AC_ERR_INVALID (-1)     /* bad argument, shape or value (reference: ValueError) */
@@ -258,6 +260,46 @@ int ac_synthesize(const float *echograms, const ac_synth_params *params, float *
  * overlap on the GPU race and must be serialised by the caller. */
 #define AC_SYNTH_STATIC_BYTES (16u << 20)
 int ac_synthesize_static(const float *echograms, const ac_synth_params *params, float *band_irs, void *stream);
+
+/* One RIR of a ragged synthesis batch: reconstruct_band_irs
+ * (steam_rt.py:2205-2232) for one echogram, with its own length, sample rate
+ * and noise.  Every output sample equals what ac_synthesize gives for the
+ * same echogram alone (same noise, same air gains). */
+typedef struct ac_synth_job {
+    const float *echogram;       /* [6, num_bins] float32 device */
+    float *band_irs;             /* [6, num_bins * samples_per_bin] float32 device */
+    const double *white;         /* AC_RNG_REFERENCE: [num_bins * samples_per_bin] device uniform(-1, 1) noise */
+    const double *air;           /* optional [6, num_bins] device air gains; NULL: computed from direct_delay */
+    uint64_t seed;               /* AC_RNG_PHILOX: noise key, the same noise as ac_synthesize with this seed */
+    double direct_delay;         /* seconds (steam_rt.py:2214) */
+    double speed_of_sound;
+    int32_t num_bins;
+    int32_t samples_per_bin;     /* ceil(bin_duration * fs) */
+    int32_t rate_index;          /* which sample rate / crossover table of the batch config */
+    int32_t rng_mode;
+} ac_synth_job;
+
+#define AC_SYNTH_MAX_RATES 4
+typedef struct ac_synth_batch_config {
+    int32_t num_rates;                               /* 1 .. AC_SYNTH_MAX_RATES */
+    int32_t sample_rates[AC_SYNTH_MAX_RATES];
+    double crossover[AC_SYNTH_MAX_RATES][100];       /* per rate, as ac_synth_params.crossover */
+    double air_coefficients[6];                      /* Np/m per band (acoustics.py:12-22) */
+} ac_synth_batch_config;
+
+/* Device workspace and pinned staging bytes for ac_synthesize_batch. */
+int ac_synth_batch_workspace_size(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                                  size_t *bytes);
+
+/* Any mix of echogram lengths and sample rates in one set of launches (three
+ * kernels whatever the batch).  Replaces the per-RIR reconstruct_band_irs
+ * calls of engine.py:64-73 / batch.py:139-185.  The job table is written to
+ * `host_staging` (pinned, ac_synth_batch_workspace_size bytes, or NULL for a
+ * pageable copy) and copied into `workspace` on `stream`; the staging must
+ * stay unchanged until the copy has run (for a captured graph: while the
+ * graph is replayed). */
+int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                        void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
 
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */

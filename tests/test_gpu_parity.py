@@ -283,3 +283,49 @@ def test_gpu_synthesis_device_air_and_batching(rt):
         scale = float(np.max(np.abs(ref)))
         # device exp() vs libm exp() in the air gains: last-place differences
         np.testing.assert_allclose(out[row].cpu().numpy(), ref, rtol=1e-6, atol=1e-7 * scale)
+
+
+def test_ragged_synthesis_batch_equals_each_rir_alone(rt):
+    """One ac_synthesize_batch over RIRs of different lengths, sample rates and noise modes.
+
+    The reference-noise RIR equals reconstruct_band_irs bit for bit (golden);
+    every Philox RIR equals ac_synthesize run on it alone with the same key.
+    """
+    from acoustic_agent_b200 import bands
+    s = np.load(GOLDEN / "synthesis.npz")
+    dev = torch.device("cuda", 0)
+    fs48, bd48, delay48, seed48 = s["furnished_f32_meta"]
+    fs16, bd16, delay16, _ = s["shoebox_f32_meta"]
+    fs48, fs16 = int(fs48), int(fs16)
+    e48 = s["furnished_f32_input"]
+    e16 = s["shoebox_f32_input"]
+    rng = np.random.default_rng(3)
+    e_odd = (rng.uniform(0, 1e-3, size=(6, 37)) * (rng.uniform(size=(6, 37)) > 0.3)).astype(np.float32)
+    spb48 = bands.samples_per_bin(float(bd48), fs48)
+    white = torch.as_tensor(np.random.default_rng(int(seed48) + 7).uniform(-1, 1, size=e48.shape[1] * spb48),
+                            device=dev)
+    air = torch.as_tensor(bands.air_gain_table(e48.shape[1], spb48, fs48, float(delay48), 343.0), device=dev)
+    cases = [  # echogram, fs, bin_dur, rng, seed, delay
+        (e48, fs48, float(bd48), "reference", int(seed48), float(delay48)),
+        (e16, fs16, float(bd16), "philox", 1736, float(delay16)),
+        (e48[:, :321] * 0.5, fs48, float(bd48), "philox", 11, 0.004),
+        (e_odd, fs16, 0.01, "philox", 5, 0.0),
+        (e16 * 2.0, fs16, float(bd16), "philox", 1736, -0.5),   # negative delay: clamped to 0 like the reference
+    ]
+    jobs = []
+    for echo, fs, bd, mode, seed, delay in cases:
+        echo_t = torch.as_tensor(np.ascontiguousarray(echo, dtype=np.float32), device=dev)
+        n = echo.shape[1] * bands.samples_per_bin(bd, fs)
+        out = torch.full((6, n), float("nan"), dtype=torch.float32, device=dev)
+        jobs.append(rt.SynthJob(echo_t, out, fs, bd, seed=seed, direct_delay=delay, rng=mode,
+                                white=white if mode == "reference" else None,
+                                air=air if mode == "reference" else None))
+    rt.synthesize_batch(jobs, rt.SynthBatchWorkspace(dev))
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(jobs[0].out.cpu().numpy(), s["furnished_f32_output"])
+    for job, (echo, fs, bd, mode, seed, delay) in zip(jobs[1:], cases[1:]):
+        delays = torch.as_tensor([max(0.0, delay)], dtype=torch.float64, device=dev)
+        p = rt.synth_params(1, echo.shape[1], bd, fs, 343.0, rng_mode="philox", seed=seed, direct_delays=delays)
+        alone = rt.synthesize(job.echogram[None].contiguous(), p, rt.SynthWorkspace(dev))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(job.out.cpu().numpy(), alone[0].cpu().numpy())

@@ -66,7 +66,7 @@ def test_library_exports_every_declared_symbol():
     missing = [name for name in sorted(declared) if not hasattr(lib, name)]
     assert not missing
     assert declared == set(_lib.SIGNATURES), "ctypes binding and header disagree"
-    assert _lib.load().ac_abi_version() == 1
+    assert _lib.load().ac_abi_version() == 2
 
 
 def test_scene_create_rejects_bad_descriptions_without_touching_the_gpu():
@@ -119,3 +119,25 @@ def test_workloads_are_seeded_and_shaped_like_the_configs():
     assert again.spec == apt.spec
     mix = workloads.mixed_batch(5, 8)
     assert len(mix) == 8 and all(1 <= len(w.sources) <= 4 and 1 <= len(w.listeners) <= 8 for w in mix)
+
+
+def test_synthesis_batch_validation_happens_on_the_host():
+    lib = _lib.load()
+    cfg = _lib.ACSynthBatchConfig()
+    cfg.num_rates = 1
+    cfg.sample_rates[0] = 16000
+    jobs = (_lib.ACSynthJob * 2)()
+    for j in jobs:
+        j.num_bins, j.samples_per_bin, j.rate_index, j.rng_mode = 10, 160, 0, _lib.AC_RNG_PHILOX
+    size = ctypes.c_size_t()
+    assert lib.ac_synth_batch_workspace_size(jobs, 2, ctypes.byref(cfg), ctypes.byref(size)) == _lib.AC_OK
+    assert size.value >= 2 * 6 * 1600 * 8          # the raw band signals alone
+    jobs[1].rate_index = 1
+    assert lib.ac_synth_batch_workspace_size(jobs, 2, ctypes.byref(cfg), ctypes.byref(size)) == _lib.AC_ERR_INVALID
+    assert b"rate_index" in lib.ac_last_error()
+    jobs[1].rate_index = 0
+    jobs[1].rng_mode = _lib.AC_RNG_REFERENCE
+    # reference noise without a noise buffer, and null echograms, are refused before any device work
+    assert lib.ac_synthesize_batch(jobs, 2, ctypes.byref(cfg), None, 0, None, None) == _lib.AC_ERR_INVALID
+    cfg.num_rates = 0
+    assert lib.ac_synth_batch_workspace_size(jobs, 2, ctypes.byref(cfg), ctypes.byref(size)) == _lib.AC_ERR_INVALID
