@@ -53,6 +53,7 @@ class ACSceneDesc(ctypes.Structure):
         ("bvh_node_count", ctypes.c_int64), ("bvh_bounds_min", c_double_p), ("bvh_bounds_max", c_double_p),
         ("bvh_start", c_int64_p), ("bvh_count", c_int64_p), ("bvh_escape", c_int64_p),
         ("bvh_primitives", c_int64_p), ("device", ctypes.c_int32), ("cluster_size", ctypes.c_int32),
+        ("traversal", ctypes.c_int32), ("bvh_leaf", ctypes.c_int32),
     ]
 
 
@@ -60,7 +61,8 @@ class ACSceneInfo(ctypes.Structure):
     _fields_ = [
         ("num_surfaces", ctypes.c_int64), ("num_corners", ctypes.c_int64), ("node_count", ctypes.c_int64),
         ("leaf_count", ctypes.c_int64), ("device_bytes", ctypes.c_int64), ("device", ctypes.c_int32),
-        ("max_leaf", ctypes.c_int32), ("num_clusters", ctypes.c_int64),
+        ("max_leaf", ctypes.c_int32), ("num_clusters", ctypes.c_int64), ("traversal", ctypes.c_int32),
+        ("bvh_depth", ctypes.c_int32), ("bvh_nodes", ctypes.c_int64),
     ]
 
 
@@ -110,6 +112,7 @@ class ACSynthParams(ctypes.Structure):
 
 
 AC_SYNTH_MAX_RATES = 4
+AC_TRAVERSAL_AUTO, AC_TRAVERSAL_SCAN, AC_TRAVERSAL_BVH = 0, 1, 2
 
 
 class ACSynthJob(ctypes.Structure):

@@ -28,7 +28,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
           f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr"]
 # Units whose float64 arithmetic must not be contracted into FMAs.
 NO_FMA = {"trace_f64.cu", "synth.cu"}
-SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "bvh_build.cpp"]
+SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "bvh_build.cpp", "fast_bvh.cpp"]
 
 
 def nvcc() -> str:

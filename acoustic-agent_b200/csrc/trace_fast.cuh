@@ -29,6 +29,7 @@
 // returns the lowest visited surface with t = 1e30 (steam_rt.py:4501).
 #pragma once
 
+#include "fast_bvh.h"
 #include "trace_kernel.cuh"
 
 namespace ac {
@@ -54,6 +55,10 @@ struct FastScene {
     int32_t num_polys;
     int32_t num_box_clusters;
     int32_t num_edges;
+    const float4 *bvh_nodes;     // BVH mode: [N][4] traversal BVH over walls and boxes (fast_bvh.h); else null
+    const float *bvh_prims;      // BVH mode: [P][12] surface records in leaf order
+    int32_t num_bvh_nodes;       // 0: scan mode
+    int32_t reserved;
 };
 
 // One group = the jobs that share a scene; chunks never straddle groups.
@@ -254,6 +259,73 @@ __device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, b
             }
         }
     }
+}
+
+// Slab test of one child box of a traversal-BVH node, with the scan's margin on max_t.
+__device__ __forceinline__ bool child_box(const FRay &r, float lx, float hx, float ly, float hy, float lz, float hz,
+                                          float max_t, float &enter) {
+    const float x0 = (lx - r.o[0]) * r.inv[0], x1 = (hx - r.o[0]) * r.inv[0];
+    const float y0 = (ly - r.o[1]) * r.inv[1], y1 = (hy - r.o[1]) * r.inv[1];
+    const float z0 = (lz - r.o[2]) * r.inv[2], z1 = (hz - r.o[2]) * r.inv[2];
+    enter = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
+    const float exit_ = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), max_t));
+    return enter <= exit_;
+}
+
+// Per-lane descent of the traversal BVH (BVH mode): nearer child first, the
+// farther one on a short stack in local memory (the builder bounds the depth
+// by kBvhStack - 1).  No warp-synchronous operation inside: lanes diverge
+// freely and reconverge after the call.  Same update rule as the scan, so
+// closest-hit and any-hit modes work as there.
+__device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r, bool any_hit, float &best_t,
+                                             int &best) {
+    int stack[kBvhStack];
+    int sp = 0;
+    int node = 0;
+#pragma unroll 1
+    while (true) {
+        if (node >= 0) {
+            const float4 *np = fs.bvh_nodes + 4 * static_cast<size_t>(node);
+            const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), k = __ldg(np + 3);
+            const float max_t = best_t * 1.000001f + 1e-5f;
+            float e0, e1;
+            const bool h0 = child_box(r, a.x, a.y, a.z, a.w, c.x, c.y, max_t, e0);
+            const bool h1 = child_box(r, b.x, b.y, b.z, b.w, c.z, c.w, max_t, e1);
+            const int k0 = __float_as_int(k.x), k1 = __float_as_int(k.y);
+            if (h0 && h1) {
+                const bool swap = e1 < e0;
+                node = swap ? k1 : k0;
+                stack[sp++] = swap ? k0 : k1;
+            } else if (h0 || h1) {
+                node = h0 ? k0 : k1;
+            } else {
+                if (sp == 0) return;
+                node = stack[--sp];
+            }
+        } else {
+            const int code = ~node;
+            const int first = code >> 3, count = (code & 7) + 1;
+#pragma unroll 1
+            for (int i = 0; i < count; ++i) {
+                const float *rec = fs.bvh_prims + static_cast<size_t>(first + i) * kPrimStride;
+                const int tag = __float_as_int(__ldg(rec + 11));
+                const float tt = (tag & 3) == 0 ? wall_t(ldq(rec), ldq(rec + 4), r) : box_t(rec, r);
+                take(tt, tag >> 2, best_t, best);
+            }
+            if (any_hit && best >= 0) return;
+            if (sp == 0) return;
+            node = stack[--sp];
+        }
+    }
+}
+
+// The closest-hit / any-hit query of one ray: the lockstep scan (walls and
+// boxes in scan mode, horizontal polygons always) and, in BVH mode, the
+// per-lane BVH descent over walls and boxes.  Every lane must call it.
+__device__ __forceinline__ void scene_query(const FastScene &fs, const FRay &r, bool active, bool any_hit,
+                                            float &best_t, int &best) {
+    scene_scan(fs, r, active, any_hit, best_t, best);
+    if (fs.num_bvh_nodes > 0 && active && !(any_hit && best >= 0)) bvh_traverse(fs, r, any_hit, best_t, best);
 }
 
 // Normal of the winning surface, oriented against the ray.
@@ -459,7 +531,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         for (int phase = 0; phase < 2; ++phase) {
             float found_t = limit;
             int found = -1;
-            scene_scan(fs, query, query_active, phase == 1, found_t, found);
+            scene_query(fs, query, query_active, phase == 1, found_t, found);
             if (phase == 1) {
                 occluded = found >= 0;
                 break;

@@ -55,7 +55,12 @@ def _stream_ptr(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
 class DeviceScene:
     """A scene uploaded with ac_scene_create; owns its device memory."""
 
-    def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0) -> None:
+    TRAVERSALS = {"auto": 0, "scan": 1, "bvh": 2}
+
+    def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0,
+                 traversal: str = "auto", bvh_leaf: int = 0) -> None:
+        if traversal not in self.TRAVERSALS:
+            raise ValueError(f"traversal must be one of {sorted(self.TRAVERSALS)}")
         require_cuda(device)
         a = arrays.arrays if isinstance(arrays, SceneArrays) else dict(arrays)
         self.names: tuple[str, ...] = tuple(a["names"])
@@ -87,6 +92,8 @@ class DeviceScene:
         desc.bvh_primitives = _ip(keep["bvh_primitives"])
         desc.device = int(device)
         desc.cluster_size = int(cluster_size)
+        desc.traversal = self.TRAVERSALS[traversal]
+        desc.bvh_leaf = int(bvh_leaf)
         if "surface_bounds_min" in a and "surface_bounds_max" in a:
             keep["surface_bounds_min"] = _f64(a["surface_bounds_min"])
             keep["surface_bounds_max"] = _f64(a["surface_bounds_max"])
@@ -102,6 +109,9 @@ class DeviceScene:
         self.device_bytes = int(info.device_bytes)
         self.node_count = int(info.node_count)
         self.num_clusters = int(info.num_clusters)
+        self.traversal = {1: "scan", 2: "bvh"}.get(int(info.traversal), "scan")
+        self.bvh_depth = int(info.bvh_depth)
+        self.bvh_nodes = int(info.bvh_nodes)
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
 
     def close(self) -> None:

@@ -329,3 +329,42 @@ def test_ragged_synthesis_batch_equals_each_rir_alone(rt):
         alone = rt.synthesize(job.echogram[None].contiguous(), p, rt.SynthWorkspace(dev))
         torch.cuda.synchronize()
         np.testing.assert_array_equal(job.out.cpu().numpy(), alone[0].cpu().numpy())
+
+
+@pytest.mark.parametrize("name", TRACE_CASES)
+def test_fp32_bvh_traversal_equals_scan(rt, name):
+    """BVH mode and scan mode find the same closest surfaces: identical rays and fixed-point bins.
+
+    Both modes only skip surfaces whose bounds lie beyond the current closest
+    hit (with the same float32 margin), and the closest hit is the minimum t
+    with ties to the lower surface index whatever the visiting order.
+    """
+    case = load_case(name)
+    spec = spec_for(rt, case, "float32")
+    got = {}
+    for mode in ("scan", "bvh"):
+        scene = rt.DeviceScene(case["arrays"], traversal=mode)
+        assert scene.traversal == mode
+        if mode == "bvh":
+            assert 1 <= scene.bvh_depth <= 31 and scene.bvh_nodes >= 1
+        buffers = rt.trace(scene, spec, record_rays=True)
+        torch.cuda.synchronize()
+        got[mode] = {"rays": buffers.ray_surfaces.cpu().numpy(), "echogram": buffers.echogram_fx.cpu().numpy(),
+                     "hits": buffers.hit_counts.cpu().numpy(), "counters": buffers.counters.cpu().numpy()}
+        scene.close()
+    for key in ("rays", "echogram", "hits", "counters"):
+        np.testing.assert_array_equal(got["bvh"][key], got["scan"][key], err_msg=key)
+
+
+@pytest.mark.parametrize("leaf", [1, 2, 8])
+def test_fp32_bvh_leaf_sizes_agree(rt, leaf):
+    case = load_case("apartment3_bvh")
+    spec = spec_for(rt, case, "float32", rng="philox", num_rays=4096)
+    got = []
+    for kw in ({"traversal": "scan"}, {"traversal": "bvh", "bvh_leaf": leaf}):
+        scene = rt.DeviceScene(case["arrays"], **kw)
+        buffers = rt.trace(scene, spec)
+        torch.cuda.synchronize()
+        got.append(buffers.echogram_fx.cpu().numpy())
+        scene.close()
+    np.testing.assert_array_equal(got[0], got[1])
