@@ -35,7 +35,7 @@ struct Offsets {
 };
 
 // Scenes with more walls + boxes than this trace in BVH mode unless the caller chooses.
-constexpr int64_t kAutoBvhSurfaces = 64;
+constexpr int64_t kAutoBvhSurfaces = 16;
 // Float32 BVH node boxes are padded by this much (metres) beyond the surface bounds.
 constexpr double kBvhPad = 1e-4;
 // Surfaces per BVH leaf unless the caller chooses: one surface per leaf measured

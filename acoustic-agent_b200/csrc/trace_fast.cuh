@@ -272,19 +272,27 @@ __device__ __forceinline__ bool child_box(const FRay &r, float lx, float hx, flo
     return enter <= exit_;
 }
 
-// Per-lane descent of the traversal BVH (BVH mode): nearer child first, the
-// farther one on a short stack in local memory (the builder bounds the depth
-// by kBvhStack - 1).  No warp-synchronous operation inside: lanes diverge
-// freely and reconverge after the call.  Same update rule as the scan, so
-// closest-hit and any-hit modes work as there.
+// Per-lane descent of the traversal BVH (BVH mode), organised "while-while"
+// (Aila and Laine, "Understanding the efficiency of ray traversal on GPUs",
+// HPG 2009): a lane descends inner nodes -- nearer child first, the farther
+// one on a short stack in local memory -- until it holds a leaf, then keeps
+// descending while other lanes of the warp still look for theirs, so leaves
+// are tested by as many lanes at once as possible.  The builder bounds the
+// depth by kBvhStack - 1.  Same update rule as the scan, so closest-hit and
+// any-hit modes work as there.
+constexpr int kBvhDone = static_cast<int>(0x80000000u);  // below every leaf reference
+
 __device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r, bool any_hit, float &best_t,
                                              int &best) {
     int stack[kBvhStack];
-    int sp = 0;
-    int node = 0;
+    stack[0] = kBvhDone;
+    int sp = 1;
+    int node = 0;      // next node to visit (>= 0 inner, < 0 leaf, kBvhDone finished)
+    int leaf = 0;      // a leaf waiting to be tested (< 0), 0 = none
 #pragma unroll 1
-    while (true) {
-        if (node >= 0) {
+    while (node != kBvhDone || leaf < 0) {
+#pragma unroll 1
+        while (node >= 0) {
             const float4 *np = fs.bvh_nodes + 4 * static_cast<size_t>(node);
             const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2), k = __ldg(np + 3);
             const float max_t = best_t * 1.000001f + 1e-5f;
@@ -299,11 +307,17 @@ __device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r,
             } else if (h0 || h1) {
                 node = h0 ? k0 : k1;
             } else {
-                if (sp == 0) return;
                 node = stack[--sp];
             }
-        } else {
-            const int code = ~node;
+            if (node < 0 && node != kBvhDone && leaf == 0) {   // park the leaf, keep descending
+                leaf = node;
+                node = stack[--sp];
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;   // every lane holds a leaf: test them
+        }
+#pragma unroll 1
+        while (leaf < 0) {
+            const int code = ~leaf;
             const int first = code >> 3, count = (code & 7) + 1;
 #pragma unroll 1
             for (int i = 0; i < count; ++i) {
@@ -313,8 +327,11 @@ __device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r,
                 take(tt, tag >> 2, best_t, best);
             }
             if (any_hit && best >= 0) return;
-            if (sp == 0) return;
-            node = stack[--sp];
+            leaf = 0;
+            if (node < 0 && node != kBvhDone) {   // the next stop is a leaf too
+                leaf = node;
+                node = stack[--sp];
+            }
         }
     }
 }
