@@ -1,0 +1,166 @@
+"""Autotuner for the tracer's schedule: per-scene traversal and per-launch shape.
+
+Every knob here changes only how the work is scheduled, never a result: the
+closest surface is the minimum distance with ties to the lower index whatever
+the visiting order, echogram bins are exact fixed-point sums, and rays are
+keyed by (seed, stream key, ray index).  The GPU tests check bit-identical
+outputs across traversal modes, leaf sizes, block sizes and chunk sizes, so
+the tuner may choose by measured time alone.
+
+Knobs
+-----
+per scene (``tune_scene``)
+    ``traversal`` -- "scan" (kind-separated clusters in warp lockstep) or
+    "bvh" (per-lane descent of a surface-area-heuristic BVH with a short stack);
+    ``bvh_leaf`` -- surfaces per BVH leaf (1, 2, 4): smaller leaves mean a
+    deeper tree and a deeper traversal stack, fewer surface tests per leaf.
+per launch (``tune_launch``)
+    ``block_size`` -- rays per block (one ray per lane: 128 or 256 threads);
+    ``chunk_rays`` -- queue granularity: rays a warp takes from the shared
+    work counter at once (16 .. 128).
+
+Choices are cached by a fingerprint of the scene's surface arrays
+(``TuneCache``), so a scene resident in a serving loop is tuned once.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import threading
+from dataclasses import asdict, dataclass, replace
+from pathlib import Path
+from typing import Any, Sequence
+
+import numpy as np
+import torch
+
+from acoustic_agent_b200 import runtime
+from acoustic_agent_b200.scene import SceneArrays
+
+SCENE_CANDIDATES: tuple[dict[str, Any], ...] = (
+    {"traversal": "scan", "bvh_leaf": 0},
+    {"traversal": "bvh", "bvh_leaf": 1},
+    {"traversal": "bvh", "bvh_leaf": 2},
+    {"traversal": "bvh", "bvh_leaf": 4},
+)
+LAUNCH_CANDIDATES: tuple[dict[str, int], ...] = tuple(
+    {"block_size": b, "chunk_rays": c} for b in (256, 128) for c in (16, 32, 64, 128))
+
+
+@dataclass(frozen=True)
+class SceneChoice:
+    traversal: str
+    bvh_leaf: int
+    ms: float
+
+    def options(self) -> dict[str, Any]:
+        return {"traversal": self.traversal, "bvh_leaf": self.bvh_leaf}
+
+
+@dataclass(frozen=True)
+class LaunchChoice:
+    block_size: int
+    chunk_rays: int
+    ms: float
+
+
+def fingerprint(arrays: SceneArrays | dict[str, Any]) -> str:
+    """Stable hash of the surface arrays the tracer reads."""
+    a = arrays.arrays if isinstance(arrays, SceneArrays) else arrays
+    h = hashlib.sha1()
+    for key in ("kinds", "wall_a", "wall_delta", "wall_z", "z_values", "box_center", "box_axis_u", "box_axis_v",
+                "box_half", "box_z", "corners"):
+        v = np.ascontiguousarray(np.asarray(a[key], dtype=np.float64))
+        h.update(key.encode())
+        h.update(str(v.shape).encode())
+        h.update(v.tobytes())
+    return h.hexdigest()
+
+
+class TuneCache:
+    """Scene choices by fingerprint; optionally persisted as JSON."""
+
+    def __init__(self, path: str | Path | None = None) -> None:
+        self.path = Path(path) if path else None
+        self.entries: dict[str, SceneChoice] = {}
+        self._lock = threading.Lock()
+        if self.path and self.path.exists():
+            for key, value in json.loads(self.path.read_text()).items():
+                self.entries[key] = SceneChoice(**value)
+
+    def get(self, key: str) -> SceneChoice | None:
+        with self._lock:
+            return self.entries.get(key)
+
+    def put(self, key: str, choice: SceneChoice) -> None:
+        with self._lock:
+            self.entries[key] = choice
+            if self.path:
+                self.path.write_text(json.dumps({k: asdict(v) for k, v in self.entries.items()}, indent=1))
+
+
+def _time_ms(fn, reps: int, stream: torch.cuda.Stream) -> float:
+    fn()  # warm-up (also sizes workspaces)
+    times = []
+    for _ in range(reps):
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        fn()
+        stop.record(stream)
+        stop.synchronize()
+        times.append(start.elapsed_time(stop))
+    return float(np.median(times))
+
+
+def tune_scene(arrays: SceneArrays, spec: runtime.TraceSpec, *, device: int = 0, sample_rays: int = 16384,
+               reps: int = 3, candidates: Sequence[dict[str, Any]] = SCENE_CANDIDATES,
+               cache: TuneCache | None = None) -> SceneChoice:
+    """Fastest traversal for one scene, timed on a sample of `spec`'s rays (float32, Philox)."""
+    key = fingerprint(arrays)
+    if cache is not None:
+        hit = cache.get(key)
+        if hit is not None:
+            return hit
+    dev = runtime.require_cuda(device)
+    stream = torch.cuda.current_stream(dev)
+    sample = replace(spec, num_rays=max(1, min(int(spec.num_rays), int(sample_rays))), precision="float32",
+                     rng="philox", render_ambisonics=False)
+    best: SceneChoice | None = None
+    for cand in candidates:
+        scene = runtime.DeviceScene(arrays, device=dev.index, **cand)
+        try:
+            if cand["traversal"] == "bvh" and scene.traversal != "bvh":
+                continue   # nothing for a BVH to hold (only horizontal surfaces)
+            buffers = runtime.TraceBuffers.allocate(scene.num_surfaces, int(sample.num_bins), dev)
+            ms = _time_ms(lambda: runtime.trace(scene, sample, buffers, stream=stream), reps, stream)
+        finally:
+            scene.close()
+        if best is None or ms < best.ms:
+            best = SceneChoice(cand["traversal"], int(cand.get("bvh_leaf", 0)), ms)
+    assert best is not None
+    if cache is not None:
+        cache.put(key, best)
+    return best
+
+
+def tune_launch(jobs: Sequence[tuple[runtime.DeviceScene, runtime.TraceSpec]], *, device: int = 0,
+                ray_fraction: float = 1.0 / 16.0, reps: int = 2,
+                candidates: Sequence[dict[str, int]] = LAUNCH_CANDIDATES) -> LaunchChoice:
+    """Fastest (block_size, chunk_rays) for one persistent launch over `jobs`.
+
+    Timed on the same jobs with their ray budgets scaled by `ray_fraction`, so
+    the mix of scenes, bounce limits and relative job sizes is the real one.
+    """
+    dev = runtime.require_cuda(device)
+    stream = torch.cuda.current_stream(dev)
+    scaled = [(scene, replace(spec, num_rays=max(1, int(round(spec.num_rays * ray_fraction)))),
+               runtime.TraceBuffers.allocate(scene.num_surfaces, int(spec.num_bins), dev)) for scene, spec in jobs]
+    workspace = runtime.BatchWorkspace(dev)
+    best: LaunchChoice | None = None
+    for cand in candidates:
+        ms = _time_ms(lambda: runtime.trace_batch(scaled, workspace, block_size=cand["block_size"],
+                                                  chunk_rays=cand["chunk_rays"], stream=stream), reps, stream)
+        if best is None or ms < best.ms:
+            best = LaunchChoice(cand["block_size"], cand["chunk_rays"], ms)
+    assert best is not None
+    return best

@@ -105,11 +105,18 @@ class RIRRenderer:
         self._trace_ws = runtime.BatchWorkspace(self.device)
         self._synth_ws = runtime.SynthBatchWorkspace(self.device)
 
-    def plan(self, scenes: Sequence[SceneArrays | dict[str, Any] | runtime.DeviceScene], jobs: Sequence[Job]) -> Plan:
+    def plan(self, scenes: Sequence[SceneArrays | dict[str, Any] | runtime.DeviceScene], jobs: Sequence[Job], *,
+             scene_options: Sequence[dict[str, Any]] | None = None) -> Plan:
+        """Upload scenes (unless already resident) and lay out every job's outputs.
+
+        `scene_options` (one dict per scene, e.g. from autotune.tune_scene)
+        chooses each uploaded scene's traversal; results do not depend on it.
+        """
+        opts = list(scene_options) if scene_options is not None else [{}] * len(scenes)
         device_scenes = [s if isinstance(s, runtime.DeviceScene) else
                          runtime.DeviceScene(s if isinstance(s, SceneArrays) else compile_scene(s),
-                                             device=self.device.index)
-                         for s in scenes]
+                                             device=self.device.index, **o)
+                         for s, o in zip(scenes, opts)]
         buffers = [runtime.TraceBuffers.allocate(device_scenes[j.scene_index].num_surfaces, j.spec.num_bins,
                                                  self.device, echogram=False) for j in jobs]
         bins = [int(j.spec.num_bins) for j in jobs]

@@ -1,0 +1,383 @@
+"""Continuous-batching RIR server on one GPU.
+
+The reference answers one request at a time: ``AcousticAgent.run`` and the
+batch helpers (api.py:477-639, batch.py:139-185, engine.py:64-73) trace each
+(source, channel) job to completion before the next starts.  This loop keeps
+the GPU fed while requests arrive:
+
+* **admission by free HBM** -- a request is admitted when its footprint (its
+  scene, unless already resident, plus the trace outputs, echograms, band IRs
+  and synthesis workspace of its jobs) fits the device budget that the
+  in-flight batches leave, and a launch slot is free;
+* **continuous batching** -- every admitted request that waits is folded into
+  the next batch: ONE persistent tracer launch over all their jobs (any mix of
+  scene sizes, ray budgets and lengths) plus one ragged synthesis and the
+  copy of the band IRs to pinned host memory.  Up to ``max_inflight`` batches
+  run on their own CUDA streams at once, so a batch formed from requests that
+  arrived while others were on the GPU starts as soon as a slot frees, and its
+  blocks fill the SMs the previous launch's tail leaves idle;
+* **resident scenes** -- scenes (BVH, surface records, material table) stay on
+  the device in an LRU cache keyed by their surface arrays and are reused by
+  later requests and by every keyframe of a moving source; only idle scenes
+  are evicted, and only when an admission needs their memory.
+
+Every job's result is independent of the batch it ran in: rays are keyed by
+(seed, stream key, ray index) with the stream key derived from the request
+identity, echogram bins are exact fixed-point sums, and synthesis noise is
+keyed by the job's own seed.  ``tests/test_gpu_serving.py`` checks that each
+served result equals the same request rendered alone.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+from typing import Any, Sequence
+
+import numpy as np
+import torch
+
+from acoustic_agent_b200 import autotune, bands, rng, runtime
+from acoustic_agent_b200.batching import NUM_BANDS
+from acoustic_agent_b200.directivity import source_directivity, source_forward
+from acoustic_agent_b200.scene import SceneArrays, compile_scene
+from acoustic_agent_b200.workloads import Workload
+
+
+@dataclass
+class Request:
+    """One RIR solve: a scene, one source (or keyframes of a moving source) and its receiver channels."""
+
+    id: int
+    workload: Workload
+    sources: list[tuple[float, float, float]]
+    arrival_s: float = 0.0
+    moving: bool = False
+
+    @property
+    def num_rirs(self) -> int:
+        return len(self.sources) * len(self.workload.listeners)
+
+
+@dataclass
+class Result:
+    request: Request
+    band_irs: list[np.ndarray]          # [6, N] float32 per (keyframe, channel), keyframe-major
+    ray_bounces: int
+    admitted_s: float
+    done_s: float
+
+    @property
+    def latency_s(self) -> float:
+        return self.done_s - self.request.arrival_s
+
+
+@dataclass
+class Report:
+    results: list[Result]
+    makespan_s: float
+    rirs: int
+    ray_bounces: int
+    batches: int
+    max_inflight_seen: int
+    scene_hits: int
+    scene_misses: int
+    evictions: int
+
+    def latency_ms(self, q: float) -> float:
+        lat = np.array([r.latency_s for r in self.results]) * 1e3
+        return float(np.percentile(lat, q)) if lat.size else float("nan")
+
+    def summary(self) -> dict[str, Any]:
+        return {
+            "requests": len(self.results), "rirs": self.rirs, "makespan_s": self.makespan_s,
+            "rirs_per_s": self.rirs / self.makespan_s if self.makespan_s > 0 else float("nan"),
+            "ray_bounces_per_s": self.ray_bounces / self.makespan_s if self.makespan_s > 0 else float("nan"),
+            "p50_ms": self.latency_ms(50), "p99_ms": self.latency_ms(99), "batches": self.batches,
+            "max_inflight": self.max_inflight_seen, "scene_cache": {"hits": self.scene_hits,
+                                                                    "misses": self.scene_misses,
+                                                                    "evictions": self.evictions},
+        }
+
+
+def request_jobs(req: Request, precision: str = "float32") -> list[runtime.TraceSpec]:
+    """TraceSpecs of a request, keyframe-major then channel; keyed by the request's identity."""
+    w = req.workload
+    cfg = w.config
+    emitter = source_directivity(w.source_model)
+    forward = source_forward(emitter)
+    specs = []
+    for k, src in enumerate(req.sources):
+        key = rng.stream_key(w.name, req.id, k)
+        for lst in w.listeners:
+            src_a = np.asarray(src, dtype=float)
+            lst_a = np.asarray(lst, dtype=float)
+            specs.append(runtime.TraceSpec(
+                source=src_a, listener=lst_a, source_forward=forward, num_rays=max(1, cfg.rt_num_rays),
+                num_bounces=cfg.rt_num_bounces, num_bins=cfg.num_bins, bin_duration=cfg.rt_bin_duration_s,
+                speed_of_sound=cfg.c, max_path_length=cfg.max_path_length,
+                direct_delay=float(np.linalg.norm(src_a - lst_a)) / cfg.c,
+                listener_radius=cfg.rt_listener_radius, source_radius=cfg.rt_source_radius,
+                irradiance_min_distance=cfg.rt_irradiance_min_distance,
+                specular_exponent=cfg.rt_specular_exponent, dipole_weight=float(emitter["dipole_weight"]),
+                dipole_power=float(emitter["dipole_power"]), use_bvh=cfg.intersection_backend == "bvh",
+                render_ambisonics=False, precision=precision, rng="philox", seed=cfg.seed, stream_key=key))
+    return specs
+
+
+def job_bytes(spec: runtime.TraceSpec, fs: int, num_surfaces: int) -> int:
+    """Device bytes one job holds while in flight (outputs, echogram, band IRs, synthesis rows)."""
+    bins = int(spec.num_bins)
+    n = bins * bands.samples_per_bin(spec.bin_duration, fs)
+    trace_out = 8 * (NUM_BANDS * bins * 2 + 4 * num_surfaces + 8) + 4 * (NUM_BANDS * bins + num_surfaces)
+    synth = 8 * (2 * NUM_BANDS * bins + NUM_BANDS * n)
+    return trace_out + 4 * NUM_BANDS * n + synth + 1024
+
+
+class SceneCache:
+    """Resident device scenes keyed by surface-array fingerprint, LRU over idle entries."""
+
+    def __init__(self, device: int, *, tune: bool = True, tune_cache: autotune.TuneCache | None = None) -> None:
+        self.device = device
+        self.tune = tune
+        self.tune_cache = tune_cache or autotune.TuneCache()
+        self.entries: OrderedDict[str, runtime.DeviceScene] = OrderedDict()
+        self.refs: dict[str, int] = {}
+        self.arrays: dict[int, tuple[str, SceneArrays]] = {}
+        self.hits = self.misses = self.evictions = 0
+
+    def resident_bytes(self) -> int:
+        return sum(s.device_bytes for s in self.entries.values())
+
+    def key_of(self, w: Workload) -> tuple[str, SceneArrays]:
+        ident = id(w.spec)
+        if ident not in self.arrays:
+            arrays = compile_scene(w.spec)
+            self.arrays[ident] = (autotune.fingerprint(arrays), arrays)
+        return self.arrays[ident]
+
+    def is_resident(self, w: Workload) -> bool:
+        return self.key_of(w)[0] in self.entries
+
+    def acquire(self, w: Workload, sample: runtime.TraceSpec) -> runtime.DeviceScene:
+        key, arrays = self.key_of(w)
+        scene = self.entries.get(key)
+        if scene is None:
+            self.misses += 1
+            options: dict[str, Any] = {}
+            if self.tune:
+                options = autotune.tune_scene(arrays, sample, device=self.device, cache=self.tune_cache).options()
+            scene = runtime.DeviceScene(arrays, device=self.device, **options)
+            self.entries[key] = scene
+        else:
+            self.hits += 1
+            self.entries.move_to_end(key)
+        self.refs[key] = self.refs.get(key, 0) + 1
+        return scene
+
+    def release(self, w: Workload) -> None:
+        key = self.key_of(w)[0]
+        self.refs[key] -= 1
+
+    def evict_idle(self, need: int) -> int:
+        """Free idle scenes, least recently used first, until `need` bytes are freed; returns bytes freed."""
+        freed = 0
+        for key in list(self.entries):
+            if freed >= need:
+                break
+            if self.refs.get(key, 0) > 0:
+                continue
+            scene = self.entries.pop(key)
+            freed += scene.device_bytes
+            scene.close()
+            self.evictions += 1
+        return freed
+
+    def close(self) -> None:
+        for scene in self.entries.values():
+            scene.close()
+        self.entries.clear()
+
+
+@dataclass
+class _Batch:
+    requests: list[Request]
+    specs: list[list[runtime.TraceSpec]]
+    stream: torch.cuda.Stream
+    done: torch.cuda.Event
+    host: torch.Tensor
+    lengths: list[list[int]]
+    buffers: list[runtime.TraceBuffers]
+    bytes: int
+    admitted_s: float
+    keep: list[Any] = field(default_factory=list)
+
+
+class Server:
+    """Continuous batching over one GPU (see the module docstring)."""
+
+    def __init__(self, device: int = 0, *, max_inflight: int = 3, hbm_budget: int | None = None,
+                 max_batch_rays: int = 400_000_000, tune: bool = True, block_size: int = 0,
+                 chunk_rays: int = 0) -> None:
+        self.dev = runtime.require_cuda(device)
+        self.max_inflight = max(1, int(max_inflight))
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.dev)
+            hbm_budget = int(free * 0.8)
+        self.budget = int(hbm_budget)
+        self.max_batch_rays = int(max_batch_rays)
+        self.scenes = SceneCache(self.dev.index, tune=tune)
+        self.block_size = block_size
+        self.chunk_rays = chunk_rays
+        self.streams = [torch.cuda.Stream(self.dev) for _ in range(self.max_inflight)]
+        self.in_use = 0     # bytes held by in-flight batches
+
+    # ---- footprint and admission
+    def footprint(self, req: Request, specs: Sequence[runtime.TraceSpec]) -> int:
+        scene = 0 if self.scenes.is_resident(req.workload) else self._scene_estimate(req.workload)
+        surfaces = self.scenes.key_of(req.workload)[1].num_surfaces
+        return scene + sum(job_bytes(s, req.workload.config.fs, surfaces) for s in specs)
+
+    def _scene_estimate(self, w: Workload) -> int:
+        arrays = self.scenes.key_of(w)[1]
+        return 4096 + 512 * arrays.num_surfaces + 64 * len(arrays.arrays["corners"])
+
+    def _fits(self, need: int) -> bool:
+        if self.scenes.resident_bytes() + self.in_use + need <= self.budget:
+            return True
+        over = self.scenes.resident_bytes() + self.in_use + need - self.budget
+        self.scenes.evict_idle(over)
+        return self.scenes.resident_bytes() + self.in_use + need <= self.budget
+
+    # ---- one batch: trace + synthesis + copy to pinned host memory, all on the batch's stream
+    def _launch(self, reqs: list[Request], specs: list[list[runtime.TraceSpec]], nbytes: int, now: float,
+                stream: torch.cuda.Stream) -> _Batch:
+        jobs, synth, lengths, keep = [], [], [], []
+        buffers: list[runtime.TraceBuffers] = []
+        total = sum(4 * NUM_BANDS * s.num_bins * bands.samples_per_bin(s.bin_duration, r.workload.config.fs)
+                    for r, ss in zip(reqs, specs) for s in ss) // 4
+        with torch.cuda.stream(stream):
+            ir_store = torch.empty(max(1, total), dtype=torch.float32, device=self.dev)
+            off = 0
+            for r, ss in zip(reqs, specs):
+                scene = self.scenes.acquire(r.workload, ss[0])
+                fs = r.workload.config.fs
+                row = []
+                for s in ss:
+                    b = runtime.TraceBuffers.allocate(scene.num_surfaces, s.num_bins, self.dev)
+                    n = s.num_bins * bands.samples_per_bin(s.bin_duration, fs)
+                    out = ir_store[off:off + NUM_BANDS * n].view(NUM_BANDS, n)
+                    off += NUM_BANDS * n
+                    jobs.append((scene, s, b))
+                    buffers.append(b)
+                    synth.append(runtime.SynthJob(b.echogram, out, fs, s.bin_duration, seed=int(s.seed) + 7,
+                                                  direct_delay=max(0.0, float(s.direct_delay)),
+                                                  speed_of_sound=s.speed_of_sound))
+                    row.append(n)
+                lengths.append(row)
+            trace_ws = runtime.BatchWorkspace(self.dev)
+            synth_ws = runtime.SynthBatchWorkspace(self.dev)
+            runtime.trace_batch(jobs, trace_ws, block_size=self.block_size, chunk_rays=self.chunk_rays,
+                                stream=stream)
+            runtime.synthesize_batch(synth, synth_ws, stream=stream)
+            host = torch.empty(ir_store.shape, dtype=torch.float32, pin_memory=True)
+            host.copy_(ir_store, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(stream)
+        keep.extend([ir_store, trace_ws, synth_ws, synth])
+        return _Batch(reqs, specs, stream, done, host, lengths, buffers, nbytes, now, keep)
+
+    def _finish(self, batch: _Batch, now: float) -> list[Result]:
+        host = batch.host.numpy()
+        out, off, k = [], 0, 0
+        for req, row in zip(batch.requests, batch.lengths):
+            irs = []
+            rb = 0
+            for n in row:
+                irs.append(host[off:off + NUM_BANDS * n].reshape(NUM_BANDS, n).copy())
+                off += NUM_BANDS * n
+                rb += int(batch.buffers[k].counters[2].item())
+                k += 1
+            out.append(Result(req, irs, rb, batch.admitted_s, now))
+            self.scenes.release(req.workload)
+        self.in_use -= batch.bytes
+        return out
+
+    def serve(self, requests: Sequence[Request], *, realtime: bool = True, idle_sleep_s: float = 2e-4) -> Report:
+        """Run every request to completion; arrivals follow `arrival_s` (wall clock) when `realtime`."""
+        pending = deque(sorted(requests, key=lambda r: r.arrival_s))
+        waiting: deque[tuple[Request, list[runtime.TraceSpec]]] = deque()
+        inflight: list[_Batch] = []
+        results: list[Result] = []
+        batches = max_seen = 0
+        free_streams = list(self.streams)
+        t0 = time.perf_counter()
+        clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
+        while pending or waiting or inflight:
+            now = clock()
+            while pending and pending[0].arrival_s <= now:
+                req = pending.popleft()
+                waiting.append((req, request_jobs(req)))
+            # completions first: they return slots and memory
+            for batch in list(inflight):
+                if batch.done.query():
+                    done_at = time.perf_counter() - t0
+                    results.extend(self._finish(batch, done_at))
+                    inflight.remove(batch)
+                    free_streams.append(batch.stream)
+            # admit everything that fits into one new batch while a slot is free
+            if waiting and free_streams:
+                reqs, specs, need_total, rays = [], [], 0, 0
+                while waiting:
+                    req, ss = waiting[0]
+                    need = self.footprint(req, ss)
+                    req_rays = sum(s.num_rays for s in ss)
+                    if reqs and rays + req_rays > self.max_batch_rays:
+                        break
+                    if not self._fits(need_total + need):
+                        if not reqs and not inflight:
+                            raise MemoryError(f"request {req.id} needs {need} bytes; the budget is {self.budget}")
+                        break
+                    waiting.popleft()
+                    reqs.append(req)
+                    specs.append(ss)
+                    need_total += need
+                    rays += req_rays
+                if reqs:
+                    self.in_use += need_total
+                    stream = free_streams.pop()
+                    inflight.append(self._launch(reqs, specs, need_total, time.perf_counter() - t0, stream))
+                    batches += 1
+                    max_seen = max(max_seen, len(inflight))
+                    continue
+            if not realtime and not inflight and not waiting and pending:
+                continue
+            if inflight or (pending and realtime):
+                time.sleep(idle_sleep_s)
+        makespan = max((r.done_s for r in results), default=0.0) - min((r.request.arrival_s for r in results),
+                                                                       default=0.0)
+        return Report(results=sorted(results, key=lambda r: r.request.id), makespan_s=makespan,
+                      rirs=sum(r.request.num_rirs for r in results),
+                      ray_bounces=sum(r.ray_bounces for r in results), batches=batches, max_inflight_seen=max_seen,
+                      scene_hits=self.scenes.hits, scene_misses=self.scenes.misses,
+                      evictions=self.scenes.evictions)
+
+    def close(self) -> None:
+        self.scenes.close()
+
+
+def requests_from_stream(stream: Sequence[dict[str, Any]]) -> list[Request]:
+    """Requests from workloads.request_stream entries."""
+    return [Request(k, e["workload"], list(e["sources"]), float(e["arrival_s"]), bool(e.get("moving", False)))
+            for k, e in enumerate(stream)]
+
+
+def render_alone(req: Request, device: int = 0) -> list[np.ndarray]:
+    """The same request rendered by itself (one batch, nothing else on the GPU)."""
+    server = Server(device, max_inflight=1, tune=False)
+    try:
+        report = server.serve([Request(req.id, req.workload, req.sources, 0.0, req.moving)], realtime=False)
+    finally:
+        server.close()
+    return report.results[0].band_irs

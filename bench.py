@@ -330,16 +330,28 @@ def main() -> int:
     parser.add_argument("--steps", type=int, default=10)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", default="u_room_20_boxes", choices=("u_room_20_boxes", "shoebox", "apartment"))
+    parser.add_argument("--workload", default="u_room_20_boxes",
+                        choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving"))
     parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     parser.add_argument("--no-cpu-baseline", action="store_true")
     parser.add_argument("--block", type=int, default=0)
+    parser.add_argument("--scenes", type=int, default=256, help="mixed_batch: scenes in the batch")
+    parser.add_argument("--plain-jobs", type=int, default=0,
+                        help="mixed_batch: jobs of the plain per-job loop to time (0: all)")
+    parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
+    parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
     if args.impl == "reference":
+        if args.workload in ("mixed_batch", "serving"):
+            parser.error("--impl reference times the reference's per-RIR path on a single-scene workload")
         run_reference_arm(args, args.workload)
         return 0
+    if args.workload == "mixed_batch":
+        return run_mixed_batch(args)
+    if args.workload == "serving":
+        return run_serving(args)
 
     import torch
     from acoustic_agent_b200 import batching, runtime, scene as scene_mod
@@ -467,6 +479,167 @@ def main() -> int:
     if dist is not None:
         dist.barrier(device_ids=[local])
         dist.destroy_process_group()
+    return 0
+
+
+def _device_timed(fn, steps: int, device, flush) -> list[float]:
+    import torch
+    stream = torch.cuda.current_stream(device)
+    out = []
+    for k in range(steps):
+        flush.fill_(float(k))
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        fn()
+        stop.record(stream)
+        stop.synchronize()
+        out.append(start.elapsed_time(stop))
+    return out
+
+
+def run_mixed_batch(args) -> int:
+    """Batched mixed-size workload: many scenes, sources and channels in one persistent launch.
+
+    256 seeded scenes log-uniform between a single room and an 8-room
+    apartment, 1-4 sources and 1-8 channels each, 1e4-1e6 rays, fs 16 kHz,
+    1-2 s: the graph-captured tracer + ragged synthesis (autotuned traversal
+    per scene and launch shape) against looping the plain per-job drop-in call
+    (one ac_trace + one ac_synthesize + a host copy per RIR).
+    """
+    import torch
+    from acoustic_agent_b200 import autotune, batching, runtime, scene as scene_mod, workloads
+    world, rank, local = _dist_setup()
+    if world > 1:
+        raise SystemExit("mixed_batch runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    t0 = time.perf_counter()
+    population = workloads.mixed_batch(1729, args.scenes)
+    specs, jobs = batching.workload_jobs(population)
+    arrays = [scene_mod.compile_scene(s) for s in specs]
+    t_compile = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cache = autotune.TuneCache()
+    first_job = {}
+    for j in jobs:
+        first_job.setdefault(j.scene_index, j)
+    options = [autotune.tune_scene(a, first_job[k].spec, device=local, cache=cache).options()
+               for k, a in enumerate(arrays)]
+    renderer = batching.RIRRenderer(local)
+    plan = renderer.plan(arrays, jobs, scene_options=options)
+    launch = autotune.tune_launch([(plan.scenes[j.scene_index], j.spec) for j in plan.jobs], device=local)
+    renderer.block_size, renderer.chunk_rays = launch.block_size, launch.chunk_rays
+    t_tune = time.perf_counter() - t0
+    if not args.no_graph:
+        renderer.capture(plan)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        renderer.launch(plan)
+    torch.cuda.synchronize(device)
+    rb = renderer.ray_bounces(plan)
+    sampler = ClockSampler(local)
+    with sampler:
+        step_ms = _device_timed(lambda: renderer.launch(plan), args.steps, device, flush)
+    ms = float(np.mean(step_ms))
+    # plain drop-in loop: one trace launch + one synthesis + one host copy per job, scenes resident
+    order = list(range(len(jobs)))
+    if args.plain_jobs > 0:
+        order = list(np.random.default_rng(0).permutation(len(jobs))[:args.plain_jobs])
+    ws = runtime.SynthWorkspace(device)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    plain_rays = 0
+    for k in order:
+        j = jobs[k]
+        b = runtime.trace(plan.scenes[j.scene_index], j.spec)
+        d = torch.tensor([max(0.0, j.spec.direct_delay)], dtype=torch.float64, device=device)
+        p = runtime.synth_params(1, j.spec.num_bins, j.spec.bin_duration, j.fs, j.spec.speed_of_sound,
+                                 rng_mode="philox", seed=int(j.spec.seed) + 7, direct_delays=d)
+        runtime.synthesize(b.echogram[None].contiguous(), p, ws).cpu()
+        plain_rays += j.spec.num_rays
+    plain_s = time.perf_counter() - t0
+    plain_rirs_per_s = len(order) / plain_s
+    # end to end: host scene arrays in, host band IRs out
+    t0 = time.perf_counter()
+    plan_e = renderer.plan(arrays, jobs, scene_options=options)
+    renderer.launch(plan_e)
+    host = plan_e.ir_store.cpu()
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(s.device_bytes for s in plan_e.scenes)
+    d2h = host.numel() * 4
+    for s in plan_e.scenes:
+        s.close()
+    value = len(jobs) / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"mixed_batch: {args.scenes} scenes, 1-8 rooms, 1-4 sources x 1-8 channels, "
+                               "1e4-1e6 rays, fs 16 kHz, 1-2 s",
+                   "rirs_per_step": len(jobs), "rays_per_step": int(sum(j.spec.num_rays for j in jobs)),
+                   "graph": not args.no_graph, "l2": "flushed between timed steps (256 MiB write)",
+                   "traversal": {m: sum(1 for s in plan.scenes if s.traversal == m) for m in ("scan", "bvh")},
+                   "launch": {"block_size": launch.block_size, "chunk_rays": launch.chunk_rays}},
+        "ray_bounces_per_step": rb, "ray_bounces_per_s": rb / (ms / 1000.0),
+        "plain": {"rirs_per_s": plain_rirs_per_s, "jobs_timed": len(order), "seconds": plain_s,
+                  "note": "per job: ac_trace + ac_synthesize + copy to host, scenes resident"},
+        "batched_vs_plain": value / plain_rirs_per_s,
+        "e2e": {"value": len(jobs) / e2e_s, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "note": "scene upload + plan + launch + host copy, one pass"},
+        "setup_s": {"compile": t_compile, "tune": t_tune}, "gpu_launches": 6 * args.steps,
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serving(args) -> int:
+    """Continuous-batching server on a Poisson request stream over the mixed-size population.
+
+    Requests arrive at `--rate` per second for `--duration` seconds; 20 % move
+    their source along a seeded 3 m path with 8 keyframes.  Scenes are uploaded
+    and tuned before the stream starts (a warm, resident scene cache).
+    Latency = arrival to band IRs in host memory.
+    """
+    import torch
+    from acoustic_agent_b200 import serving, workloads
+    world, rank, local = _dist_setup()
+    if world > 1:
+        raise SystemExit("serving runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    population = workloads.mixed_batch(1730, 64)
+    stream = workloads.request_stream(1729, rate_hz=args.rate, duration_s=args.duration, population=population)
+    requests = serving.requests_from_stream(stream)
+    server = serving.Server(local, max_inflight=3)
+    t0 = time.perf_counter()
+    for w in population:   # warm the resident scene cache (upload + tune) before the clock starts
+        req = serving.Request(-1, w, [w.sources[0]])
+        server.scenes.acquire(w, serving.request_jobs(req)[0])
+        server.scenes.release(w)
+    warm_s = time.perf_counter() - t0
+    # warm-up: a short burst of the same mix (kernels, allocator, pinned pool)
+    server.serve(requests[: min(len(requests), 8)], realtime=False)
+    sampler = ClockSampler(local)
+    with sampler:
+        report = server.serve(requests, realtime=True)
+    server.close()
+    s = report.summary()
+    line = {
+        "metric": METRIC, "value": s["rirs_per_s"], "unit": "RIRs/s", "n_gpus": 1, "steps": len(requests),
+        "warmup": min(len(requests), 8), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, Poisson arrivals)",
+        "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s over 64 mixed scenes, "
+                               "20% moving sources x 8 keyframes", "requests": len(requests),
+                   "moving": sum(r.moving for r in requests), "max_inflight": server.max_inflight},
+        "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]},
+        "ray_bounces_per_s": s["ray_bounces_per_s"], "rirs": s["rirs"], "makespan_s": s["makespan_s"],
+        "batches": s["batches"], "max_inflight_seen": s["max_inflight"], "scene_cache": s["scene_cache"],
+        "offered_rirs_per_s": s["rirs"] / args.duration, "warm_cache_s": warm_s,
+        "e2e": {"value": s["rirs_per_s"], "unit": "RIRs/s", "note": "arrival to host band IRs"},
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
     return 0
 
 
