@@ -57,6 +57,10 @@ class Plan:
     synth_workspace: runtime.SynthBatchWorkspace
     graph: torch.cuda.CUDAGraph | None = None
     keepalive: list[Any] = field(default_factory=list)
+    # pipelined steps (launch_pipelined): a copy of the previous step's echograms and its synthesis jobs
+    echo_prev: torch.Tensor | None = None
+    synth_jobs_prev: Any = None
+    pipe_graph: torch.cuda.CUDAGraph | None = None
 
     @property
     def num_rirs(self) -> int:
@@ -167,6 +171,69 @@ class RIRRenderer:
             self._enqueue(plan, side)
         torch.cuda.current_stream(self.device).wait_stream(side)
         plan.graph = graph
+
+    # ---- pipelined steps: the trace of step k runs beside the synthesis of step k-1
+    def _pipe_setup(self, plan: Plan) -> None:
+        if plan.echo_prev is not None:
+            return
+        plan.echo_prev = torch.zeros_like(plan.echo_store)
+        synth, off = [], 0
+        for k, j in enumerate(plan.jobs):
+            bins = int(j.spec.num_bins)
+            view = plan.echo_prev[off:off + NUM_BANDS * bins].view(NUM_BANDS, bins)
+            off += NUM_BANDS * bins
+            synth.append(runtime.SynthJob(view, plan.irs[k], j.fs, j.spec.bin_duration, seed=int(j.spec.seed) + 7,
+                                          direct_delay=max(0.0, float(j.spec.direct_delay)),
+                                          speed_of_sound=j.spec.speed_of_sound))
+        plan.synth_jobs_prev = runtime.synth_job_array(synth, plan.synth_config)
+        plan.keepalive.append(synth)
+        plan.pipe_side = torch.cuda.Stream(self.device)  # type: ignore[attr-defined]
+        # private staged workspaces: the synthesis and the trace now run on different streams
+        plan.workspace = runtime.BatchWorkspace(self.device)
+        plan.synth_workspace = runtime.SynthBatchWorkspace(self.device)
+
+    def _enqueue_pipelined(self, plan: Plan, main: torch.cuda.Stream) -> None:
+        side: torch.cuda.Stream = plan.pipe_side  # type: ignore[attr-defined]
+        side.wait_stream(main)
+        copied = torch.cuda.Event()
+        with torch.cuda.stream(side):
+            plan.echo_prev.copy_(plan.echo_store)   # the previous step's echograms
+            copied.record(side)
+            runtime.synthesize_batch((plan.synth_jobs_prev, len(plan.jobs), plan.synth_config), plan.synth_workspace,
+                                     stream=side)
+        main.wait_event(copied)
+        with torch.cuda.stream(main):
+            runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
+                                plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
+                                chunk_rays=self.chunk_rays, stream=main)
+        main.wait_stream(side)
+
+    def launch_pipelined(self, plan: Plan) -> None:
+        """One pipelined step: trace every job while synthesising the echograms the previous step traced.
+
+        Every step does the full trace and the full synthesis; the band IRs in
+        `plan.irs` after a step belong to the echograms of the step before it
+        (after `launch`, or a first pipelined step, to that launch's trace).
+        """
+        self._pipe_setup(plan)
+        if plan.pipe_graph is not None:
+            plan.pipe_graph.replay()
+            return
+        self._enqueue_pipelined(plan, torch.cuda.current_stream(self.device))
+
+    def capture_pipelined(self, plan: Plan) -> None:
+        """Record one pipelined step as a CUDA graph (two streams forked and joined inside the graph)."""
+        self._pipe_setup(plan)
+        main = torch.cuda.Stream(self.device)
+        main.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(main):
+            self._enqueue_pipelined(plan, main)   # warm-up: sizes workspaces
+        main.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=main):
+            self._enqueue_pipelined(plan, main)
+        torch.cuda.current_stream(self.device).wait_stream(main)
+        plan.pipe_graph = graph
 
     def ray_bounces(self, plan: Plan) -> int:
         return int(sum(int(b.counters[2].item()) for b in plan.buffers))

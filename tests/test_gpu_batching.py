@@ -61,3 +61,27 @@ def test_graph_replay_equals_eager_launch(mix):
     graphed, _ = _render(batching, arrays, jobs, graph=True)
     for a, b in zip(eager, graphed):
         np.testing.assert_array_equal(a, b)
+
+
+def test_pipelined_steps_synthesise_the_previous_trace(mix):
+    """A pipelined step traces every job beside the synthesis of the previous step's echograms."""
+    batching, arrays, jobs = mix
+    renderer = batching.RIRRenderer(0)
+    plan = renderer.plan(arrays, jobs)
+    renderer.launch(plan)
+    torch.cuda.synchronize()
+    expected = renderer.results(plan)
+    plan.ir_store.fill_(float("nan"))
+    renderer.launch_pipelined(plan)          # eager: synthesises the echograms traced by launch()
+    torch.cuda.synchronize()
+    for a, b in zip(renderer.results(plan), expected):
+        np.testing.assert_array_equal(a, b)
+    renderer.capture_pipelined(plan)
+    plan.ir_store.fill_(float("nan"))
+    for _ in range(2):
+        renderer.launch_pipelined(plan)      # graph replays
+    torch.cuda.synchronize()
+    for a, b in zip(renderer.results(plan), expected):
+        np.testing.assert_array_equal(a, b)
+    for s in plan.scenes:
+        s.close()
