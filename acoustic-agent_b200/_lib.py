@@ -79,7 +79,8 @@ class ACTraceParams(ctypes.Structure):
         ("rng_mode", ctypes.c_int32), ("seed", ctypes.c_uint64), ("stream_key", ctypes.c_uint64),
         ("directions", ctypes.c_void_p), ("diffuse_random", ctypes.c_void_p), ("diffuse_indices", ctypes.c_void_p),
         ("diffuse_bank", ctypes.c_void_p), ("num_bank", ctypes.c_int32), ("block_size", ctypes.c_int32),
-        ("energy_scale", ctypes.c_double), ("grid_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("energy_scale", ctypes.c_double), ("grid_blocks", ctypes.c_int32), ("visual_limit", ctypes.c_int32),
+        ("visual_stride", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -89,6 +90,9 @@ class ACTraceOutputs(ctypes.Structure):
         ("contrib_counts", ctypes.c_void_p), ("surface_energy_fx", ctypes.c_void_p), ("counters", ctypes.c_void_p),
         ("echogram", ctypes.c_void_p), ("ambisonic", ctypes.c_void_p), ("surface_energy", ctypes.c_void_p),
         ("ray_surfaces", ctypes.c_void_p), ("scale_out", c_double_p),
+        ("visual_hit_points", ctypes.c_void_p), ("visual_surfaces", ctypes.c_void_p),
+        ("visual_rays", ctypes.c_void_p), ("visual_orders", ctypes.c_void_p),
+        ("visual_distances", ctypes.c_void_p), ("visual_gains", ctypes.c_void_p),
     ]
 
 

@@ -124,9 +124,9 @@ def trace_energy_field(scene: Any, source: np.ndarray, listener: np.ndarray, con
     src = np.asarray(source, dtype=float)
     lst = np.asarray(listener, dtype=float)
     direct_delay = float(np.linalg.norm(src - lst)) / float(config.c)
-    if getattr(config, "collect_visual_paths", False):
-        raise NotImplementedError("visual path candidates are not produced by the B200 backend yet; "
-                                  "set collect_visual_paths=False")
+    collect_visual = bool(getattr(config, "collect_visual_paths", False))
+    visual_limit, visual_stride = runtime.visual_candidate_layout(
+        num_rays, collect_visual, getattr(config, "rt_visual_num_rays", None), retain_limit=_VISUAL_RETAIN_LIMIT)
     mode = rng or _DEFAULT_RNG
     spec = runtime.TraceSpec(
         source=src, listener=lst, source_forward=source_forward(emitter), num_rays=num_rays,
@@ -137,14 +137,15 @@ def trace_energy_field(scene: Any, source: np.ndarray, listener: np.ndarray, con
         specular_exponent=float(config.rt_specular_exponent), dipole_weight=float(emitter["dipole_weight"]),
         dipole_power=float(emitter["dipole_power"]), use_bvh=intersection_backend == "bvh",
         render_ambisonics=bool(render_ambisonics), precision=precision, rng=mode, seed=int(config.seed),
-        stream_key=0,
+        stream_key=0, visual_limit=visual_limit, visual_stride=visual_stride,
     )
     transfer_started = time.perf_counter()
     hits_before, misses_before = runtime.STREAMS.hits, runtime.STREAMS.misses
     device_scene, scene_hit = SCENES.get(arrays, device_id)
     stream = torch.cuda.current_stream(device)
     buffers = runtime.TraceBuffers.allocate(device_scene.num_surfaces, num_bins, device,
-                                            ambisonics=bool(render_ambisonics))
+                                            ambisonics=bool(render_ambisonics),
+                                            visual=(visual_limit, num_bounces, spec.dtype) if visual_limit else None)
     if mode == "reference":
         runtime.reference_stream(spec, device)
     runtime.diffuse_bank(spec.dtype, device)
@@ -173,7 +174,7 @@ def trace_energy_field(scene: Any, source: np.ndarray, listener: np.ndarray, con
         "surface_hit_count": field["surface_hit_count"],
         "surface_contribution_count": field["surface_contribution_count"],
         "surface_energy": field["surface_energy"],
-        "visual_candidates": None,
+        "visual_candidates": field.get("visual_candidates") if collect_visual else None,
         "accelerator": ACCELERATOR_NAME,
         "precision": precision,
         "cuda": {k: v for k, v in runtime.device_info(device_id).items() if k != "sm_count"},

@@ -79,6 +79,11 @@ int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_t
         return fail(AC_ERR_INVALID, "render_ambisonics needs the ambisonic accumulator");
     if (p->energy_scale < 0.0 || !std::isfinite(p->energy_scale))
         return fail(AC_ERR_INVALID, "energy_scale must be zero (automatic) or positive");
+    if (p->visual_limit < 0 || (p->visual_limit > 0 && p->visual_stride < 1))
+        return fail(AC_ERR_INVALID, "visual_limit must be >= 0 and visual_stride >= 1 when candidates are recorded");
+    if (p->visual_limit > 0 && (!o->visual_hit_points || !o->visual_surfaces || !o->visual_rays || !o->visual_orders ||
+                                !o->visual_distances || !o->visual_gains))
+        return fail(AC_ERR_INVALID, "visual_limit > 0 needs every visual-candidate output");
     // Each ray deposits at most once per bounce: fewer than 2^32 quanta per accumulator.
     if (static_cast<double>(p->num_rays) * static_cast<double>(std::max<int32_t>(1, p->num_bounces)) >= 4294967296.0)
         return fail(AC_ERR_CAPACITY, "num_rays * num_bounces must stay below 2^32; split the rays over several jobs");
@@ -112,8 +117,9 @@ std::vector<Partition> partition_jobs(const ac_job *jobs, int32_t count) {
     std::vector<Partition> parts;
     for (int32_t j = 0; j < count; ++j) {
         const bool fp64 = jobs[j].params.precision == AC_PRECISION_FP64;
-        const int key = fp64 ? 4 : ((jobs[j].params.rng_mode == AC_RNG_PHILOX ? 2 : 0) |
-                                    (jobs[j].params.render_ambisonics ? 1 : 0));
+        const int key = fp64 ? 8 : ((jobs[j].params.rng_mode == AC_RNG_PHILOX ? 2 : 0) |
+                                    (jobs[j].params.render_ambisonics ? 1 : 0) |
+                                    (jobs[j].params.visual_limit > 0 ? 4 : 0));
         Partition *found = nullptr;
         for (Partition &p : parts)
             if (p.key == key) found = &p;
@@ -180,7 +186,7 @@ int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch
     return AC_OK;
 }
 
-// Jobs run in one launch per (precision, random stream, ambisonics) partition;
+// Jobs run in one launch per (precision, random stream, ambisonics, visual candidates) partition;
 // each partition has its own region of the workspace, so the launches are
 // simply enqueued one after another on the stream.
 int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,

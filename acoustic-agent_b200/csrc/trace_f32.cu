@@ -13,10 +13,16 @@ constexpr int kDefaultChunkRays = 32;
 
 using FastKernel = void (*)(const Job<float>, const FastScene, const FastTable);
 
+template <bool kSingle, bool kVisual>
+FastKernel pick_variant(bool philox, bool amb) {
+    if (philox)
+        return amb ? trace_fast_kernel<kSingle, true, true, kVisual> : trace_fast_kernel<kSingle, true, false, kVisual>;
+    return amb ? trace_fast_kernel<kSingle, false, true, kVisual> : trace_fast_kernel<kSingle, false, false, kVisual>;
+}
+
 template <bool kSingle>
-FastKernel pick_kernel(bool philox, bool amb) {
-    if (philox) return amb ? trace_fast_kernel<kSingle, true, true> : trace_fast_kernel<kSingle, true, false>;
-    return amb ? trace_fast_kernel<kSingle, false, true> : trace_fast_kernel<kSingle, false, false>;
+FastKernel pick_kernel(bool philox, bool amb, bool visual) {
+    return visual ? pick_variant<kSingle, true>(philox, amb) : pick_variant<kSingle, false>(philox, amb);
 }
 
 int fast_grid(FastKernel kernel, int device, int block, int64_t total_rays, int requested) {
@@ -86,12 +92,19 @@ int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac
     AC_CUDA_TRY(cudaMemsetAsync(o->contrib_counts, 0, ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->surface_energy_fx, 0, 2 * ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->counters, 0, 8 * sizeof(int64_t), stream));
+    if (job.visual_limit > 0) {
+        const size_t cells = 3 * static_cast<size_t>(job.visual_limit) * job.num_bounces;
+        init_visual_single_kernel<float><<<static_cast<int>(std::min<size_t>((cells + 255) / 256, 1024)), 256, 0,
+                                           stream>>>(job);
+        AC_CUDA_TRY(cudaGetLastError());
+    }
     const int block = p->block_size > 0 ? p->block_size : kDefaultBlock;
     if (block % 32 != 0 || block > 256) return fail(AC_ERR_INVALID, "block_size must be a multiple of 32 up to 256");
     FastTable table{};
     table.chunk_rays = kDefaultChunkRays;
     table.chunk_counter = reinterpret_cast<unsigned long long *>(o->counters) + 4;
-    const FastKernel kernel = pick_kernel<true>(p->rng_mode == AC_RNG_PHILOX, p->render_ambisonics != 0);
+    const FastKernel kernel = pick_kernel<true>(p->rng_mode == AC_RNG_PHILOX, p->render_ambisonics != 0,
+                                                p->visual_limit > 0);
     const int grid = fast_grid(kernel, scene->device, block, p->num_rays, p->grid_blocks);
     kernel<<<grid, block, 0, stream>>>(job, scene->fast, table);
     AC_CUDA_TRY(cudaGetLastError());
@@ -149,8 +162,10 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         double scale = in.params.energy_scale;
         if (!(scale > 0.0)) scale = choose_energy_scale(in.scene, &in.params);
         fill_job<float>(in.scene, &in.params, &in.outputs, scale, jobs[k]);
-        if (k > 0 && (jobs[k].rng_mode != jobs[0].rng_mode || jobs[k].render_ambisonics != jobs[0].render_ambisonics))
-            return fail(AC_ERR_INVALID, "one float32 launch needs one random-stream mode and ambisonics setting");
+        if (k > 0 && (jobs[k].rng_mode != jobs[0].rng_mode || jobs[k].render_ambisonics != jobs[0].render_ambisonics ||
+                      (jobs[k].visual_limit > 0) != (jobs[0].visual_limit > 0)))
+            return fail(AC_ERR_INVALID,
+                        "one float32 launch needs one random-stream mode, ambisonics and visual-candidate setting");
         if (in.outputs.scale_out) *in.outputs.scale_out = scale;
         prefix[k] = total;
         jobs[k].ray_begin = total;
@@ -187,7 +202,8 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         std::memset(&unused, 0, sizeof(unused));
         FastScene none{};
         // ac_trace_batch partitions jobs so that one launch has one kernel variant.
-        const FastKernel kernel = pick_kernel<false>(jobs[0].rng_mode == AC_RNG_PHILOX, jobs[0].render_ambisonics != 0);
+        const FastKernel kernel = pick_kernel<false>(jobs[0].rng_mode == AC_RNG_PHILOX, jobs[0].render_ambisonics != 0,
+                                                     jobs[0].visual_limit > 0);
         const int grid = fast_grid(kernel, device, block, total, cfg ? cfg->grid_blocks : 0);
         kernel<<<grid, block, 0, stream>>>(unused, none, table);
         AC_CUDA_TRY(cudaGetLastError());

@@ -1,5 +1,9 @@
 // Float32 production tracer for sm_100a: warp-uniform scene scan.
 //
+// Specialised at compile time on (single job, Philox stream, ambisonics,
+// visual-path candidates), so no variant carries the state or the branches
+// of an option it does not use.
+//
 // Same per-ray algorithm as trace_kernel.cuh (steam_rt.py:4708-4850), but the
 // intersection queries are organised for SIMT instead of restating the
 // reference's per-thread escape-link walk.  A warp always works on ONE scene;
@@ -416,6 +420,7 @@ struct FastLane {
     int bounce;
     int queries;
     int shadows;
+    int vslot;    // visual-candidate slot, -1 for none
 };
 
 __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int hi, int64_t g) {
@@ -426,7 +431,7 @@ __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int
     return lo;
 }
 
-template <bool kSingle, bool kPhilox, bool kAmb>
+template <bool kSingle, bool kPhilox, bool kAmb, bool kVisual>
 __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(const __grid_constant__ Job<float> single,
                                                          const __grid_constant__ FastScene single_fast,
                                                          const __grid_constant__ FastTable table) {
@@ -494,6 +499,10 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 s.queries = 0;
                 s.shadows = 0;
                 s.path = 0.0;
+                if (kVisual) {
+                    s.vslot = visual_slot(job, ri);
+                    if (s.vslot >= 0) job.visual_rays[s.vslot] = static_cast<int32_t>(ri);
+                }
                 s.o[0] = job.lst[0]; s.o[1] = job.lst[1]; s.o[2] = job.lst[2];
                 if (kPhilox) {
                     const double3 v = philox_direction(job.seed, job.stream_key, job.num_rays, ri);
@@ -588,6 +597,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     hx = s.o[0] + t * s.d[0] + 1e-2f * n[0];
                     hy = s.o[1] + t * s.d[1] + 1e-2f * n[1];
                     hz = s.o[2] + t * s.d[2] + 1e-2f * n[2];
+                    if (kVisual && s.vslot >= 0) visual_hit(job, s.vslot, s.bounce, hx, hy, hz, surf);
                     const float tsx = job.src[0] - hx, tsy = job.src[1] - hy, tsz = job.src[2] - hz;
                     const float d2 = tsx * tsx + tsy * tsy + tsz * tsz;
                     const float inv = rsqrtf(fmaxf(d2, 1e-30f));
@@ -641,9 +651,11 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                         const int bin = static_cast<int>(q);
                         const float common = job.ray_scale * source_gain * distance_term * (diffuse + specular);
                         long long esum = 0;
+                        float energy_sum = 0.0f;
 #pragma unroll
                         for (int b = 0; b < kBands; ++b) {
                             const float e = common * refl[b] * s.acc[b];
+                            if (kVisual) energy_sum += e;
                             const long long qe = quantize(e, job.energy_scale);
                             add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
                             if (kAmb) {
@@ -660,6 +672,10 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                         }
                         atomicAdd(job.contrib_counts + surf, 1ull);
                         add_fixed(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
+                        if (kVisual && s.vslot >= 0)
+                            visual_contribution(job, s.vslot, s.bounce, energy_sum,
+                                                static_cast<float>(s.path + static_cast<double>(t) +
+                                                                   static_cast<double>(dist)));
                     }
                 }
             }

@@ -142,7 +142,46 @@ struct Job {
     unsigned long long *surface_energy_fx; // [S,2]
     unsigned long long *counters;      // [8]
     int32_t *ray_surfaces;             // [R,B] or null
+    // visual-path candidates (steam_rt.py:4718-4731): slot = ray / stride for rays with ray % stride == 0
+    int32_t visual_limit;              // 0: none
+    int32_t visual_stride;
+    T *visual_hit_points;              // [L,B,3]
+    int32_t *visual_surfaces;          // [L,B]
+    int32_t *visual_rays;              // [L]
+    int32_t *visual_orders;            // [L]
+    T *visual_distances;               // [L]
+    T *visual_gains;                   // [L]
 };
+
+// Visual slot of a ray, -1 for none (steam_rt.py:4726-4731).
+template <typename T>
+__device__ __forceinline__ int visual_slot(const Job<T> &job, int64_t ray) {
+    if (job.visual_limit <= 0 || ray % job.visual_stride != 0) return -1;
+    const int64_t slot = ray / job.visual_stride;
+    return slot < job.visual_limit ? static_cast<int>(slot) : -1;
+}
+
+// A hit of a candidate ray (steam_rt.py:4765-4769).
+template <typename T>
+__device__ __forceinline__ void visual_hit(const Job<T> &job, int slot, int bounce, T hx, T hy, T hz, int surf) {
+    const size_t k = static_cast<size_t>(slot) * job.num_bounces + bounce;
+    job.visual_hit_points[3 * k] = hx;
+    job.visual_hit_points[3 * k + 1] = hy;
+    job.visual_hit_points[3 * k + 2] = hz;
+    job.visual_surfaces[k] = surf;
+}
+
+// The strongest contribution of a candidate ray so far (steam_rt.py:4821-4824).
+template <typename T>
+__device__ __forceinline__ void visual_contribution(const Job<T> &job, int slot, int bounce, T energy_sum,
+                                                    T distance) {
+    const T g = job.visual_gains[slot];
+    if (energy_sum > g * g) {
+        job.visual_orders[slot] = bounce + 1;
+        job.visual_distances[slot] = distance;
+        job.visual_gains[slot] = sqrt(energy_sum > T(0) ? energy_sum : T(0));
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Intersection routines (steam_rt.py:4259-4426)
@@ -503,6 +542,7 @@ struct Lane {
     int bounce;
     int queries;
     int shadows;
+    int vslot;   // visual-candidate slot, -1 for none
 };
 
 template <typename T, bool kSingle>
@@ -544,6 +584,8 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                     s.queries = 0;
                     s.shadows = 0;
                     s.path = 0.0;
+                    s.vslot = visual_slot(job, ri);
+                    if (s.vslot >= 0) job.visual_rays[s.vslot] = static_cast<int32_t>(ri);
                     s.o[0] = job.lst[0]; s.o[1] = job.lst[1]; s.o[2] = job.lst[2];
                     initial_direction(job, ri, s.d);
                     s.d0[0] = s.d[0]; s.d0[1] = s.d[1]; s.d0[2] = s.d[2];
@@ -590,6 +632,7 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                 const T hx = s.o[0] + t * s.d[0] + T(1e-2) * n[0];
                 const T hy = s.o[1] + t * s.d[1] + T(1e-2) * n[1];
                 const T hz = s.o[2] + t * s.d[2] + T(1e-2) * n[2];
+                if (s.vslot >= 0) visual_hit(job, s.vslot, s.bounce, hx, hy, hz, surf);
                 const T tsx = job.src[0] - hx, tsy = job.src[1] - hy, tsz = job.src[2] - hz;
                 const T dist = sqrt(tsx * tsx + tsy * tsy + tsz * tsz);
                 const Quad<T> m0 = ldq(sc.mats + static_cast<size_t>(surf) * kMatStride);
@@ -626,9 +669,11 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                                 const int bin = static_cast<int>(q);
                                 const T common = job.ray_scale * source_gain * distance_term * (diffuse + specular);
                                 long long esum = 0;
+                                T energy_sum = T(0);
 #pragma unroll
                                 for (int b = 0; b < kBands; ++b) {
                                     const T e = common * refl[b] * s.acc[b];
+                                    energy_sum += e;
                                     const long long qe = quantize(e, job.energy_scale);
                                     add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
                                     if (job.ambisonic_fx) {
@@ -644,6 +689,10 @@ __global__ void __launch_bounds__(256) trace_kernel(const __grid_constant__ Job<
                                 }
                                 atomicAdd(job.contrib_counts + surf, 1ull);
                                 add_fixed(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
+                                if (s.vslot >= 0)
+                                    visual_contribution(job, s.vslot, s.bounce, energy_sum,
+                                                        static_cast<T>((s.path + static_cast<double>(t)) +
+                                                                       static_cast<double>(dist)));
                             }
                         }
                     }

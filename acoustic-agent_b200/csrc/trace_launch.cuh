@@ -16,6 +16,21 @@ namespace ac {
 
 constexpr int kDefaultBlock = 256;
 
+// Reference initial values of the visual-candidate arrays (steam_rt.py:4718-4723).
+template <typename T>
+__device__ __forceinline__ void init_visual(const Job<T> &job, size_t first, size_t step) {
+    if (job.visual_limit <= 0) return;
+    const size_t L = static_cast<size_t>(job.visual_limit), LB = L * static_cast<size_t>(job.num_bounces);
+    for (size_t i = first; i < 3 * LB; i += step) job.visual_hit_points[i] = T(0);
+    for (size_t i = first; i < LB; i += step) job.visual_surfaces[i] = -1;
+    for (size_t i = first; i < L; i += step) {
+        job.visual_rays[i] = -1;
+        job.visual_orders[i] = 0;
+        job.visual_distances[i] = T(0);
+        job.visual_gains[i] = T(0);
+    }
+}
+
 // Zero every job's accumulators and the work counter (one launch for all jobs).
 template <typename T>
 __global__ void zero_outputs_kernel(const Job<T> *jobs, int num_jobs, unsigned long long *work_counter) {
@@ -35,7 +50,14 @@ __global__ void zero_outputs_kernel(const Job<T> *jobs, int num_jobs, unsigned l
             else if (i < nb + na + 4 * ns) job.surface_energy_fx[i - nb - na - 2 * ns] = 0ull;
             else job.counters[i - nb - na - 4 * ns] = 0ull;
         }
+        init_visual(job, blockIdx.x * blockDim.x + threadIdx.x, static_cast<size_t>(gridDim.x) * blockDim.x);
     }
+}
+
+template <typename T>
+__global__ void init_visual_single_kernel(const __grid_constant__ Job<T> job) {
+    init_visual(job, blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x,
+                static_cast<size_t>(gridDim.x) * blockDim.x);
 }
 
 struct FinalizeTargets {
@@ -124,6 +146,16 @@ inline void fill_job(const ac_scene_s *scene, const ac_trace_params *p, const ac
     job.surface_energy_fx = reinterpret_cast<unsigned long long *>(o->surface_energy_fx);
     job.counters = reinterpret_cast<unsigned long long *>(o->counters);
     job.ray_surfaces = o->ray_surfaces;
+    if (p->visual_limit > 0) {
+        job.visual_limit = p->visual_limit;
+        job.visual_stride = p->visual_stride;
+        job.visual_hit_points = static_cast<T *>(o->visual_hit_points);
+        job.visual_surfaces = o->visual_surfaces;
+        job.visual_rays = o->visual_rays;
+        job.visual_orders = o->visual_orders;
+        job.visual_distances = static_cast<T *>(o->visual_distances);
+        job.visual_gains = static_cast<T *>(o->visual_gains);
+    }
 }
 
 template <typename T, bool kSingle>
@@ -155,6 +187,12 @@ inline int launch_single(const ac_scene_s *scene, const ac_trace_params *p, cons
     AC_CUDA_TRY(cudaMemsetAsync(o->contrib_counts, 0, ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->surface_energy_fx, 0, 2 * ns, stream));
     AC_CUDA_TRY(cudaMemsetAsync(o->counters, 0, 8 * sizeof(int64_t), stream));
+    if (job.visual_limit > 0) {
+        const size_t cells = 3 * static_cast<size_t>(job.visual_limit) * job.num_bounces;
+        init_visual_single_kernel<T><<<static_cast<int>(std::min<size_t>((cells + 255) / 256, 1024)), 256, 0,
+                                       stream>>>(job);
+        AC_CUDA_TRY(cudaGetLastError());
+    }
     const int block = p->block_size > 0 ? p->block_size : kDefaultBlock;
     if (block % 32 != 0 || block > 256) return fail(AC_ERR_INVALID, "block_size must be a multiple of 32 up to 256");
     if (p->num_rays > 0) {

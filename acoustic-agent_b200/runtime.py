@@ -155,6 +155,8 @@ class TraceSpec:
     energy_scale: float = 0.0
     block_size: int = 0
     grid_blocks: int = 0
+    visual_limit: int = 0      # visual-path candidate slots (0: none)
+    visual_stride: int = 1
 
     @property
     def dtype(self) -> torch.dtype:
@@ -228,13 +230,26 @@ class TraceBuffers:
     ambisonic: torch.Tensor | None = None
     ray_surfaces: torch.Tensor | None = None
     scale: ctypes.c_double = field(default_factory=lambda: ctypes.c_double(0.0))
+    visual: dict[str, torch.Tensor] | None = None   # visual-path candidate arrays (allocate(visual=...))
 
     @classmethod
     def allocate(cls, num_surfaces: int, num_bins: int, device: torch.device, *, ambisonics: bool = False,
-                 record_rays: tuple[int, int] | None = None, echogram: bool = True) -> "TraceBuffers":
-        """Zeroed device outputs; echogram=False leaves `echogram` for the caller to point at its own storage."""
+                 record_rays: tuple[int, int] | None = None, echogram: bool = True,
+                 visual: tuple[int, int, torch.dtype] | None = None) -> "TraceBuffers":
+        """Zeroed device outputs; echogram=False leaves `echogram` for the caller to point at its own storage.
+
+        visual=(limit, bounces, dtype) adds the visual-candidate arrays (the trace initialises them).
+        """
         z64 = lambda *shape: torch.zeros(*shape, dtype=torch.int64, device=device)
-        return cls(
+        vis = None
+        if visual is not None and visual[0] > 0:
+            limit, bounces, dtype = visual
+            e = lambda *shape, dt: torch.empty(*shape, dtype=dt, device=device)  # noqa: E731
+            vis = {"hit_points": e(limit, max(1, bounces), 3, dt=dtype),
+                   "surface_indices": e(limit, max(1, bounces), dt=torch.int32),
+                   "ray_indices": e(limit, dt=torch.int32), "orders": e(limit, dt=torch.int32),
+                   "distances": e(limit, dt=dtype), "gains": e(limit, dt=dtype)}
+        return cls(visual=vis, **dict(
             echogram_fx=z64(NUM_BANDS, num_bins, 2), hit_counts=z64(num_surfaces), contrib_counts=z64(num_surfaces),
             surface_energy_fx=z64(num_surfaces, 2), counters=z64(8),
             echogram=(torch.zeros(NUM_BANDS, num_bins, dtype=torch.float32, device=device) if echogram
@@ -244,7 +259,7 @@ class TraceBuffers:
             ambisonic=torch.zeros(NUM_BANDS, 4, num_bins, dtype=torch.float32, device=device) if ambisonics else None,
             ray_surfaces=(torch.empty(record_rays[0], record_rays[1], dtype=torch.int32, device=device)
                           if record_rays else None),
-        )
+        ))
 
     def outputs_struct(self) -> _lib.ACTraceOutputs:
         o = _lib.ACTraceOutputs()
@@ -259,6 +274,13 @@ class TraceBuffers:
         o.surface_energy = self.surface_energy.data_ptr()
         o.ray_surfaces = self.ray_surfaces.data_ptr() if self.ray_surfaces is not None else None
         o.scale_out = ctypes.pointer(self.scale)
+        if self.visual is not None:
+            o.visual_hit_points = self.visual["hit_points"].data_ptr()
+            o.visual_surfaces = self.visual["surface_indices"].data_ptr()
+            o.visual_rays = self.visual["ray_indices"].data_ptr()
+            o.visual_orders = self.visual["orders"].data_ptr()
+            o.visual_distances = self.visual["distances"].data_ptr()
+            o.visual_gains = self.visual["gains"].data_ptr()
         return o
 
 
@@ -306,6 +328,8 @@ def params_struct(spec: TraceSpec, device: torch.device,
     p.energy_scale = float(spec.energy_scale)
     p.block_size = int(spec.block_size)
     p.grid_blocks = int(spec.grid_blocks)
+    p.visual_limit = int(spec.visual_limit)
+    p.visual_stride = int(spec.visual_stride)
     return p
 
 
@@ -429,7 +453,25 @@ def host_field(buffers: TraceBuffers, names: Sequence[str], spec: TraceSpec) -> 
     }
     if buffers.ray_surfaces is not None:
         out["ray_surfaces"] = buffers.ray_surfaces.cpu().numpy()
+    if buffers.visual is not None and spec.visual_limit > 0:
+        vis = {k: v.cpu().numpy() for k, v in buffers.visual.items()}
+        if spec.num_bounces < 1:   # [L, 0, ...] like the reference when there are no bounces
+            vis["hit_points"] = vis["hit_points"][:, :0]
+            vis["surface_indices"] = vis["surface_indices"][:, :0]
+        vis.update({"surface_names": tuple(names), "candidate_limit": int(spec.visual_limit),
+                    "stride": int(spec.visual_stride)})
+        out["visual_candidates"] = vis
     return out
+
+
+def visual_candidate_layout(num_rays: int, collect: bool, visual_num_rays: int | None = None,
+                            retain_limit: int = 512) -> tuple[int, int]:
+    """(limit, stride) of the visual-candidate slots, as steam_rt.py:1853-1860 sets them."""
+    default = int(retain_limit * 4)
+    requested = default if visual_num_rays is None else max(1, min(int(visual_num_rays), default))
+    limit = min(int(num_rays), requested) if collect else 0
+    stride = max(1, int(num_rays) // max(limit, 1))
+    return limit, stride
 
 
 # ---------------------------------------------------------------------------

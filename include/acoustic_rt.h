@@ -156,6 +156,12 @@ typedef struct ac_trace_params {
     int32_t block_size;          /* 0: library default */
     double energy_scale;         /* fixed-point scale (a power of two); 0: library picks (ac_energy_scale) */
     int32_t grid_blocks;         /* 0: library default (persistent, SM-count based) */
+    /* Visual-path candidates (steam_rt.py:1853-1860, kernel :4718-4731, :4765-4769,
+     * :4821-4824): rays with ray % visual_stride == 0 and ray / visual_stride <
+     * visual_limit record their hit points and their strongest contribution.
+     * visual_limit = 0: none. */
+    int32_t visual_limit;
+    int32_t visual_stride;
     int32_t reserved;
 } ac_trace_params;
 
@@ -182,6 +188,15 @@ typedef struct ac_trace_outputs {
     float *surface_energy;       /* [S] optional */
     int32_t *ray_surfaces;       /* [R,B] optional per-ray hit surface per bounce, -1 after termination */
     double *scale_out;           /* optional host pointer: receives the fixed-point scale used */
+    /* Visual-path candidates, required when visual_limit > 0 (L = visual_limit,
+     * B = num_bounces; element type float for FP32, double for FP64); the call
+     * initialises them like the reference (0, and -1 for the index arrays). */
+    void *visual_hit_points;     /* [L,B,3] offset hit point of each bounce */
+    int32_t *visual_surfaces;    /* [L,B] hit surface of each bounce */
+    int32_t *visual_rays;        /* [L] ray index of the slot */
+    int32_t *visual_orders;      /* [L] bounce + 1 of the strongest contribution */
+    void *visual_distances;      /* [L] its path length */
+    void *visual_gains;          /* [L] sqrt of its six-band energy */
 } ac_trace_outputs;
 
 /* One job of a batched launch: a scene, its trace parameters and outputs. */

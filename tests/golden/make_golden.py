@@ -85,6 +85,8 @@ def reference_arrays(steam_rt, models, spec):
     return scene, arrays
 
 
+VISUAL_POINT_RAYS = 64
+
 ARRAY_KEYS = ("kinds", "wall_a", "wall_delta", "wall_z", "z_values", "box_center", "box_axis_u", "box_axis_v",
               "box_half", "box_z", "normals", "reflection", "scattering", "corners", "surface_bounds_min",
               "surface_bounds_max", "bvh_bounds_min", "bvh_bounds_max", "bvh_start", "bvh_count", "bvh_escape",
@@ -115,11 +117,16 @@ def run_trace(steam_rt, directivity, arrays, trace):
         arrays["reflection"], arrays["scattering"], arrays["corners"], float(arrays["height"]), B, num_bins,
         bin_dur, c, duration * c, direct_delay, 0.1, 0.1, 1.0, 100.0, np.asarray(forward, dtype=float),
         float(emitter["dipole_weight"]), float(emitter["dipole_power"]), R, 1, bool(trace.get("ambisonics", False)))
-    (echogram, ambisonic, hits, contrib, energy, actual, active, _vhp, vsurf, _vray, _vord, _vdist, _vgain) = res
+    (echogram, ambisonic, hits, contrib, energy, actual, active, vhp, vsurf, vray, vord, vdist, vgain) = res
     return {
         "echogram": echogram, "ambisonic": ambisonic, "hit_counts": hits, "contrib_counts": contrib,
         "surface_energy": energy, "actual_bounces": int(actual), "active_ray_count": int(active),
         "ray_surfaces": vsurf.astype(np.int16), "num_bins": num_bins, "direct_delay": direct_delay,
+        # visual-candidate slots with one slot per ray: every ray's strongest contribution, and
+        # the hit points of the first VISUAL_POINT_RAYS rays
+        "visual_rays": vray.astype(np.int32), "visual_orders": vord.astype(np.int32),
+        "visual_distances": vdist, "visual_gains": vgain,
+        "visual_hit_points": vhp[:VISUAL_POINT_RAYS],
         "source_forward": np.asarray(forward), "dipole_weight": float(emitter["dipole_weight"]),
         "dipole_power": float(emitter["dipole_power"]),
     }

@@ -368,3 +368,63 @@ def test_fp32_bvh_leaf_sizes_agree(rt, leaf):
         got.append(buffers.echogram_fx.cpu().numpy())
         scene.close()
     np.testing.assert_array_equal(got[0], got[1])
+
+
+@pytest.mark.parametrize("name", TRACE_CASES)
+def test_fp64_visual_candidates_equal_reference(rt, name):
+    """Visual-path candidate slots (one per ray) against the reference kernel's own slots.
+
+    Ray indices, per-bounce surfaces, strongest-contribution bounce and hit
+    points are identical; path lengths and gains agree to rounding (the gain
+    carries the float64 pow of the specular and directivity terms).
+    """
+    case = load_case(name)
+    tr = case["trace"]
+    R, B = max(1, tr["rays"]), tr["bounces"]
+    spec = spec_for(rt, case, "float64", visual_limit=R, visual_stride=1)
+    dev = torch.device("cuda", 0)
+    scene = rt.DeviceScene(case["arrays"])
+    buffers = rt.TraceBuffers.allocate(scene.num_surfaces, int(case["num_bins"]), dev,
+                                       ambisonics=spec.render_ambisonics, visual=(R, B, torch.float64))
+    rt.trace(scene, spec, buffers)
+    torch.cuda.synchronize()
+    v = {k: t.cpu().numpy() for k, t in buffers.visual.items()}
+    scene.close()
+    np.testing.assert_array_equal(v["ray_indices"], case["visual_rays"])
+    np.testing.assert_array_equal(v["surface_indices"], case["ray_surfaces"])
+    np.testing.assert_array_equal(v["orders"], case["visual_orders"])
+    np.testing.assert_allclose(v["distances"], case["visual_distances"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(v["gains"], case["visual_gains"], rtol=1e-9, atol=0)
+    n = case["visual_hit_points"].shape[0]
+    np.testing.assert_array_equal(v["hit_points"][:n], case["visual_hit_points"])
+
+
+def test_fp32_visual_candidates_follow_the_reference_layout(rt):
+    """Float32 drop-in with collect_visual_paths=True: slot layout, dtypes and agreement with the float64 slots."""
+    from dataclasses import replace
+    from acoustic_agent_b200 import backend
+    from acoustic_agent_b200.workloads import TraceConfig
+    case = load_case("u_furnished_bvh")
+    tr = case["trace"]
+    cfg = TraceConfig(duration_s=tr["duration"], rt_duration_s=tr["duration"], rt_num_rays=tr["rays"],
+                      rt_num_bounces=tr["bounces"], rt_bin_duration_s=tr["bin_dur"], seed=tr["seed"],
+                      intersection_backend="bvh", rt_precision="float32")
+    cfg = replace(cfg, collect_visual_paths=True)
+    field = backend.trace_energy_field(case["arrays"], np.asarray(tr["source"]), np.asarray(tr["listener"]), cfg,
+                                       source_model=tr.get("source_model"), render_ambisonics=False,
+                                       rng="reference")
+    vc = field["visual_candidates"]
+    R, B = tr["rays"], tr["bounces"]
+    L = min(R, 2048)
+    assert vc["candidate_limit"] == L and vc["stride"] == max(1, R // L)
+    assert vc["hit_points"].shape == (L, B, 3) and vc["hit_points"].dtype == np.float32
+    assert vc["surface_indices"].shape == (L, B) and vc["orders"].shape == (L,)
+    np.testing.assert_array_equal(vc["ray_indices"], np.arange(L) * vc["stride"])
+    rays = vc["ray_indices"]
+    same_path = np.all(vc["surface_indices"] == case["ray_surfaces"][rays], axis=1)
+    assert same_path.mean() > 0.7
+    # float32 energies: the strongest bounce can flip only at near-equal contributions
+    same_order = vc["orders"] == case["visual_orders"][rays]
+    assert same_order[same_path].mean() >= 0.99
+    both = same_path & same_order
+    np.testing.assert_allclose(vc["gains"][both], case["visual_gains"][rays][both], rtol=2e-3)
