@@ -208,9 +208,11 @@ def reference_stream(spec: TraceSpec, device: torch.device) -> tuple[torch.Tenso
     def build():
         directions = rng.sphere_samples(spec.num_rays, spec.seed)
         random_values, indices = rng.diffuse_random_sequence(spec.num_rays, spec.num_bounces, NUM_BANK, spec.seed)
-        return (torch.as_tensor(directions, dtype=spec.dtype, device=device),
-                torch.as_tensor(random_values, dtype=spec.dtype, device=device),
-                torch.as_tensor(np.ascontiguousarray(indices), dtype=torch.int32, device=device))
+        # numpy may hand out read-only views; torch wants writable host memory to copy from
+        host = [np.array(a, copy=True) for a in (directions, random_values, indices)]
+        return (torch.as_tensor(host[0], dtype=spec.dtype, device=device),
+                torch.as_tensor(host[1], dtype=spec.dtype, device=device),
+                torch.as_tensor(host[2], dtype=torch.int32, device=device))
 
     return STREAMS.get(key, build)
 

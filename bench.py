@@ -113,6 +113,19 @@ class ClockSampler:
                 "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
 
 
+def replica_throughput(ms_per_step: float, rirs_per_step: int, dist=None, device=None) -> tuple[float, float]:
+    """Whole-job throughput of independent replicas: every rank ran the same step count on its own
+    jobs; the job took as long as the slowest rank (MAX over ranks), and the RIRs of all ranks count."""
+    world = 1
+    if dist is not None and dist.is_initialized():
+        import torch
+        world = dist.get_world_size()
+        t = torch.tensor([ms_per_step], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+    return ms_per_step, world * rirs_per_step / (ms_per_step / 1000.0)
+
+
 def _dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -408,12 +421,8 @@ def main() -> int:
     barrier()
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
     ms_per_step = float(np.mean(step_ms))
-    if dist is not None:
-        t = torch.tensor([ms_per_step], dtype=torch.float64, device=device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_per_step = float(t.item())
     rirs_per_step = plan.num_rirs
-    value = world * rirs_per_step / (ms_per_step / 1000.0)
+    ms_per_step, value = replica_throughput(ms_per_step, rirs_per_step, dist, device)
 
     # Tracer kernel alone (for the roofline): eager trace_batch launches timed with events.
     trace_ms = []
