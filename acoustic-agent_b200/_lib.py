@@ -161,6 +161,14 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_synthesize_batch": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
                                            ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_synthesize_batch_raw": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
+                                               ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
+                                               ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_synthesize_batch_filter": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
+                                                  ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p,
+                                                  ctypes.c_size_t, ctypes.c_void_p]),
+    "ac_read_bandwidth_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
     "ac_synthesize_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
                                             ctypes.c_void_p]),
     "ac_philox_workspace": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,

@@ -195,17 +195,21 @@ class RIRRenderer:
     def _enqueue_pipelined(self, plan: Plan, main: torch.cuda.Stream) -> None:
         side: torch.cuda.Stream = plan.pipe_side  # type: ignore[attr-defined]
         side.wait_stream(main)
-        copied = torch.cuda.Event()
+        raw_done = torch.cuda.Event()
+        synth = (plan.synth_jobs_prev, len(plan.jobs), plan.synth_config)
         with torch.cuda.stream(side):
-            plan.echo_prev.copy_(plan.echo_store)   # the previous step's echograms
-            copied.record(side)
-            runtime.synthesize_batch((plan.synth_jobs_prev, len(plan.jobs), plan.synth_config), plan.synth_workspace,
-                                     stream=side)
-        main.wait_event(copied)
+            # the previous step's echograms, then their raw band signals -- before the trace takes every SM
+            plan.echo_prev.copy_(plan.echo_store)
+            runtime.synthesize_batch(synth, plan.synth_workspace, stream=side, phase="raw")
+            raw_done.record(side)
+        main.wait_event(raw_done)
         with torch.cuda.stream(main):
             runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
                                 plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
                                 chunk_rays=self.chunk_rays, stream=main)
+        with torch.cuda.stream(side):
+            # the recursion runs as one-warp blocks beside the persistent trace blocks
+            runtime.synthesize_batch(synth, plan.synth_workspace, stream=side, phase="filter")
         main.wait_stream(side)
 
     def launch_pipelined(self, plan: Plan) -> None:

@@ -141,6 +141,24 @@ size_t partition_bytes(const ac_job *jobs, const Partition &part, const ac_batch
 
 }  // namespace ac
 
+namespace ac {
+namespace {
+
+// Reads n 16-byte words `repeats` times through L2 (ld.global.cg: not cached in L1).
+__global__ void read_probe_kernel(const uint4 *buf, size_t n, int repeats, unsigned long long *sink) {
+    unsigned acc = 0u;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    for (int r = 0; r < repeats; ++r)
+        for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += stride) {
+            const uint4 v = __ldcg(buf + i);
+            acc ^= v.x ^ v.y ^ v.z ^ v.w;
+        }
+    if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // a data dependence that keeps every load
+}
+
+}  // namespace
+}  // namespace ac
+
 extern "C" {
 
 const char *ac_last_error(void) { return ac::last_error_slot().c_str(); }
@@ -229,6 +247,19 @@ int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, in
         ac::philox_workspace_kernel<float><<<grid, block, 0, s>>>(seed, stream_key, num_rays, num_bounces, num_bank,
                                                                   static_cast<float *>(directions),
                                                                   static_cast<float *>(random), indices);
+    AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}
+
+int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, unsigned long long *sink,
+                            void *stream) {
+    if (!buffer || !sink || repeats < 1 || bytes < 16 || (reinterpret_cast<uintptr_t>(buffer) & 15u) != 0)
+        return ac::fail(AC_ERR_INVALID, "ac_read_bandwidth_probe: needs a 16-byte aligned buffer and a sink");
+    int device = 0;
+    AC_CUDA_TRY(cudaGetDevice(&device));
+    const int grid = 8 * ac::device_sm_count(device);
+    ac::read_probe_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const uint4 *>(buffer),
+                                                                                bytes / 16, repeats, sink);
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
 }

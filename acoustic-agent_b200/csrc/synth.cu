@@ -477,14 +477,32 @@ extern "C" int ac_synth_batch_workspace_size(const ac_synth_job *jobs, int32_t n
     return AC_OK;
 }
 
-extern "C" int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
-                                   void *workspace, size_t workspace_bytes, void *host_staging, void *stream_ptr) {
+namespace {
+
+// Phase 1 (table copy, envelopes and air gains, raw band signals) and phase 2
+// (the crossover recursion) of a ragged batch; phase 2 reads only what phase 1
+// left in the workspace.
+int synth_batch_phase(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                      void *workspace, size_t workspace_bytes, void *host_staging, void *stream_ptr, bool raw_phase,
+                      bool filter_phase) {
     ac::SynthBatchLayout l;
     const int rc = ac::check_batch(jobs, num_jobs, config, true, &l);
     if (rc != AC_OK) return rc;
     if (num_jobs == 0) return AC_OK;
     if (!workspace || workspace_bytes < l.total)
         return ac::fail(AC_ERR_CAPACITY, "synthesis batch workspace too small: %zu < %zu", workspace_bytes, l.total);
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    const ac::SynthJobDev *d_jobs = reinterpret_cast<const ac::SynthJobDev *>(ws + l.jobs);
+    const int32_t *d_units = reinterpret_cast<const int32_t *>(ws + l.units);
+    double *raw = reinterpret_cast<double *>(ws + l.raw);
+    if (!raw_phase) {
+        if (filter_phase) {
+            ac::synth_batch_filter_kernel<<<l.num_units / 4, 32, 0, stream>>>(d_jobs, d_units, l.num_units, *config, raw);
+            AC_CUDA_TRY(cudaGetLastError());
+        }
+        return AC_OK;
+    }
     std::vector<unsigned char> local;
     unsigned char *host = static_cast<unsigned char *>(host_staging);
     if (!host) {
@@ -532,26 +550,41 @@ extern "C" int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, c
         for (int band = 0; band < 6; ++band) units[u++] = (j << 3) | band;
     for (; u < l.num_units; ++u) units[u] = -1;
 
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    unsigned char *ws = static_cast<unsigned char *>(workspace);
     AC_CUDA_TRY(cudaMemcpyAsync(ws, host, l.table_end, cudaMemcpyHostToDevice, stream));
     if (!host_staging) AC_CUDA_TRY(cudaStreamSynchronize(stream));  // pageable source must stay alive
-    const ac::SynthJobDev *d_jobs = reinterpret_cast<const ac::SynthJobDev *>(ws + l.jobs);
     const int64_t *d_cells = reinterpret_cast<const int64_t *>(ws + l.cell_prefix);
     const int64_t *d_samples = reinterpret_cast<const int64_t *>(ws + l.sample_prefix);
-    const int32_t *d_units = reinterpret_cast<const int32_t *>(ws + l.units);
     double *amps = reinterpret_cast<double *>(ws + l.amps);
     double *air = reinterpret_cast<double *>(ws + l.air);
-    double *raw = reinterpret_cast<double *>(ws + l.raw);
     const int prep_grid = static_cast<int>(std::min<int64_t>((cells + 255) / 256, 8192));
     ac::synth_batch_prepare_kernel<<<prep_grid, 256, 0, stream>>>(d_jobs, d_cells, num_jobs, *config, amps, air);
     AC_CUDA_TRY(cudaGetLastError());
     const int raw_grid = static_cast<int>(std::min<int64_t>((samples + 255) / 256, 65536));
     ac::synth_batch_raw_kernel<<<raw_grid, 256, 0, stream>>>(d_jobs, d_samples, num_jobs, amps, air, raw);
     AC_CUDA_TRY(cudaGetLastError());
-    ac::synth_batch_filter_kernel<<<l.num_units / 4, 32, 0, stream>>>(d_jobs, d_units, l.num_units, *config, raw);
-    AC_CUDA_TRY(cudaGetLastError());
+    if (filter_phase) {
+        ac::synth_batch_filter_kernel<<<l.num_units / 4, 32, 0, stream>>>(d_jobs, d_units, l.num_units, *config, raw);
+        AC_CUDA_TRY(cudaGetLastError());
+    }
     return AC_OK;
+}
+
+}  // namespace
+
+extern "C" int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                                   void *workspace, size_t workspace_bytes, void *host_staging, void *stream) {
+    return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, host_staging, stream, true, true);
+}
+
+extern "C" int ac_synthesize_batch_raw(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                                       void *workspace, size_t workspace_bytes, void *host_staging, void *stream) {
+    return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, host_staging, stream, true, false);
+}
+
+extern "C" int ac_synthesize_batch_filter(const ac_synth_job *jobs, int32_t num_jobs,
+                                          const ac_synth_batch_config *config, void *workspace,
+                                          size_t workspace_bytes, void *stream) {
+    return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, nullptr, stream, false, true);
 }
 
 // ---------------------------------------------------------------------------

@@ -592,8 +592,16 @@ class SynthBatchWorkspace(_StagedWorkspace):
 
 
 def synthesize_batch(jobs: Sequence[SynthJob] | tuple[ctypes.Array, int, _lib.ACSynthBatchConfig],
-                     workspace: SynthBatchWorkspace, *, stream: torch.cuda.Stream | None = None) -> None:
-    """Band IRs of every job in three launches (ac_synthesize_batch); outputs land in each job's `out`."""
+                     workspace: SynthBatchWorkspace, *, stream: torch.cuda.Stream | None = None,
+                     phase: str = "all") -> None:
+    """Band IRs of every job in three launches (ac_synthesize_batch); outputs land in each job's `out`.
+
+    phase="raw" then phase="filter" (same jobs and workspace, the second
+    ordered after the first, possibly on another stream) split the work at
+    the crossover recursion (ac_synthesize_batch_raw / _filter).
+    """
+    if phase not in ("all", "raw", "filter"):
+        raise ValueError("phase must be 'all', 'raw' or 'filter'")
     if isinstance(jobs, tuple):
         arr, n, cfg = jobs
     else:
@@ -603,10 +611,43 @@ def synthesize_batch(jobs: Sequence[SynthJob] | tuple[ctypes.Array, int, _lib.AC
         arr, n = synth_job_array(jobs, cfg), len(jobs)
     if n == 0:
         return
+    lib = _lib.load()
+    if phase == "filter":
+        if workspace.device_buffer is None:
+            raise RuntimeError("the filter phase needs the workspace of a preceding raw phase")
+        _lib.check(lib.ac_synthesize_batch_filter(arr, n, ctypes.byref(cfg),
+                                                  ctypes.c_void_p(workspace.device_buffer.data_ptr()),
+                                                  workspace.device_buffer.numel(), _stream_ptr(stream)),
+                   "ac_synthesize_batch_filter")
+        return
     ws, ws_bytes, host = workspace.ensure(arr, n, cfg)
-    _lib.check(_lib.load().ac_synthesize_batch(arr, n, ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
-                                               ctypes.c_void_p(host), _stream_ptr(stream)), "ac_synthesize_batch")
+    fn = lib.ac_synthesize_batch if phase == "all" else lib.ac_synthesize_batch_raw
+    _lib.check(fn(arr, n, ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes, ctypes.c_void_p(host),
+                  _stream_ptr(stream)), "ac_synthesize_batch")
     workspace.launched(stream)
+
+
+def read_bandwidth_gbs(device: torch.device, nbytes: int, *, repeats: int = 10, launches: int = 20) -> float:
+    """Measured read bandwidth (GB/s) over a buffer of `nbytes`: L2 when it fits, HBM otherwise."""
+    buf = torch.ones(nbytes // 4, dtype=torch.float32, device=device)
+    sink = torch.zeros(1, dtype=torch.int64, device=device)
+    stream = torch.cuda.current_stream(device)
+    lib = _lib.load()
+
+    def launch():
+        _lib.check(lib.ac_read_bandwidth_probe(ctypes.c_void_p(buf.data_ptr()), buf.numel() * 4, int(repeats),
+                                               ctypes.c_void_p(sink.data_ptr()), _stream_ptr(stream)),
+                   "ac_read_bandwidth_probe")
+
+    for _ in range(3):
+        launch()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(launches):
+        launch()
+    stop.record(stream)
+    stop.synchronize()
+    return (buf.numel() // 4) * 16 * repeats * launches / (start.elapsed_time(stop) / 1000.0) / 1e9
 
 
 def device_info(device: int = 0) -> dict[str, Any]:

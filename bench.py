@@ -467,6 +467,7 @@ def main() -> int:
             ref_cpu = reference_rirs(workloads_[0], 1, 1, accelerator="numba", precision="float64")
             ref_cuda = reference_rirs(workloads_[0], 3, 1, accelerator="cuda", precision="float32")
         bytes_per_rb = cpu["bytes_per_ray_bounce"] if cpu else None
+        l2_gbs = l2_read_gbs(device)
         achieved = (bytes_per_rb * ray_bounces_per_step / (trace_launch_ms / 1000.0) / 1e9) if bytes_per_rb else None
         traffic = _profiled_traffic(args.workload)
         result = {
@@ -492,6 +493,8 @@ def main() -> int:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
                          "peak_source": peaks["source"],
+                         "l2_peak": l2_gbs, "frac_of_l2": (achieved / l2_gbs) if achieved else None,
+                         "l2_peak_source": "measured in this run: L2-cached 16-byte loads over a 32 MiB buffer",
                          "kernel": "trace_kernel (ac_trace_batch)",
                          "bytes_per_ray_bounce": bytes_per_rb},
             "cpu_baseline": _cpu_baseline(cpu, ref_cpu),
@@ -686,6 +689,16 @@ def _reference_cuda_line(ref_cuda):
         return {"unavailable": ref_cuda["unavailable"]}
     return {"value": ref_cuda["value"], "unit": "RIRs/s", "seconds_per_rir": ref_cuda["seconds_per_rir"],
             "trace_seconds_per_rir": ref_cuda["trace_seconds"], "sample": ref_cuda["sample"]}
+
+
+def l2_read_gbs(device) -> float:
+    """Measured L2 read bandwidth: 16-byte loads cached in L2 only over a 32 MiB buffer (ac_read_bandwidth_probe).
+
+    The tracer's scenes (tens of KB) live in L1/L2, so this, beside the HBM
+    copy peak, is the roof its node and surface fetches run against.
+    """
+    from acoustic_agent_b200 import runtime
+    return runtime.read_bandwidth_gbs(device, 32 << 20)
 
 
 def _profiled_traffic(workload: str):

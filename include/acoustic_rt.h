@@ -327,6 +327,24 @@ int ac_synth_batch_workspace_size(const ac_synth_job *jobs, int32_t num_jobs, co
 int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
                         void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
 
+/* ac_synthesize_batch in two phases on possibly different streams, for a
+ * caller that overlaps the recursion with other work: _raw copies the job
+ * table and writes the raw band signals (fully parallel, a fraction of a
+ * millisecond); _filter runs the crossover recursion (one warp per four band
+ * signals, latency-bound) from what _raw left in `workspace`.  Same jobs,
+ * config and workspace for both; _filter must be ordered after _raw. */
+int ac_synthesize_batch_raw(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                            void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
+int ac_synthesize_batch_filter(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                               void *workspace, size_t workspace_bytes, void *stream);
+
+/* Measurement helper, no counterpart in the reference: reads `bytes` (a
+ * multiple of 16 is used) of device memory `repeats` times with 16-byte loads
+ * cached in L2 only, on `stream`; time it with events to get the L2 (buffer
+ * smaller than L2) or HBM (larger) read bandwidth the tracer's roofline is
+ * reported against.  `sink` is one device word the kernel may write. */
+int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, unsigned long long *sink, void *stream);
+
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */
 int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces,

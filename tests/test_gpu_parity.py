@@ -428,3 +428,33 @@ def test_fp32_visual_candidates_follow_the_reference_layout(rt):
     assert same_order[same_path].mean() >= 0.99
     both = same_path & same_order
     np.testing.assert_allclose(vc["gains"][both], case["visual_gains"][rays][both], rtol=2e-3)
+
+
+def test_two_phase_synthesis_equals_one_call(rt):
+    """ac_synthesize_batch_raw + _filter on two streams == ac_synthesize_batch."""
+    s = np.load(GOLDEN / "synthesis.npz")
+    dev = torch.device("cuda", 0)
+    fs, bd, delay, _ = s["furnished_f32_meta"]
+    echo = torch.as_tensor(np.stack([s["furnished_f32_input"], s["furnished_f32_input"] * 0.3]), device=dev)
+    n = echo.shape[2] * 48
+    outs = [torch.full((2, 6, n), float("nan"), device=dev) for _ in range(2)]
+
+    def jobs(out):
+        return [rt.SynthJob(echo[k], out[k], int(fs), float(bd), seed=100 + k, direct_delay=float(delay))
+                for k in range(2)]
+
+    rt.synthesize_batch(jobs(outs[0]), rt.SynthBatchWorkspace(dev))
+    ws = rt.SynthBatchWorkspace(dev)
+    side = torch.cuda.Stream(dev)
+    j1 = jobs(outs[1])
+    rt.synthesize_batch(j1, ws, phase="raw")
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        rt.synthesize_batch(j1, ws, stream=side, phase="filter")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(outs[0].cpu().numpy(), outs[1].cpu().numpy())
+
+
+def test_read_bandwidth_probe_reports_a_plausible_l2_rate(rt):
+    gbs = rt.read_bandwidth_gbs(torch.device("cuda", 0), 32 << 20, repeats=4, launches=4)
+    assert 1000.0 < gbs < 100000.0
