@@ -116,7 +116,7 @@ class ACSynthParams(ctypes.Structure):
 
 
 AC_SYNTH_MAX_RATES = 4
-AC_TRAVERSAL_AUTO, AC_TRAVERSAL_SCAN, AC_TRAVERSAL_BVH = 0, 1, 2
+AC_TRAVERSAL_AUTO, AC_TRAVERSAL_SCAN, AC_TRAVERSAL_BVH, AC_TRAVERSAL_HYBRID = 0, 1, 2, 3
 
 
 class ACSynthJob(ctypes.Structure):

@@ -10,8 +10,9 @@ the tuner may choose by measured time alone.
 Knobs
 -----
 per scene (``tune_scene``)
-    ``traversal`` -- "scan" (kind-separated clusters in warp lockstep) or
-    "bvh" (per-lane descent of a surface-area-heuristic BVH with a short stack);
+    ``traversal`` -- "scan" (kind-separated clusters in warp lockstep), "bvh"
+    (per-lane descent of a surface-area-heuristic BVH with a short stack) or
+    "hybrid" (walls in lockstep, a BVH over the boxes);
     ``bvh_leaf`` -- surfaces per BVH leaf (1, 2, 4): smaller leaves mean a
     deeper tree and a deeper traversal stack, fewer surface tests per leaf.
 per launch (``tune_launch``)
@@ -42,6 +43,7 @@ SCENE_CANDIDATES: tuple[dict[str, Any], ...] = (
     {"traversal": "bvh", "bvh_leaf": 1},
     {"traversal": "bvh", "bvh_leaf": 2},
     {"traversal": "bvh", "bvh_leaf": 4},
+    {"traversal": "hybrid", "bvh_leaf": 1},
 )
 LAUNCH_CANDIDATES: tuple[dict[str, int], ...] = tuple(
     {"block_size": b, "chunk_rays": c} for b in (256, 128) for c in (16, 32, 64, 128))
@@ -129,8 +131,8 @@ def tune_scene(arrays: SceneArrays, spec: runtime.TraceSpec, *, device: int = 0,
     for cand in candidates:
         scene = runtime.DeviceScene(arrays, device=dev.index, **cand)
         try:
-            if cand["traversal"] == "bvh" and scene.traversal != "bvh":
-                continue   # nothing for a BVH to hold (only horizontal surfaces)
+            if scene.traversal != cand["traversal"]:
+                continue   # nothing for a BVH to hold (no boxes, or only horizontal surfaces)
             buffers = runtime.TraceBuffers.allocate(scene.num_surfaces, int(sample.num_bins), dev)
             ms = _time_ms(lambda: runtime.trace(scene, sample, buffers, stream=stream), reps, stream)
         finally:

@@ -34,8 +34,12 @@ struct Offsets {
         box_bounds, boxes, edges, bvh_nodes, bvh_prims, total;  // elements
 };
 
-// Scenes with more walls + boxes than this trace in BVH mode unless the caller chooses.
+// Scenes with more walls + boxes than this trace in BVH mode unless the caller chooses;
+// with at most kAutoHybridWalls walls (one room) in hybrid mode.  Measured on B200:
+// U room (8 walls, 20 boxes) hybrid 11.4 ms < BVH 11.8 < scan 12.3; 8-room apartment
+// (52 walls, 374 boxes) BVH 5.1 ms < hybrid 6.3 < scan 9.6.
 constexpr int64_t kAutoBvhSurfaces = 16;
+constexpr int64_t kAutoHybridWalls = 16;
 // Float32 BVH node boxes are padded by this much (metres) beyond the surface bounds.
 constexpr double kBvhPad = 1e-4;
 // Surfaces per BVH leaf unless the caller chooses: one surface per leaf measured
@@ -50,8 +54,9 @@ struct FastLists {
     std::vector<int64_t> wall_slots, box_slots, polys;                    // surface index per slot
     std::vector<std::array<int64_t, 2>> wall_clusters, box_clusters;      // {first slot, count}
     std::vector<std::array<double, 6>> wall_cluster_bounds, box_cluster_bounds;
-    bool use_bvh = false;
-    ac::TraversalBvh bvh;                                                 // BVH mode: walls and boxes
+    bool use_bvh = false;                                                 // BVH or hybrid mode
+    bool hybrid = false;                                                  // walls stay in the scan
+    ac::TraversalBvh bvh;                                                 // walls and boxes (hybrid: boxes)
 };
 
 int cluster_kind(const ac_scene_desc *d, const double *blo, const double *bhi, int64_t kind, int leaf,
@@ -304,11 +309,12 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const FastLists *
         s->fast.num_edges = static_cast<int32_t>(C);
         s->num_clusters = static_cast<int64_t>(f->wall_clusters.size() + f->box_clusters.size());
         if (f->use_bvh) {
-            // BVH mode: walls and boxes come from the traversal BVH, only polygons stay in the scan
+            // BVH mode: walls and boxes come from the traversal BVH, only polygons stay in the scan;
+            // hybrid mode: boxes from the BVH, walls and polygons in the scan
             s->fast.bvh_nodes = reinterpret_cast<const float4 *>(fbase + o.bvh_nodes);
             s->fast.bvh_prims = fbase + o.bvh_prims;
             s->fast.num_bvh_nodes = static_cast<int32_t>(f->bvh.num_nodes());
-            s->fast.num_wall_clusters = 0;
+            if (!f->hybrid) s->fast.num_wall_clusters = 0;
             s->fast.num_box_clusters = 0;
         }
     }
@@ -430,15 +436,25 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
         rc = cluster_kind(d, blo, bhi, AC_KIND_BOX, s->cluster_size, lists.box_slots, lists.box_clusters,
                           lists.box_cluster_bounds);
     if (rc == AC_OK) {
-        if (d->traversal < AC_TRAVERSAL_AUTO || d->traversal > AC_TRAVERSAL_BVH) {
+        if (d->traversal < AC_TRAVERSAL_AUTO || d->traversal > AC_TRAVERSAL_HYBRID) {
             rc = ac::fail(AC_ERR_INVALID, "unknown traversal %d", d->traversal);
         } else {
+            int64_t walls = 0, boxes = 0;
+            for (int64_t i = 0; i < S; ++i) {
+                walls += d->kinds[i] == AC_KIND_WALL;
+                boxes += d->kinds[i] == AC_KIND_BOX;
+            }
+            // AUTO: a single room's few walls are cheapest in lockstep, its furniture in a BVH
+            lists.hybrid = d->traversal == AC_TRAVERSAL_HYBRID ||
+                           (d->traversal == AC_TRAVERSAL_AUTO && walls + boxes > kAutoBvhSurfaces &&
+                            walls <= kAutoHybridWalls && boxes > 0);
             std::vector<int64_t> members;
             for (int64_t i = 0; i < S; ++i)
-                if (d->kinds[i] != AC_KIND_HORIZONTAL) members.push_back(i);
+                if (d->kinds[i] == AC_KIND_BOX || (d->kinds[i] == AC_KIND_WALL && !lists.hybrid)) members.push_back(i);
             lists.use_bvh = !members.empty() &&
-                            (d->traversal == AC_TRAVERSAL_BVH ||
+                            (d->traversal == AC_TRAVERSAL_BVH || lists.hybrid ||
                              (d->traversal == AC_TRAVERSAL_AUTO && static_cast<int64_t>(members.size()) > kAutoBvhSurfaces));
+            if (!lists.use_bvh) lists.hybrid = false;   // no boxes: plain scan
             if (lists.use_bvh)
                 rc = ac::build_traversal_bvh(members, blo, bhi, d->bvh_leaf > 0 ? d->bvh_leaf : kDefaultBvhLeaf, kBvhPad,
                                              &lists.bvh);
@@ -448,7 +464,7 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
         delete s;
         return rc;
     }
-    s->traversal = lists.use_bvh ? AC_TRAVERSAL_BVH : AC_TRAVERSAL_SCAN;
+    s->traversal = lists.hybrid ? AC_TRAVERSAL_HYBRID : (lists.use_bvh ? AC_TRAVERSAL_BVH : AC_TRAVERSAL_SCAN);
     s->bvh_depth = lists.use_bvh ? lists.bvh.depth : 0;
     s->bvh_nodes = lists.use_bvh ? lists.bvh.num_nodes() : 0;
     rc = pack_and_upload<float>(d, bvh, &lists, blo, bhi, s, &s->storage_f32, &s->bytes_f32, &s->f32);

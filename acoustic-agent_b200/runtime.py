@@ -55,7 +55,7 @@ def _stream_ptr(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
 class DeviceScene:
     """A scene uploaded with ac_scene_create; owns its device memory."""
 
-    TRAVERSALS = {"auto": 0, "scan": 1, "bvh": 2}
+    TRAVERSALS = {"auto": 0, "scan": 1, "bvh": 2, "hybrid": 3}
 
     def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0,
                  traversal: str = "auto", bvh_leaf: int = 0) -> None:
@@ -109,7 +109,7 @@ class DeviceScene:
         self.device_bytes = int(info.device_bytes)
         self.node_count = int(info.node_count)
         self.num_clusters = int(info.num_clusters)
-        self.traversal = {1: "scan", 2: "bvh"}.get(int(info.traversal), "scan")
+        self.traversal = {1: "scan", 2: "bvh", 3: "hybrid"}.get(int(info.traversal), "scan")
         self.bvh_depth = int(info.bvh_depth)
         self.bvh_nodes = int(info.bvh_nodes)
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0

@@ -52,8 +52,10 @@ enum { AC_RNG_REFERENCE = 0, AC_RNG_PHILOX = 1 };
  * SCAN walks kind-separated clusters of surfaces in warp lockstep (best for a
  * room with tens of surfaces); BVH lets every lane descend its own path of a
  * surface-area-heuristic BVH over walls and boxes with a short stack (best
- * for multi-room scenes with hundreds of surfaces); AUTO picks by size. */
-enum { AC_TRAVERSAL_AUTO = 0, AC_TRAVERSAL_SCAN = 1, AC_TRAVERSAL_BVH = 2 };
+ * for multi-room scenes with hundreds of surfaces); HYBRID scans the walls in
+ * lockstep and descends a BVH over the boxes only; AUTO picks by size (scan
+ * up to 16 walls and boxes, hybrid with up to 16 walls, BVH beyond). */
+enum { AC_TRAVERSAL_AUTO = 0, AC_TRAVERSAL_SCAN = 1, AC_TRAVERSAL_BVH = 2, AC_TRAVERSAL_HYBRID = 3 };
 
 typedef struct ac_scene_s *ac_scene_t;
 
@@ -102,7 +104,7 @@ typedef struct ac_scene_desc {
     const int64_t *bvh_primitives;
     int32_t device;              /* CUDA device ordinal that will own the scene */
     int32_t cluster_size;        /* surfaces per cluster of the float32 scan (0: 32) */
-    int32_t traversal;           /* float32 kernel: AC_TRAVERSAL_AUTO / _SCAN / _BVH */
+    int32_t traversal;           /* float32 kernel: AC_TRAVERSAL_AUTO / _SCAN / _BVH / _HYBRID */
     int32_t bvh_leaf;            /* float32 BVH: surfaces per leaf, 1..8 (0: 1) */
 } ac_scene_desc;
 
@@ -115,7 +117,7 @@ typedef struct ac_scene_info {
     int32_t device;
     int32_t max_leaf;
     int64_t num_clusters;        /* clusters of the float32 scan */
-    int32_t traversal;           /* what the float32 kernel uses: AC_TRAVERSAL_SCAN or AC_TRAVERSAL_BVH */
+    int32_t traversal;           /* what the float32 kernel uses: AC_TRAVERSAL_SCAN, _BVH or _HYBRID */
     int32_t bvh_depth;           /* float32 BVH: inner-node levels (0 in scan mode) */
     int64_t bvh_nodes;           /* float32 BVH: inner nodes (0 in scan mode) */
 } ac_scene_info;

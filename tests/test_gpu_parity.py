@@ -341,19 +341,21 @@ def test_fp32_bvh_traversal_equals_scan(rt, name):
     """
     case = load_case(name)
     spec = spec_for(rt, case, "float32")
+    has_boxes = bool(np.any(np.asarray(case["arrays"]["kinds"]) == 2))
     got = {}
-    for mode in ("scan", "bvh"):
+    for mode in ("scan", "bvh", "hybrid"):
         scene = rt.DeviceScene(case["arrays"], traversal=mode)
-        assert scene.traversal == mode
-        if mode == "bvh":
+        assert scene.traversal == (mode if mode != "hybrid" or has_boxes else "scan")
+        if scene.traversal != "scan":
             assert 1 <= scene.bvh_depth <= 31 and scene.bvh_nodes >= 1
         buffers = rt.trace(scene, spec, record_rays=True)
         torch.cuda.synchronize()
         got[mode] = {"rays": buffers.ray_surfaces.cpu().numpy(), "echogram": buffers.echogram_fx.cpu().numpy(),
                      "hits": buffers.hit_counts.cpu().numpy(), "counters": buffers.counters.cpu().numpy()}
         scene.close()
-    for key in ("rays", "echogram", "hits", "counters"):
-        np.testing.assert_array_equal(got["bvh"][key], got["scan"][key], err_msg=key)
+    for mode in ("bvh", "hybrid"):
+        for key in ("rays", "echogram", "hits", "counters"):
+            np.testing.assert_array_equal(got[mode][key], got["scan"][key], err_msg=f"{mode} {key}")
 
 
 @pytest.mark.parametrize("leaf", [1, 2, 8])
