@@ -185,6 +185,7 @@ int ac_energy_scale(ac_scene_t scene, const ac_trace_params *params, double *sca
 }
 
 int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_outputs *outputs, void *stream) {
+    ac::NvtxRange nvtx_range("ac_trace");
     int rc = ac::validate_trace(scene, params, outputs);
     if (rc != AC_OK) return rc;
     const double scale = params->energy_scale > 0.0 ? params->energy_scale : ac::choose_energy_scale(scene, params);
@@ -209,6 +210,7 @@ int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch
 // simply enqueued one after another on the stream.
 int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
                    size_t workspace_bytes, void *host_staging, void *stream) {
+    ac::NvtxRange nvtx_range("ac_trace_batch");
     if (num_jobs < 0 || (num_jobs > 0 && (!jobs || !workspace)))
         return ac::fail(AC_ERR_INVALID, "ac_trace_batch: bad argument");
     for (int32_t j = 0; j < num_jobs; ++j) {
@@ -233,6 +235,7 @@ int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *
 
 int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces, int32_t num_bank,
                         int32_t precision, void *directions, void *random, int32_t *indices, void *stream) {
+    ac::NvtxRange nvtx_range("ac_philox_workspace");
     if (num_rays < 1 || num_rays > 0x7FFFFFFF || num_bounces < 0 || num_bank < 1 || !directions ||
         (num_bounces > 0 && (!random || !indices)))
         return ac::fail(AC_ERR_INVALID, "ac_philox_workspace: bad argument");
@@ -253,6 +256,7 @@ int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, in
 
 int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, unsigned long long *sink,
                             void *stream) {
+    ac::NvtxRange nvtx_range("ac_read_bandwidth_probe");
     if (!buffer || !sink || repeats < 1 || bytes < 16 || (reinterpret_cast<uintptr_t>(buffer) & 15u) != 0)
         return ac::fail(AC_ERR_INVALID, "ac_read_bandwidth_probe: needs a 16-byte aligned buffer and a sink");
     int device = 0;

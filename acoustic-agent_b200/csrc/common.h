@@ -1,13 +1,24 @@
-// Shared host helpers for the C ABI: thread-local error reporting and CUDA checks.
+// Shared host helpers for the C ABI: thread-local error reporting, CUDA
+// checks and NVTX ranges (one named range per entry point, visible in
+// Nsight Systems / ncu range filters; a no-op when no tool is attached).
 #pragma once
 
 #include <cstdarg>
 #include <cstdio>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "acoustic_rt.h"
 
 namespace ac {
+
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 std::string &last_error_slot();
 

@@ -330,6 +330,7 @@ bool finite_all(const double *p, size_t n) {
 }  // namespace
 
 extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
+    ac::NvtxRange nvtx_range("ac_scene_create");
     if (!d || !out) return ac::fail(AC_ERR_INVALID, "ac_scene_create: null argument");
     *out = nullptr;
     const int64_t S = d->num_surfaces;
@@ -480,6 +481,7 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
 }
 
 extern "C" int ac_scene_destroy(ac_scene_t s) {
+    ac::NvtxRange nvtx_range("ac_scene_destroy");
     if (!s) return AC_OK;
     cudaSetDevice(s->device);
     if (s->storage_f32) cudaFree(s->storage_f32);

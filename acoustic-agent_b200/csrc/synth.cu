@@ -361,6 +361,7 @@ extern "C" int ac_synth_workspace_size(const ac_synth_params *p, size_t *bytes) 
 
 extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, float *band_irs, void *workspace,
                              size_t workspace_bytes, void *stream_ptr) {
+    ac::NvtxRange nvtx_range("ac_synthesize");
     if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize: null argument");
     if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
         return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
@@ -573,17 +574,20 @@ int synth_batch_phase(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth
 
 extern "C" int ac_synthesize_batch(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
                                    void *workspace, size_t workspace_bytes, void *host_staging, void *stream) {
+    ac::NvtxRange nvtx_range("ac_synthesize_batch");
     return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, host_staging, stream, true, true);
 }
 
 extern "C" int ac_synthesize_batch_raw(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
                                        void *workspace, size_t workspace_bytes, void *host_staging, void *stream) {
+    ac::NvtxRange nvtx_range("ac_synthesize_batch_raw");
     return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, host_staging, stream, true, false);
 }
 
 extern "C" int ac_synthesize_batch_filter(const ac_synth_job *jobs, int32_t num_jobs,
                                           const ac_synth_batch_config *config, void *workspace,
                                           size_t workspace_bytes, void *stream) {
+    ac::NvtxRange nvtx_range("ac_synthesize_batch_filter");
     return synth_batch_phase(jobs, num_jobs, config, workspace, workspace_bytes, nullptr, stream, false, true);
 }
 
@@ -627,6 +631,7 @@ int static_scratch(void **out) {
 
 extern "C" int ac_synthesize_static(const float *echograms, const ac_synth_params *p, float *band_irs,
                                     void *stream_ptr) {
+    ac::NvtxRange nvtx_range("ac_synthesize_static");
     if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize_static: null argument");
     if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
         return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");

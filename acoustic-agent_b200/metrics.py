@@ -8,7 +8,8 @@ not expected (float32 arithmetic, or a different random stream):
   steam_rt.py:2727-2792 ``_schroeder_fit_rt60``);
 * T30: decay time from a least-squares line over -5 .. -35 dB, times 2;
 * EDT: same over 0 .. -10 dB, times 6;
-* C50: early-to-late energy ratio at 50 ms after the first arrival bin.
+* C50: early-to-late energy ratio at 50 ms after the first arrival bin;
+* the reference's own traced RT60 fit (``schroeder_rt60``).
 """
 from __future__ import annotations
 
@@ -33,6 +34,27 @@ def edc_error_db(a: np.ndarray, b: np.ndarray, range_db: float = 30.0) -> np.nda
         if np.any(mask):
             out[band] = float(np.max(np.abs(ea[band, mask] - eb[band, mask])))
     return out
+
+
+def schroeder_rt60(energy: np.ndarray, bin_dur: float, *, min_total_energy: float = 1e-12) -> float:
+    """The reference's traced RT60 of one band (steam_rt.py:3052-3067): least-squares line through the
+    Schroeder curve between -5 and -25 dB, bins timed at their start, extrapolated to -60 dB."""
+    e = np.asarray(energy, dtype=np.float64)
+    total = float(np.sum(e))
+    if total < float(min_total_energy):
+        return 0.0
+    edc = np.cumsum(e[::-1])[::-1]
+    db = 10.0 * np.log10(np.clip(edc / total, 1e-12, None))
+    x = float(bin_dur) * np.arange(edc.size, dtype=np.float64)
+    fit = (db <= -5.0) & (db >= -25.0)
+    if int(np.count_nonzero(fit)) < 2:
+        return 0.0
+    xs, ys = x[fit], db[fit]
+    n = xs.size
+    denom = n * np.sum(xs * xs) - np.sum(xs) ** 2
+    numer = n * np.sum(xs * ys) - np.sum(xs) * np.sum(ys)
+    slope = numer / denom if abs(denom) > 1e-12 else 0.0
+    return float(max(0.0, -60.0 / slope)) if slope < -1e-9 else 0.0
 
 
 def _decay_time(edc: np.ndarray, bin_dur: float, hi_db: float, lo_db: float, factor: float) -> float:

@@ -8,7 +8,9 @@ the GPU fed while requests arrive:
 * **admission by free HBM** -- a request is admitted when its footprint (its
   scene, unless already resident, plus the trace outputs, echograms, band IRs
   and synthesis workspace of its jobs) fits the device budget that the
-  in-flight batches leave, and a launch slot is free;
+  in-flight batches leave, and a launch slot is free; a request that cannot
+  fit even on an idle device is rejected (its result carries the reason) and
+  the others are served;
 * **continuous batching** -- every admitted request that waits is folded into
   the next batch: ONE persistent tracer launch over all their jobs (any mix of
   scene sizes, ray budgets and lengths) plus one ragged synthesis and the
@@ -67,6 +69,7 @@ class Result:
     ray_bounces: int
     admitted_s: float
     done_s: float
+    error: str | None = None            # set when the request was rejected (its band_irs are empty)
 
     @property
     def latency_s(self) -> float:
@@ -84,14 +87,20 @@ class Report:
     scene_hits: int
     scene_misses: int
     evictions: int
+    peak_bytes: int = 0                 # device bytes held by resident scenes and in-flight batches, at most
+
+    @property
+    def rejected(self) -> list[Result]:
+        return [r for r in self.results if r.error is not None]
 
     def latency_ms(self, q: float) -> float:
-        lat = np.array([r.latency_s for r in self.results]) * 1e3
+        lat = np.array([r.latency_s for r in self.results if r.error is None]) * 1e3
         return float(np.percentile(lat, q)) if lat.size else float("nan")
 
     def summary(self) -> dict[str, Any]:
         return {
-            "requests": len(self.results), "rirs": self.rirs, "makespan_s": self.makespan_s,
+            "requests": len(self.results), "rejected": len(self.rejected), "rirs": self.rirs,
+            "makespan_s": self.makespan_s, "peak_device_bytes": self.peak_bytes,
             "rirs_per_s": self.rirs / self.makespan_s if self.makespan_s > 0 else float("nan"),
             "ray_bounces_per_s": self.ray_bounces / self.makespan_s if self.makespan_s > 0 else float("nan"),
             "p50_ms": self.latency_ms(50), "p99_ms": self.latency_ms(99), "batches": self.batches,
@@ -310,7 +319,7 @@ class Server:
         waiting: deque[tuple[Request, list[runtime.TraceSpec]]] = deque()
         inflight: list[_Batch] = []
         results: list[Result] = []
-        batches = max_seen = 0
+        batches = max_seen = peak = 0
         free_streams = list(self.streams)
         t0 = time.perf_counter()
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
@@ -336,8 +345,13 @@ class Server:
                     if reqs and rays + req_rays > self.max_batch_rays:
                         break
                     if not self._fits(need_total + need):
-                        if not reqs and not inflight:
-                            raise MemoryError(f"request {req.id} needs {need} bytes; the budget is {self.budget}")
+                        if not reqs and not inflight and self.scenes.resident_bytes() + need > self.budget:
+                            # cannot fit even on an idle device: reject it, keep serving the others
+                            waiting.popleft()
+                            t = time.perf_counter() - t0
+                            results.append(Result(req, [], 0, t, t, error=f"needs {need} bytes of device memory; "
+                                                                              f"the budget is {self.budget}"))
+                            continue
                         break
                     waiting.popleft()
                     reqs.append(req)
@@ -346,6 +360,7 @@ class Server:
                     rays += req_rays
                 if reqs:
                     self.in_use += need_total
+                    peak = max(peak, self.in_use + self.scenes.resident_bytes())
                     stream = free_streams.pop()
                     inflight.append(self._launch(reqs, specs, need_total, time.perf_counter() - t0, stream))
                     batches += 1
@@ -355,13 +370,14 @@ class Server:
                 continue
             if inflight or (pending and realtime):
                 time.sleep(idle_sleep_s)
-        makespan = max((r.done_s for r in results), default=0.0) - min((r.request.arrival_s for r in results),
-                                                                       default=0.0)
+        served = [r for r in results if r.error is None]
+        makespan = max((r.done_s for r in served), default=0.0) - min((r.request.arrival_s for r in served),
+                                                                      default=0.0)
         return Report(results=sorted(results, key=lambda r: r.request.id), makespan_s=makespan,
-                      rirs=sum(r.request.num_rirs for r in results),
-                      ray_bounces=sum(r.ray_bounces for r in results), batches=batches, max_inflight_seen=max_seen,
+                      rirs=sum(r.request.num_rirs for r in served),
+                      ray_bounces=sum(r.ray_bounces for r in served), batches=batches, max_inflight_seen=max_seen,
                       scene_hits=self.scenes.hits, scene_misses=self.scenes.misses,
-                      evictions=self.scenes.evictions)
+                      evictions=self.scenes.evictions, peak_bytes=peak)
 
     def close(self) -> None:
         self.scenes.close()

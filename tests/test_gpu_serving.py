@@ -84,3 +84,20 @@ def test_served_result_tracks_the_float64_oracle(served):
 
     err = metrics.edc_error_db(bin_energy(res.band_irs[0]), bin_energy(expected))
     assert float(err.max()) <= 0.5, err
+
+
+def test_a_request_larger_than_the_budget_is_rejected_not_fatal(served):
+    serving, requests, report = served
+    small = requests[:3]
+    sizer = serving.Server(0, max_inflight=2, tune=False)
+    sizes = [sizer.footprint(r, serving.request_jobs(r)) for r in small]
+    sizer.close()
+    budget = sorted(sizes)[1] + (64 << 10)       # the largest of the three cannot fit
+    big = small[int(np.argmax(sizes))]
+    server = serving.Server(0, max_inflight=2, hbm_budget=budget, tune=False)
+    out = server.serve([serving.Request(r.id, r.workload, r.sources, 0.0, r.moving) for r in small], realtime=False)
+    server.close()
+    rejected = [r.request.id for r in out.rejected]
+    assert big.id in rejected and "budget" in out.results[[r.request.id for r in out.results].index(big.id)].error
+    assert all(r.band_irs for r in out.results if r.error is None)
+    assert out.summary()["rejected"] == len(rejected) >= 1

@@ -115,3 +115,13 @@ def test_planted_error_is_caught():
     case["arrays"]["reflection"] = refl
     changed = run_oracle(case, record_rays=False)
     assert not np.allclose(changed["echogram"], base["echogram"], rtol=1e-6)
+
+
+def test_reference_rt60_fit_restatement_on_a_known_decay():
+    """schroeder_rt60 (steam_rt.py:3052-3067) on an exact exponential decay returns its RT60."""
+    from acoustic_agent_b200 import metrics
+    bin_dur, rt60 = 0.01, 0.5
+    t = np.arange(200) * bin_dur
+    energy = 10.0 ** (-6.0 * t / rt60)          # -60 dB per rt60 seconds
+    assert abs(metrics.schroeder_rt60(energy, bin_dur) - rt60) < 1e-3
+    assert metrics.schroeder_rt60(np.zeros(10), bin_dur) == 0.0
