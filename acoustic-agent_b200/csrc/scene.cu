@@ -275,11 +275,15 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const FastLists *
 
     *bytes = o.total * sizeof(T);
     void *dev = nullptr;
-    cudaError_t err = cudaMalloc(&dev, *bytes);
+    // Stream-ordered allocation on the legacy default stream: unlike cudaMalloc/cudaFree it does not
+    // wait for the whole device, so uploading or destroying a scene does not stall work that other
+    // (non-blocking) streams have in flight.  The upload is complete when this function returns.
+    cudaError_t err = cudaMallocAsync(&dev, *bytes, cudaStreamLegacy);
     if (err != cudaSuccess) return ac::fail(AC_ERR_NOMEM, "scene allocation of %zu bytes failed: %s", *bytes, cudaGetErrorString(err));
-    err = cudaMemcpy(dev, host.data(), *bytes, cudaMemcpyHostToDevice);
+    err = cudaMemcpyAsync(dev, host.data(), *bytes, cudaMemcpyHostToDevice, cudaStreamLegacy);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(cudaStreamLegacy);
     if (err != cudaSuccess) {
-        cudaFree(dev);
+        cudaFreeAsync(dev, cudaStreamLegacy);
         return ac::fail(AC_ERR_CUDA, "scene upload failed: %s", cudaGetErrorString(err));
     }
     *storage = dev;
@@ -472,7 +476,7 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
     if (rc == AC_OK)
         rc = pack_and_upload<double>(d, bvh, nullptr, blo, bhi, s, &s->storage_f64, &s->bytes_f64, &s->f64);
     if (rc != AC_OK) {
-        if (s->storage_f32) cudaFree(s->storage_f32);
+        if (s->storage_f32) cudaFreeAsync(s->storage_f32, cudaStreamLegacy);
         delete s;
         return rc;
     }
@@ -484,8 +488,9 @@ extern "C" int ac_scene_destroy(ac_scene_t s) {
     ac::NvtxRange nvtx_range("ac_scene_destroy");
     if (!s) return AC_OK;
     cudaSetDevice(s->device);
-    if (s->storage_f32) cudaFree(s->storage_f32);
-    if (s->storage_f64) cudaFree(s->storage_f64);
+    // the caller destroys a scene only after the work that reads it has finished
+    if (s->storage_f32) cudaFreeAsync(s->storage_f32, cudaStreamLegacy);
+    if (s->storage_f64) cudaFreeAsync(s->storage_f64, cudaStreamLegacy);
     delete s;
     return AC_OK;
 }

@@ -246,6 +246,10 @@ int ac_bvh_build(const double *bounds_min, const double *bounds_max, int64_t num
 int ac_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major, int32_t *cc_minor,
                    int32_t *sm_count);
 
+/* The scene's device memory comes from the device's stream-ordered pool, so
+ * creating or destroying a scene does not wait for work that other streams
+ * have in flight; ac_scene_create returns once the upload is complete.
+ * Destroy a scene only after the work that reads it has finished. */
 int ac_scene_create(const ac_scene_desc *desc, ac_scene_t *out);
 int ac_scene_destroy(ac_scene_t scene);
 int ac_scene_get_info(ac_scene_t scene, ac_scene_info *info);
