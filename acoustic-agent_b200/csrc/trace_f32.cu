@@ -10,6 +10,9 @@ namespace ac {
 namespace {
 
 constexpr int kDefaultChunkRays = 32;
+// A scene group holds at most this many consecutive jobs, so that (job index mod 1024,
+// surface) identifies a (job, surface) pair among the lanes of one warp (hit-count keys).
+constexpr int64_t kMaxGroupJobs = 1024;
 
 using FastKernel = void (*)(const Job<float>, const FastScene, const FastTable);
 
@@ -70,7 +73,11 @@ void count_groups_chunks(const ac_job *jobs, const std::vector<int32_t> &order, 
     while (k < order.size()) {
         const ac_scene_t scene = jobs[order[k]].scene;
         int64_t rays = 0;
-        while (k < order.size() && jobs[order[k]].scene == scene) rays += jobs[order[k++]].params.num_rays;
+        int64_t members = 0;
+        while (k < order.size() && jobs[order[k]].scene == scene && members < kMaxGroupJobs) {
+            rays += jobs[order[k++]].params.num_rays;
+            ++members;
+        }
         *groups += 1;
         *chunks += (rays + chunk_rays - 1) / chunk_rays;
     }
@@ -151,7 +158,7 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         const ac_job &in = jobs_in[order[k]];
         if (device < 0) device = in.scene->device;
         if (in.scene->device != device) return fail(AC_ERR_INVALID, "batch jobs must share one device");
-        if (in.scene != current) {
+        if (in.scene != current || groups[g].num_jobs >= kMaxGroupJobs) {
             if (g >= 0) close_group(total);
             ++g;
             current = in.scene;

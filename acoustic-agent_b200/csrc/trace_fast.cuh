@@ -610,11 +610,16 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     }
                 }
             }
-            // per-surface hit counters: one atomic per distinct (job, surface) in the warp
+            // per-surface hit counters: one atomic per distinct (job, surface) in the warp.  The
+            // lanes of a warp trace jobs of one scene group of at most 1024 consecutive jobs
+            // (surfaces < 2^22), so (job mod 1024, surface) is a 32-bit key -- cheaper to match
+            // than a 64-bit one.
             const unsigned counting = __ballot_sync(full, count_hit);
             if (count_hit) {
-                warp_count(counting, (static_cast<unsigned long long>(s.job) << 32) | static_cast<unsigned>(surf), 1u,
-                           job.hit_counts + surf);
+                const unsigned key = ((static_cast<unsigned>(s.job) & 1023u) << 22) | static_cast<unsigned>(surf);
+                const unsigned same = __match_any_sync(counting, key);
+                if (lane_id == __ffs(same) - 1)
+                    atomicAdd(job.hit_counts + surf, static_cast<unsigned long long>(__popc(same)));
             }
             const float h[3] = {hx, hy, hz};
             make_ray(query, h, sd);

@@ -460,3 +460,22 @@ def test_two_phase_synthesis_equals_one_call(rt):
 def test_read_bandwidth_probe_reports_a_plausible_l2_rate(rt):
     gbs = rt.read_bandwidth_gbs(torch.device("cuda", 0), 32 << 20, repeats=4, launches=4)
     assert 1000.0 < gbs < 100000.0
+
+
+def test_batch_of_more_than_1024_jobs_on_one_scene_counts_every_job(rt):
+    """Scene groups hold at most 1024 jobs: jobs 1024 apart never share a warp's hit-count keys."""
+    case = load_case("u_room_kat")
+    dev = torch.device("cuda", 0)
+    scene = rt.DeviceScene(case["arrays"])
+    n = 1030
+    specs = [spec_for(rt, case, "float32", rng="philox", num_rays=64, stream_key=k % 7, render_ambisonics=False)
+             for k in range(n)]
+    buffers = [rt.TraceBuffers.allocate(scene.num_surfaces, int(case["num_bins"]), dev) for _ in range(n)]
+    rt.trace_batch([(scene, s, b) for s, b in zip(specs, buffers)], rt.BatchWorkspace(dev))
+    torch.cuda.synchronize()
+    for k in (0, 5, 1023, 1024, 1029):
+        alone = rt.trace(scene, specs[k])
+        torch.cuda.synchronize()
+        assert torch.equal(alone.hit_counts, buffers[k].hit_counts)
+        assert torch.equal(alone.echogram_fx, buffers[k].echogram_fx)
+    scene.close()
