@@ -142,9 +142,16 @@ struct Section {
     }
 };
 
-constexpr int kPrefetch = 8;
-constexpr int kSkew = 2;  // iterations between consecutive sections
+#ifndef AC_SYNTH_PREFETCH
+#define AC_SYNTH_PREFETCH 16
+#endif
+#ifndef AC_SYNTH_SKEW
+#define AC_SYNTH_SKEW 4
+#endif
+constexpr int kPrefetch = AC_SYNTH_PREFETCH;
+constexpr int kSkew = AC_SYNTH_SKEW;  // iterations between consecutive sections
 constexpr int kLag = kSkew * 3;  // section 3 runs kLag samples behind section 0
+static_assert(kSkew >= 3 && kLag + 2 <= kPrefetch, "the prefetch window must hold the lagged input");
 
 // Lane (unit, chain, stage): section `stage` works on sample it - kSkew*stage.
 // The float32 output it produces at iteration it is shuffled one lane up at
@@ -183,7 +190,14 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
         ahead[u] = (valid_unit && u < n_len) ? __ldg(x + u) : 0.0;
         prev[u] = 0.0;
     }
-    float q1 = 0.0f;  // value the previous section sent last iteration (this section's input next iteration)
+    // q[d]: the value the previous section produced at iteration it - 1 - d (received through the
+    // shuffle issued one iteration after it was produced, so no shuffle result is used in the
+    // iteration that receives it); q[kSkew - 2] is this section's input at the next iteration.
+    float q[kSkew - 1];
+#pragma unroll
+    for (int i = 0; i < kSkew - 1; ++i) q[i] = 0.0f;
+    float y1f = 0.0f, y2f = 0.0f;   // this lane's float outputs of iterations it - 1 and it - 2
+    float lower2 = 0.0f;            // the lower chain's output of iteration it - 2
     // input part of the first sample (its input is ahead[0] for section 0 and +0.0 otherwise)
     double v = sec.feed(is_first ? ahead[0] : 0.0);
     const int last = n_len + kLag;  // this lane's own end
@@ -197,19 +211,27 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
             const int it = base + u;
-            const float y = sec.step(v);
-            // input of the next iteration: section 0 reads the prefetched signal,
-            // later sections the value their predecessor sent two iterations ago
-            const double in_next = is_first ? (u + 1 < kPrefetch ? ahead[u + 1] : next[0]) : static_cast<double>(q1);
+            const float y = sec.step(v);   // the recursion: the only chain carried from one iteration to the next
+            // exchange the outputs of the previous iteration, already rounded to float32
+            const float sent = __shfl_up_sync(full, y1f, 1);
+            const float lower = __shfl_down_sync(full, y1f, 4);
+#pragma unroll
+            for (int i = kSkew - 2; i > 0; --i) q[i] = q[i - 1];
+            q[0] = sent;
+            // input part of the next iteration: section 0 reads the prefetched signal, later
+            // sections the value their predecessor produced kSkew - 1 iterations before it
+            const double in_next =
+                is_first ? (u + 1 < kPrefetch ? ahead[u + 1] : next[0]) : static_cast<double>(q[kSkew - 2]);
             v = sec.feed(in_next);
-            const float sent = __shfl_up_sync(full, y, 1);
-            const float lower = __shfl_down_sync(full, y, 4);
-            q1 = sent;
-            // x[it - kLag] is still in registers from the prefetch
-            const double x_n = (u >= kLag) ? ahead[u - kLag] : prev[u + kPrefetch - kLag];
-            const float band5 = static_cast<float>(x_n - static_cast<double>(y));
-            const float o = mode == 0 ? y : (mode == 2 ? band5 : y - lower);
-            if (emits && it >= kLag && it < last) out_row[it - kLag] = o;
+            // output of iteration it - 2; x[it - 2 - kLag] is still in registers from the prefetch
+            const int k = u - 2 - kLag;
+            const double x_n = k >= 0 ? ahead[k] : prev[k + kPrefetch];
+            const float band5 = static_cast<float>(x_n - static_cast<double>(y2f));
+            const float o = mode == 0 ? y2f : (mode == 2 ? band5 : y2f - lower2);
+            if (emits && it - 2 >= kLag && it - 2 < last) out_row[it - 2 - kLag] = o;
+            lower2 = lower;
+            y2f = y1f;
+            y1f = y;
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
@@ -230,7 +252,7 @@ __global__ void __launch_bounds__(128) synth_filter_kernel(const double *raw, co
     const int N = a.num_bins * a.spb;
     const double *x = raw + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
     float *out_row = out + static_cast<size_t>(valid_unit ? unit : 0) * static_cast<size_t>(N);
-    filter_units(x, out_row, N, valid_unit, band, a.crossover, N + kLag);
+    filter_units(x, out_row, N, valid_unit, band, a.crossover, N + kLag + 2);
 }
 
 // ---- ragged batches (ac_synthesize_batch) ----------------------------------
@@ -345,7 +367,7 @@ __global__ void __launch_bounds__(32) synth_batch_filter_kernel(const SynthJobDe
     const double *x = raw + 6 * job.samples + static_cast<int64_t>(band) * n_len;
     float *out_row = job.band_irs + static_cast<int64_t>(band) * n_len;
     filter_units(x, out_row, n_len, valid_unit, band, cfg.crossover[valid_unit ? job.rate_index : 0],
-                 longest + kLag);
+                 longest + kLag + 2);
 }
 
 }  // namespace
