@@ -101,3 +101,21 @@ def test_install_routes_only_the_b200_accelerator(backend):
     handle.uninstall()
     with pytest.raises(ValueError):
         fake._normalize_rt_accelerator("b200")
+
+
+def test_capacity_and_sizes_are_checked_before_launch(backend):
+    """num_rays * num_bounces must stay below 2^32 (exact fixed-point sums); bad sizes never launch."""
+    from acoustic_agent_b200 import _lib, runtime, scene, workloads
+    w = workloads.shoebox(3)
+    dev = runtime.DeviceScene(scene.compile_scene(w.spec))
+    buffers = runtime.TraceBuffers.allocate(dev.num_surfaces, 10, torch.device("cuda", 0))
+    base = dict(source=w.sources[0], listener=w.listeners[0], num_bins=10, bin_duration=0.01,
+                speed_of_sound=343.0, max_path_length=343.0, direct_delay=0.01, rng="philox")
+    too_big = runtime.TraceSpec(num_rays=(1 << 31) - 1, num_bounces=3, **base)
+    with pytest.raises(_lib.BackendError) as err:   # AC_ERR_CAPACITY, with the library's message
+        runtime.trace(dev, too_big, buffers)
+    assert err.value.code == _lib.AC_ERR_CAPACITY and "2^32" in str(err.value)
+    with pytest.raises(ValueError):
+        runtime.trace(dev, runtime.TraceSpec(num_rays=0, num_bounces=3, **base), buffers)
+    torch.cuda.synchronize()
+    dev.close()

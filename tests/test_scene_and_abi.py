@@ -141,3 +141,24 @@ def test_synthesis_batch_validation_happens_on_the_host():
     assert lib.ac_synthesize_batch(jobs, 2, ctypes.byref(cfg), None, 0, None, None) == _lib.AC_ERR_INVALID
     cfg.num_rates = 0
     assert lib.ac_synth_batch_workspace_size(jobs, 2, ctypes.byref(cfg), ctypes.byref(size)) == _lib.AC_ERR_INVALID
+
+
+def test_scene_size_limit_is_checked_before_any_device_work():
+    lib = _lib.load()
+    desc = _lib.ACSceneDesc()
+    desc.num_surfaces = 1 << 22
+    handle = ctypes.c_void_p()
+    assert lib.ac_scene_create(ctypes.byref(desc), ctypes.byref(handle)) == _lib.AC_ERR_CAPACITY
+    assert b"surfaces" in lib.ac_last_error()
+
+
+def test_empty_batches_are_accepted():
+    lib = _lib.load()
+    cfg = _lib.ACBatchConfig(0, 0, 0, 0)
+    size = ctypes.c_size_t()
+    assert lib.ac_batch_workspace_size(None, 0, ctypes.byref(cfg), ctypes.byref(size)) == _lib.AC_OK
+    scfg = _lib.ACSynthBatchConfig()
+    scfg.num_rates = 1
+    scfg.sample_rates[0] = 16000
+    assert lib.ac_synth_batch_workspace_size(None, 0, ctypes.byref(scfg), ctypes.byref(size)) == _lib.AC_OK
+    assert lib.ac_synthesize_batch(None, 0, ctypes.byref(scfg), None, 0, None, None) == _lib.AC_OK
