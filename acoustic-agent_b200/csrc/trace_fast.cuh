@@ -97,9 +97,16 @@ struct FRay {
     float inv[3];
 };
 
+// Approximate reciprocal (MUFU, ~1 ulp): the float32 path needs no correctly rounded division.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ float safe_inv(float d) {
     const float m = fabsf(d) < 1e-20f ? copysignf(1e-20f, d) : d;
-    return __frcp_rn(m);
+    return rcp_approx(m);
 }
 
 __device__ __forceinline__ void make_ray(FRay &r, const float *o, const float *d) {
@@ -142,7 +149,7 @@ __device__ __forceinline__ bool point_in_polygon_fast(float x, float y, const fl
 __device__ __forceinline__ float wall_t(const Quad<float> &A, const Quad<float> &B, const FRay &r) {
     const float det = A.z * r.d[1] - A.w * r.d[0];
     if (fabsf(det) > 1e-12f) {
-        const float inv = __frcp_rn(det);
+        const float inv = rcp_approx(det);
         const float relx = r.o[0] - A.x, rely = r.o[1] - A.y;
         const float t = (relx * A.w - rely * A.z) * inv;
         const float u = (relx * r.d[1] - rely * r.d[0]) * inv;
@@ -164,7 +171,7 @@ __device__ __forceinline__ float box_t(const float *rec, const FRay &r) {
     if (fabsf(dx) <= 1e-12f) {
         if (ox < -B.z || ox > B.z) return 1e30f;
     } else {
-        const float ix = __frcp_rn(dx);
+        const float ix = rcp_approx(dx);
         const float a = (-B.z - ox) * ix, b = (B.z - ox) * ix;
         t_min = fminf(a, b);
         t_max = fmaxf(a, b);
@@ -172,7 +179,7 @@ __device__ __forceinline__ float box_t(const float *rec, const FRay &r) {
     if (fabsf(dy) <= 1e-12f) {
         if (oy < -B.w || oy > B.w) return 1e30f;
     } else {
-        const float iy = __frcp_rn(dy);
+        const float iy = rcp_approx(dy);
         const float a = (-B.w - oy) * iy, b = (B.w - oy) * iy;
         t_min = fmaxf(t_min, fminf(a, b));
         t_max = fminf(t_max, fmaxf(a, b));
