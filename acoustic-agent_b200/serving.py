@@ -153,18 +153,21 @@ class SceneCache:
         self.tune_cache = tune_cache or autotune.TuneCache()
         self.entries: OrderedDict[str, runtime.DeviceScene] = OrderedDict()
         self.refs: dict[str, int] = {}
-        self.arrays: dict[int, tuple[str, SceneArrays]] = {}
+        # compiled arrays by the identity of the workload's spec dict; the spec is kept with its
+        # entry, so an id reused by a later object can never alias an earlier scene
+        self.arrays: dict[int, tuple[Any, str, SceneArrays]] = {}
         self.hits = self.misses = self.evictions = 0
 
     def resident_bytes(self) -> int:
         return sum(s.device_bytes for s in self.entries.values())
 
     def key_of(self, w: Workload) -> tuple[str, SceneArrays]:
-        ident = id(w.spec)
-        if ident not in self.arrays:
+        entry = self.arrays.get(id(w.spec))
+        if entry is None or entry[0] is not w.spec:
             arrays = compile_scene(w.spec)
-            self.arrays[ident] = (autotune.fingerprint(arrays), arrays)
-        return self.arrays[ident]
+            entry = (w.spec, autotune.fingerprint(arrays), arrays)
+            self.arrays[id(w.spec)] = entry
+        return entry[1], entry[2]
 
     def is_resident(self, w: Workload) -> bool:
         return self.key_of(w)[0] in self.entries
