@@ -11,9 +11,9 @@
 // recursion itself is sequential in time, so parallelism comes from elsewhere:
 // one warp is a systolic array of 8 four-section low-pass chains.  Lane
 // (unit, chain, stage) runs one biquad section and passes its float32 output
-// one lane up; section s runs two samples behind section s-1.  A "unit" is one band of one RIR: bands 1-4 need
-// two chains (the low-pass at the upper and lower crossover, subtracted),
-// bands 0 and 5 one.  Four units per warp.
+// one lane up; section s runs kSkew samples behind section s-1.  A "unit" is
+// one band of one RIR: bands 1-4 need two chains (the low-pass at the upper
+// and lower crossover, subtracted), bands 0 and 5 one.  Four units per warp.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -155,8 +155,10 @@ static_assert(kSkew >= 3 && kLag + 2 <= kPrefetch, "the prefetch window must hol
 
 // Lane (unit, chain, stage): section `stage` works on sample it - kSkew*stage.
 // The float32 output it produces at iteration it is shuffled one lane up at
-// once but consumed there only at it + kSkew, so the shuffle latency never sits
-// on the recursion's critical path -- only the section's own y dependency does.
+// iteration it + 1 and consumed there at it + kSkew - 1 (as the input part of
+// its step at it + kSkew); the outputs are written two iterations late.  So
+// no instruction waits on a shuffle issued in its own iteration, and only the
+// section's own y dependency is carried from one iteration to the next.
 //
 // The body is branch-free: before a section's first real sample its input is
 // +0.0, and a section whose inputs and state are all +0.0 produces exactly +0.0
@@ -164,7 +166,7 @@ static_assert(kSkew >= 3 && kLag + 2 <= kPrefetch, "the prefetch window must hol
 // out +0.0), so the steps while the pipeline fills change nothing.
 // The per-lane recursion of one warp.  `x` / `out_row` / `n_len` belong to the
 // lane's unit (band of one RIR); `co` points at the lane's section
-// coefficients.  `iterations` (the longest unit of the warp + kLag) is
+// coefficients.  `iterations` (the longest unit of the warp + kLag + 2) is
 // warp-uniform: every lane runs every iteration, so the shuffles stay full-warp.
 __device__ __forceinline__ void filter_units(const double *x, float *out_row, int n_len, bool valid_unit, int band,
                                              const double *co, int iterations) {
