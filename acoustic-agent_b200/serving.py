@@ -229,9 +229,18 @@ class _Batch:
 class Server:
     """Continuous batching over one GPU (see the module docstring)."""
 
+    POLICIES = ("small_first", "fifo")
+
     def __init__(self, device: int = 0, *, max_inflight: int = 3, hbm_budget: int | None = None,
                  max_batch_rays: int = 400_000_000, tune: bool = True, block_size: int = 0,
-                 chunk_rays: int = 0) -> None:
+                 chunk_rays: int = 0, policy: str = "small_first", starve_s: float = 1.0) -> None:
+        """`policy` orders the waiting requests when a batch is formed: "fifo" by arrival, or
+        "small_first" by ray count, except that requests waiting longer than `starve_s` go first
+        (in arrival order), so a stream of small requests cannot hold a large one back for ever."""
+        if policy not in self.POLICIES:
+            raise ValueError(f"policy must be one of {self.POLICIES}")
+        self.policy = policy
+        self.starve_s = float(starve_s)
         self.dev = runtime.require_cuda(device)
         self.max_inflight = max(1, int(max_inflight))
         if hbm_budget is None:
@@ -316,6 +325,18 @@ class Server:
         self.in_use -= batch.bytes
         return out
 
+    def _order(self, waiting, now: float) -> list[tuple[Request, list[runtime.TraceSpec]]]:
+        if self.policy == "fifo":
+            return list(waiting)
+
+        def key(entry):
+            req, ss = entry
+            if now - req.arrival_s > self.starve_s:
+                return (0, req.arrival_s)
+            return (1, sum(s.num_rays for s in ss), req.arrival_s)
+
+        return sorted(waiting, key=key)
+
     def serve(self, requests: Sequence[Request], *, realtime: bool = True, idle_sleep_s: float = 2e-4) -> Report:
         """Run every request to completion; arrivals follow `arrival_s` (wall clock) when `realtime`."""
         pending = deque(sorted(requests, key=lambda r: r.arrival_s))
@@ -338,11 +359,11 @@ class Server:
                     results.extend(self._finish(batch, done_at))
                     inflight.remove(batch)
                     free_streams.append(batch.stream)
-            # admit everything that fits into one new batch while a slot is free
+            # admit what fits into one new batch while a slot is free
             if waiting and free_streams:
                 reqs, specs, need_total, rays = [], [], 0, 0
-                while waiting:
-                    req, ss = waiting[0]
+                for entry in self._order(waiting, time.perf_counter() - t0 if realtime else 0.0):
+                    req, ss = entry
                     need = self.footprint(req, ss)
                     req_rays = sum(s.num_rays for s in ss)
                     if reqs and rays + req_rays > self.max_batch_rays:
@@ -350,13 +371,13 @@ class Server:
                     if not self._fits(need_total + need):
                         if not reqs and not inflight and self.scenes.resident_bytes() + need > self.budget:
                             # cannot fit even on an idle device: reject it, keep serving the others
-                            waiting.popleft()
+                            waiting.remove(entry)
                             t = time.perf_counter() - t0
                             results.append(Result(req, [], 0, t, t, error=f"needs {need} bytes of device memory; "
                                                                               f"the budget is {self.budget}"))
                             continue
                         break
-                    waiting.popleft()
+                    waiting.remove(entry)
                     reqs.append(req)
                     specs.append(ss)
                     need_total += need

@@ -355,6 +355,10 @@ def main() -> int:
                         help="mixed_batch: jobs of the plain per-job loop to time (0: all)")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
     parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
+    parser.add_argument("--policy", default="small_first", choices=("small_first", "fifo"),
+                        help="serving: order in which waiting requests join a batch")
+    parser.add_argument("--max-batch-rays", type=int, default=400_000_000, help="serving: rays per batch at most")
+    parser.add_argument("--max-inflight", type=int, default=3, help="serving: batches on the GPU at once")
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
@@ -662,7 +666,8 @@ def run_serving(args) -> int:
     population = workloads.mixed_batch(1730, 64)
     stream = workloads.request_stream(1729, rate_hz=args.rate, duration_s=args.duration, population=population)
     requests = serving.requests_from_stream(stream)
-    server = serving.Server(local, max_inflight=3)
+    server = serving.Server(local, max_inflight=args.max_inflight, policy=args.policy,
+                            max_batch_rays=args.max_batch_rays)
     t0 = time.perf_counter()
     for w in population:   # warm the resident scene cache (upload + tune) before the clock starts
         req = serving.Request(-1, w, [w.sources[0]])
@@ -681,7 +686,8 @@ def run_serving(args) -> int:
         "warmup": min(len(requests), 8), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, Poisson arrivals)",
         "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s over 64 mixed scenes, "
-                               "20% moving sources x 8 keyframes", "requests": len(requests),
+                               "20% moving sources x 8 keyframes", "requests": len(requests), "policy": args.policy,
+                   "max_batch_rays": args.max_batch_rays,
                    "moving": sum(r.moving for r in requests), "max_inflight": server.max_inflight},
         "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]},
         "ray_bounces_per_s": s["ray_bounces_per_s"], "rirs": s["rirs"], "makespan_s": s["makespan_s"],
