@@ -135,6 +135,30 @@ class ACSynthBatchConfig(ctypes.Structure):
     ]
 
 
+AC_FDN_LINES, AC_FDN_ALLPASS, AC_FDN_MIN_DELAY, AC_FDN_MAX_ALLPASS = 16, 4, 72, 4096
+AC_LATE_STATS = 8
+(AC_LATE_SCALE, AC_LATE_POWER, AC_LATE_FDN_ENERGY, AC_LATE_TRACED_TAIL, AC_LATE_RENDERED_TAIL, AC_LATE_COMPONENT,
+ AC_LATE_CHANGED) = range(7)
+
+
+class ACFdnJob(ctypes.Structure):
+    _fields_ = [
+        ("absorptive", ctypes.c_double * (AC_FDN_LINES * 6 * 5)), ("tone", ctypes.c_double * 30),
+        ("delays", ctypes.c_int32 * AC_FDN_LINES), ("allpass_delays", ctypes.c_int32 * AC_FDN_ALLPASS),
+        ("num_samples", ctypes.c_int32), ("preroll", ctypes.c_int32), ("out", ctypes.c_void_p),
+    ]
+
+
+class ACLateTailJob(ctypes.Structure):
+    _fields_ = [
+        ("traced", ctypes.c_void_p), ("fdn", ctypes.c_void_p), ("out", ctypes.c_void_p),
+        ("fdn_component", ctypes.c_void_p), ("stats", ctypes.c_void_p), ("rt60", ctypes.c_double * 6),
+        ("start", ctypes.c_int32 * 6), ("end", ctypes.c_int32 * 6), ("anchor", ctypes.c_int32 * 6),
+        ("changed_from", ctypes.c_int32), ("num_samples", ctypes.c_int32), ("bin_samples", ctypes.c_int32),
+        ("rate_index", ctypes.c_int32),
+    ]
+
+
 # Every symbol include/acoustic_rt.h declares, with (restype, argtypes).
 SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_last_error": (ctypes.c_char_p, []),
@@ -167,6 +191,16 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_synthesize_batch_filter": (ctypes.c_int, [ctypes.POINTER(ACSynthJob), ctypes.c_int32,
                                                   ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p,
                                                   ctypes.c_size_t, ctypes.c_void_p]),
+    "ac_fdn_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACFdnJob), ctypes.c_int32,
+                                             ctypes.POINTER(ctypes.c_size_t)]),
+    "ac_fdn_impulse": (ctypes.c_int, [ctypes.POINTER(ACFdnJob), ctypes.c_int32, ctypes.c_void_p, ctypes.c_size_t,
+                                      ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_late_tail_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACLateTailJob), ctypes.c_int32,
+                                                   ctypes.POINTER(ACSynthBatchConfig),
+                                                   ctypes.POINTER(ctypes.c_size_t)]),
+    "ac_late_tail": (ctypes.c_int, [ctypes.POINTER(ACLateTailJob), ctypes.c_int32,
+                                    ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
+                                    ctypes.c_void_p, ctypes.c_void_p]),
     "ac_read_bandwidth_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_void_p,
                                                ctypes.c_void_p]),
     "ac_synthesize_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,

@@ -203,7 +203,9 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
 
     After ``install()``, ``rt_accelerator="b200"`` selects the GPU tracer here; with
     ``route_cuda=True`` the reference's ``"cuda"`` setting is routed here too.  Other
-    settings keep the reference's own dispatch (steam_rt.py:1757-1811).
+    settings keep the reference's own dispatch (steam_rt.py:1757-1811).  The same
+    setting routes the FDN late tail (``_render_parametric_fdn_late_reverb``,
+    steam_rt.py:2500, called by the renderer at :1029) to ``late_reverb``.
     """
     if steam_rt_module is None:
         import acoustic_agent.steam_rt as steam_rt_module  # type: ignore[import-not-found]
@@ -224,7 +226,18 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
                                       render_ambisonics=render_ambisonics)
         return original_trace(scene, source, listener, config, source_model, render_ambisonics=render_ambisonics)
 
+    original_late = steam_rt_module._render_parametric_fdn_late_reverb
+
+    def routed_late(traced_band_irs, field, rt60_bands, config, *, decay_profiles=None):
+        if normalize(config.rt_accelerator) in handled:
+            from acoustic_agent_b200 import late_reverb
+            return late_reverb.render_parametric_fdn_late_reverb(traced_band_irs, field, rt60_bands, config,
+                                                                 decay_profiles=decay_profiles)
+        return original_late(traced_band_irs, field, rt60_bands, config, decay_profiles=decay_profiles)
+
     steam_rt_module.trace_energy_field = routed_trace
     steam_rt_module._normalize_rt_accelerator = normalize
+    steam_rt_module._render_parametric_fdn_late_reverb = routed_late
     return Installation(steam_rt_module, {"trace_energy_field": original_trace,
-                                          "_normalize_rt_accelerator": original_normalize})
+                                          "_normalize_rt_accelerator": original_normalize,
+                                          "_render_parametric_fdn_late_reverb": original_late})

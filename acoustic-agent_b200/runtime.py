@@ -370,10 +370,10 @@ class _StagedWorkspace:
         self.host_buffer: torch.Tensor | None = None
         self._copied: torch.cuda.Event | None = None
 
-    def ensure(self, jobs, num_jobs: int, cfg) -> tuple[int, int, int]:
+    def ensure(self, jobs, num_jobs: int, cfg=None) -> tuple[int, int, int]:
         size = ctypes.c_size_t()
-        _lib.check(getattr(_lib.load(), self.SIZE_FN)(jobs, num_jobs, ctypes.byref(cfg), ctypes.byref(size)),
-                   self.SIZE_FN)
+        args = (jobs, num_jobs) + ((ctypes.byref(cfg),) if cfg is not None else ()) + (ctypes.byref(size),)
+        _lib.check(getattr(_lib.load(), self.SIZE_FN)(*args), self.SIZE_FN)
         need = max(int(size.value), 256)
         if self._copied is not None and not torch.cuda.is_current_stream_capturing():
             self._copied.synchronize()   # host waits are not allowed inside a capture (nor needed there)
@@ -624,6 +624,44 @@ def synthesize_batch(jobs: Sequence[SynthJob] | tuple[ctypes.Array, int, _lib.AC
     fn = lib.ac_synthesize_batch if phase == "all" else lib.ac_synthesize_batch_raw
     _lib.check(fn(arr, n, ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes, ctypes.c_void_p(host),
                   _stream_ptr(stream)), "ac_synthesize_batch")
+    workspace.launched(stream)
+
+
+# ---------------------------------------------------------------------------
+# Late reverberation (FDN impulse + hybrid tail)
+
+
+class FdnWorkspace(_StagedWorkspace):
+    """Reusable device workspace + pinned staging for ac_fdn_impulse."""
+
+    SIZE_FN = "ac_fdn_workspace_size"
+
+
+class LateTailWorkspace(_StagedWorkspace):
+    """Reusable device workspace + pinned staging for ac_late_tail."""
+
+    SIZE_FN = "ac_late_tail_workspace_size"
+
+
+def fdn_impulse(jobs: ctypes.Array, num_jobs: int, workspace: FdnWorkspace, *,
+                stream: torch.cuda.Stream | None = None) -> None:
+    """Every job's FDN impulse response into its `out` (ac_fdn_impulse), one launch."""
+    if num_jobs == 0:
+        return
+    ws, ws_bytes, host = workspace.ensure(jobs, num_jobs)
+    _lib.check(_lib.load().ac_fdn_impulse(jobs, num_jobs, ctypes.c_void_p(ws), ws_bytes, ctypes.c_void_p(host),
+                                          _stream_ptr(stream)), "ac_fdn_impulse")
+    workspace.launched(stream)
+
+
+def late_tail(jobs: ctypes.Array, num_jobs: int, config: _lib.ACSynthBatchConfig, workspace: LateTailWorkspace, *,
+              stream: torch.cuda.Stream | None = None) -> None:
+    """Band-limit, scale and crossfade every job's FDN into its traced band signals (ac_late_tail)."""
+    if num_jobs == 0:
+        return
+    ws, ws_bytes, host = workspace.ensure(jobs, num_jobs, config)
+    _lib.check(_lib.load().ac_late_tail(jobs, num_jobs, ctypes.byref(config), ctypes.c_void_p(ws), ws_bytes,
+                                        ctypes.c_void_p(host), _stream_ptr(stream)), "ac_late_tail")
     workspace.launched(stream)
 
 

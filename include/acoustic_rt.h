@@ -344,6 +344,75 @@ int ac_synthesize_batch_raw(const ac_synth_job *jobs, int32_t num_jobs, const ac
 int ac_synthesize_batch_filter(const ac_synth_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
                                void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- late reverberation (steam_rt.py:2235-2640) ------------------------
+ *
+ * One FDN impulse response: _fdn_impulse_kernel(delays, absorptive,
+ * preroll + num_samples, allpass_delays, tone)[preroll:]
+ * (steam_rt.py:2235-2327, called at :2579-2586).  The delay and filter design
+ * (_steam_fdn_delays, _steam_fdn_filter_coefficients, :2330-2470) is host
+ * work and arrives here as numbers.  Every output sample is bit-identical to
+ * the reference's float64 kernel given the same design. */
+#define AC_FDN_LINES 16
+#define AC_FDN_ALLPASS 4
+#define AC_FDN_MIN_DELAY 72      /* delay lines shorter than this are refused (fs below about 1 kHz) */
+#define AC_FDN_MAX_ALLPASS 4096  /* longest all-pass stage; the shortest must exceed 32 */
+typedef struct ac_fdn_job {
+    double absorptive[AC_FDN_LINES][6][5];  /* per line and band: b0 b1 b2 a1 a2 */
+    double tone[6][5];                      /* output tone-correction sections */
+    int32_t delays[AC_FDN_LINES];           /* delay-line lengths in samples */
+    int32_t allpass_delays[AC_FDN_ALLPASS]; /* Schroeder all-pass lengths (225, 341, 441, 556 in the reference) */
+    int32_t num_samples;                    /* samples written to `out` */
+    int32_t preroll;                        /* samples run before the first one written */
+    double *out;                            /* device [num_samples] float64 */
+} ac_fdn_job;
+
+/* Device workspace (job table + delay lines) and pinned staging bytes for ac_fdn_impulse. */
+int ac_fdn_workspace_size(const ac_fdn_job *jobs, int32_t num_jobs, size_t *bytes);
+
+/* Any number of FDN impulse responses in one launch (one 64-thread block per
+ * job); the job table is staged as for ac_synthesize_batch. */
+int ac_fdn_impulse(const ac_fdn_job *jobs, int32_t num_jobs, void *workspace, size_t workspace_bytes,
+                   void *host_staging, void *stream);
+
+/* The hybrid tail of _render_parametric_fdn_late_reverb
+ * (steam_rt.py:2588-2640) for one RIR: the FDN impulse is split into six
+ * bands by bandlimit_band_signals, each band is scaled so that its energy
+ * after `anchor` equals the traced power there decaying at the band's RT60
+ * (_late_tail_start_power, :2473-2497), and crossfaded into the traced band
+ * signal with the equal-power ramp over [start, end).  Bands with rt60 <= 0
+ * keep the unscaled FDN, as in the reference.  Outputs are the float32 casts
+ * the reference returns; `stats` receives per band AC_LATE_STATS doubles. */
+#define AC_LATE_STATS 8
+enum {
+    AC_LATE_SCALE = 0,          /* scale_by_band (1 for rt60 <= 0) */
+    AC_LATE_POWER = 1,          /* anchor_power_by_band */
+    AC_LATE_FDN_ENERGY = 2,     /* fdn_energy_by_band: sum of the scaled FDN band from start */
+    AC_LATE_TRACED_TAIL = 3,    /* sum of traced^2 from start */
+    AC_LATE_RENDERED_TAIL = 4,  /* sum of out^2 (float64, before the cast) from start */
+    AC_LATE_COMPONENT = 5,      /* sum of fdn_component^2 (float64) over the band */
+    AC_LATE_CHANGED = 6,        /* 1 if any sample from `changed_from` fails allclose(out, traced, 1e-7, 1e-12) */
+};
+typedef struct ac_late_tail_job {
+    const double *traced;     /* device [6, num_samples] float64 traced band signals */
+    const double *fdn;        /* device [num_samples] float64 FDN impulse (ac_fdn_impulse's out) */
+    float *out;               /* device [6, num_samples] hybrid band signals */
+    float *fdn_component;     /* device [6, num_samples] the crossfaded FDN part of `out` */
+    double *stats;            /* device [6, AC_LATE_STATS] */
+    double rt60[6];           /* target RT60 per band in seconds */
+    int32_t start[6];         /* crossfade start sample per band */
+    int32_t end[6];           /* crossfade end sample per band (> start) */
+    int32_t anchor[6];        /* sample where the tail power is measured (start, or end at a fitted breakpoint) */
+    int32_t changed_from;     /* first sample of the `changed` test (the smallest start) */
+    int32_t num_samples;
+    int32_t bin_samples;      /* round(bin_duration * fs), at least 1 */
+    int32_t rate_index;       /* sample rate / crossover table of the config */
+} ac_late_tail_job;
+
+int ac_late_tail_workspace_size(const ac_late_tail_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                                size_t *bytes);
+int ac_late_tail(const ac_late_tail_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
+                 void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
+
 /* Measurement helper, no counterpart in the reference: reads `bytes` (a
  * multiple of 16 is used) of device memory `repeats` times with 16-byte loads
  * cached in L2 only, on `stream`; time it with events to get the L2 (buffer

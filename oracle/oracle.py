@@ -9,6 +9,9 @@ never as part of the product path.
 * ``synthesize``   echogram -> band signals (steam_rt.py:2205-2232, 3070-3083, 4131-4212)
 * ``build_bvh``    numpy restatement of acoustic_agent/bvh.py:8-77
 * ``workspace``    the reference's random workspace (steam_rt.py:3959-4044)
+* ``fdn_impulse``  the sixteen-line FDN of steam_rt.py:2235-2327, restated in C
+* ``fdn_design`` / ``late_reverb``  the FDN's delay and filter design and the
+                   hybrid late-tail render (steam_rt.py:2330-2640), restated in numpy
 * ``philox_workspace`` numpy Philox4x32-10 (Salmon et al., SC'11) producing the
                    directions / uniforms / bank indices the GPU's counter-based
                    mode draws, so that mode can be checked ray by ray
@@ -94,6 +97,11 @@ def _lib() -> ctypes.CDLL:
         lib.oracle_closest_hit.argtypes = [ctypes.POINTER(_Scene), _d, _d, _d, _d]
         lib.oracle_synthesize.restype = ctypes.c_int
         lib.oracle_synthesize.argtypes = [_d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _d, _d, _d, _f32]
+        lib.oracle_bandlimit.restype = ctypes.c_int
+        lib.oracle_bandlimit.argtypes = [_d, ctypes.c_int64, _d, _f32]
+        lib.oracle_fdn_impulse.restype = ctypes.c_int
+        lib.oracle_fdn_impulse.argtypes = [_i64, ctypes.c_int64, _d, ctypes.c_int64, ctypes.c_int64, _i64,
+                                           ctypes.c_int64, _d, _d]
         _LIB = lib
     return _LIB
 
@@ -376,3 +384,233 @@ def philox_noise(num_samples: int, seed: int) -> np.ndarray:
     out[0::2] = -1.0 + 2.0 * _u01_53(x, y)
     out[1::2] = -1.0 + 2.0 * _u01_53(z, w)
     return out[:num_samples]
+
+
+# ---- late reverberation: FDN design, impulse and hybrid tail ------------------
+
+BANDS = ("125", "250", "500", "1000", "2000", "4000")
+_INNER_EDGES = (176.78, 353.55, 707.11, 1414.2, 2828.4)
+FDN_PRIMES = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53)
+FDN_ALLPASS = (225, 341, 441, 556)
+
+
+def bandlimit(signals: np.ndarray, fs: int) -> np.ndarray:
+    """bandlimit_band_signals (steam_rt.py:3070-3083): float64 [6, n] -> float32 [6, n]."""
+    x = np.ascontiguousarray(signals, dtype=np.float64)
+    out = np.zeros(x.shape, dtype=np.float32)
+    rc = _lib().oracle_bandlimit(_p(x, _d), x.shape[1], _p(crossover_table(fs), _d), _p(out, _f32))
+    if rc != 0:
+        raise RuntimeError(f"oracle_bandlimit failed ({rc})")
+    return out
+
+
+def fdn_delays(fs: int, seed: int) -> np.ndarray:
+    """steam_rt.py:2330-2340: prime powers near 0.15 s / 16 lines plus a seeded 0-100 sample jitter."""
+    target0 = max(1, int(0.15 * 10.0 * max(int(fs), 1) / len(FDN_PRIMES)))
+    jitter = np.random.default_rng(int(seed) + 1701).integers(0, 101, size=len(FDN_PRIMES))
+    out = np.empty(len(FDN_PRIMES), dtype=np.int64)
+    for i, p in enumerate(FDN_PRIMES):
+        target = max(1, target0 + int(jitter[i]))
+        power = max(1, int(round(math.log(target) / math.log(p))))
+        out[i] = max(1, p ** power)
+    return out
+
+
+def _shelf(cutoff: float, gain: float, fs: int, high: bool) -> np.ndarray:
+    """RBJ shelving section, Q = 0.707 (steam_rt.py:2343-2378); `high` flips the sign of the (A-1) terms."""
+    w0 = 2.0 * math.pi * float(cutoff) / max(float(fs), 1.0)
+    cw, sw = math.cos(w0), math.sin(w0)
+    alpha = sw / (2.0 * 0.707)
+    A = math.sqrt(max(float(gain), 1e-6))
+    ra = math.sqrt(A)
+    if not high:
+        a0 = (A + 1.0) + (A - 1.0) * cw + 2.0 * ra * alpha
+        return np.asarray((A * ((A + 1.0) - (A - 1.0) * cw + 2.0 * ra * alpha) / a0,
+                           2.0 * A * ((A - 1.0) - (A + 1.0) * cw) / a0,
+                           A * ((A + 1.0) - (A - 1.0) * cw - 2.0 * ra * alpha) / a0,
+                           -2.0 * ((A - 1.0) + (A + 1.0) * cw) / a0,
+                           ((A + 1.0) + (A - 1.0) * cw - 2.0 * ra * alpha) / a0))
+    a0 = (A + 1.0) - (A - 1.0) * cw + 2.0 * ra * alpha
+    return np.asarray((A * ((A + 1.0) + (A - 1.0) * cw + 2.0 * ra * alpha) / a0,
+                       -2.0 * A * ((A - 1.0) + (A + 1.0) * cw) / a0,
+                       A * ((A + 1.0) + (A - 1.0) * cw - 2.0 * ra * alpha) / a0,
+                       2.0 * ((A - 1.0) - (A + 1.0) * cw) / a0,
+                       ((A + 1.0) - (A - 1.0) * cw - 2.0 * ra * alpha) / a0))
+
+
+def _peak(low: float, high: float, gain: float, fs: int) -> np.ndarray:
+    """RBJ peaking section between two edges (steam_rt.py:2381-2398)."""
+    centre = math.sqrt(max(float(low) * float(high), 1e-12))
+    bw = (float(high) - float(low)) / centre
+    w0 = 2.0 * math.pi * centre / max(float(fs), 1.0)
+    cw, sw = math.cos(w0), math.sin(w0)
+    alpha = sw * bw / 2.0
+    A = math.sqrt(max(float(gain), 1e-6))
+    a0 = 1.0 + alpha / A
+    return np.asarray(((1.0 + alpha * A) / a0, -2.0 * cw / a0, (1.0 - alpha * A) / a0, -2.0 * cw / a0,
+                       (1.0 - alpha / A) / a0))
+
+
+def multiband_sections(gains, fs: int) -> np.ndarray:
+    """steam_rt.py:2401-2416: low shelf, four peaking sections, high shelf -> [6, 5]."""
+    g = np.asarray(gains, dtype=np.float64).reshape(6)
+    nyq = max(1.0, 0.5 * float(fs))
+    edges = [0.0, *_INNER_EDGES, float(fs) * 0.5]
+    rows = []
+    for b in range(6):
+        lo, hi = edges[b], edges[b + 1]
+        if b == 0:
+            rows.append(_shelf(min(max(hi, 1e-3), nyq * 0.999), g[b], fs, False))
+        elif b == 5:
+            rows.append(_shelf(min(max(lo, 1e-3), nyq * 0.999), g[b], fs, True))
+        else:
+            lower = min(max(lo, 1e-3), nyq * 0.998)
+            upper = min(max(hi, lower + 1e-3), nyq * 0.999)
+            rows.append(_peak(lower, upper, g[b], fs))
+    return np.asarray(rows, dtype=np.float64)
+
+
+def multiband_response(fs: int) -> np.ndarray:
+    """steam_rt.py:2419-2435: log-gain response of the cascade at the band centres per unit log-gain of
+    each section (probe gain 0.5)."""
+    centres = np.minimum(np.asarray([float(b) for b in BANDS]), 0.9 * 0.5 * max(float(fs), 1.0))
+    z = np.exp(-2.0j * math.pi * centres / max(float(fs), 1.0))
+    m = np.empty((6, 6))
+    for k in range(6):
+        g = np.ones(6)
+        g[k] = 0.5
+        h = np.ones(6, dtype=np.complex128)
+        for c in multiband_sections(g, fs):
+            h *= (c[0] + c[1] * z + c[2] * z * z) / (1.0 + c[3] * z + c[4] * z * z)
+        m[:, k] = np.log(np.maximum(np.abs(h), 1e-12)) / math.log(0.5)
+    return m
+
+
+def compensated_sections(gains, fs: int, response: np.ndarray | None = None) -> np.ndarray:
+    """steam_rt.py:2438-2452: solve for section gains whose cascade hits the six targets."""
+    want = np.clip(np.asarray(gains, dtype=np.float64).reshape(6), 1e-3, 0.999999)
+    m = multiband_response(fs) if response is None else response
+    try:
+        logs = np.linalg.solve(m, np.log(want))
+    except np.linalg.LinAlgError:
+        logs = np.linalg.pinv(m) @ np.log(want)
+    return multiband_sections(np.clip(np.exp(logs), 1e-3, 4.0), fs)
+
+
+def fdn_design(fs: int, seed: int, rt60) -> dict[str, np.ndarray]:
+    """Delays, per-line absorptive sections [16, 6, 5] and tone sections [6, 5] (steam_rt.py:2455-2470)."""
+    delays = fdn_delays(fs, seed)
+    t60 = np.asarray([max(0.1, float(v or 0.0)) for v in rt60], dtype=np.float64)
+    m = multiband_response(fs)
+    absorptive = np.empty((delays.size, 6, 5))
+    for line, d in enumerate(delays.astype(np.float64)):
+        g = np.maximum(np.exp(-(6.91 * d) / (t60 * max(float(fs), 1.0))), 1e-3)
+        absorptive[line] = compensated_sections(g, fs, m)
+    tone = np.sqrt(1.0 / t60)
+    tone /= max(float(np.max(tone)), 1e-12)
+    return {"delays": delays, "absorptive": absorptive, "tone": multiband_sections(tone, fs),
+            "allpass": np.asarray(FDN_ALLPASS, dtype=np.int64)}
+
+
+def fdn_impulse(delays, absorptive, num_samples: int, allpass, tone) -> np.ndarray:
+    """_fdn_impulse_kernel (steam_rt.py:2235-2327): float64 [num_samples]."""
+    d = np.ascontiguousarray(delays, dtype=np.int64)
+    a = np.ascontiguousarray(absorptive, dtype=np.float64)
+    ap = np.ascontiguousarray(allpass, dtype=np.int64)
+    t = np.ascontiguousarray(tone, dtype=np.float64)
+    out = np.zeros(int(num_samples))
+    rc = _lib().oracle_fdn_impulse(_p(d, _i64), d.size, _p(a, _d), a.shape[1], int(num_samples), _p(ap, _i64),
+                                   ap.size, _p(t, _d), _p(out, _d))
+    if rc != 0:
+        raise RuntimeError(f"oracle_fdn_impulse failed ({rc})")
+    return out
+
+
+def late_tail_start_power(signal: np.ndarray, start: int, rt60: float, fs: int, bin_samples: int) -> float:
+    """steam_rt.py:2473-2497: power at the tail start, from the bin there and the last five non-empty
+    bins before it, each decayed to the start at the target RT60."""
+    sq = np.square(np.asarray(signal, dtype=np.float64))
+    start = min(max(0, int(start)), sq.size)
+    here = sq[start:min(sq.size, start + bin_samples)]
+    power = float(np.mean(here)) if here.size else 0.0
+    if start <= 0:
+        return power
+    nb = int(math.ceil(start / bin_samples))
+    energy = np.asarray([float(np.sum(sq[i * bin_samples:min(start, (i + 1) * bin_samples)])) for i in range(nb)])
+    nonempty = np.flatnonzero(energy > 1e-18)
+    if nonempty.size == 0:
+        return power
+    k = 6.0 * math.log(10.0) / max(float(rt60), 0.1)
+    guesses = [(energy[i] / bin_samples) * math.exp(-k * max(0.0, (start - (float(i) + 0.5) * bin_samples)
+                                                               / max(float(fs), 1.0)))
+               for i in nonempty[-min(5, nonempty.size):]]
+    return max(power, float(np.median(guesses)))
+
+
+def late_tail_windows(num_samples: int, fs: int, transition_s: float, overlap_fraction: float,
+                      decay_profiles=None):
+    """Per-band crossfade start / end samples and models (steam_rt.py:2508-2541)."""
+    N = int(num_samples)
+    fs = max(1, int(fs))
+    duration = N / fs
+    trans = min(max(1.0 / fs, float(transition_s)), max(1.0 / fs, (N - 1) / fs))
+    ov = float(np.clip(overlap_fraction, 0.0, 0.95))
+    s0 = min(N, max(0, int(math.floor((1.0 - ov) * trans * fs))))
+    e0 = min(N, max(s0 + 1, int(math.ceil(trans * fs))))
+    starts, ends, models = [s0] * 6, [e0] * 6, ["configured_hybrid_transition"] * 6
+    profiles = decay_profiles if isinstance(decay_profiles, Mapping) else {}
+    for b, band in enumerate(BANDS):
+        prof = profiles.get(band)
+        if not isinstance(prof, Mapping):
+            continue
+        bp = float(prof.get("transition_time_s", 0.0) or 0.0)
+        if str(prof.get("selected_target_source", "")) == "fitted_late_slope" and 0.0 < bp < duration:
+            starts[b] = min(N - 1, max(0, int(math.floor((1.0 - ov) * bp * fs))))
+            ends[b] = min(N, max(starts[b] + 1, int(math.ceil(bp * fs))))
+            models[b] = "coupled_space_breakpoint"
+    return starts, ends, models, trans, ov, (1.0 - ov) * trans
+
+
+def late_reverb(traced: np.ndarray, bin_duration_s: float, rt60_bands: Mapping[str, float], *, fs: int, seed: int,
+                transition_s: float, overlap_fraction: float, late_tail: bool = True, decay_profiles=None):
+    """_render_parametric_fdn_late_reverb (steam_rt.py:2500-2640) without the metadata: float32 (out, fdn
+    component) plus per-band scales and anchor powers.  Returns None for the pass-through cases."""
+    x = np.asarray(traced, dtype=np.float64)
+    N = x.shape[1]
+    fs = max(1, int(fs))
+    starts, ends, models, _, _, _ = late_tail_windows(N, fs, transition_s, overlap_fraction, decay_profiles)
+    if not late_tail or min(starts) >= N:
+        return None
+    rt60 = [float(rt60_bands.get(b, 0.0) or 0.0) for b in BANDS]
+    design = fdn_design(fs, seed, rt60)
+    pre = int(np.max(design["delays"]) + np.sum(design["allpass"]))
+    raw = fdn_impulse(design["delays"], design["absorptive"], N + pre, design["allpass"], design["tone"])[pre:]
+    fdn = bandlimit(np.repeat(raw[None, :], 6, axis=0), fs).astype(np.float64)
+    bin_samples = max(1, int(round(float(bin_duration_s) * fs)))
+    scales, powers = [1.0] * 6, [0.0] * 6
+    for b in range(6):
+        if rt60[b] <= 0.0:
+            continue
+        anchor = ends[b] if models[b] == "coupled_space_breakpoint" else starts[b]
+        p = late_tail_start_power(x[b], anchor, rt60[b], fs, bin_samples)
+        k = 6.0 * math.log(10.0) / max(rt60[b], 0.1)
+        target = float(np.sum(p * np.exp(-k * np.arange(N - anchor, dtype=np.float64) / fs)))
+        unit = float(np.sum(np.square(fdn[b, anchor:])))
+        scales[b] = math.sqrt(target / max(unit, 1e-24)) if target > 0.0 else 0.0
+        powers[b] = p
+        fdn[b, starts[b]:] *= scales[b]
+    out = x.copy()
+    comp = np.zeros_like(x)
+    for b in range(6):
+        s, e = starts[b], ends[b]
+        ramp = max(1, e - s)
+        alpha = np.linspace(1.0, 0.0, ramp, endpoint=False)
+        out[b, s:e] *= np.sqrt(alpha)
+        if e < N:
+            out[b, e:] = 0.0
+        w = np.ones(N - s)
+        w[:ramp] = np.sqrt(1.0 - alpha)
+        comp[b, s:] = fdn[b, s:] * w
+    out += comp
+    return out.astype(np.float32), comp.astype(np.float32), {"scales": scales, "powers": powers,
+                                                             "starts": starts, "ends": ends}

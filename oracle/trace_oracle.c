@@ -18,6 +18,7 @@
  *   - acoustic_agent/steam_rt.py:4131-4146  _biquad_filter_jit
  *   - acoustic_agent/steam_rt.py:2205-2232  reconstruct_band_irs envelope
  *   - acoustic_agent/steam_rt.py:3070-3083  bandlimit_band_signals
+ *   - acoustic_agent/steam_rt.py:2235-2327  _fdn_impulse_kernel (16-line FDN)
  *
  * Build with -ffp-contract=off and without -ffast-math: Numba evaluates
  * every multiply and add separately in IEEE double, and so must this file.
@@ -572,5 +573,110 @@ int oracle_synthesize(const double *echogram, int64_t echogram_f32, int64_t num_
     lowpass8(raw + (NB - 1) * N, lp_lo, tmp, N, crossover + 20 * (NB - 2));
     for (int64_t i = 0; i < N; ++i) out[(NB - 1) * N + i] = (float)(raw[(NB - 1) * N + i] - (double)lp_lo[i]);
     free(raw); free(tmp); free(lp_hi); free(lp_lo); free(amps);
+    return 0;
+}
+
+/* bandlimit_band_signals (steam_rt.py:3070-3083) on six float64 signals [6, n]. */
+int oracle_bandlimit(const double *signals, int64_t n, const double *crossover, float *out)
+{
+    double *tmp = malloc(sizeof(double) * (n > 0 ? n : 1));
+    float *lp_hi = malloc(sizeof(float) * (n > 0 ? n : 1));
+    float *lp_lo = malloc(sizeof(float) * (n > 0 ? n : 1));
+    if (!tmp || !lp_hi || !lp_lo) {
+        free(tmp); free(lp_hi); free(lp_lo);
+        return -2;
+    }
+    lowpass8(signals, out, tmp, n, crossover);
+    for (int bi = 1; bi < NB - 1; ++bi) {
+        lowpass8(signals + bi * n, lp_hi, tmp, n, crossover + 20 * bi);
+        lowpass8(signals + bi * n, lp_lo, tmp, n, crossover + 20 * (bi - 1));
+        for (int64_t i = 0; i < n; ++i) out[bi * n + i] = lp_hi[i] - lp_lo[i];
+    }
+    lowpass8(signals + (NB - 1) * n, lp_lo, tmp, n, crossover + 20 * (NB - 2));
+    for (int64_t i = 0; i < n; ++i) out[(NB - 1) * n + i] = (float)(signals[(NB - 1) * n + i] - (double)lp_lo[i]);
+    free(tmp); free(lp_hi); free(lp_lo);
+    return 0;
+}
+
+/* One direct-form-I section y = b0*x + b1*x1 + b2*x2 - a1*y1 - a2*y2, left to right; state {x1, x2, y1, y2}. */
+static double fdn_section(const double *co, double *st, double x)
+{
+    double y = co[0] * x + co[1] * st[0] + co[2] * st[1] - co[3] * st[2] - co[4] * st[3];
+    st[1] = st[0];
+    st[0] = x;
+    st[3] = st[2];
+    st[2] = y;
+    return y;
+}
+
+/*
+ * The sixteen-line feedback delay network of steam_rt.py:2235-2327, one
+ * sample at a time in the reference's order: each line reads its delay
+ * line and runs its absorptive sections (absorptive[line][band][5]); the
+ * line outputs are mixed by an unnormalised Hadamard butterfly (strides 1,
+ * 2, 4, ...) and written back scaled by 0.25 (plus the unit impulse at
+ * sample 0); the output is the mean of the line outputs through the
+ * Schroeder all-pass stages (gain 0.5) and the tone sections tone[band][5].
+ */
+int oracle_fdn_impulse(const int64_t *delays, int64_t num_delays, const double *absorptive, int64_t num_bands,
+                       int64_t num_samples, const int64_t *allpass_delays, int64_t num_allpass, const double *tone,
+                       double *out)
+{
+    int64_t max_delay = 0, max_allpass = 0;
+    for (int64_t l = 0; l < num_delays; ++l) max_delay = delays[l] > max_delay ? delays[l] : max_delay;
+    for (int64_t s = 0; s < num_allpass; ++s) max_allpass = allpass_delays[s] > max_allpass ? allpass_delays[s] : max_allpass;
+    max_delay += 1;
+    max_allpass += 1;
+    double *lines = calloc((size_t)(num_delays * max_delay), sizeof(double));
+    int64_t *pos = calloc((size_t)num_delays, sizeof(int64_t));
+    double *delayed = calloc((size_t)num_delays, sizeof(double));
+    double *mixed = calloc((size_t)num_delays, sizeof(double));
+    double *line_state = calloc((size_t)(num_delays * num_bands * 4), sizeof(double));
+    double *tone_state = calloc((size_t)(num_bands * 4), sizeof(double));
+    double *ap = calloc((size_t)(num_allpass * max_allpass), sizeof(double));
+    int64_t *ap_pos = calloc((size_t)(num_allpass > 0 ? num_allpass : 1), sizeof(int64_t));
+    if (!lines || !pos || !delayed || !mixed || !line_state || !tone_state || !ap || !ap_pos) {
+        free(lines); free(pos); free(delayed); free(mixed); free(line_state); free(tone_state); free(ap); free(ap_pos);
+        return -2;
+    }
+    for (int64_t n = 0; n < num_samples; ++n) {
+        for (int64_t l = 0; l < num_delays; ++l) {
+            double v = lines[l * max_delay + pos[l]];
+            for (int64_t b = 0; b < num_bands; ++b)
+                v = fdn_section(absorptive + (l * num_bands + b) * 5, line_state + (l * num_bands + b) * 4, v);
+            delayed[l] = v;
+            mixed[l] = v;
+        }
+        for (int64_t stride = 1; stride < num_delays; stride *= 2) {
+            for (int64_t base = 0; base < num_delays; base += 2 * stride) {
+                for (int64_t o = 0; o < stride; ++o) {
+                    double first = mixed[base + o], second = mixed[base + o + stride];
+                    mixed[base + o] = first + second;
+                    mixed[base + o + stride] = first - second;
+                }
+            }
+        }
+        double injection = n == 0 ? 1.0 : 0.0;
+        for (int64_t l = 0; l < num_delays; ++l) {
+            lines[l * max_delay + pos[l]] = injection + 0.25 * mixed[l];
+            pos[l] += 1;
+            if (pos[l] >= delays[l]) pos[l] = 0;
+        }
+        double value = 0.0;
+        for (int64_t l = 0; l < num_delays; ++l) value += delayed[l];
+        value /= (double)num_delays;
+        for (int64_t s = 0; s < num_allpass; ++s) {
+            double *buf = ap + s * max_allpass;
+            double previous = buf[ap_pos[s]];
+            double internal = value + 0.5 * previous;
+            buf[ap_pos[s]] = internal;
+            value = previous - 0.5 * internal;
+            ap_pos[s] += 1;
+            if (ap_pos[s] >= allpass_delays[s]) ap_pos[s] = 0;
+        }
+        for (int64_t b = 0; b < num_bands; ++b) value = fdn_section(tone + b * 5, tone_state + b * 4, value);
+        out[n] = value;
+    }
+    free(lines); free(pos); free(delayed); free(mixed); free(line_state); free(tone_state); free(ap); free(ap_pos);
     return 0;
 }

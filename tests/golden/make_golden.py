@@ -188,11 +188,64 @@ def cases():
     return out
 
 
+BANDS = ("125", "250", "500", "1000", "2000", "4000")
+DESIGN_CASES = ((16000, 1729, (1.2, 1.0, 0.9, 0.8, 0.6, 0.4)), (48000, 7, (0.5, 0.5, 0.45, 0.4, 0.35, 0.3)),
+                (8000, 81, (1.2, 0.0, 0.9, 0.05, 0.6, 2.5)))
+RENDER_CASES = (
+    ("basic", {"rt60": (1.2,) * 6}, {}),
+    ("breakpoint", {"rt60": (1.0, 0.9, 0.8, 0.8, 0.7, 0.6),
+                    "profiles": {"125": {"model": "double_slope", "transition_time_s": 0.2,
+                                         "selected_target_source": "fitted_late_slope"},
+                                 "250": {"model": "double_slope", "transition_time_s": 0.15,
+                                         "selected_target_source": "steam_single_slope"}}}, {}),
+    ("zero_band", {"rt60": (1.2, 0.9, 0.0, 0.05, 0.6, 0.4)}, {}),
+    ("disabled", {"rt60": (1.2,) * 6}, {"late_tail": False}),
+)
+
+
+def late_reverb_golden(steam_rt, SimConfig) -> None:
+    """FDN design, FDN impulse and the hybrid late-tail render (steam_rt.py:2235-2640)."""
+    out = {}
+    for k, (fs, seed, rt60) in enumerate(DESIGN_CASES):
+        delays = steam_rt._steam_fdn_delays(fs, seed)
+        absorptive, tone = steam_rt._steam_fdn_filter_coefficients(delays, dict(zip(BANDS, rt60)), fs)
+        out[f"design{k}_meta"] = np.asarray([fs, seed, *rt60], dtype=np.float64)
+        out[f"design{k}_delays"] = delays
+        out[f"design{k}_absorptive"] = absorptive
+        out[f"design{k}_tone"] = tone
+    # the network alone, at 8 kHz with the third design (a zero and a short RT60 band)
+    allpass = np.asarray((225, 341, 441, 556), dtype=np.int64)
+    out["impulse"] = steam_rt._fdn_impulse_kernel_jit(out["design2_delays"], out["design2_absorptive"], 6000,
+                                                      allpass, out["design2_tone"])
+    fs, N = 8000, 4000
+    rng = np.random.default_rng(81)
+    env = np.exp(-3.0 * math.log(10.0) * (np.arange(N, dtype=np.float64) / fs) / 1.2)
+    traced = np.vstack([rng.uniform(-1.0, 1.0, N) * env for _ in BANDS]).astype(np.float32)
+    out["render_traced"] = traced
+    for name, case, overrides in RENDER_CASES:
+        cfg = SimConfig(fs=fs, duration_s=N / fs, hybrid_transition_s=0.3, hybrid_overlap_fraction=0.25, seed=1729,
+                        **overrides)
+        rendered, fdn, meta = steam_rt._render_parametric_fdn_late_reverb(
+            traced, {"bin_duration_s": 0.01}, dict(zip(BANDS, case["rt60"])), cfg,
+            decay_profiles=case.get("profiles"))
+        out[f"render_{name}_out"] = rendered
+        out[f"render_{name}_fdn"] = fdn
+        out[f"render_{name}_meta"] = np.asarray(json.dumps(meta))
+        out[f"render_{name}_case"] = np.asarray(json.dumps({"rt60": case["rt60"], "profiles": case.get("profiles"),
+                                                            **overrides}))
+    np.savez_compressed(HERE / "late_reverb.npz", **out)
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", choices=("late_reverb",), help="regenerate one fixture file only")
     args = parser.parse_args()
     steam_rt, models, directivity = import_reference(args.reference)
+    if args.only == "late_reverb":
+        from acoustic_agent.models import SimConfig  # noqa: E402
+        late_reverb_golden(steam_rt, SimConfig)
+        return 0
     written = []
     for name, spec, trace in cases():
         scene, arrays = reference_arrays(steam_rt, models, spec)
@@ -233,7 +286,8 @@ def main() -> int:
     rnd, idx = steam_rt._diffuse_random_sequence(1000, 5, 128, 1729)
     np.savez_compressed(HERE / "workspace.npz", sphere=steam_rt._sphere_samples(1000, 1729),
                         bank=steam_rt._diffuse_sample_bank(128), random=rnd, indices=idx)
-    print("wrote", written, "synthesis", "workspace")
+    late_reverb_golden(steam_rt, SimConfig)
+    print("wrote", written, "synthesis", "workspace", "late_reverb")
     return 0
 
 

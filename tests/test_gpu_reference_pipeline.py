@@ -57,3 +57,34 @@ def test_simulate_steam_room_renders_through_the_b200_backend(reference):
     t32 = np.array(list(renders["float32"].rt60_bands.values()))
     assert (t64 > 0).all()
     np.testing.assert_allclose(t32, t64, rtol=0.02)
+
+
+def test_late_tail_routes_to_the_gpu_fdn(reference):
+    """With late_tail on, install() also routes _render_parametric_fdn_late_reverb (steam_rt.py:1029) to the GPU
+    FDN; the rendered RIR equals the one with the reference's own CPU FDN to float32 rounding."""
+    bench, (steam_rt, models) = reference
+    from acoustic_agent_b200 import backend, workloads
+    spec = {"corners": [(0.0, 0.0), (6.0, 0.0), (6.0, 4.0), (0.0, 4.0)], "height": 3.0,
+            "materials": workloads._uniform_materials()}
+    room = bench.reference_scene(steam_rt, models, spec).room
+    cfg = models.SimConfig(fs=16000, duration_s=1.0, rt_duration_s=1.0, rt_num_rays=4000, rt_num_bounces=64,
+                           late_tail=True, hybrid_transition_s=0.5, adaptive_geometry_bounces=False,
+                           rt_accelerator="b200", rt_precision="float64", seed=11)
+    handle = backend.install(steam_rt)
+    try:
+        gpu = steam_rt.simulate_steam_room(room, [1.5, 1.2, 1.5], [4.2, 2.9, 1.6], cfg)
+        routed = steam_rt._render_parametric_fdn_late_reverb
+        steam_rt._render_parametric_fdn_late_reverb = handle.originals["_render_parametric_fdn_late_reverb"]
+        try:
+            cpu = steam_rt.simulate_steam_room(room, [1.5, 1.2, 1.5], [4.2, 2.9, 1.6], cfg)
+        finally:
+            steam_rt._render_parametric_fdn_late_reverb = routed
+    finally:
+        handle.uninstall()
+    g_meta, c_meta = gpu.metadata["reflections"]["late_tail"], cpu.metadata["reflections"]["late_tail"]
+    assert g_meta["applied"] and c_meta["applied"]
+    assert g_meta["delay_samples"] == c_meta["delay_samples"]
+    for band, scale in c_meta["scale_by_band"].items():
+        assert g_meta["scale_by_band"][band] == pytest.approx(scale, rel=1e-7)
+    scale = float(np.abs(cpu.rir).max())
+    np.testing.assert_allclose(gpu.rir, cpu.rir, rtol=1e-5, atol=1e-6 * scale)
