@@ -135,7 +135,7 @@ class ACSynthBatchConfig(ctypes.Structure):
     ]
 
 
-AC_FDN_LINES, AC_FDN_ALLPASS, AC_FDN_MIN_DELAY, AC_FDN_MAX_ALLPASS = 16, 4, 72, 4096
+AC_FDN_LINES, AC_FDN_ALLPASS, AC_FDN_MIN_DELAY, AC_FDN_MAX_ALLPASS = 16, 4, 128, 4096
 AC_LATE_STATS = 8
 (AC_LATE_SCALE, AC_LATE_POWER, AC_LATE_FDN_ENERGY, AC_LATE_TRACED_TAIL, AC_LATE_RENDERED_TAIL, AC_LATE_COMPONENT,
  AC_LATE_CHANGED) = range(7)

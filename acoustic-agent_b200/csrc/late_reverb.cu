@@ -6,26 +6,32 @@
 // compiled with -fmad=false and every expression keeps the reference's
 // operation order.  The network is sequential in time, but its feedback runs
 // through delay lines of at least AC_FDN_MIN_DELAY samples, so nothing a
-// sample computes is needed by the next few samples except each biquad's own
-// state.  One 64-thread block renders one impulse response:
+// sample computes is needed by the next hundred samples except each biquad's
+// own state.  A biquad's state recursion ((S - a1*y1) - a2*y2) is three
+// dependent float64 operations per sample; a sample needs 96 absorptive
+// sections, and one warp issuing three of them per lane is bound by the
+// float64 issue rate, so the sections are spread one per lane.  One
+// 192-thread block renders one impulse response:
 //
-//   warp 0 (the lines): lane (line, half) runs three of its line's six
-//     absorptive sections, the lower half bands 0-2 and the upper half bands
-//     3-5.  Section k of the lower half works on sample n - k at step n; the
-//     upper half gets the lower half's band-2 output through a shuffle and
-//     runs one step later (band 3 on sample n - 4), so band 5 of sample m runs
-//     at step m + 6.  The Hadamard butterfly of the sixteen band-5 outputs is
-//     four xor-shuffles inside the upper half, whose lanes then write their
-//     delay lines (global memory, L2-resident) and their pre-mix outputs to a
-//     shared ring.  Delay-line inputs are fetched one 32-sample block ahead
-//     with cp.async, which the minimum delay makes safe.
-//   warp 1 (the output): one 32-sample block behind, lane i sums sample i's
-//     sixteen line outputs in line order, runs the four all-pass stages (their
-//     delays exceed 32, so a block's samples are independent) and hands the
-//     block to the six tone sections, a systolic chain over lanes 0-5 with a
-//     skew of four steps.
+//   warps 0-3 (the lines): lane 6j + b of warp w runs absorptive section
+//     (band) b of line 4w + j, kLineSkew steps behind band b - 1, whose
+//     output reaches it by a shuffle; the input part of each biquad is
+//     computed a step ahead, so only its three-operation recursion is on the
+//     per-sample path.  Lanes 24-31 idle.  Band 5 of sample m runs at step m + kLineLag and is
+//     stored to a shared ring.  Each warp fetches its four delay lines one
+//     32-sample block ahead by cp.async.
+//   warp 4 (the mix): one block behind, lane i takes sample i of the block
+//     from the ring and, in registers, sums its sixteen line outputs in line
+//     order, runs the Hadamard butterfly and writes the sixteen delay lines
+//     (global memory, L2-resident; coalesced per line), and runs the four
+//     all-pass stages (their delays exceed 32, so a block's samples are
+//     independent).
+//   warp 5 (the tone): two blocks behind, the six tone sections as a
+//     systolic chain over lanes 0-5, kToneSkew steps apart.
 //
-// The two warps meet at one named barrier per block.
+// The six warps meet at one named barrier per block.  A delay-line value
+// written by the mix warp is visible to the line warps two barriers later,
+// which is why the delays must be at least 128 samples (see check_fdn).
 //
 // ac_late_tail restates the rest of _render_parametric_fdn_late_reverb
 // (:2588-2640): bandlimit_band_signals of the impulse (the systolic crossover
@@ -50,15 +56,23 @@ namespace {
 
 constexpr int kLines = AC_FDN_LINES;
 constexpr int kBlk = 32;                   // samples per block
-constexpr int kLineLag = 6;                // band 5 of sample m runs at step m + 6
+constexpr int kLineSkew = 2;               // steps between consecutive absorptive sections of a line
+constexpr int kLineWarps = 4;              // line warps, four lines each
+constexpr int kLinesPerWarp = kLines / kLineWarps;
+constexpr int kLineLag = 5 * kLineSkew;        // band 5 of sample m runs at step m + kLineLag
 constexpr int kRing = 4 * kBlk;            // samples of line outputs kept for the output warp
 constexpr int kRowStride = kLines + 1;     // doubles per ring row: column reads without bank conflicts
-constexpr int kToneSkew = 4;               // steps between consecutive tone sections
-constexpr int kToneLag = 5 * kToneSkew;    // tone section 5 finishes sample g - 20 at step g
-constexpr int kStageDoubles = 2 * kLines * kBlk;
-constexpr int kFixedSmem = (kStageDoubles + kRing * kRowStride + kBlk) * static_cast<int>(sizeof(double));
-static_assert(AC_FDN_MIN_DELAY >= 2 * kBlk + kLineLag + 2,
-              "a prefetched delay-line value must have been written at least one block earlier");
+constexpr int kToneSkew = 2;               // steps between consecutive tone sections
+constexpr int kToneLag = 5 * kToneSkew;    // tone section 5 finishes sample g - kToneLag at step g
+constexpr int kStageRow = kLines + 1;      // staged inputs: one padded row of 16 lines per sample
+constexpr int kStageBlock = kBlk * kStageRow;
+constexpr int kStageDoubles = 2 * kStageBlock;
+constexpr int kFixedSmem = (kStageDoubles + kRing * kRowStride + 2 * kBlk) * static_cast<int>(sizeof(double));
+constexpr int kFdnThreads = 32 * (kLineWarps + 2);
+// Warp 1 writes the delay-line values of sample block b between barriers b+1
+// and b+2; warp 0's prefetch after barrier j-1 reads samples up to 32j + 63,
+// whose delayed sources must lie in blocks <= j - 3: delays of 128 or more.
+static_assert(AC_FDN_MIN_DELAY >= 4 * kBlk, "a prefetched delay-line value must be visible to warp 0");
 
 inline size_t align256(size_t v) { return (v + 255) & ~static_cast<size_t>(255); }
 
@@ -77,6 +91,9 @@ struct FdnJobDev {
 
 // y = b0*x + b1*x1 + b2*x2 - a1*y1 - a2*y2, left to right, all in float64
 // (the absorptive and tone sections of steam_rt.py:2261-2275 / :2312-2325).
+// feed() is the input part ((b0*x + b1*x1) + b2*x2), which does not depend on
+// y and is computed one sample ahead; step() is the recursion
+// (v - a1*y1) - a2*y2.  Same operations in the same order as run().
 struct Biquad {
     double b0, b1, b2, a1, a2, x1, x2, y1, y2;
 
@@ -85,10 +102,15 @@ struct Biquad {
         x1 = x2 = y1 = y2 = 0.0;
     }
 
-    __device__ __forceinline__ double run(double x) {
-        const double y = b0 * x + b1 * x1 + b2 * x2 - a1 * y1 - a2 * y2;
+    __device__ __forceinline__ double feed(double x) {
+        const double v = b0 * x + b1 * x1 + b2 * x2;
         x2 = x1;
         x1 = x;
+        return v;
+    }
+
+    __device__ __forceinline__ double step(double v) {
+        const double y = v - a1 * y1 - a2 * y2;
         y2 = y1;
         y1 = y;
         return y;
@@ -103,116 +125,112 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// The two warps of a block meet here once per sample block.
-__device__ __forceinline__ void pair_barrier() { asm volatile("bar.sync 1, 64;" ::: "memory"); }
+// The six warps of a block meet here once per sample block.
+__device__ __forceinline__ void block_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kFdnThreads) : "memory"); }
 
-// One Hadamard butterfly stage across lanes line ^ s: the lower lane of the
-// pair keeps first + second, the upper one first - second (steam_rt.py:2281-2289).
-__device__ __forceinline__ double butterfly(double mine, int line, int s) {
-    const double other = __shfl_xor_sync(0xFFFFFFFFu, mine, s);
-    return (line & s) ? other - mine : mine + other;
-}
-
-// Block k's delay-line inputs: element `lane` of line l is sample 32k + lane,
-// at position pos[l] of the line; advance the positions by one block.
+// Block k's delay-line inputs for lines first .. first + 3: lane i fetches
+// sample 32k + i of each into row i of the stage; advance the positions by
+// one block.
 __device__ __forceinline__ void prefetch_block(const double *lines, const int *line_start, const int *delays,
-                                               int *pos, double *stage, int lane) {
+                                               int first, int *pos, double *stage, int lane) {
 #pragma unroll
-    for (int l = 0; l < kLines; ++l) {
-        cp_async8(stage + l * kBlk + lane, lines + line_start[l] + pos[l]);
-        const int p = pos[l] + kBlk;
-        pos[l] = p >= delays[l] ? p - delays[l] : p;
+    for (int j = 0; j < kLinesPerWarp; ++j) {
+        const int l = first + j;
+        cp_async8(stage + lane * kStageRow + l, lines + line_start[l] + pos[j]);
+        const int p = pos[j] + kBlk;
+        pos[j] = p >= delays[l] ? p - delays[l] : p;
     }
     cp_async_commit();
 }
 
-__device__ void fdn_lines(const FdnJobDev &job, double *lines, double *stage, double *rows, const int *s_start,
-                          const int *s_delay, int blocks) {
+__device__ void fdn_lines(const FdnJobDev &job, const double *lines, double *stage, double *rows, const int *s_start,
+                          const int *s_delay, int iterations) {
     const unsigned full = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
-    const int line = lane & 15;
-    const int half = lane >> 4;
-    Biquad s0, s1, s2;
-    s0.load(job.absorptive[line][3 * half + 0]);
-    s1.load(job.absorptive[line][3 * half + 1]);
-    s2.load(job.absorptive[line][3 * half + 2]);
-    const int D = job.delays[line];
-    double *my_line = lines + job.line_start[line];
-    int pos[kLines];
+    const int first = (threadIdx.x >> 5) * kLinesPerWarp;
+    const bool valid = lane < 6 * kLinesPerWarp;
+    const int line = first + (valid ? lane / 6 : 0);
+    const int band = valid ? lane % 6 : 0;
+    Biquad sec;
+    sec.load(job.absorptive[line][band]);
+    if (!valid) sec.b0 = sec.b1 = sec.b2 = sec.a1 = sec.a2 = 0.0;
+    const bool stores = valid && band == 5;
+    int pos[kLinesPerWarp];
 #pragma unroll
-    for (int l = 0; l < kLines; ++l) pos[l] = lane;  // every delay exceeds 32
-    double h0 = 0.0, h1 = 0.0;    // sections 0 and 1 outputs of the previous step
-    double rq0 = 0.0, rq1 = 0.0;  // band-2 outputs received one and two steps ago (upper half)
-    int wpos = 0;                 // delay-line position of sample m = step - kLineLag
-    prefetch_block(lines, s_start, s_delay, pos, stage, lane);
-    for (int k = 0; k <= blocks; ++k) {
-        prefetch_block(lines, s_start, s_delay, pos, stage + ((k + 1) & 1) * kLines * kBlk, lane);
+    for (int j = 0; j < kLinesPerWarp; ++j) pos[j] = lane;  // every delay exceeds 32
+    // band b works on sample n - kLineSkew * b at step n; its input is band b - 1's output of step
+    // n - kLineSkew, which arrives by a shuffle issued at step n - kLineSkew and is fed (the input part
+    // of the biquad) one step ahead, at step n - 1
+    static_assert(kLineSkew == 2, "the shuffle is consumed one step after it is issued");
+    double received = 0.0;   // band b - 1's output of the previous step
+    double carry = 0.0;      // band b - 1's input for the first step of the next block
+    double v = 0.0;          // input part for the current step
+    prefetch_block(lines, s_start, s_delay, first, pos, stage, lane);
+    for (int k = 0; k < iterations; ++k) {
+        prefetch_block(lines, s_start, s_delay, first, pos, stage + ((k + 1) & 1) * kStageBlock, lane);
         cp_async_wait<1>();
         __syncwarp();
-        const double *in = stage + (k & 1) * kLines * kBlk + line * kBlk;
-#pragma unroll 4
+        const double *in = stage + (k & 1) * kStageBlock + line;
+        v = sec.feed(band == 0 ? in[0] : carry);
+        const int m0 = k * kBlk - kLineLag;
+        // fully unrolled, so that band 0's staged reads are issued well ahead of their use
+#pragma unroll
         for (int t = 0; t < kBlk; ++t) {
-            const double x0 = half ? rq1 : in[t];
-            const double o0 = s0.run(x0);
-            const double o1 = s1.run(h0);
-            const double o2 = s2.run(h1);
-            h0 = o0;
-            h1 = o1;
-            rq1 = rq0;
-            rq0 = __shfl_up_sync(full, o2, 16);
-            double mixed = butterfly(o2, line, 1);
-            mixed = butterfly(mixed, line, 2);
-            mixed = butterfly(mixed, line, 4);
-            mixed = butterfly(mixed, line, 8);
-            const int m = k * kBlk + t - kLineLag;
-            if (m >= 0) {
-                if (half) {
-                    const double injection = m == 0 ? 1.0 : 0.0;
-                    my_line[wpos] = injection + 0.25 * mixed;
-                    rows[(m & (kRing - 1)) * kRowStride + line] = o2;
-                }
-                wpos = wpos + 1 == D ? 0 : wpos + 1;
-            }
+            const double y = sec.step(v);                      // the only chain carried between steps
+            const double next_in = band == 0 ? in[((t + 1) & (kBlk - 1)) * kStageRow] : received;
+            received = __shfl_up_sync(full, y, 1);
+            if (t + 1 < kBlk) v = sec.feed(next_in);          // the next block's first input is fed after its fetch
+            else carry = next_in;
+            const int m = m0 + t;
+            if (stores && m >= 0) rows[(m & (kRing - 1)) * kRowStride + line] = y;
         }
         __syncwarp();
-        pair_barrier();
+        block_barrier();
     }
     cp_async_wait<0>();
 }
 
-__device__ void fdn_output(const FdnJobDev &job, const double *rows, double *tone_in, double *ap, int blocks,
-                           int total) {
-    const unsigned full = 0xFFFFFFFFu;
+__device__ void fdn_mix(const FdnJobDev &job, double *lines, const double *rows, double *tone_in, double *ap,
+                        const int *s_start, const int *s_delay, int blocks, int iterations) {
     const int lane = threadIdx.x & 31;
-    Biquad tone;
-    tone.load(job.tone[lane < 6 ? lane : 0]);
-    if (lane >= 6) tone.b0 = tone.b1 = tone.b2 = tone.a1 = tone.a2 = 0.0;
-    double q0 = 0.0, q1 = 0.0, q2 = 0.0, q3 = 0.0;  // the previous lane's outputs of steps g-1 .. g-4
     int apos[AC_FDN_ALLPASS];
 #pragma unroll
     for (int s = 0; s < AC_FDN_ALLPASS; ++s) apos[s] = 0;
-    const int preroll = job.preroll;
-    double *out = job.out;
-    // Tone section `lane` works on sample g - kToneSkew * lane at step g.
-    auto tone_step = [&](int g, double x_first) {
-        const double x = lane == 0 ? x_first : q3;
-        const double y = tone.run(x);
-        q3 = q2;
-        q2 = q1;
-        q1 = q0;
-        q0 = __shfl_up_sync(full, y, 1);
-        const int m = g - kToneLag;
-        if (lane == 5 && m >= preroll && m < total) out[m - preroll] = y;
-    };
-    for (int k = 0; k <= blocks; ++k) {
-        pair_barrier();
-        if (k == 0) continue;
-        const int base = (k - 1) * kBlk;  // this pass finishes samples base .. base + 31
-        const double *row = rows + ((base + lane) & (kRing - 1)) * kRowStride;
+    int wpos[kLines];   // delay-line position of this lane's sample in the current block
+#pragma unroll
+    for (int l = 0; l < kLines; ++l) wpos[l] = lane;
+    for (int k = 0; k < iterations; ++k) {
+        block_barrier();
+        if (k == 0 || k > blocks) continue;
+        const int base = (k - 1) * kBlk;  // samples base .. base + 31 are complete in the ring
+        const int m = base + lane;
+        const double *row = rows + (m & (kRing - 1)) * kRowStride;
+        double d[kLines];
+#pragma unroll
+        for (int l = 0; l < kLines; ++l) d[l] = row[l];
+        // output: the line outputs summed in line order, over the line count (steam_rt.py:2297-2300)
         double v = 0.0;
 #pragma unroll
-        for (int l = 0; l < kLines; ++l) v += row[l];
+        for (int l = 0; l < kLines; ++l) v += d[l];
         v /= static_cast<double>(kLines);
+        // feedback: unnormalised Hadamard butterfly, strides 1, 2, 4, 8, written back with gain 0.25
+        // and the unit impulse at sample 0 (steam_rt.py:2279-2295)
+#pragma unroll
+        for (int stride = 1; stride < kLines; stride *= 2)
+#pragma unroll
+            for (int a = 0; a < kLines; ++a)
+                if ((a & stride) == 0) {
+                    const double first = d[a], second = d[a + stride];
+                    d[a] = first + second;
+                    d[a + stride] = first - second;
+                }
+        const double injection = m == 0 ? 1.0 : 0.0;
+#pragma unroll
+        for (int l = 0; l < kLines; ++l) {
+            lines[s_start[l] + wpos[l]] = injection + 0.25 * d[l];
+            const int p = wpos[l] + kBlk;
+            wpos[l] = p >= s_delay[l] ? p - s_delay[l] : p;
+        }
 #pragma unroll
         for (int s = 0; s < AC_FDN_ALLPASS; ++s) {
             const int D = job.allpass[s];
@@ -226,24 +244,66 @@ __device__ void fdn_output(const FdnJobDev &job, const double *rows, double *ton
             const int p = apos[s] + kBlk;
             apos[s] = p >= D ? p - D : p;
         }
-        tone_in[lane] = v;
-        __syncwarp();
-        for (int t = 0; t < kBlk; ++t) tone_step(base + t, tone_in[t]);
-        __syncwarp();
+        tone_in[((k - 1) & 1) * kBlk + lane] = v;
     }
-    for (int t = 0; t < kToneLag; ++t) tone_step(blocks * kBlk + t, 0.0);
 }
 
-__global__ void __launch_bounds__(64) fdn_kernel(const FdnJobDev *jobs, double *pool) {
+__device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, int blocks, int iterations, int total) {
+    const unsigned full = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    Biquad tone;
+    tone.load(job.tone[lane < 6 ? lane : 0]);
+    if (lane >= 6) tone.b0 = tone.b1 = tone.b2 = tone.a1 = tone.a2 = 0.0;
+    static_assert(kToneSkew == 2, "the shuffle is consumed one step after it is issued");
+    // Tone section `lane` works on sample g - kToneSkew * lane at step g; its input is the previous
+    // section's output of step g - kToneSkew, fed one step ahead like the line sections.
+    double received = 0.0, carry = 0.0, v = 0.0;
+    const int preroll = job.preroll;
+    double *out = job.out;
+    auto emit = [&](int g, double y) {
+        const int m = g - kToneLag;
+        if (lane == 5 && m >= preroll && m < total) out[m - preroll] = y;
+    };
+    for (int k = 0; k < iterations; ++k) {
+        block_barrier();
+        if (k < 2 || k > blocks + 1) continue;
+        const int base = (k - 2) * kBlk;
+        const double *in = tone_in + ((k - 2) & 1) * kBlk;
+        v = tone.feed(lane == 0 ? in[0] : carry);
+#pragma unroll
+        for (int t = 0; t < kBlk; ++t) {
+            const double y = tone.step(v);
+            const double next_in = lane == 0 ? in[(t + 1) & (kBlk - 1)] : received;
+            received = __shfl_up_sync(full, y, 1);
+            if (t + 1 < kBlk) v = tone.feed(next_in);
+            else carry = next_in;
+            emit(base + t, y);
+        }
+    }
+    // drain: inputs past the last sample are zero
+    v = tone.feed(lane == 0 ? 0.0 : carry);
+    for (int t = 0; t < kToneLag; ++t) {
+        const double y = tone.step(v);
+        const double next_in = lane == 0 ? 0.0 : received;
+        received = __shfl_up_sync(full, y, 1);
+        v = tone.feed(next_in);
+        emit(blocks * kBlk + t, y);
+    }
+}
+
+__global__ void __launch_bounds__(kFdnThreads) fdn_kernel(const FdnJobDev *jobs, double *pool) {
     extern __shared__ __align__(16) double smem[];
     double *stage = smem;
     double *rows = stage + kStageDoubles;
     double *tone_in = rows + kRing * kRowStride;
-    double *ap = tone_in + kBlk;
+    double *ap = tone_in + 2 * kBlk;
     __shared__ int s_start[kLines], s_delay[kLines];
     const FdnJobDev &job = jobs[blockIdx.x];
     const int total = job.preroll + job.num_samples;
     const int blocks = (total + kBlk - 1) / kBlk;
+    // every warp passes the block barrier `iterations` times: the lines finish block b in iteration b + 1,
+    // the mix takes it in iteration b + 1 and the tone in iteration b + 2
+    const int iterations = blocks + 2;
     const int ap_total = job.allpass_start[AC_FDN_ALLPASS - 1] + job.allpass[AC_FDN_ALLPASS - 1];
     for (int i = threadIdx.x; i < ap_total; i += blockDim.x) ap[i] = 0.0;
     if (threadIdx.x < kLines) {
@@ -251,10 +311,13 @@ __global__ void __launch_bounds__(64) fdn_kernel(const FdnJobDev *jobs, double *
         s_delay[threadIdx.x] = job.delays[threadIdx.x];
     }
     __syncthreads();
-    if (threadIdx.x < 32)
-        fdn_lines(job, pool + job.pool, stage, rows, s_start, s_delay, blocks);
+    const int warp = threadIdx.x >> 5;
+    if (warp < kLineWarps)
+        fdn_lines(job, pool + job.pool, stage, rows, s_start, s_delay, iterations);
+    else if (warp == kLineWarps)
+        fdn_mix(job, pool + job.pool, rows, tone_in, ap, s_start, s_delay, blocks, iterations);
     else
-        fdn_output(job, rows, tone_in, ap, blocks, total);
+        fdn_tone(job, tone_in, blocks, iterations, total);
 }
 
 // ---- the hybrid tail ------------------------------------------------------
@@ -612,7 +675,7 @@ extern "C" int ac_fdn_impulse(const ac_fdn_job *jobs, int32_t num_jobs, void *wo
     const int smem = ac::kFixedSmem + l.max_allpass_doubles * static_cast<int>(sizeof(double));
     const int prc = ac::ensure_fdn_smem(smem);
     if (prc != AC_OK) return prc;
-    ac::fdn_kernel<<<num_jobs, 64, smem, stream>>>(reinterpret_cast<const ac::FdnJobDev *>(ws + l.jobs),
+    ac::fdn_kernel<<<num_jobs, ac::kFdnThreads, smem, stream>>>(reinterpret_cast<const ac::FdnJobDev *>(ws + l.jobs),
                                                    reinterpret_cast<double *>(ws + l.pool));
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;

@@ -21,7 +21,6 @@ path: without the library or a CUDA device the calls raise.
 """
 from __future__ import annotations
 
-import ctypes
 import math
 from dataclasses import dataclass
 from typing import Any, Mapping, Sequence
@@ -241,10 +240,12 @@ class LateReverbRenderer:
             self._designs[key] = design(fs, seed, rt60)
         return self._designs[key]
 
-    def render(self, jobs: Sequence[LateReverbJob], *, stream: torch.cuda.Stream | None = None
+    def render(self, jobs: Sequence[LateReverbJob], *, stream: torch.cuda.Stream | None = None,
+               fdn_events: tuple[torch.cuda.Event, torch.cuda.Event] | None = None
                ) -> tuple[torch.Tensor, list[FdnDesign], list[Windows]]:
         """Enqueue every job on `stream`; returns the [J, 6, AC_LATE_STATS] float64 stats tensor, the designs
-        and the windows.  Jobs whose tail starts outside the signal must not be passed."""
+        and the windows.  Jobs whose tail starts outside the signal must not be passed.  `fdn_events`, if
+        given, are recorded around the FDN launch (to time the network alone)."""
         J = len(jobs)
         stats = torch.zeros(max(J, 1), 6, _lib.AC_LATE_STATS, dtype=torch.float64, device=self.device)
         if J == 0:
@@ -292,10 +293,15 @@ class LateReverbRenderer:
             t.bin_samples = max(1, int(round(float(job.bin_duration_s) * fs)))
             t.rate_index = rate_index[fs]
             offset += N
+        launch_stream = stream if stream is not None else torch.cuda.current_stream(self.device)
+        if fdn_events is not None:
+            fdn_events[0].record(launch_stream)
         runtime.fdn_impulse(fdn_jobs, J, self.fdn_ws, stream=stream)
+        if fdn_events is not None:
+            fdn_events[1].record(launch_stream)
         runtime.late_tail(tail_jobs, J, cfg, self.tail_ws, stream=stream)
         # keep the FDN scratch alive until the stream has used it
-        raw.record_stream(stream if stream is not None else torch.cuda.current_stream(self.device))
+        raw.record_stream(launch_stream)
         return stats, designs, wins
 
 

@@ -108,6 +108,9 @@ class ClockSampler:
         if self._thread is not None:
             self._thread.join()
 
+    def median_mhz(self) -> int | None:
+        return int(statistics.median(self.samples)) if self.samples else None
+
     def summary(self) -> dict:
         return {"sm_mhz": int(statistics.median(self.samples)) if self.samples else None,
                 "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons), "samples": len(self.samples)}
@@ -344,7 +347,7 @@ def main() -> int:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--workload", default="u_room_20_boxes",
-                        choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving"))
+                        choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving", "late_reverb"))
     parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     parser.add_argument("--no-pipeline", action="store_true",
                         help="run each step's synthesis after its own trace instead of beside the next trace")
@@ -362,6 +365,21 @@ def main() -> int:
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
+    if args.impl == "reference" and args.workload == "late_reverb":
+        world, rank, _ = _dist_setup()
+        if rank == 0:
+            ref = reference_late_tails(args.steps, args.warmup)
+            print(json.dumps({
+                "impl": "reference", "metric": "late tails/s", "value": ref["value"], "unit": "tails/s",
+                "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ref["seconds_per_tail"] * 1000.0, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded decaying noise)",
+                "config": {"workload": "late_reverb: one 48 kHz x 2 s channel per step"},
+                "cpu_baseline": {"value": ref["value"], "unit": "tails/s", "cores": ref["cores"], "kind": ref["kind"],
+                                 "sample": ref["sample"]},
+                "e2e": {"value": ref["value"], "unit": "tails/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
+                flush=True)
+        return 0
     if args.impl == "reference":
         if args.workload in ("mixed_batch", "serving"):
             parser.error("--impl reference times the reference's per-RIR path on a single-scene workload")
@@ -371,6 +389,8 @@ def main() -> int:
         return run_mixed_batch(args)
     if args.workload == "serving":
         return run_serving(args)
+    if args.workload == "late_reverb":
+        return run_late_reverb(args)
 
     import torch
     from acoustic_agent_b200 import batching, runtime, scene as scene_mod
@@ -694,6 +714,182 @@ def run_serving(args) -> int:
         "batches": s["batches"], "max_inflight_seen": s["max_inflight"], "scene_cache": s["scene_cache"],
         "offered_rirs_per_s": s["rirs"] / args.duration, "warm_cache_s": warm_s,
         "e2e": {"value": s["rirs_per_s"], "unit": "RIRs/s", "note": "arrival to host band IRs"},
+        "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+LATE_FS, LATE_SAMPLES, LATE_CHANNELS = 48000, 96000, 8
+LATE_RT60 = (0.72, 0.68, 0.62, 0.57, 0.50, 0.41)
+# float64 operations per FDN sample: 96 absorptive sections x 9, Hadamard 64, line writes 32, output mean 17,
+# all-pass 16, tone sections 6 x 9 (steam_rt.py:2257-2326)
+FDN_FLOPS_PER_SAMPLE = 96 * 9 + 64 + 32 + 17 + 16 + 6 * 9
+
+
+def late_reverb_inputs(channels: int, seed: int = 1729):
+    """Traced band IRs of the U-room RIR set (48 kHz, 2 s, 8 channels): seeded noise under per-band
+    exponential decays, each channel with its own RT60 targets, as float32 [6, N] arrays."""
+    rng = np.random.default_rng(seed)
+    t = np.arange(LATE_SAMPLES) / LATE_FS
+    out = []
+    for ch in range(channels):
+        rt60 = tuple(v * (1.0 + 0.01 * ch) for v in LATE_RT60)
+        env = np.stack([np.exp(-3.0 * math.log(10.0) * t / r) for r in rt60])
+        out.append((((rng.uniform(-1.0, 1.0, env.shape) * env) * 1e-2).astype(np.float32), rt60))
+    return out
+
+
+def _late_config(seed: int = 1729):
+    return types.SimpleNamespace(fs=LATE_FS, seed=seed, late_tail=True, hybrid_transition_s=1.0,
+                                 hybrid_overlap_fraction=0.25, rt_bin_duration_s=0.001)
+
+
+def reference_late_tails(steps: int, warmup: int) -> dict:
+    """The reference's _render_parametric_fdn_late_reverb (float64 Numba FDN, one host thread) on one
+    channel per step; the oracle's restatement when the reference package is absent."""
+    traced, rt60 = late_reverb_inputs(1)[0]
+    rt60_bands = dict(zip(("125", "250", "500", "1000", "2000", "4000"), rt60))
+    ref, reason = import_reference_package()
+    times = []
+    if ref is not None:
+        steam_rt, models = ref
+        cfg = models.SimConfig(fs=LATE_FS, duration_s=2.0, hybrid_transition_s=1.0, hybrid_overlap_fraction=0.25,
+                               seed=1729)
+        kind, what = "reference", "steam_rt._render_parametric_fdn_late_reverb (baseline/_ref, Numba float64)"
+        for k in range(warmup + steps):
+            t0 = time.perf_counter()
+            steam_rt._render_parametric_fdn_late_reverb(traced, {"bin_duration_s": 0.001}, rt60_bands, cfg)
+            if k >= warmup:
+                times.append(time.perf_counter() - t0)
+    else:
+        from oracle import oracle
+        kind, what = "port", f"{reason}; oracle restatement (C float64 FDN + numpy)"
+        for k in range(warmup + steps):
+            t0 = time.perf_counter()
+            oracle.late_reverb(traced, 0.001, rt60_bands, fs=LATE_FS, seed=1729, transition_s=1.0,
+                               overlap_fraction=0.25)
+            if k >= warmup:
+                times.append(time.perf_counter() - t0)
+    per = float(np.mean(times))
+    return {"value": 1.0 / per, "seconds_per_tail": per, "cores": 1, "kind": kind,
+            "sample": f"one 48 kHz x 2 s channel per step, {what}, mean of {steps} after {warmup} warm-up"}
+
+
+def run_late_reverb(args) -> int:
+    """Hybrid FDN late tails of the U-room RIR set: 8 channels x 48 kHz x 2 s per step.
+
+    value: ``LateReverbRenderer.render`` with traced band IRs resident (one FDN
+    launch + one band split + one mix launch for the 8 tails; designs cached).
+    e2e: the reference-facing drop-in ``render_parametric_fdn_late_reverb``
+    per channel from host arrays, with a fresh design per call (RT60 changes
+    every step), host<->device copies included.  A second launch of 1184 FDN
+    impulses (8 per SM) gives the network's saturated throughput.
+    """
+    import torch
+    from acoustic_agent_b200 import _lib, late_reverb, runtime
+    world, rank, local = _dist_setup()
+    if world > 1:
+        raise SystemExit("late_reverb runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    stream = torch.cuda.current_stream(device)
+    inputs = late_reverb_inputs(LATE_CHANNELS)
+    r = late_reverb.LateReverbRenderer(local)
+    traced = [torch.from_numpy(t.astype(np.float64)).to(device) for t, _ in inputs]
+    jobs = [late_reverb.LateReverbJob(t, torch.empty(t.shape, dtype=torch.float32, device=device),
+                                      torch.empty(t.shape, dtype=torch.float32, device=device), LATE_FS, 1729, rt60,
+                                      0.001, 1.0, 0.25) for t, (_, rt60) in zip(traced, inputs)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    for _ in range(args.warmup):
+        r.render(jobs, stream=stream)
+    torch.cuda.synchronize()
+    fdn_ms, steps_ms = [], []
+    sampler = ClockSampler(local)
+    with sampler:
+        for k in range(args.steps):
+            flush.fill_(k & 0xFF)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            ev[0].record(stream)
+            r.render(jobs, stream=stream, fdn_events=(ev[1], ev[2]))
+            ev[3].record(stream)
+            ev[3].synchronize()
+            steps_ms.append(ev[0].elapsed_time(ev[3]))
+            fdn_ms.append(ev[1].elapsed_time(ev[2]))
+    step_ms = float(np.mean(steps_ms))
+    fdn_kernel_ms = float(np.mean(fdn_ms))
+    design = r.design(LATE_FS, 1729, inputs[0][1])
+    samples_per_tail = LATE_SAMPLES + design.preroll
+    fdn_flops = FDN_FLOPS_PER_SAMPLE * samples_per_tail * LATE_CHANNELS
+    # saturated FDN throughput: 1184 impulses in one launch
+    sat_jobs = 8 * torch.cuda.get_device_properties(device).multi_processor_count
+    designs = [r.design(LATE_FS, 1729, rt60) for _, rt60 in inputs]
+    sat_out = torch.empty(sat_jobs, LATE_SAMPLES, dtype=torch.float64, device=device)
+    arr = (_lib.ACFdnJob * sat_jobs)()
+    for k in range(sat_jobs):
+        d = designs[k % len(designs)]
+        arr[k].absorptive[:] = d.absorptive.reshape(-1).tolist()
+        arr[k].tone[:] = d.tone.reshape(-1).tolist()
+        arr[k].delays[:] = [int(v) for v in d.delays]
+        arr[k].allpass_delays[:] = list(d.allpass)
+        arr[k].num_samples = LATE_SAMPLES
+        arr[k].preroll = d.preroll
+        arr[k].out = sat_out[k].data_ptr()
+    ws = runtime.FdnWorkspace(device)
+    for _ in range(2):
+        runtime.fdn_impulse(arr, sat_jobs, ws, stream=stream)
+    torch.cuda.synchronize()
+    sat_ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        runtime.fdn_impulse(arr, sat_jobs, ws, stream=stream)
+        e1.record(stream)
+        e1.synchronize()
+        sat_ms.append(e0.elapsed_time(e1))
+    sat = float(np.median(sat_ms))
+    sat_flops = FDN_FLOPS_PER_SAMPLE * samples_per_tail * sat_jobs
+    del sat_out
+    # end to end through the drop-in, a new RT60 (so a new design) every call
+    h2d = d2h = 0
+    e2e_times = []
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for ch, (t, rt60) in enumerate(inputs):
+            bands_rt60 = dict(zip(("125", "250", "500", "1000", "2000", "4000"), (v * (1.0 + 1e-6 * k) for v in rt60)))
+            out, comp, _ = late_reverb.render_parametric_fdn_late_reverb(t, {"bin_duration_s": 0.001}, bands_rt60,
+                                                                         _late_config())
+            if k == 0:
+                h2d += t.size * 8
+                d2h += out.nbytes + comp.nbytes + 6 * _lib.AC_LATE_STATS * 8
+        if k >= args.warmup:
+            e2e_times.append(time.perf_counter() - t0)
+    e2e_step = float(np.mean(e2e_times))
+    cpu = None if args.no_cpu_baseline else reference_late_tails(2, 1)
+    peak_fp64 = 37.0   # TFLOP/s, nominal B200 FP64 (no measured figure is available)
+    achieved = fdn_flops / (fdn_kernel_ms * 1e-3) / 1e12
+    sat_achieved = sat_flops / (sat * 1e-3) / 1e12
+    line = {
+        "metric": "late tails/s", "value": LATE_CHANNELS / (step_ms * 1e-3), "unit": "tails/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded decaying noise)",
+        "config": {"workload": "late_reverb: hybrid FDN tails of the U-room RIR set, 8 channels x 48 kHz x 2 s, "
+                               "transition 1 s, overlap 0.25", "samples_per_tail": LATE_SAMPLES,
+                   "fdn_samples_per_tail": samples_per_tail, "l2": "256 MiB buffer written between steps"},
+        "fdn_kernel_ms": fdn_kernel_ms,
+        "fdn_cycles_per_sample": fdn_kernel_ms * 1e-3 * sampler.median_mhz() * 1e6 / samples_per_tail
+        if sampler.median_mhz() else None,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_fp64, "unit": "TFLOP/s",
+                     "frac": achieved / peak_fp64, "traffic": None,
+                     "note": "8 tails occupy 8 of 148 SMs and run latency-bound; peak is the nominal FP64 rate"},
+        "saturated_fdn": {"tails": sat_jobs, "ms": sat, "tails_per_s": sat_jobs / (sat * 1e-3),
+                          "achieved_tflops": sat_achieved, "frac_of_nominal_fp64": sat_achieved / peak_fp64},
+        "e2e": {"value": LATE_CHANNELS / e2e_step, "unit": "tails/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "note": "drop-in per channel from host arrays, new design per call"},
+        "cpu_baseline": None if cpu is None else {"value": cpu["value"], "unit": "tails/s", "cores": cpu["cores"],
+                                                  "kind": cpu["kind"], "sample": cpu["sample"]},
+        "gpu_launches": 3 * args.steps,
         "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)

@@ -354,7 +354,8 @@ int ac_synthesize_batch_filter(const ac_synth_job *jobs, int32_t num_jobs, const
  * the reference's float64 kernel given the same design. */
 #define AC_FDN_LINES 16
 #define AC_FDN_ALLPASS 4
-#define AC_FDN_MIN_DELAY 72      /* delay lines shorter than this are refused (fs below about 1 kHz) */
+#define AC_FDN_MIN_DELAY 128     /* delay lines shorter than this are refused (the reference design keeps them
+                                    above 280 samples from 8 kHz up) */
 #define AC_FDN_MAX_ALLPASS 4096  /* longest all-pass stage; the shortest must exceed 32 */
 typedef struct ac_fdn_job {
     double absorptive[AC_FDN_LINES][6][5];  /* per line and band: b0 b1 b2 a1 a2 */
@@ -369,7 +370,7 @@ typedef struct ac_fdn_job {
 /* Device workspace (job table + delay lines) and pinned staging bytes for ac_fdn_impulse. */
 int ac_fdn_workspace_size(const ac_fdn_job *jobs, int32_t num_jobs, size_t *bytes);
 
-/* Any number of FDN impulse responses in one launch (one 64-thread block per
+/* Any number of FDN impulse responses in one launch (one 192-thread block per
  * job); the job table is staged as for ac_synthesize_batch. */
 int ac_fdn_impulse(const ac_fdn_job *jobs, int32_t num_jobs, void *workspace, size_t workspace_bytes,
                    void *host_staging, void *stream);
