@@ -201,6 +201,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_late_tail": (ctypes.c_int, [ctypes.POINTER(ACLateTailJob), ctypes.c_int32,
                                     ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
                                     ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_fp64_rate_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
+                                          ctypes.c_void_p]),
     "ac_read_bandwidth_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_void_p,
                                                ctypes.c_void_p]),
     "ac_synthesize_static": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,

@@ -156,6 +156,28 @@ __global__ void read_probe_kernel(const uint4 *buf, size_t n, int repeats, unsig
     if (acc == 0x9E3779B9u) atomicAdd(sink, 1ull);  // a data dependence that keeps every load
 }
 
+// Float64 issue-rate probe: eight independent add chains and eight independent
+// multiply chains per thread (separate instructions, no fused multiply-add).
+__global__ void fp64_probe_kernel(int iterations, double c, double f, unsigned long long *sink) {
+    double a[8], m[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        a[j] = threadIdx.x + j;
+        m[j] = 1.0 + 1e-9 * (threadIdx.x + j);
+    }
+    for (int i = 0; i < iterations; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            a[j] = a[j] + c;
+            m[j] = m[j] * f;
+        }
+    }
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc += a[j] + m[j];
+    if (acc == -1.0) atomicAdd(sink, 1ull);  // a data dependence that keeps every chain
+}
+
 }  // namespace
 }  // namespace ac
 
@@ -265,6 +287,19 @@ int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, u
     ac::read_probe_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<const uint4 *>(buffer),
                                                                                 bytes / 16, repeats, sink);
     AC_CUDA_TRY(cudaGetLastError());
+    return AC_OK;
+}
+
+int ac_fp64_rate_probe(int32_t iterations, unsigned long long *sink, int64_t *ops, void *stream) {
+    if (iterations < 1 || !sink || !ops) return ac::fail(AC_ERR_INVALID, "ac_fp64_rate_probe: bad argument");
+    int dev = 0, sms = 0;
+    AC_CUDA_TRY(cudaGetDevice(&dev));
+    AC_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int blocks = 2 * sms, threads = 256;   // sixteen warps per SM
+    ac::fp64_probe_kernel<<<blocks, threads, 0, static_cast<cudaStream_t>(stream)>>>(iterations, 1e-3, 1.0000000001,
+                                                                                    sink);
+    AC_CUDA_TRY(cudaGetLastError());
+    *ops = static_cast<int64_t>(blocks) * threads * iterations * 16;
     return AC_OK;
 }
 

@@ -665,6 +665,29 @@ def late_tail(jobs: ctypes.Array, num_jobs: int, config: _lib.ACSynthBatchConfig
     workspace.launched(stream)
 
 
+def fp64_rate_tops(device: torch.device, *, iterations: int = 8192, launches: int = 5) -> float:
+    """Measured float64 add/multiply issue rate of the whole GPU in 10^12 operations/s (ac_fp64_rate_probe)."""
+    sink = torch.zeros(1, dtype=torch.int64, device=device)
+    stream = torch.cuda.current_stream(device)
+    lib = _lib.load()
+    ops = ctypes.c_int64()
+
+    def launch():
+        _lib.check(lib.ac_fp64_rate_probe(int(iterations), ctypes.c_void_p(sink.data_ptr()), ctypes.byref(ops),
+                                          _stream_ptr(stream)), "ac_fp64_rate_probe")
+
+    launch()
+    best = 0.0
+    for _ in range(launches):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        launch()
+        e1.record(stream)
+        e1.synchronize()
+        best = max(best, ops.value / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    return best
+
+
 def read_bandwidth_gbs(device: torch.device, nbytes: int, *, repeats: int = 10, launches: int = 20) -> float:
     """Measured read bandwidth (GB/s) over a buffer of `nbytes`: L2 when it fits, HBM otherwise."""
     buf = torch.ones(nbytes // 4, dtype=torch.float32, device=device)

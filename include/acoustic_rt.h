@@ -421,6 +421,13 @@ int ac_late_tail(const ac_late_tail_job *jobs, int32_t num_jobs, const ac_synth_
  * reported against.  `sink` is one device word the kernel may write. */
 int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, unsigned long long *sink, void *stream);
 
+/* Measurement helper, no counterpart in the reference: launches independent
+ * float64 add and multiply chains (separate instructions, as the bit-exact
+ * float64 kernels issue them) over every SM on `stream` and returns in *ops
+ * the operations launched; time it with events for the float64 issue rate
+ * the FDN's roofline is reported against.  `sink` is one device word. */
+int ac_fp64_rate_probe(int32_t iterations, unsigned long long *sink, int64_t *ops, void *stream);
+
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */
 int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces,
