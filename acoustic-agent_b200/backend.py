@@ -226,18 +226,19 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
                                       render_ambisonics=render_ambisonics)
         return original_trace(scene, source, listener, config, source_model, render_ambisonics=render_ambisonics)
 
-    original_late = steam_rt_module._render_parametric_fdn_late_reverb
-
-    def routed_late(traced_band_irs, field, rt60_bands, config, *, decay_profiles=None):
-        if normalize(config.rt_accelerator) in handled:
-            from acoustic_agent_b200 import late_reverb
-            return late_reverb.render_parametric_fdn_late_reverb(traced_band_irs, field, rt60_bands, config,
-                                                                 decay_profiles=decay_profiles)
-        return original_late(traced_band_irs, field, rt60_bands, config, decay_profiles=decay_profiles)
-
+    originals = {"trace_energy_field": original_trace, "_normalize_rt_accelerator": original_normalize}
     steam_rt_module.trace_energy_field = routed_trace
     steam_rt_module._normalize_rt_accelerator = normalize
-    steam_rt_module._render_parametric_fdn_late_reverb = routed_late
-    return Installation(steam_rt_module, {"trace_energy_field": original_trace,
-                                          "_normalize_rt_accelerator": original_normalize,
-                                          "_render_parametric_fdn_late_reverb": original_late})
+    original_late = getattr(steam_rt_module, "_render_parametric_fdn_late_reverb", None)
+    if original_late is not None:
+
+        def routed_late(traced_band_irs, field, rt60_bands, config, *, decay_profiles=None):
+            if normalize(config.rt_accelerator) in handled:
+                from acoustic_agent_b200 import late_reverb
+                return late_reverb.render_parametric_fdn_late_reverb(traced_band_irs, field, rt60_bands, config,
+                                                                     decay_profiles=decay_profiles)
+            return original_late(traced_band_irs, field, rt60_bands, config, decay_profiles=decay_profiles)
+
+        steam_rt_module._render_parametric_fdn_late_reverb = routed_late
+        originals["_render_parametric_fdn_late_reverb"] = original_late
+    return Installation(steam_rt_module, originals)

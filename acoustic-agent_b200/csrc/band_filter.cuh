@@ -52,9 +52,11 @@ static_assert(kSkew >= 3 && kLag + 2 <= kPrefetch, "the prefetch window must hol
 // Lane (unit, chain, stage): section `stage` works on sample it - kSkew*stage.
 // The float32 output it produces at iteration it is shuffled one lane up at
 // iteration it + 1 and consumed there at it + kSkew - 1 (as the input part of
-// its step at it + kSkew); the outputs are written two iterations late.  So
-// no instruction waits on a shuffle issued in its own iteration, and only the
-// section's own y dependency is carried from one iteration to the next.
+// its step at it + kSkew); the outputs are formed two iterations late and
+// written once per chunk of kPrefetch iterations.  So no instruction waits on
+// a shuffle issued in its own iteration, no store or bounds test sits in the
+// per-sample loop, and only the section's own y dependency is carried from one
+// iteration to the next.
 //
 // The body is branch-free: before a section's first real sample its input is
 // +0.0, and a section whose inputs and state are all +0.0 produces exactly +0.0
@@ -98,9 +100,9 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
     float lower2 = 0.0f;            // the lower chain's output of iteration it - 2
     // input part of the first sample (its input is ahead[0] for section 0 and +0.0 otherwise)
     double v = sec.feed(is_first ? ahead[0] : 0.0);
-    const int last = n_len + kLag;  // this lane's own end
     for (int base = 0; base < iterations; base += kPrefetch) {
         double next[kPrefetch];
+        float emitted[kPrefetch];   // this chunk's outputs, written after the chunk (off the recursion's path)
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {
             const int m = base + kPrefetch + u;
@@ -125,11 +127,22 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
             const int k = u - 2 - kLag;
             const double x_n = k >= 0 ? ahead[k] : prev[k + kPrefetch];
             const float band5 = static_cast<float>(x_n - static_cast<double>(y2f));
-            const float o = mode == 0 ? y2f : (mode == 2 ? band5 : y2f - lower2);
-            if (emits && it - 2 >= kLag && it - 2 < last) out_row[it - 2 - kLag] = o;
+            emitted[u] = mode == 0 ? y2f : (mode == 2 ? band5 : y2f - lower2);
             lower2 = lower;
             y2f = y1f;
             y1f = y;
+        }
+        // iteration base + u produced output sample base + u - 2 - kLag
+        const int first = base - 2 - kLag;
+        if (emits) {
+            if (first >= 0 && first + kPrefetch <= n_len) {
+#pragma unroll
+                for (int u = 0; u < kPrefetch; ++u) out_row[first + u] = emitted[u];
+            } else {
+#pragma unroll
+                for (int u = 0; u < kPrefetch; ++u)
+                    if (first + u >= 0 && first + u < n_len) out_row[first + u] = emitted[u];
+            }
         }
 #pragma unroll
         for (int u = 0; u < kPrefetch; ++u) {

@@ -67,7 +67,7 @@ constexpr int kToneLag = 5 * kToneSkew;    // tone section 5 finishes sample g -
 constexpr int kStageRow = kLines + 1;      // staged inputs: one padded row of 16 lines per sample
 constexpr int kStageBlock = kBlk * kStageRow;
 constexpr int kStageDoubles = 2 * kStageBlock;
-constexpr int kFixedSmem = (kStageDoubles + kRing * kRowStride + 2 * kBlk) * static_cast<int>(sizeof(double));
+constexpr int kFixedSmem = (kStageDoubles + kRing * kRowStride + 3 * kBlk) * static_cast<int>(sizeof(double));
 constexpr int kFdnThreads = 32 * (kLineWarps + 2);
 // Warp 1 writes the delay-line values of sample block b between barriers b+1
 // and b+2; warp 0's prefetch after barrier j-1 reads samples up to 32j + 63,
@@ -181,8 +181,9 @@ __device__ void fdn_lines(const FdnJobDev &job, const double *lines, double *sta
             received = __shfl_up_sync(full, y, 1);
             if (t + 1 < kBlk) v = sec.feed(next_in);          // the next block's first input is fed after its fetch
             else carry = next_in;
-            const int m = m0 + t;
-            if (stores && m >= 0) rows[(m & (kRing - 1)) * kRowStride + line] = y;
+            // band 5 of sample m0 + t; the ring slots written while m0 + t < 0 (zeros) are
+            // rewritten with their real samples before the mix warp reads them
+            if (stores) rows[((m0 + t) & (kRing - 1)) * kRowStride + line] = y;
         }
         __syncwarp();
         block_barrier();
@@ -248,7 +249,8 @@ __device__ void fdn_mix(const FdnJobDev &job, double *lines, const double *rows,
     }
 }
 
-__device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, int blocks, int iterations, int total) {
+__device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, double *tone_out, int blocks, int iterations,
+                         int total) {
     const unsigned full = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     Biquad tone;
@@ -260,9 +262,13 @@ __device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, int blocks
     double received = 0.0, carry = 0.0, v = 0.0;
     const int preroll = job.preroll;
     double *out = job.out;
-    auto emit = [&](int g, double y) {
-        const int m = g - kToneLag;
-        if (lane == 5 && m >= preroll && m < total) out[m - preroll] = y;
+    // section 5 stages its output of step base + t in tone_out[t]; the warp writes the block out after it
+    const bool last_section = lane == 5;
+    auto flush = [&](int base, int count) {
+        __syncwarp();
+        const int m = base + lane - kToneLag;
+        if (lane < count && m >= preroll && m < total) out[m - preroll] = tone_out[lane];
+        __syncwarp();
     };
     for (int k = 0; k < iterations; ++k) {
         block_barrier();
@@ -277,8 +283,9 @@ __device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, int blocks
             received = __shfl_up_sync(full, y, 1);
             if (t + 1 < kBlk) v = tone.feed(next_in);
             else carry = next_in;
-            emit(base + t, y);
+            if (last_section) tone_out[t] = y;
         }
+        flush(base, kBlk);
     }
     // drain: inputs past the last sample are zero
     v = tone.feed(lane == 0 ? 0.0 : carry);
@@ -287,8 +294,9 @@ __device__ void fdn_tone(const FdnJobDev &job, const double *tone_in, int blocks
         const double next_in = lane == 0 ? 0.0 : received;
         received = __shfl_up_sync(full, y, 1);
         v = tone.feed(next_in);
-        emit(blocks * kBlk + t, y);
+        if (last_section) tone_out[t] = y;
     }
+    flush(blocks * kBlk, kToneLag);
 }
 
 __global__ void __launch_bounds__(kFdnThreads) fdn_kernel(const FdnJobDev *jobs, double *pool) {
@@ -296,7 +304,8 @@ __global__ void __launch_bounds__(kFdnThreads) fdn_kernel(const FdnJobDev *jobs,
     double *stage = smem;
     double *rows = stage + kStageDoubles;
     double *tone_in = rows + kRing * kRowStride;
-    double *ap = tone_in + 2 * kBlk;
+    double *tone_out = tone_in + 2 * kBlk;
+    double *ap = tone_out + kBlk;
     __shared__ int s_start[kLines], s_delay[kLines];
     const FdnJobDev &job = jobs[blockIdx.x];
     const int total = job.preroll + job.num_samples;
@@ -317,7 +326,7 @@ __global__ void __launch_bounds__(kFdnThreads) fdn_kernel(const FdnJobDev *jobs,
     else if (warp == kLineWarps)
         fdn_mix(job, pool + job.pool, rows, tone_in, ap, s_start, s_delay, blocks, iterations);
     else
-        fdn_tone(job, tone_in, blocks, iterations, total);
+        fdn_tone(job, tone_in, tone_out, blocks, iterations, total);
 }
 
 // ---- the hybrid tail ------------------------------------------------------

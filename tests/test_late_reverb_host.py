@@ -159,3 +159,28 @@ def test_every_reference_rate_has_long_enough_delay_lines():
     for fs in (8000, 11025, 16000, 22050, 32000, 44100, 48000, 96000):
         for seed in range(20):
             assert int(np.min(late_reverb.line_delays(fs, seed))) >= _lib.AC_FDN_MIN_DELAY
+
+
+def test_install_routes_the_late_tail_only_for_the_b200_accelerator():
+    import types
+    from acoustic_agent_b200 import backend
+    calls = []
+    fake = types.SimpleNamespace(
+        trace_energy_field=lambda *a, **k: {"accelerator": "numba"},
+        _normalize_rt_accelerator=lambda v: v if v in {"auto", "numba", "cuda"} else (_ for _ in ()).throw(
+            ValueError("rt_accelerator must be auto, numba, or cuda")),
+        _render_parametric_fdn_late_reverb=lambda *a, **k: calls.append("reference") or "reference")
+    handle = backend.install(fake)
+    traced = np.zeros((6, 100))
+    cfg = sim_config(rt_accelerator="numba")
+    assert fake._render_parametric_fdn_late_reverb(traced, {}, {}, cfg) == "reference"
+    # the b200 accelerator takes the GPU renderer; with the tail disabled it returns without a device
+    out, comp, meta = fake._render_parametric_fdn_late_reverb(traced, {}, {}, sim_config(rt_accelerator="b200",
+                                                                                        late_tail=False))
+    assert meta["reason"] == "disabled" and calls == ["reference"]
+    handle.uninstall()
+    assert fake._render_parametric_fdn_late_reverb(traced, {}, {}, cfg) == "reference"
+    # a module without the late-tail function still installs
+    bare = types.SimpleNamespace(trace_energy_field=fake.trace_energy_field,
+                                 _normalize_rt_accelerator=fake._normalize_rt_accelerator)
+    backend.install(bare).uninstall()
