@@ -159,6 +159,27 @@ class ACLateTailJob(ctypes.Structure):
     ]
 
 
+AC_DIRECT_MAX_LAYERS = 64
+
+
+class ACDirectQuery(ctypes.Structure):
+    _fields_ = [
+        ("source", ctypes.c_double * 3), ("listener", ctypes.c_double * 3), ("radius", ctypes.c_double),
+        ("occlusion", ctypes.c_int32), ("volumetric", ctypes.c_int32), ("transmission", ctypes.c_int32),
+        ("max_layers", ctypes.c_int32),
+    ]
+
+
+class ACDirectResult(ctypes.Structure):
+    _fields_ = [("occlusion", ctypes.c_double), ("transmission", ctypes.c_double * 6),
+                ("occlusion_surface", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class ACDirectTables(ctypes.Structure):
+    _fields_ = [("unit_samples", ctypes.c_void_p), ("num_samples", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("transmission", ctypes.c_void_p), ("surface_group", ctypes.c_void_p)]
+
+
 # Every symbol include/acoustic_rt.h declares, with (restype, argtypes).
 SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_last_error": (ctypes.c_char_p, []),
@@ -201,6 +222,10 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_late_tail": (ctypes.c_int, [ctypes.POINTER(ACLateTailJob), ctypes.c_int32,
                                     ctypes.POINTER(ACSynthBatchConfig), ctypes.c_void_p, ctypes.c_size_t,
                                     ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_direct_workspace_size": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t)]),
+    "ac_direct": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACDirectQuery), ctypes.c_int32,
+                                 ctypes.POINTER(ACDirectTables), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                 ctypes.c_void_p, ctypes.c_void_p]),
     "ac_fp64_rate_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64),
                                           ctypes.c_void_p]),
     "ac_read_bandwidth_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_void_p,

@@ -205,7 +205,8 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
     ``route_cuda=True`` the reference's ``"cuda"`` setting is routed here too.  Other
     settings keep the reference's own dispatch (steam_rt.py:1757-1811).  The same
     setting routes the FDN late tail (``_render_parametric_fdn_late_reverb``,
-    steam_rt.py:2500, called by the renderer at :1029) to ``late_reverb``.
+    steam_rt.py:2500, called by the renderer at :1029) to ``late_reverb`` and the
+    direct path (``simulate_direct``, :1315, called at :942) to ``direct``.
     """
     if steam_rt_module is None:
         import acoustic_agent.steam_rt as steam_rt_module  # type: ignore[import-not-found]
@@ -241,4 +242,15 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
 
         steam_rt_module._render_parametric_fdn_late_reverb = routed_late
         originals["_render_parametric_fdn_late_reverb"] = original_late
+    original_direct = getattr(steam_rt_module, "simulate_direct", None)
+    if original_direct is not None:
+
+        def routed_direct(scene, source, listener, config, source_model=None):
+            if normalize(config.rt_accelerator) in handled:
+                from acoustic_agent_b200 import direct
+                return direct.simulate_direct(scene, source, listener, config, source_model)
+            return original_direct(scene, source, listener, config, source_model)
+
+        steam_rt_module.simulate_direct = routed_direct
+        originals["simulate_direct"] = original_direct
     return Installation(steam_rt_module, originals)

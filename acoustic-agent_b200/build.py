@@ -2,7 +2,7 @@
 
 Usage: ``python acoustic-agent_b200/build.py [--force]``.  Every translation
 unit targets ``-gencode arch=compute_100a,code=sm_100a``.  The float64 tracer,
-the band synthesis and the late reverberation are compiled with ``-fmad=false`` so that their
+the band synthesis, the late reverberation and the direct-path queries are compiled with ``-fmad=false`` so that their
 arithmetic rounds operation by operation like the reference's float64 code;
 the float32 tracer keeps FMA contraction.
 """
@@ -27,9 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr"]
 # Units whose float64 arithmetic must not be contracted into FMAs.
-NO_FMA = {"trace_f64.cu", "synth.cu", "late_reverb.cu"}
-SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "late_reverb.cu", "bvh_build.cpp",
-           "fast_bvh.cpp"]
+NO_FMA = {"trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu"}
+SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu",
+           "bvh_build.cpp", "fast_bvh.cpp"]
 
 
 def nvcc() -> str:

@@ -414,6 +414,50 @@ int ac_late_tail_workspace_size(const ac_late_tail_job *jobs, int32_t num_jobs, 
 int ac_late_tail(const ac_late_tail_job *jobs, int32_t num_jobs, const ac_synth_batch_config *config,
                  void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
 
+/* ---- direct path (steam_rt.py:1315-1350) ------------------------------
+ *
+ * The occlusion part of simulate_direct for any number of (source,
+ * listener) pairs of one scene, in float64 with the reference's own surface
+ * tests (RoomRayScene.closest_hit / any_hit, steam_rt.py:320-352, where a
+ * point on the room outline counts as inside): the first surface between
+ * listener and source, the volumetric visibility fraction over a sphere of
+ * sample points around the source (_volumetric_occlusion, :4215-4240) and,
+ * when that is below one, the per-band transmission through the distinct
+ * surfaces crossed from both ends (_transmission, :3437-3462).  Distances,
+ * gains and delays stay host arithmetic. */
+#define AC_DIRECT_MAX_LAYERS 64
+typedef struct ac_direct_query {
+    double source[3];
+    double listener[3];
+    double radius;            /* direct_occlusion_radius_m */
+    int32_t occlusion;        /* direct_occlusion: 0 leaves occlusion 1 and transmission 1 */
+    int32_t volumetric;       /* direct_occlusion_mode == "volumetric"; 0: the blocking surface decides */
+    int32_t transmission;     /* direct_transmission: 0 gives zero transmission when occluded */
+    int32_t max_layers;       /* max(1, num_transmission_rays), at most AC_DIRECT_MAX_LAYERS */
+} ac_direct_query;
+
+typedef struct ac_direct_result {
+    double occlusion;         /* visible fraction of the source sphere (or 0 / 1) */
+    double transmission[6];
+    int32_t occlusion_surface;  /* surface index between listener and source, -1 if none */
+    int32_t reserved;
+} ac_direct_result;
+
+typedef struct ac_direct_tables {
+    const double *unit_samples;   /* device [num_samples, 3]: _sphere_volume_samples(num_samples) */
+    int32_t num_samples;          /* direct_occlusion_samples */
+    int32_t reserved;
+    const double *transmission;   /* device [S, 6] per-surface band transmission */
+    const int32_t *surface_group; /* device [S]: surfaces that share a name share a group */
+} ac_direct_tables;
+
+/* Device workspace and pinned staging bytes for ac_direct. */
+int ac_direct_workspace_size(int32_t num_queries, size_t *bytes);
+
+/* One warp per query on `stream`; results is device memory [num_queries]. */
+int ac_direct(ac_scene_t scene, const ac_direct_query *queries, int32_t num_queries, const ac_direct_tables *tables,
+              ac_direct_result *results, void *workspace, size_t workspace_bytes, void *host_staging, void *stream);
+
 /* Measurement helper, no counterpart in the reference: reads `bytes` (a
  * multiple of 16 is used) of device memory `repeats` times with 16-byte loads
  * cached in L2 only, on `stream`; time it with events to get the L2 (buffer

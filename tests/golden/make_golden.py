@@ -236,15 +236,62 @@ def late_reverb_golden(steam_rt, SimConfig) -> None:
     np.savez_compressed(HERE / "late_reverb.npz", **out)
 
 
+DIRECT_SCENES = ("shoebox_linear", "u_furnished_bvh", "objects_mix_bvh", "apartment3_bvh", "open_room_bvh")
+DIRECT_CONFIGS = (
+    ("volumetric", {}),
+    ("raycast", {"direct_occlusion_mode": "raycast"}),
+    ("wide_opaque", {"direct_occlusion_samples": 45, "direct_occlusion_radius_m": 0.4, "direct_transmission": False,
+                     "num_transmission_rays": 2}),
+)
+
+
+def direct_golden(steam_rt, models, SimConfig) -> None:
+    """simulate_direct (steam_rt.py:1315-1350) on seeded source/listener pairs of five golden scenes."""
+    out = {}
+    for name in DIRECT_SCENES:
+        g = np.load(HERE / f"{name}.npz")
+        spec = json.loads(str(g["spec_json"]))
+        trace = json.loads(str(g["trace_json"]))
+        scene, _ = reference_arrays(steam_rt, models, spec)
+        corners = np.asarray(spec["corners"], dtype=float)
+        lo, hi = corners.min(axis=0), corners.max(axis=0)
+        rng = np.random.default_rng(31)
+        pairs = [(trace["source"], trace["listener"])]
+        for _ in range(15):
+            a = np.r_[rng.uniform(lo, hi), rng.uniform(0.3, float(spec["height"]) - 0.3)]
+            b = np.r_[rng.uniform(lo, hi), rng.uniform(0.3, float(spec["height"]) - 0.3)]
+            pairs.append((a, b))
+        pairs = np.asarray(pairs, dtype=float)
+        out[f"{name}_pairs"] = pairs
+        out[f"{name}_names"] = np.asarray([str(srf.name) for srf in scene.surfaces])
+        out[f"{name}_transmission"] = np.stack([np.asarray(srf.transmission, dtype=float) for srf in scene.surfaces])
+        for label, overrides in DIRECT_CONFIGS:
+            cfg = SimConfig(**overrides)
+            res = [steam_rt.simulate_direct(scene, p[0], p[1], cfg, "cardioid") for p in pairs]
+            out[f"{name}_{label}_occlusion"] = np.asarray([r["occlusion"] for r in res])
+            out[f"{name}_{label}_transmission"] = np.stack([np.asarray(r["transmission"], dtype=float) for r in res])
+            out[f"{name}_{label}_surface"] = np.asarray([r["occlusion_surface"] or "" for r in res])
+            out[f"{name}_{label}_gains"] = np.asarray([[r["band_gains"][b] for b in BANDS] for r in res])
+    for count in (32, 45):
+        out[f"sphere_samples_{count}"] = steam_rt._sphere_volume_samples(count)
+    out["configs_json"] = np.asarray(json.dumps({label: {k: getattr(SimConfig(**o), k) for k in (
+        "direct_occlusion", "direct_occlusion_mode", "direct_occlusion_radius_m", "direct_occlusion_samples",
+        "direct_transmission", "num_transmission_rays", "min_distance_m", "c")} for label, o in DIRECT_CONFIGS}))
+    np.savez_compressed(HERE / "direct.npz", **out)
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
-    parser.add_argument("--only", choices=("late_reverb",), help="regenerate one fixture file only")
+    parser.add_argument("--only", choices=("late_reverb", "direct"), help="regenerate one fixture file only")
     args = parser.parse_args()
     steam_rt, models, directivity = import_reference(args.reference)
-    if args.only == "late_reverb":
+    if args.only is not None:
         from acoustic_agent.models import SimConfig  # noqa: E402
-        late_reverb_golden(steam_rt, SimConfig)
+        if args.only == "late_reverb":
+            late_reverb_golden(steam_rt, SimConfig)
+        else:
+            direct_golden(steam_rt, models, SimConfig)
         return 0
     written = []
     for name, spec, trace in cases():
@@ -287,7 +334,8 @@ def main() -> int:
     np.savez_compressed(HERE / "workspace.npz", sphere=steam_rt._sphere_samples(1000, 1729),
                         bank=steam_rt._diffuse_sample_bank(128), random=rnd, indices=idx)
     late_reverb_golden(steam_rt, SimConfig)
-    print("wrote", written, "synthesis", "workspace", "late_reverb")
+    direct_golden(steam_rt, models, SimConfig)
+    print("wrote", written, "synthesis", "workspace", "late_reverb", "direct")
     return 0
 
 

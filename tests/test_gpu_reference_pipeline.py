@@ -88,3 +88,27 @@ def test_late_tail_routes_to_the_gpu_fdn(reference):
         assert g_meta["scale_by_band"][band] == pytest.approx(scale, rel=1e-7)
     scale = float(np.abs(cpu.rir).max())
     np.testing.assert_allclose(gpu.rir, cpu.rir, rtol=1e-5, atol=1e-6 * scale)
+
+
+def test_direct_path_routes_to_the_gpu(reference):
+    """install() also routes simulate_direct (steam_rt.py:942) to the GPU queries; in the furnished U room, where
+    walls and cabinets block the direct path, the render equals the one with the reference's own Python queries."""
+    bench, (steam_rt, models) = reference
+    from acoustic_agent_b200 import backend, workloads
+    w = workloads.u_furnished(1729)
+    room = bench.reference_scene(steam_rt, models, w.spec).room
+    cfg = models.SimConfig(fs=16000, duration_s=0.5, rt_duration_s=0.5, rt_num_rays=2000, rt_num_bounces=32,
+                           late_tail=False, adaptive_geometry_bounces=False, rt_accelerator="b200",
+                           rt_precision="float64", seed=5)
+    handle = backend.install(steam_rt)
+    try:
+        gpu = steam_rt.simulate_steam_room(room, list(w.sources[0]), list(w.listeners[0]), cfg, "cardioid")
+        routed = steam_rt.simulate_direct
+        steam_rt.simulate_direct = handle.originals["simulate_direct"]
+        try:
+            cpu = steam_rt.simulate_steam_room(room, list(w.sources[0]), list(w.listeners[0]), cfg, "cardioid")
+        finally:
+            steam_rt.simulate_direct = routed
+    finally:
+        handle.uninstall()
+    np.testing.assert_array_equal(gpu.rir, cpu.rir)

@@ -184,3 +184,11 @@ def test_install_routes_the_late_tail_only_for_the_b200_accelerator():
     bare = types.SimpleNamespace(trace_energy_field=fake.trace_energy_field,
                                  _normalize_rt_accelerator=fake._normalize_rt_accelerator)
     backend.install(bare).uninstall()
+
+
+def test_direct_sample_sphere_matches_reference():
+    from acoustic_agent_b200 import direct
+    g = np.load(GOLDEN / "direct.npz")
+    for count in (32, 45):
+        np.testing.assert_array_equal(direct.sphere_volume_samples(count), g[f"sphere_samples_{count}"])
+    assert list(direct.surface_groups(["a", "b", "a", "c", "b"])) == [0, 1, 0, 2, 1]
