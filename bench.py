@@ -22,6 +22,7 @@ prints one JSON line.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -347,7 +348,8 @@ def main() -> int:
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--workload", default="u_room_20_boxes",
-                        choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving", "late_reverb"))
+                        choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving", "late_reverb",
+                                 "direct"))
     parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     parser.add_argument("--no-pipeline", action="store_true",
                         help="run each step's synthesis after its own trace instead of beside the next trace")
@@ -380,6 +382,26 @@ def main() -> int:
                 "e2e": {"value": ref["value"], "unit": "tails/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}),
                 flush=True)
         return 0
+    if args.impl == "reference" and args.workload == "direct":
+        world, rank, _ = _dist_setup()
+        if rank == 0:
+            from acoustic_agent_b200 import workloads
+            w = workloads.u_furnished(1729)
+            ref = reference_direct(w, direct_pairs(w, DIRECT_PAIRS), max(20, args.steps))
+            if "unavailable" in ref:
+                print(json.dumps({"impl": "reference", "unavailable": ref["unavailable"]}), flush=True)
+            else:
+                print(json.dumps({
+                    "impl": "reference", "metric": "direct paths/s", "value": ref["value"], "unit": "paths/s",
+                    "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                    "ms_per_step": ref["seconds_per_pair"] * 1000.0, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pairs)",
+                    "config": {"workload": "direct: one source/listener pair per step, furnished U room"},
+                    "cpu_baseline": {"value": ref["value"], "unit": "paths/s", "cores": 1, "kind": "reference",
+                                     "sample": ref["sample"]},
+                    "e2e": {"value": ref["value"], "unit": "paths/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
     if args.impl == "reference":
         if args.workload in ("mixed_batch", "serving"):
             parser.error("--impl reference times the reference's per-RIR path on a single-scene workload")
@@ -391,6 +413,8 @@ def main() -> int:
         return run_serving(args)
     if args.workload == "late_reverb":
         return run_late_reverb(args)
+    if args.workload == "direct":
+        return run_direct(args)
 
     import torch
     from acoustic_agent_b200 import batching, runtime, scene as scene_mod
@@ -896,6 +920,121 @@ def run_late_reverb(args) -> int:
         "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+DIRECT_PAIRS = 1024
+
+
+def direct_pairs(workload, count: int, seed: int = 11) -> list[tuple[np.ndarray, np.ndarray]]:
+    """Seeded source/listener pairs inside the workload's footprint (0.3 m off floor and ceiling)."""
+    corners = np.asarray(workload.spec["corners"], dtype=float)
+    lo, hi = corners.min(axis=0), corners.max(axis=0)
+    h = float(workload.spec["height"])
+    rng = np.random.default_rng(seed)
+    return [(np.r_[rng.uniform(lo, hi), rng.uniform(0.3, h - 0.3)], np.r_[rng.uniform(lo, hi), rng.uniform(0.3, h - 0.3)])
+            for _ in range(count)]
+
+
+def reference_direct(workload, pairs, steps: int) -> dict:
+    """The reference's simulate_direct (Python surface objects, one host thread) on the first pairs."""
+    ref, reason = import_reference_package()
+    if ref is None:
+        return {"unavailable": reason}
+    steam_rt, models = ref
+    scene = reference_scene(steam_rt, models, workload.spec)
+    cfg = models.SimConfig()
+    steam_rt.simulate_direct(scene, pairs[0][0], pairs[0][1], cfg, "cardioid")
+    t0 = time.perf_counter()
+    for src, lst in pairs[:steps]:
+        steam_rt.simulate_direct(scene, src, lst, cfg, "cardioid")
+    per = (time.perf_counter() - t0) / steps
+    return {"value": 1.0 / per, "seconds_per_pair": per, "cores": 1, "kind": "reference",
+            "sample": f"{steps} pairs of {workload.name}, steam_rt.simulate_direct (baseline/_ref), one host thread"}
+
+
+def run_direct(args) -> int:
+    """Direct sound of 1024 seeded source/listener pairs in the furnished U room per step.
+
+    value: one ac_direct launch over the pairs (scene and tables resident;
+    volumetric occlusion with 32 samples, 8 transmission layers), device time.
+    e2e: the batch drop-in simulate_direct_batch from host arrays to the
+    reference's result dicts.  The reference's Python simulate_direct runs
+    beside it on a sample of the pairs.
+    """
+    import torch
+    from acoustic_agent_b200 import _lib, direct, runtime, workloads
+    world, rank, local = _dist_setup()
+    if world > 1:
+        raise SystemExit("the direct workload runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    w = workloads.u_furnished(1729)
+    pairs = direct_pairs(w, DIRECT_PAIRS)
+    cfg = types.SimpleNamespace(direct_occlusion=True, direct_occlusion_mode="volumetric", direct_occlusion_radius_m=0.1,
+                                direct_occlusion_samples=32, direct_transmission=True, num_transmission_rays=8,
+                                min_distance_m=1.0, c=343.0, rt_cuda_device=local)
+    ref, why = import_reference_package()
+    if ref is None:
+        raise SystemExit(f"the direct workload needs the reference scene objects: {why}")
+    steam_rt, models = ref
+    ref_scene = reference_scene(steam_rt, models, w.spec)
+    device_scene = runtime.DeviceScene(steam_rt._scene_kernel_arrays(ref_scene), device=local)
+    names, transmission = direct.scene_surfaces(ref_scene)
+    tables = direct.DirectTables(names, transmission, device)
+    queries = (_lib.ACDirectQuery * len(pairs))()
+    for k, (a, b) in enumerate(pairs):
+        queries[k] = direct.make_query(a, b, cfg)
+    stream = torch.cuda.current_stream(device)
+    for _ in range(args.warmup):
+        direct.run_queries(device_scene, tables, queries, len(pairs), samples=32, stream=stream)
+    times = []
+    sampler = ClockSampler(local)
+    with sampler:
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            # device time of the launch alone (the table copy and the result read are in e2e)
+            lib = _lib.load()
+            t = _lib.ACDirectTables()
+            t.unit_samples = tables.samples(32).data_ptr()
+            t.num_samples = 32
+            t.transmission = tables.transmission.data_ptr()
+            t.surface_group = tables.groups.data_ptr()
+            size = ctypes.c_size_t()
+            lib.ac_direct_workspace_size(len(pairs), ctypes.byref(size))
+            ws = torch.empty(int(size.value), dtype=torch.uint8, device=device)
+            res = torch.empty(len(pairs) * ctypes.sizeof(_lib.ACDirectResult), dtype=torch.uint8, device=device)
+            staging = torch.empty(int(size.value), dtype=torch.uint8, pin_memory=True)
+            e0.record(stream)
+            _lib.check(lib.ac_direct(device_scene.handle, queries, len(pairs), ctypes.byref(t),
+                                     ctypes.c_void_p(res.data_ptr()), ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                     ctypes.c_void_p(staging.data_ptr()), ctypes.c_void_p(stream.cuda_stream)),
+                       "ac_direct")
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+    step_ms = float(np.median(times))
+    e2e = []
+    for _ in range(max(3, args.steps)):
+        t0 = time.perf_counter()
+        direct.direct_results(device_scene, tables, pairs, cfg, "cardioid")
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e))
+    cpu = None if args.no_cpu_baseline else reference_direct(w, pairs, 40)
+    line = {
+        "metric": "direct paths/s", "value": len(pairs) / (step_ms * 1e-3), "unit": "paths/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pairs)",
+        "config": {"workload": f"direct: {len(pairs)} source/listener pairs in the furnished U room "
+                               f"({len(names)} surfaces), volumetric occlusion 32 samples, 8 transmission layers"},
+        "e2e": {"value": len(pairs) / e2e_s, "unit": "paths/s", "h2d_bytes_per_step": len(pairs) * 72,
+                "d2h_bytes_per_step": len(pairs) * 64, "note": "direct_results from host pairs to result dicts"},
+        "cpu_baseline": None if cpu is None or "unavailable" in cpu else {
+            "value": cpu["value"], "unit": "paths/s", "cores": 1, "kind": "reference", "sample": cpu["sample"]},
+        "gpu_launches": args.steps, "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    device_scene.close()
     return 0
 
 
