@@ -354,6 +354,7 @@ def main() -> int:
     parser.add_argument("--no-pipeline", action="store_true",
                         help="run each step's synthesis after its own trace instead of beside the next trace")
     parser.add_argument("--no-cpu-baseline", action="store_true")
+    parser.add_argument("--e2e-slots", type=int, default=3, help="end-to-end steps kept in flight (streams)")
     parser.add_argument("--block", type=int, default=0)
     parser.add_argument("--scenes", type=int, default=256, help="mixed_batch: scenes in the batch")
     parser.add_argument("--plain-jobs", type=int, default=0,
@@ -487,11 +488,11 @@ def main() -> int:
 
     # End to end through the public API: every step uploads the scene from host arrays
     # (ac_scene_create), lays out the jobs' outputs, traces and synthesises, and copies the band IRs
-    # to pinned host memory.  Two steps are in flight on two streams (one renderer each), so a step's
-    # synthesis and copy overlap the next step's upload and trace, as a streaming caller would run it.
+    # to pinned host memory.  Several steps are in flight on their own streams (one renderer each), so a
+    # step's synthesis and copy overlap the next steps' upload and trace, as a streaming caller would run it.
     slots = [{"stream": torch.cuda.Stream(device), "renderer": batching.RIRRenderer(local, block_size=args.block),
               "out": torch.empty(plan.ir_store.shape, dtype=plan.ir_store.dtype, pin_memory=True), "busy": None}
-             for _ in range(2)]
+             for _ in range(max(1, args.e2e_slots))]
 
     def e2e_drain(slot):
         if slot["busy"] is not None:
@@ -514,13 +515,13 @@ def main() -> int:
         return scenes_k, plan_k
 
     for k in range(args.warmup):
-        e2e_step(slots[k % 2])
+        e2e_step(slots[k % len(slots)])
     for slot in slots:
         e2e_drain(slot)
     e2e_steps = max(4, args.steps)
     t0 = time.perf_counter()
     for k in range(e2e_steps):
-        scenes_k, plan_k = e2e_step(slots[k % 2])
+        scenes_k, plan_k = e2e_step(slots[k % len(slots)])
     for slot in slots:
         e2e_drain(slot)
     e2e_s = time.perf_counter() - t0
@@ -559,9 +560,9 @@ def main() -> int:
             "ray_bounces_per_s": world * ray_bounces_per_step / (ms_per_step / 1000.0),
             "trace_launch_ms": trace_launch_ms,
             "e2e": {"value": e2e_value, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                    "d2h_bytes_per_step": int(d2h), "steps": e2e_steps, "in_flight": len(slots),
                     "step": "upload the scene, plan, trace + synthesise, band IRs to pinned host memory; "
-                            "two steps in flight on two streams"},
+                            f"{len(slots)} steps in flight on {len(slots)} streams"},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
