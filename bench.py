@@ -357,6 +357,8 @@ def main() -> int:
     parser.add_argument("--e2e-slots", type=int, default=3, help="end-to-end steps kept in flight (streams)")
     parser.add_argument("--block", type=int, default=0)
     parser.add_argument("--scenes", type=int, default=256, help="mixed_batch: scenes in the batch")
+    parser.add_argument("--reference-jobs", type=int, default=16,
+                        help="mixed_batch: jobs of the reference's plain per-scene CUDA path to time")
     parser.add_argument("--plain-jobs", type=int, default=0,
                         help="mixed_batch: jobs of the plain per-job loop to time (0: all)")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
@@ -597,6 +599,59 @@ def _device_timed(fn, steps: int, device, flush) -> list[float]:
     return out
 
 
+def reference_plain_sample(population, jobs, count: int, seed: int = 0) -> dict:
+    """The reference's own plain per-scene GPU path on a random sample of the batch's jobs.
+
+    One call per job, as the reference's job loops make them (engine.py:64-73,
+    batch.py:139-185): ``trace_energy_field`` with its Numba-CUDA float32
+    kernel (``rt_accelerator="cuda"``) and ``reconstruct_band_irs`` on the
+    host.  The jobs are drawn uniformly, so their mean time estimates the mean
+    over the whole batch; the first call (kernel compilation) is not timed.
+    """
+    ref, reason = import_reference_package()
+    if ref is None:
+        return {"unavailable": reason}
+    steam_rt, models = ref
+    try:
+        from acoustic_agent.steam_rt_cuda import cuda_available
+        if not cuda_available(0):
+            return {"unavailable": "the reference's Numba-CUDA backend reports no usable CUDA device"}
+    except Exception as exc:  # pragma: no cover - depends on the box
+        return {"unavailable": f"reference CUDA backend import failed: {type(exc).__name__}: {exc}"}
+    rng = np.random.default_rng(seed)
+    pick = [int(k) for k in rng.choice(len(jobs), size=min(count, len(jobs)), replace=False)]
+    scenes: dict[int, object] = {}
+
+    def run(k):
+        j = jobs[k]
+        w = population[j.workload]
+        cfg = w.config
+        if j.workload not in scenes:
+            scenes[j.workload] = reference_scene(steam_rt, models, w.spec)
+        sim = models.SimConfig(fs=cfg.fs, c=cfg.c, duration_s=cfg.duration_s, rt_duration_s=cfg.rt_duration_s,
+                               rt_num_rays=cfg.rt_num_rays, rt_num_bounces=cfg.rt_num_bounces,
+                               rt_bin_duration_s=cfg.rt_bin_duration_s, rt_specular_exponent=cfg.rt_specular_exponent,
+                               rt_irradiance_min_distance=cfg.rt_irradiance_min_distance,
+                               rt_source_radius=cfg.rt_source_radius, rt_listener_radius=cfg.rt_listener_radius,
+                               intersection_backend=cfg.intersection_backend, seed=cfg.seed, rt_accelerator="cuda",
+                               rt_precision="float32", collect_visual_paths=False, render_ambisonics=False)
+        field = steam_rt.trace_energy_field(scenes[j.workload], np.asarray(w.sources[j.source], dtype=float),
+                                            np.asarray(w.listeners[j.channel], dtype=float), sim, w.source_model,
+                                            render_ambisonics=False)
+        steam_rt.reconstruct_band_irs(field, sim)
+
+    smallest = min(range(len(jobs)), key=lambda k: jobs[k].spec.num_rays)
+    run(smallest)   # compiles the reference's kernels
+    t0 = time.perf_counter()
+    for k in pick:
+        run(k)
+    seconds = time.perf_counter() - t0
+    return {"rirs_per_s": len(pick) / seconds, "jobs_timed": len(pick), "seconds": seconds,
+            "rays_timed": int(sum(jobs[k].spec.num_rays for k in pick)),
+            "note": "the reference's trace_energy_field (Numba-CUDA float32, this GPU) + reconstruct_band_irs "
+                    "(host) per job, on uniformly drawn jobs of this batch"}
+
+
 def run_mixed_batch(args) -> int:
     """Batched mixed-size workload: many scenes, sources and channels in one persistent launch.
 
@@ -670,6 +725,12 @@ def run_mixed_batch(args) -> int:
     for s in plan_e.scenes:
         s.close()
     value = len(jobs) / (ms / 1000.0)
+    ref_plain = None if args.no_cpu_baseline else reference_plain_sample(population, jobs, args.reference_jobs)
+    if ref_plain and "rirs_per_s" in ref_plain:
+        # the sample's rays differ from the batch's: also extrapolate its time in proportion to rays
+        total_rays = sum(j.spec.num_rays for j in jobs)
+        ref_plain["rays_weighted_rirs_per_s"] = len(jobs) / (ref_plain["seconds"] * total_rays /
+                                                           max(ref_plain["rays_timed"], 1))
     line = {
         "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -684,6 +745,9 @@ def run_mixed_batch(args) -> int:
         "plain": {"rirs_per_s": plain_rirs_per_s, "jobs_timed": len(order), "seconds": plain_s,
                   "note": "per job: ac_trace + ac_synthesize + copy to host, scenes resident"},
         "batched_vs_plain": value / plain_rirs_per_s,
+        "reference_plain": ref_plain,
+        "batched_vs_reference_plain": (value / ref_plain["rirs_per_s"]) if ref_plain and "rirs_per_s" in ref_plain
+        else None,
         "e2e": {"value": len(jobs) / e2e_s, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h), "note": "scene upload + plan + launch + host copy, one pass"},
         "setup_s": {"compile": t_compile, "tune": t_tune}, "gpu_launches": 6 * args.steps,
