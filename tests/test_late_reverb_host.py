@@ -192,3 +192,23 @@ def test_direct_sample_sphere_matches_reference():
     for count in (32, 45):
         np.testing.assert_array_equal(direct.sphere_volume_samples(count), g[f"sphere_samples_{count}"])
     assert list(direct.surface_groups(["a", "b", "a", "c", "b"])) == [0, 1, 0, 2, 1]
+
+
+def test_direct_query_and_sizes_are_checked_on_the_host():
+    import ctypes
+    from acoustic_agent_b200 import direct
+    cfg = SimpleNamespace(direct_occlusion=True, direct_occlusion_mode="raycast", direct_occlusion_radius_m=0.0,
+                          direct_occlusion_samples=32, direct_transmission=False, num_transmission_rays=0)
+    q = direct.make_query(np.array([1.0, 2.0, 3.0]), np.array([4.0, 5.0, 6.0]), cfg)
+    assert (q.occlusion, q.volumetric, q.transmission, q.max_layers) == (1, 0, 0, 1)
+    assert q.radius == 1e-4   # the reference's max(1e-4, radius)
+    with pytest.raises(ValueError):
+        direct.make_query(np.zeros(3), np.ones(3), SimpleNamespace(**{**vars(cfg), "num_transmission_rays": 65}))
+    lib = _lib.load()
+    size = ctypes.c_size_t()
+    assert lib.ac_direct_workspace_size(10, ctypes.byref(size)) == _lib.AC_OK and size.value >= 10 * 72
+    assert lib.ac_direct_workspace_size(-1, ctypes.byref(size)) == _lib.AC_ERR_INVALID
+    # a null scene is refused before anything reaches a device
+    tables = _lib.ACDirectTables()
+    assert lib.ac_direct(None, (_lib.ACDirectQuery * 1)(), 1, ctypes.byref(tables), None, None, 0, None,
+                         None) == _lib.AC_ERR_INVALID
