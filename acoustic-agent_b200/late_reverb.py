@@ -21,6 +21,7 @@ path: without the library or a CUDA device the calls raise.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 from dataclasses import dataclass
 from typing import Any, Mapping, Sequence
@@ -166,6 +167,80 @@ def design(fs: int, seed: int, rt60: Sequence[float]) -> FdnDesign:
     return FdnDesign(delays, absorptive, eq_cascade(tone, fs), ALLPASS_DELAYS)
 
 
+def _cascade_many(gains: np.ndarray, fs: int) -> np.ndarray:
+    """eq_cascade for many gain rows at once: [M, 6] -> [M, 6, 5], the same operations element by element."""
+    g = np.asarray(gains, dtype=np.float64).reshape(-1, 6)
+    nyquist = max(1.0, 0.5 * float(fs))
+    out = np.empty((g.shape[0], 6, 5), dtype=np.float64)
+    for b, (lo, hi) in enumerate(bands.band_edges(fs)):
+        A = np.sqrt(np.maximum(g[:, b], 1e-6))
+        if b == 0 or b == 5:
+            cutoff = float(np.clip(hi if b == 0 else lo, 1e-3, nyquist * 0.999))
+            cw, alpha, _, _ = _rbj_terms(cutoff, 1.0, fs, 0.707)
+            r = np.sqrt(A)
+            if b == 0:
+                a0 = (A + 1.0) + (A - 1.0) * cw + 2.0 * r * alpha
+                rows = (A * ((A + 1.0) - (A - 1.0) * cw + 2.0 * r * alpha) / a0,
+                        2.0 * A * ((A - 1.0) - (A + 1.0) * cw) / a0,
+                        A * ((A + 1.0) - (A - 1.0) * cw - 2.0 * r * alpha) / a0,
+                        -2.0 * ((A - 1.0) + (A + 1.0) * cw) / a0,
+                        ((A + 1.0) + (A - 1.0) * cw - 2.0 * r * alpha) / a0)
+            else:
+                a0 = (A + 1.0) - (A - 1.0) * cw + 2.0 * r * alpha
+                rows = (A * ((A + 1.0) + (A - 1.0) * cw + 2.0 * r * alpha) / a0,
+                        -2.0 * A * ((A - 1.0) + (A + 1.0) * cw) / a0,
+                        A * ((A + 1.0) + (A - 1.0) * cw - 2.0 * r * alpha) / a0,
+                        2.0 * ((A - 1.0) - (A + 1.0) * cw) / a0,
+                        ((A + 1.0) - (A - 1.0) * cw - 2.0 * r * alpha) / a0)
+        else:
+            lower = float(np.clip(lo, 1e-3, nyquist * 0.998))
+            upper = float(np.clip(hi, lower + 1e-3, nyquist * 0.999))
+            centre = math.sqrt(max(lower * upper, 1e-12))
+            w0 = 2.0 * math.pi * centre / max(float(fs), 1.0)
+            cw, sw = math.cos(w0), math.sin(w0)
+            alpha = sw * ((upper - lower) / centre) / 2.0
+            a0 = 1.0 + alpha / A
+            rows = ((1.0 + alpha * A) / a0, -2.0 * cw / a0, (1.0 - alpha * A) / a0, -2.0 * cw / a0,
+                    (1.0 - alpha / A) / a0)
+        out[:, b] = np.stack(rows, axis=-1)
+    return out
+
+
+def design_many(fs: int, seed: int, rt60s: np.ndarray) -> list[FdnDesign]:
+    """design() for many RT60 rows of one sample rate and seed, with the per-line solves batched."""
+    t60 = np.maximum(0.1, np.nan_to_num(np.asarray(rt60s, dtype=np.float64).reshape(-1, 6)))
+    if t60.shape[0] == 0:
+        return []
+    delays = line_delays(fs, seed)
+    d = np.asarray(delays, dtype=np.float64)
+    gains = np.maximum(np.exp(-(6.91 * d)[None, :, None] / (t60[:, None, :] * max(float(fs), 1.0))), 1e-3)
+    want = np.clip(gains.reshape(-1, 6), 1e-3, 0.999999)
+    m = eq_response(fs)
+    logs = np.linalg.solve(np.broadcast_to(m, (want.shape[0], 6, 6)), np.log(want)[..., None])[..., 0]
+    absorptive = _cascade_many(np.clip(np.exp(logs), 1e-3, 4.0), fs).reshape(t60.shape[0], delays.size, 6, 5)
+    tone_gains = np.sqrt(1.0 / t60)
+    tone_gains /= np.maximum(np.max(tone_gains, axis=1, keepdims=True), 1e-12)
+    tones = _cascade_many(tone_gains, fs)
+    return [FdnDesign(delays, absorptive[k], tones[k], ALLPASS_DELAYS) for k in range(t60.shape[0])]
+
+
+_Y00 = 1.0 / math.sqrt(4.0 * math.pi)   # steam_rt.py:37-38
+
+
+def estimate_reverb_times(echogram: np.ndarray, bin_duration_s: float, speed_of_sound: float) -> list[float]:
+    """The reference's traced RT60 per band (steam_rt.py:2727-2742): the Schroeder fit of Y00 * E, weighted
+    by the band's air absorption over the bin start times (:2196-2202), with a 1e-4 energy floor."""
+    from acoustic_agent_b200 import metrics
+    e = np.asarray(echogram)
+    times = float(bin_duration_s) * np.arange(e.shape[1], dtype=np.float64)
+    distances = np.maximum(times, 0.0) * max(0.0, float(speed_of_sound))
+    out = []
+    for b, coeff in enumerate(bands.AIR_ABSORPTION_NP_PER_M):
+        weights = np.exp(-2.0 * max(0.0, float(coeff)) * distances)
+        out.append(metrics.schroeder_rt60((_Y00 * e[b]) * weights, bin_duration_s, min_total_energy=1e-4))
+    return out
+
+
 # ---- crossfade windows -----------------------------------------------------
 
 @dataclass
@@ -241,11 +316,13 @@ class LateReverbRenderer:
         return self._designs[key]
 
     def render(self, jobs: Sequence[LateReverbJob], *, stream: torch.cuda.Stream | None = None,
-               fdn_events: tuple[torch.cuda.Event, torch.cuda.Event] | None = None
+               fdn_events: tuple[torch.cuda.Event, torch.cuda.Event] | None = None,
+               designs: Sequence[FdnDesign] | None = None
                ) -> tuple[torch.Tensor, list[FdnDesign], list[Windows]]:
         """Enqueue every job on `stream`; returns the [J, 6, AC_LATE_STATS] float64 stats tensor, the designs
         and the windows.  Jobs whose tail starts outside the signal must not be passed.  `fdn_events`, if
-        given, are recorded around the FDN launch (to time the network alone)."""
+        given, are recorded around the FDN launch (to time the network alone); `designs`, if given, are
+        the jobs' FDN designs (from design_many), else they are made here."""
         J = len(jobs)
         stats = torch.zeros(max(J, 1), 6, _lib.AC_LATE_STATS, dtype=torch.float64, device=self.device)
         if J == 0:
@@ -256,6 +333,9 @@ class LateReverbRenderer:
         rate_index = {int(cfg.sample_rates[k]): k for k in range(cfg.num_rates)}
         fdn_jobs = (_lib.ACFdnJob * J)()
         tail_jobs = (_lib.ACLateTailJob * J)()
+        given = list(designs) if designs is not None else None
+        if given is not None and len(given) != J:
+            raise ValueError("one design per job")
         designs, wins = [], []
         offset = 0
         for k, job in enumerate(jobs):
@@ -264,15 +344,16 @@ class LateReverbRenderer:
                 if t.dtype != dtype or not t.is_contiguous() or tuple(t.shape) != (6, N) or t.device != self.device:
                     raise ValueError(f"late reverb job {k}: expected contiguous [6, {N}] {dtype} on {self.device}")
             fs = max(1, int(job.fs))
-            d = self.design(fs, job.seed, job.rt60)
+            d = given[k] if given is not None else self.design(fs, job.seed, job.rt60)
             w = windows(N, fs, job.transition_s, job.overlap_fraction, job.decay_profiles)
             if min(w.start) >= N:
                 raise ValueError(f"late reverb job {k}: the tail starts after the signal ends")
             designs.append(d)
             wins.append(w)
             f = fdn_jobs[k]
-            f.absorptive[:] = d.absorptive.reshape(-1).tolist()
-            f.tone[:] = d.tone.reshape(-1).tolist()
+            ctypes.memmove(ctypes.addressof(f.absorptive), np.ascontiguousarray(d.absorptive).ctypes.data,
+                           ctypes.sizeof(f.absorptive))
+            ctypes.memmove(ctypes.addressof(f.tone), np.ascontiguousarray(d.tone).ctypes.data, ctypes.sizeof(f.tone))
             f.delays[:] = [int(v) for v in d.delays]
             f.allpass_delays[:] = list(d.allpass)
             f.num_samples = N

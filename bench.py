@@ -725,6 +725,20 @@ def run_mixed_batch(args) -> int:
     for s in plan_e.scenes:
         s.close()
     value = len(jobs) / (ms / 1000.0)
+    # hybrid FDN late tails of every job of the batch (RT60 from each echogram, batched designs, one FDN
+    # launch and one tail launch), after a warm-up call
+    renderer.launch(plan)
+    renderer.late_tails(plan)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    tails = renderer.late_tails(plan)
+    torch.cuda.synchronize(device)
+    tails_s = time.perf_counter() - t0
+    late = {"tails": len(jobs), "seconds": tails_s, "host_seconds": tails.host_seconds,
+            "tails_per_s": len(jobs) / tails_s,
+            "note": "RIRRenderer.late_tails after a step: RT60 estimates and FDN designs on the host, "
+                    "ac_fdn_impulse + ac_late_tail over all jobs"}
+    del tails
     ref_plain = None if args.no_cpu_baseline else reference_plain_sample(population, jobs, args.reference_jobs)
     if ref_plain and "rirs_per_s" in ref_plain:
         # the sample's rays differ from the batch's: also extrapolate its time in proportion to rays
@@ -746,6 +760,7 @@ def run_mixed_batch(args) -> int:
                   "note": "per job: ac_trace + ac_synthesize + copy to host, scenes resident"},
         "batched_vs_plain": value / plain_rirs_per_s,
         "reference_plain": ref_plain,
+        "late_tails": late,
         "batched_vs_reference_plain": (value / ref_plain["rirs_per_s"]) if ref_plain and "rirs_per_s" in ref_plain
         else None,
         "e2e": {"value": len(jobs) / e2e_s, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),

@@ -280,16 +280,37 @@ def direct_golden(steam_rt, models, SimConfig) -> None:
     np.savez_compressed(HERE / "direct.npz", **out)
 
 
+RT60_CASES = (("shoebox_linear", 0.01), ("u_furnished_bvh", 0.001), ("apartment3_bvh", 0.01),
+              ("objects_mix_bvh", 0.01))
+
+
+def rt60_golden(steam_rt, SimConfig) -> None:
+    """estimate_reverb_times (steam_rt.py:2727-2742) on golden echograms, as float64 and as float32."""
+    out = {}
+    cfg = SimConfig()
+    for name, bin_dur in RT60_CASES:
+        echogram = np.load(HERE / f"{name}.npz")["echogram"]
+        for label, e in (("f64", echogram.astype(np.float64)), ("f32", echogram.astype(np.float32))):
+            field = {"echogram": e, "bin_duration_s": bin_dur, "num_bins": e.shape[1]}
+            rt = steam_rt.estimate_reverb_times(field, cfg)
+            out[f"{name}_{label}"] = np.asarray([rt[b] for b in BANDS])
+        out[f"{name}_bin"] = np.asarray(bin_dur)
+    out["speed_of_sound"] = np.asarray(float(cfg.c))
+    np.savez_compressed(HERE / "rt60.npz", **out)
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
-    parser.add_argument("--only", choices=("late_reverb", "direct"), help="regenerate one fixture file only")
+    parser.add_argument("--only", choices=("late_reverb", "direct", "rt60"), help="regenerate one fixture file only")
     args = parser.parse_args()
     steam_rt, models, directivity = import_reference(args.reference)
     if args.only is not None:
         from acoustic_agent.models import SimConfig  # noqa: E402
         if args.only == "late_reverb":
             late_reverb_golden(steam_rt, SimConfig)
+        elif args.only == "rt60":
+            rt60_golden(steam_rt, SimConfig)
         else:
             direct_golden(steam_rt, models, SimConfig)
         return 0
@@ -335,7 +356,8 @@ def main() -> int:
                         bank=steam_rt._diffuse_sample_bank(128), random=rnd, indices=idx)
     late_reverb_golden(steam_rt, SimConfig)
     direct_golden(steam_rt, models, SimConfig)
-    print("wrote", written, "synthesis", "workspace", "late_reverb", "direct")
+    rt60_golden(steam_rt, SimConfig)
+    print("wrote", written, "synthesis", "workspace", "late_reverb", "direct", "rt60")
     return 0
 
 

@@ -206,3 +206,33 @@ def test_full_length_tail_matches_the_oracle():
         np.testing.assert_allclose(got, want, rtol=2e-7, atol=2e-7 * float(np.abs(want).max()))
     for b, band in enumerate(bands.FREQUENCY_BANDS):
         assert meta["scale_by_band"][band] == pytest.approx(info["scales"][b], rel=1e-7)
+
+
+def test_batched_late_tails_equal_the_drop_in_per_job():
+    """RIRRenderer.late_tails over a mixed plan (16 and 48 kHz) equals render_parametric_fdn_late_reverb on
+    each job's band IRs, with the RT60s estimated from its echogram, bit for bit."""
+    from acoustic_agent_b200 import batching, scene, workloads
+    ws = [workloads.shoebox(1729, rays=20000, bounces=50), workloads.u_furnished(1729, rays=20000)]
+    specs, jobs = batching.workload_jobs(ws)
+    jobs = jobs[:4]   # the shoebox RIR and three U-room channels
+    renderer = batching.RIRRenderer(0)
+    plan = renderer.plan([scene.compile_scene(s) for s in specs], jobs)
+    renderer.launch(plan)
+    tails = renderer.late_tails(plan)
+    torch.cuda.synchronize()
+    band_irs = renderer.results(plan)
+    # the shoebox's traced energy gives RT60s; the U room's stays under the estimator's 1e-4 floor, so its
+    # tails take the reference's zero-RT60 path (design at 0.1 s, FDN bands left unscaled)
+    assert (tails.rt60[0] > 0).all()
+    for k, j in enumerate(plan.jobs):
+        rt60 = dict(zip(bands.FREQUENCY_BANDS, tails.rt60[k]))
+        cfg = sim_config(fs=j.fs, seed=int(j.spec.seed), hybrid_transition_s=1.0, hybrid_overlap_fraction=0.25,
+                         rt_bin_duration_s=j.spec.bin_duration)
+        out, comp, _ = late_reverb.render_parametric_fdn_late_reverb(band_irs[k], {"bin_duration_s": j.spec.bin_duration},
+                                                                     rt60, cfg)
+        np.testing.assert_array_equal(tails.irs[k].cpu().numpy(), out)
+        n = out.size
+        start = sum(t.numel() for t in plan.irs[:k])
+        np.testing.assert_array_equal(tails.component[start:start + n].cpu().numpy().reshape(out.shape), comp)
+    for s in plan.scenes:
+        s.close()

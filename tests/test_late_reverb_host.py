@@ -212,3 +212,25 @@ def test_direct_query_and_sizes_are_checked_on_the_host():
     tables = _lib.ACDirectTables()
     assert lib.ac_direct(None, (_lib.ACDirectQuery * 1)(), 1, ctypes.byref(tables), None, None, 0, None,
                          None) == _lib.AC_ERR_INVALID
+
+
+def test_batched_design_equals_the_per_call_design():
+    rng = np.random.default_rng(5)
+    for fs in (16000, 48000):
+        rt60s = rng.uniform(0.05, 3.0, (24, 6))
+        rt60s[3] = 0.0
+        rt60s[7, 2] = 0.0
+        for got, r in zip(late_reverb.design_many(fs, 11, rt60s), rt60s):
+            want = late_reverb.design(fs, 11, r)
+            np.testing.assert_array_equal(got.delays, want.delays)
+            np.testing.assert_array_equal(got.absorptive, want.absorptive)
+            np.testing.assert_array_equal(got.tone, want.tone)
+
+
+@pytest.mark.parametrize("name", ("shoebox_linear", "u_furnished_bvh", "apartment3_bvh", "objects_mix_bvh"))
+def test_rt60_estimate_matches_reference(name):
+    g = np.load(GOLDEN / "rt60.npz")
+    echogram = np.load(GOLDEN / f"{name}.npz")["echogram"]
+    for label, e in (("f64", echogram.astype(np.float64)), ("f32", echogram.astype(np.float32))):
+        got = late_reverb.estimate_reverb_times(e, float(g[f"{name}_bin"]), float(g["speed_of_sound"]))
+        np.testing.assert_array_equal(np.asarray(got), g[f"{name}_{label}"])
