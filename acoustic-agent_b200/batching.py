@@ -17,14 +17,13 @@ bins), which the tests check.
 from __future__ import annotations
 
 import math
-import time
 from dataclasses import dataclass, field
 from typing import Any, Iterable, Sequence
 
 import numpy as np
 import torch
 
-from acoustic_agent_b200 import _lib, bands, rng, runtime
+from acoustic_agent_b200 import bands, rng, runtime
 from acoustic_agent_b200.directivity import source_directivity, source_forward
 from acoustic_agent_b200.scene import SceneArrays, compile_scene
 from acoustic_agent_b200.workloads import TraceConfig, Workload
@@ -241,7 +240,7 @@ class RIRRenderer:
         plan.pipe_graph = graph
 
     def late_tails(self, plan: Plan, *, transition_s: float = 1.0, overlap_fraction: float = 0.25,
-                   stream: torch.cuda.Stream | None = None) -> LateTails:
+                   stream: torch.cuda.Stream | None = None):
         """Hybrid FDN late tails of every job of `plan` (see plan_late_tails)."""
         return plan_late_tails(self, plan, transition_s=transition_s, overlap_fraction=overlap_fraction,
                                stream=stream)
@@ -259,79 +258,27 @@ class RIRRenderer:
         return out
 
 
-@dataclass
-class LateTails:
-    """Hybrid band IRs of a plan's jobs: traced band IRs crossfaded into their FDN late tails."""
-
-    out: torch.Tensor             # float32, every job's [6, N] hybrid band IRs back to back (as ir_store)
-    component: torch.Tensor       # float32, the FDN part of `out`
-    irs: list[torch.Tensor]       # per job: its [6, N] view of `out`
-    rt60: np.ndarray              # [J, 6] target RT60s estimated from the jobs' echograms
-    stats: torch.Tensor           # [J, 6, AC_LATE_STATS] float64 (zeros for a job without a tail)
-    host_seconds: float           # RT60 estimates, designs and job tables on the host
-
-
 def plan_late_tails(renderer: "RIRRenderer", plan: Plan, *, transition_s: float = 1.0,
-                    overlap_fraction: float = 0.25, stream: torch.cuda.Stream | None = None) -> LateTails:
-    """Late tails for every job of a plan whose trace and synthesis have been enqueued on `stream`.
-
-    Per job, as the reference's renderer does for one RIR (steam_rt.py:1014-1035, single room): the
-    six target RT60s from the job's echogram (``late_reverb.estimate_reverb_times``), an FDN designed for
-    them (``late_reverb.design_many``, the same numbers as the per-call design), and the hybrid tail over
-    the job's band IRs; all FDN impulses in one ``ac_fdn_impulse`` launch and all tails in one
-    ``ac_late_tail``.  Each job's result equals ``render_parametric_fdn_late_reverb`` on that job's band
-    IRs.  The coupled-space breakpoint model of multi-room renders is not applied here.
-    """
+                    overlap_fraction: float = 0.25, stream: torch.cuda.Stream | None = None):
+    """Late tails for every job of a plan whose trace and synthesis have been enqueued on `stream`
+    (late_reverb.batch_late_tails over the plan's band IRs and echograms); returns its BatchTails."""
     from acoustic_agent_b200 import late_reverb
     stream = stream if stream is not None else torch.cuda.current_stream(renderer.device)
-    t0 = time.perf_counter()
     with torch.cuda.stream(stream):
         echo_host = plan.echo_store.to("cpu", non_blocking=True)
-        traced = plan.ir_store.to(torch.float64)
-        out = torch.empty_like(plan.ir_store)
-        component = torch.zeros_like(plan.ir_store)
     stream.synchronize()
     echo = echo_host.numpy()
-    rt60 = np.zeros((len(plan.jobs), NUM_BANDS), dtype=np.float64)
-    off = 0
-    for k, j in enumerate(plan.jobs):
+    echograms, off = [], 0
+    for j in plan.jobs:
         bins = int(j.spec.num_bins)
-        e = echo[off:off + NUM_BANDS * bins].reshape(NUM_BANDS, bins)
+        echograms.append(echo[off:off + NUM_BANDS * bins].reshape(NUM_BANDS, bins))
         off += NUM_BANDS * bins
-        rt60[k] = late_reverb.estimate_reverb_times(e, j.spec.bin_duration, j.spec.speed_of_sound)
-    designs: list[Any] = [None] * len(plan.jobs)
-    groups: dict[tuple[int, int], list[int]] = {}
-    for k, j in enumerate(plan.jobs):
-        groups.setdefault((int(j.fs), int(j.spec.seed)), []).append(k)
-    for (fs, seed), members in groups.items():
-        for k, d in zip(members, late_reverb.design_many(fs, seed, rt60[members])):
-            designs[k] = d
-    views, comp_views, jobs, chosen = [], [], [], []
-    i_off = 0
-    for k, (j, ir) in enumerate(zip(plan.jobs, plan.irs)):
-        n = ir.numel()
-        shape = tuple(ir.shape)
-        views.append(out[i_off:i_off + n].view(shape))
-        comp_views.append(component[i_off:i_off + n].view(shape))
-        w = late_reverb.windows(shape[1], j.fs, transition_s, overlap_fraction)
-        if min(w.start) >= shape[1]:
-            views[-1].copy_(ir)   # no tail fits: the traced band IRs stand (steam_rt.py:2542-2552)
-        else:
-            jobs.append(late_reverb.LateReverbJob(traced[i_off:i_off + n].view(shape), views[-1], comp_views[-1],
-                                                  j.fs, int(j.spec.seed), rt60[k], j.spec.bin_duration,
-                                                  transition_s, overlap_fraction))
-            chosen.append(k)
-        i_off += n
-    host_seconds = time.perf_counter() - t0
-    stats = torch.zeros(len(plan.jobs), NUM_BANDS, _lib.AC_LATE_STATS, dtype=torch.float64, device=renderer.device)
-    if jobs:
-        if getattr(renderer, "_late", None) is None:
-            renderer._late = late_reverb.LateReverbRenderer(renderer.device)
-        got, _, _ = renderer._late.render(jobs, stream=stream, designs=[designs[k] for k in chosen])
-        with torch.cuda.stream(stream):
-            stats[chosen] = got
-    traced.record_stream(stream)
-    return LateTails(out, component, views, rt60, stats, host_seconds)
+    if getattr(renderer, "_late", None) is None:
+        renderer._late = late_reverb.LateReverbRenderer(renderer.device)
+    return late_reverb.batch_late_tails(
+        renderer._late, plan.irs, echograms, [j.fs for j in plan.jobs], [int(j.spec.seed) for j in plan.jobs],
+        [j.spec.bin_duration for j in plan.jobs], [j.spec.speed_of_sound for j in plan.jobs],
+        transition_s=transition_s, overlap_fraction=overlap_fraction, stream=stream)
 
 
 def render(workloads: Sequence[Workload], *, device: int = 0, precision: str = "float32",

@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 from dataclasses import dataclass
 from typing import Any, Mapping, Sequence
 
@@ -384,6 +385,81 @@ class LateReverbRenderer:
         # keep the FDN scratch alive until the stream has used it
         raw.record_stream(launch_stream)
         return stats, designs, wins
+
+
+@dataclass
+class BatchTails:
+    """Hybrid band IRs of a batch: every job's traced band IRs crossfaded into its FDN late tail."""
+
+    out: torch.Tensor             # float32, the jobs' [6, N] hybrid band IRs back to back
+    component: torch.Tensor       # float32, the FDN part of `out`, same layout
+    irs: list[torch.Tensor]       # per job: its [6, N] view of `out`
+    rt60: np.ndarray              # [J, 6] target RT60s estimated from the jobs' echograms
+    stats: torch.Tensor           # [J, 6, AC_LATE_STATS] float64 (zeros for a job without a tail)
+    host_seconds: float           # RT60 estimates, designs and job tables on the host
+
+
+def batch_late_tails(renderer: LateReverbRenderer, band_irs: Sequence[torch.Tensor], echograms: Sequence[np.ndarray],
+                     fs: Sequence[int], seeds: Sequence[int], bin_durations: Sequence[float],
+                     speeds: Sequence[float], *, transition_s: float = 1.0, overlap_fraction: float = 0.25,
+                     stream: torch.cuda.Stream | None = None) -> BatchTails:
+    """Late tails of many RIRs, as the reference's renderer makes one (steam_rt.py:1014-1035, single room).
+
+    `band_irs` are the jobs' float32 [6, N] device band IRs (contiguous and back to back in one buffer, in
+    job order), `echograms` their [6, bins] host echograms.  Per job: the six target RT60s from the
+    echogram (estimate_reverb_times), an FDN designed for them (design_many: the same numbers as the
+    per-call design) and the hybrid tail; all FDN impulses go in one ac_fdn_impulse launch and all tails
+    in one ac_late_tail, enqueued on `stream` after whatever produced `band_irs` there.  Each job's result
+    equals render_parametric_fdn_late_reverb on its band IRs.  The coupled-space breakpoint model of
+    multi-room renders is not applied.
+    """
+    t0 = time.perf_counter()
+    J = len(band_irs)
+    stream = stream if stream is not None else torch.cuda.current_stream(renderer.device)
+    total = sum(t.numel() for t in band_irs)
+    base = band_irs[0] if J else None
+    if J and any(t.data_ptr() != base.data_ptr() + 4 * sum(u.numel() for u in band_irs[:k])
+                 for k, t in enumerate(band_irs)):
+        raise ValueError("band_irs must lie back to back in one buffer, in job order")
+    flat = torch.as_strided(base, (total,), (1,)) if J else torch.empty(0, device=renderer.device)
+    with torch.cuda.stream(stream):
+        traced = flat.to(torch.float64)
+        out = torch.empty_like(flat)
+        component = torch.zeros_like(flat)
+    rt60 = np.zeros((J, 6), dtype=np.float64)
+    for k in range(J):
+        rt60[k] = estimate_reverb_times(echograms[k], bin_durations[k], speeds[k])
+    designs: list[Any] = [None] * J
+    groups: dict[tuple[int, int], list[int]] = {}
+    for k in range(J):
+        groups.setdefault((max(1, int(fs[k])), int(seeds[k])), []).append(k)
+    for (rate, seed), members in groups.items():
+        for k, d in zip(members, design_many(rate, seed, rt60[members])):
+            designs[k] = d
+    views, jobs, chosen = [], [], []
+    off = 0
+    for k, ir in enumerate(band_irs):
+        n = ir.numel()
+        shape = tuple(ir.shape)
+        views.append(out[off:off + n].view(shape))
+        w = windows(shape[1], fs[k], transition_s, overlap_fraction)
+        if min(w.start) >= shape[1]:
+            with torch.cuda.stream(stream):
+                views[-1].copy_(ir)   # no tail fits: the traced band IRs stand (steam_rt.py:2542-2552)
+        else:
+            jobs.append(LateReverbJob(traced[off:off + n].view(shape), views[-1],
+                                      component[off:off + n].view(shape), int(fs[k]), int(seeds[k]), rt60[k],
+                                      bin_durations[k], transition_s, overlap_fraction))
+            chosen.append(k)
+        off += n
+    host_seconds = time.perf_counter() - t0
+    stats = torch.zeros(J, 6, _lib.AC_LATE_STATS, dtype=torch.float64, device=renderer.device)
+    if jobs:
+        got, _, _ = renderer.render(jobs, stream=stream, designs=[designs[k] for k in chosen])
+        with torch.cuda.stream(stream):
+            stats[chosen] = got
+    traced.record_stream(stream)
+    return BatchTails(out, component, views, rt60, stats, host_seconds)
 
 
 def metadata(stats: np.ndarray, d: FdnDesign, w: Windows, fs: int, rt60_bands: Mapping[str, float]) -> dict[str, Any]:

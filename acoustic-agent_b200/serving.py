@@ -135,13 +135,15 @@ def request_jobs(req: Request, precision: str = "float32") -> list[runtime.Trace
     return specs
 
 
-def job_bytes(spec: runtime.TraceSpec, fs: int, num_surfaces: int) -> int:
-    """Device bytes one job holds while in flight (outputs, echogram, band IRs, synthesis rows)."""
+def job_bytes(spec: runtime.TraceSpec, fs: int, num_surfaces: int, *, late_tail: bool = False) -> int:
+    """Device bytes one job holds while in flight (outputs, echogram, band IRs, synthesis rows, and with
+    `late_tail` the float64 copy, hybrid outputs, FDN impulse, band split and delay lines)."""
     bins = int(spec.num_bins)
     n = bins * bands.samples_per_bin(spec.bin_duration, fs)
     trace_out = 8 * (NUM_BANDS * bins * 2 + 4 * num_surfaces + 8) + 4 * (NUM_BANDS * bins + num_surfaces)
     synth = 8 * (2 * NUM_BANDS * bins + NUM_BANDS * n)
-    return trace_out + 4 * NUM_BANDS * n + synth + 1024
+    tail = (8 + 4 + 4 + 4) * NUM_BANDS * n + 8 * n + (1 << 20) if late_tail else 0
+    return trace_out + 4 * NUM_BANDS * n + synth + tail + 1024
 
 
 class SceneCache:
@@ -224,6 +226,10 @@ class _Batch:
     bytes: int
     admitted_s: float
     keep: list[Any] = field(default_factory=list)
+    # late tails: the band IRs and host echograms wait for the tail phase, which replaces `done`
+    ir_store: torch.Tensor | None = None
+    echograms: list[torch.Tensor] | None = None
+    tails_pending: bool = False
 
 
 class Server:
@@ -233,10 +239,13 @@ class Server:
 
     def __init__(self, device: int = 0, *, max_inflight: int = 3, hbm_budget: int | None = None,
                  max_batch_rays: int = 400_000_000, tune: bool = True, block_size: int = 0,
-                 chunk_rays: int = 0, policy: str = "small_first", starve_s: float = 1.0) -> None:
+                 chunk_rays: int = 0, policy: str = "small_first", starve_s: float = 1.0,
+                 late_tail: bool = False, transition_s: float = 1.0, overlap_fraction: float = 0.25) -> None:
         """`policy` orders the waiting requests when a batch is formed: "fifo" by arrival, or
         "small_first" by ray count, except that requests waiting longer than `starve_s` go first
-        (in arrival order), so a stream of small requests cannot hold a large one back for ever."""
+        (in arrival order), so a stream of small requests cannot hold a large one back for ever.
+        With `late_tail`, every served RIR is crossfaded into its FDN late tail as the reference's
+        renderer does with late_tail=True (late_reverb.batch_late_tails, one launch pair per batch)."""
         if policy not in self.POLICIES:
             raise ValueError(f"policy must be one of {self.POLICIES}")
         self.policy = policy
@@ -253,12 +262,16 @@ class Server:
         self.chunk_rays = chunk_rays
         self.streams = [torch.cuda.Stream(self.dev) for _ in range(self.max_inflight)]
         self.in_use = 0     # bytes held by in-flight batches
+        self.late_tail = bool(late_tail)
+        self.transition_s = float(transition_s)
+        self.overlap_fraction = float(overlap_fraction)
+        self._late: dict[int, Any] = {}
 
     # ---- footprint and admission
     def footprint(self, req: Request, specs: Sequence[runtime.TraceSpec]) -> int:
         scene = 0 if self.scenes.is_resident(req.workload) else self._scene_estimate(req.workload)
         surfaces = self.scenes.key_of(req.workload)[1].num_surfaces
-        return scene + sum(job_bytes(s, req.workload.config.fs, surfaces) for s in specs)
+        return scene + sum(job_bytes(s, req.workload.config.fs, surfaces, late_tail=self.late_tail) for s in specs)
 
     def _scene_estimate(self, w: Workload) -> int:
         arrays = self.scenes.key_of(w)[1]
@@ -303,11 +316,50 @@ class Server:
                                 stream=stream)
             runtime.synthesize_batch(synth, synth_ws, stream=stream)
             host = torch.empty(ir_store.shape, dtype=torch.float32, pin_memory=True)
-            host.copy_(ir_store, non_blocking=True)
+            echograms = None
+            if self.late_tail:   # the tails need the echograms on the host first
+                echograms = []
+                for b in buffers:
+                    e = torch.empty(b.echogram.shape, dtype=torch.float32, pin_memory=True)
+                    e.copy_(b.echogram, non_blocking=True)
+                    echograms.append(e)
+            else:
+                host.copy_(ir_store, non_blocking=True)
             done = torch.cuda.Event()
             done.record(stream)
         keep.extend([ir_store, trace_ws, synth_ws, synth])
-        return _Batch(reqs, specs, stream, done, host, lengths, buffers, nbytes, now, keep)
+        return _Batch(reqs, specs, stream, done, host, lengths, buffers, nbytes, now, keep, ir_store=ir_store,
+                      echograms=echograms, tails_pending=self.late_tail)
+
+    def _start_tails(self, batch: _Batch) -> None:
+        """Second phase of a late-tail batch: RT60s from the echograms, the FDN tails of every job in one
+        launch pair on the batch's stream, and the hybrid band IRs to pinned host memory."""
+        from acoustic_agent_b200 import late_reverb
+        # one renderer (and so one device workspace) per stream: batches in flight on other streams
+        # must not share delay lines or band-split scratch with this one
+        key = id(batch.stream)
+        if key not in self._late:
+            self._late[key] = late_reverb.LateReverbRenderer(self.dev)
+        irs, fs, seeds, bins, speeds = [], [], [], [], []
+        off = 0
+        for req, ss, row in zip(batch.requests, batch.specs, batch.lengths):
+            for s, n in zip(ss, row):
+                irs.append(batch.ir_store[off:off + NUM_BANDS * n].view(NUM_BANDS, n))
+                off += NUM_BANDS * n
+                fs.append(req.workload.config.fs)
+                seeds.append(int(s.seed))
+                bins.append(s.bin_duration)
+                speeds.append(s.speed_of_sound)
+        tails = late_reverb.batch_late_tails(self._late[key], irs, [e.numpy() for e in batch.echograms], fs, seeds,
+                                             bins, speeds, transition_s=self.transition_s,
+                                             overlap_fraction=self.overlap_fraction, stream=batch.stream)
+        with torch.cuda.stream(batch.stream):
+            batch.host.copy_(tails.out, non_blocking=True)
+            done = torch.cuda.Event()
+            done.record(batch.stream)
+        batch.keep.append(tails)
+        batch.done = done
+        batch.tails_pending = False
 
     def _finish(self, batch: _Batch, now: float) -> list[Result]:
         host = batch.host.numpy()
@@ -354,6 +406,9 @@ class Server:
                 waiting.append((req, request_jobs(req)))
             # completions first: they return slots and memory
             for batch in list(inflight):
+                if batch.done.query() and batch.tails_pending:
+                    self._start_tails(batch)
+                    continue
                 if batch.done.query():
                     done_at = time.perf_counter() - t0
                     results.extend(self._finish(batch, done_at))
@@ -413,9 +468,9 @@ def requests_from_stream(stream: Sequence[dict[str, Any]]) -> list[Request]:
             for k, e in enumerate(stream)]
 
 
-def render_alone(req: Request, device: int = 0) -> list[np.ndarray]:
+def render_alone(req: Request, device: int = 0, *, late_tail: bool = False) -> list[np.ndarray]:
     """The same request rendered by itself (one batch, nothing else on the GPU)."""
-    server = Server(device, max_inflight=1, tune=False)
+    server = Server(device, max_inflight=1, tune=False, late_tail=late_tail)
     try:
         report = server.serve([Request(req.id, req.workload, req.sources, 0.0, req.moving)], realtime=False)
     finally:

@@ -101,3 +101,39 @@ def test_a_request_larger_than_the_budget_is_rejected_not_fatal(served):
     assert big.id in rejected and "budget" in out.results[[r.request.id for r in out.results].index(big.id)].error
     assert all(r.band_irs for r in out.results if r.error is None)
     assert out.summary()["rejected"] == len(rejected) >= 1
+
+
+def test_served_late_tails_equal_the_request_alone():
+    """With late_tail, each served RIR is its band IRs crossfaded into the FDN late tail; a request gives the
+    same hybrid band IRs in the mix (two batches in flight) as alone, and its tail equals the per-call
+    drop-in on its band IRs."""
+    from types import SimpleNamespace
+    from acoustic_agent_b200 import bands, late_reverb, runtime, serving, workloads
+    population = workloads.mixed_batch(23, 4, max_rays=20_000, min_rays=5_000)
+    stream = workloads.request_stream(9, rate_hz=200.0, duration_s=0.05, population=population, keyframes=2)
+    requests = serving.requests_from_stream(stream)[:6]
+    server = serving.Server(0, max_inflight=2, tune=False, late_tail=True)
+    report = server.serve(requests, realtime=True)
+    server.close()
+    assert all(r.error is None for r in report.results)
+    for res in (report.results[0], report.results[-1]):
+        alone = serving.render_alone(res.request, late_tail=True)
+        plain = serving.render_alone(res.request)
+        for a, b, p in zip(alone, res.band_irs, plain):
+            np.testing.assert_array_equal(a, b)
+            assert not np.array_equal(a, p)   # the tail changed the band IRs
+    # the first RIR's tail against the drop-in, with the RT60s estimated from its own trace
+    res = report.results[0]
+    spec = serving.request_jobs(res.request)[0]
+    w = res.request.workload
+    scene = runtime.DeviceScene(serving.SceneCache(0, tune=False).key_of(w)[1])
+    b = runtime.trace(scene, spec)
+    echogram = b.echogram.cpu().numpy()
+    scene.close()
+    rt60 = late_reverb.estimate_reverb_times(echogram, spec.bin_duration, spec.speed_of_sound)
+    cfg = SimpleNamespace(fs=w.config.fs, seed=int(spec.seed), late_tail=True, hybrid_transition_s=1.0,
+                          hybrid_overlap_fraction=0.25, rt_bin_duration_s=spec.bin_duration)
+    plain_first = serving.render_alone(res.request)[0]
+    out, _, _ = late_reverb.render_parametric_fdn_late_reverb(plain_first, {"bin_duration_s": spec.bin_duration},
+                                                              dict(zip(bands.FREQUENCY_BANDS, rt60)), cfg)
+    np.testing.assert_array_equal(out, res.band_irs[0])
