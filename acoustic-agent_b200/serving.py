@@ -240,12 +240,16 @@ class Server:
     def __init__(self, device: int = 0, *, max_inflight: int = 3, hbm_budget: int | None = None,
                  max_batch_rays: int = 400_000_000, tune: bool = True, block_size: int = 0,
                  chunk_rays: int = 0, policy: str = "small_first", starve_s: float = 1.0,
-                 late_tail: bool = False, transition_s: float = 1.0, overlap_fraction: float = 0.25) -> None:
+                 late_tail: bool = False, transition_s: float = 1.0, overlap_fraction: float = 0.25,
+                 trace_blocks_per_sm: int = 2) -> None:
         """`policy` orders the waiting requests when a batch is formed: "fifo" by arrival, or
         "small_first" by ray count, except that requests waiting longer than `starve_s` go first
         (in arrival order), so a stream of small requests cannot hold a large one back for ever.
         With `late_tail`, every served RIR is crossfaded into its FDN late tail as the reference's
-        renderer does with late_tail=True (late_reverb.batch_late_tails, one launch pair per batch)."""
+        renderer does with late_tail=True (late_reverb.batch_late_tails, one launch pair per batch).
+        `trace_blocks_per_sm` > 0 caps each batch's persistent trace grid at that many blocks per SM
+        (0: the library's choice, three).  Two leave room for other batches' synthesis recursion beside a
+        trace, whose one-warp blocks do not fit next to three trace blocks' registers."""
         if policy not in self.POLICIES:
             raise ValueError(f"policy must be one of {self.POLICIES}")
         self.policy = policy
@@ -266,6 +270,8 @@ class Server:
         self.transition_s = float(transition_s)
         self.overlap_fraction = float(overlap_fraction)
         self._late: dict[int, Any] = {}
+        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
+        self.trace_grid = max(0, int(trace_blocks_per_sm)) * sms
 
     # ---- footprint and admission
     def footprint(self, req: Request, specs: Sequence[runtime.TraceSpec]) -> int:
@@ -313,7 +319,7 @@ class Server:
             trace_ws = runtime.BatchWorkspace(self.dev)
             synth_ws = runtime.SynthBatchWorkspace(self.dev)
             runtime.trace_batch(jobs, trace_ws, block_size=self.block_size, chunk_rays=self.chunk_rays,
-                                stream=stream)
+                                grid_blocks=self.trace_grid, stream=stream)
             runtime.synthesize_batch(synth, synth_ws, stream=stream)
             host = torch.empty(ir_store.shape, dtype=torch.float32, pin_memory=True)
             echograms = None

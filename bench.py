@@ -369,6 +369,8 @@ def main() -> int:
     parser.add_argument("--max-inflight", type=int, default=3, help="serving: batches on the GPU at once")
     parser.add_argument("--late-tail", action="store_true",
                         help="serving: crossfade every served RIR into its FDN late tail")
+    parser.add_argument("--trace-blocks-per-sm", type=int, default=2,
+                        help="serving: cap each batch's trace grid (0: the library's choice)")
     args = parser.parse_args()
     if args.warmup < 3:
         parser.error("--warmup must be at least 3")
@@ -793,7 +795,8 @@ def run_serving(args) -> int:
     stream = workloads.request_stream(1729, rate_hz=args.rate, duration_s=args.duration, population=population)
     requests = serving.requests_from_stream(stream)
     server = serving.Server(local, max_inflight=args.max_inflight, policy=args.policy,
-                            max_batch_rays=args.max_batch_rays, late_tail=args.late_tail)
+                            max_batch_rays=args.max_batch_rays, late_tail=args.late_tail,
+                            trace_blocks_per_sm=args.trace_blocks_per_sm)
     t0 = time.perf_counter()
     for w in population:   # warm the resident scene cache (upload + tune) before the clock starts
         req = serving.Request(-1, w, [w.sources[0]])
@@ -814,6 +817,7 @@ def run_serving(args) -> int:
         "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s over 64 mixed scenes, "
                                "20% moving sources x 8 keyframes", "requests": len(requests), "policy": args.policy,
                    "max_batch_rays": args.max_batch_rays, "late_tail": args.late_tail,
+                   "trace_blocks_per_sm": args.trace_blocks_per_sm,
                    "moving": sum(r.moving for r in requests), "max_inflight": server.max_inflight},
         "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]},
         "ray_bounces_per_s": s["ray_bounces_per_s"], "rirs": s["rirs"], "makespan_s": s["makespan_s"],
