@@ -27,6 +27,10 @@ AC_PRECISION_FP32 = 0
 AC_PRECISION_FP64 = 1
 AC_RNG_REFERENCE = 0
 AC_RNG_PHILOX = 1
+AC_BVH_STATUS_NONFINITE = 1
+AC_BVH_STATUS_ORDER = 2
+AC_BVH_STATUS_TIMEOUT = 4
+AC_BVH_STATUS_INTERNAL = 8
 AC_SYNTH_STATIC_BYTES = 16 << 20
 
 c_double_p = ctypes.POINTER(ctypes.c_double)
@@ -185,6 +189,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_last_error": (ctypes.c_char_p, []),
     "ac_abi_version": (ctypes.c_int, []),
     "ac_bvh_build": (ctypes.c_int, [c_double_p, c_double_p, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ACBvh)]),
+    "ac_bvh_device_workspace_size": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t),
+                                                    ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int64)]),
+    "ac_bvh_build_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
+                                           ctypes.POINTER(ACBvh), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
     "ac_device_info": (ctypes.c_int, [ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t, c_int32_p, c_int32_p,
                                       c_int32_p]),
     "ac_scene_create": (ctypes.c_int, [ctypes.POINTER(ACSceneDesc), ctypes.POINTER(ctypes.c_void_p)]),
@@ -277,6 +286,15 @@ def check(code: int, what: str) -> None:
 
 def _ptr(array: np.ndarray, ctype):
     return array.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def device_bvh_plan(num_surfaces: int, leaf_size: int = 4) -> tuple[int, int, int]:
+    """(device workspace bytes, plan staging bytes, node count) of ac_bvh_build_device; host only."""
+    ws, staging, nodes = ctypes.c_size_t(), ctypes.c_size_t(), ctypes.c_int64()
+    check(load().ac_bvh_device_workspace_size(int(num_surfaces), int(leaf_size), ctypes.byref(ws),
+                                              ctypes.byref(staging), ctypes.byref(nodes)),
+          "ac_bvh_device_workspace_size")
+    return int(ws.value), int(staging.value), int(nodes.value)
 
 
 def build_bvh(bounds_min: np.ndarray, bounds_max: np.ndarray, leaf_size: int = 4) -> dict[str, Any]:

@@ -27,9 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
           f"-I{INCLUDE}", f"-I{CSRC}", "--expt-relaxed-constexpr"]
 # Units whose float64 arithmetic must not be contracted into FMAs.
-NO_FMA = {"trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu"}
+NO_FMA = {"trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu", "bvh_device.cu"}
 SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu",
-           "bvh_build.cpp", "fast_bvh.cpp"]
+           "bvh_device.cu", "bvh_build.cpp", "fast_bvh.cpp"]
 
 
 def nvcc() -> str:

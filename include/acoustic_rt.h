@@ -15,6 +15,7 @@
  *
  * Reference interfaces replaced (paths inside the Acoustic Agent project):
  *   ac_bvh_build        acoustic_agent/bvh.py:8-77                   build_bvh
+ *   ac_bvh_build_device the same, on the GPU (steam_rt.py:881 calls build_bvh)
  *   ac_scene_create     acoustic_agent/steam_rt.py:834-924           _scene_kernel_arrays
  *                       + acoustic_agent/steam_rt_cuda.py:76-115     device upload / cache
  *   ac_trace            acoustic_agent/steam_rt.py:1757-1804         trace_energy_field
@@ -241,6 +242,35 @@ int ac_abi_version(void);
 /* Host-only: build the preorder escape-link BVH of bvh.py:8-77. */
 int ac_bvh_build(const double *bounds_min, const double *bounds_max, int64_t num_surfaces, int32_t leaf_size,
                  ac_bvh *out);
+
+/* The same tree built on the GPU from device-resident bounds (bvh.py:8-77,
+ * build_bvh, for scenes of thousands to millions of surfaces).  The tree's
+ * shape depends only on num_surfaces and leaf_size (every split is at n/2),
+ * so the host plans it; the device chooses each node's axis and partitions its
+ * surfaces about the median of the reference's stable sort order.
+ *
+ * Host-only sizing: *workspace_bytes of device workspace (256-byte aligned),
+ * *staging_bytes of the plan copied to the device each call (pass a pinned
+ * buffer of that size as host_staging to keep the call asynchronous; with
+ * NULL the call synchronizes `stream` after the copy), *node_count nodes. */
+int ac_bvh_device_workspace_size(int64_t num_surfaces, int32_t leaf_size, size_t *workspace_bytes,
+                                 size_t *staging_bytes, int64_t *node_count);
+
+/* bounds_min/max: device [S,3] float64.  `out` holds device arrays with room
+ * for *node_count nodes and S primitive slots; node_count, leaf_count and
+ * max_depth are filled on return.  `status` is one device int32, zeroed by the
+ * call and, once the stream reaches the end of the build, OR of
+ * AC_BVH_STATUS_*; the arrays are only valid when it reads 0.  S >= 1,
+ * S < 2^30, 1 <= leaf_size <= 255. */
+enum {
+    AC_BVH_STATUS_NONFINITE = 1,   /* reference: "BVH bounds must be finite" */
+    AC_BVH_STATUS_ORDER = 2,       /* reference: "BVH maximum bounds must not be below minimum bounds" */
+    AC_BVH_STATUS_TIMEOUT = 4,     /* a grid barrier gave up waiting (the build is abandoned) */
+    AC_BVH_STATUS_INTERNAL = 8     /* a median search ended without its element (a defect) */
+};
+int ac_bvh_build_device(const double *bounds_min, const double *bounds_max, int64_t num_surfaces,
+                        int32_t leaf_size, ac_bvh *out, int32_t *status, void *workspace, size_t workspace_bytes,
+                        void *host_staging, void *stream);
 
 /* Device info for the reference's `cuda` result field. */
 int ac_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major, int32_t *cc_minor,

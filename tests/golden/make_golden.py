@@ -299,11 +299,34 @@ def rt60_golden(steam_rt, SimConfig) -> None:
     np.savez_compressed(HERE / "rt60.npz", **out)
 
 
+BVH_KEYS = ("bounds_min", "bounds_max", "start", "count", "escape", "primitives")
+
+
+def bvh_golden(reference_path: str) -> None:
+    """The reference's build_bvh (bvh.py:8-77) on the seeded inputs of bvh_cases.py."""
+    sys.path.insert(0, str(HERE))
+    import bvh_cases  # noqa: E402
+    import_reference(reference_path)
+    from acoustic_agent.bvh import build_bvh  # noqa: E402
+    out = {}
+    for name in bvh_cases.CASES:
+        lo, hi, leaf = bvh_cases.inputs(name)
+        tree = build_bvh(lo, hi, leaf_size=leaf)
+        for k in BVH_KEYS:
+            out[f"{name}_{k}"] = np.asarray(tree[k])
+        out[f"{name}_meta"] = np.asarray([tree["node_count"], tree["leaf_count"], tree["max_depth"], tree["leaf_size"]])
+    np.savez_compressed(HERE / "bvh.npz", **out)
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference")
-    parser.add_argument("--only", choices=("late_reverb", "direct", "rt60"), help="regenerate one fixture file only")
+    parser.add_argument("--only", choices=("late_reverb", "direct", "rt60", "bvh"),
+                        help="regenerate one fixture file only")
     args = parser.parse_args()
+    if args.only == "bvh":
+        bvh_golden(args.reference)
+        return 0
     steam_rt, models, directivity = import_reference(args.reference)
     if args.only is not None:
         from acoustic_agent.models import SimConfig  # noqa: E402
@@ -357,7 +380,8 @@ def main() -> int:
     late_reverb_golden(steam_rt, SimConfig)
     direct_golden(steam_rt, models, SimConfig)
     rt60_golden(steam_rt, SimConfig)
-    print("wrote", written, "synthesis", "workspace", "late_reverb", "direct", "rt60")
+    bvh_golden(args.reference)
+    print("wrote", written, "synthesis", "workspace", "late_reverb", "direct", "rt60", "bvh")
     return 0
 
 

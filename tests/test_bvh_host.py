@@ -1,0 +1,65 @@
+"""BVH fixture pins (CPU): the oracle and the host builder reproduce the reference's trees, and the
+device build's host plan gives the reference's node counts (acoustic_agent/bvh.py:8-77)."""
+from __future__ import annotations
+
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+sys.path.insert(0, str(GOLDEN))
+import bvh_cases  # noqa: E402
+
+KEYS = ("bounds_min", "bounds_max", "start", "count", "escape", "primitives")
+
+
+def golden(name: str) -> dict:
+    g = np.load(GOLDEN / "bvh.npz")
+    out = {k: g[f"{name}_{k}"] for k in KEYS}
+    out["node_count"], out["leaf_count"], out["max_depth"], out["leaf_size"] = (int(v) for v in g[f"{name}_meta"])
+    return out
+
+
+@pytest.mark.parametrize("name", list(bvh_cases.CASES))
+def test_oracle_and_host_builder_match_the_reference_tree(name):
+    from acoustic_agent_b200 import _lib
+    from oracle import oracle
+    lo, hi, leaf = bvh_cases.inputs(name)
+    ref = golden(name)
+    for tree in (oracle.build_bvh(lo, hi, leaf), _lib.build_bvh(lo, hi, leaf)):
+        for k in KEYS:
+            np.testing.assert_array_equal(np.asarray(tree[k]), ref[k], err_msg=f"{name} {k}")
+        assert (tree["node_count"], tree["leaf_count"], tree["max_depth"]) == (
+            ref["node_count"], ref["leaf_count"], ref["max_depth"])
+
+
+@pytest.mark.parametrize("name", list(bvh_cases.CASES))
+def test_device_plan_node_count_matches_the_reference(name):
+    from acoustic_agent_b200 import _lib
+    n, leaf = bvh_cases.CASES[name]
+    _, _, nodes = _lib.device_bvh_plan(n, leaf)
+    assert nodes == golden(name)["node_count"]
+
+
+def test_device_plan_sizes_over_a_sweep():
+    """Node counts of the plan equal the host builder's for sizes around the shared-memory subtree limit."""
+    from acoustic_agent_b200 import _lib
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 3, 7, 8, 9, 1023, 2047, 2048, 2049, 4095, 4096, 4097, 8193, 20000):
+        for leaf in (1, 3, 4, 8, 255):
+            ws, staging, nodes = _lib.device_bvh_plan(n, leaf)
+            lo = rng.random((n, 3))
+            assert nodes == _lib.build_bvh(lo, lo + 1.0, leaf)["node_count"], (n, leaf)
+            assert ws % 256 == 0 and ws >= 32 * n and staging > 0
+
+
+def test_device_plan_rejects_bad_sizes():
+    from acoustic_agent_b200 import _lib
+    with pytest.raises(ValueError, match="at least one surface"):
+        _lib.device_bvh_plan(0, 4)
+    with pytest.raises(ValueError, match="leaf size"):
+        _lib.device_bvh_plan(10, 0)
+    with pytest.raises(_lib.BackendError):
+        _lib.device_bvh_plan(1 << 30, 4)
