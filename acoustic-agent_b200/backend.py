@@ -198,7 +198,8 @@ class Installation:
             setattr(self.module, name, fn)
 
 
-def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Installation:
+def install(steam_rt_module: Any = None, *, route_cuda: bool = False,
+            gpu_bvh_min_surfaces: int | None = None) -> Installation:
     """Route Acoustic Agent's reflection trace to this backend.
 
     After ``install()``, ``rt_accelerator="b200"`` selects the GPU tracer here; with
@@ -207,6 +208,11 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
     setting routes the FDN late tail (``_render_parametric_fdn_late_reverb``,
     steam_rt.py:2500, called by the renderer at :1029) to ``late_reverb`` and the
     direct path (``simulate_direct``, :1315, called at :942) to ``direct``.
+
+    ``gpu_bvh_min_surfaces=N`` also routes the scene BVH build (``build_bvh``,
+    called by ``_scene_kernel_arrays`` at steam_rt.py:881 with no accelerator
+    setting in reach) to the GPU build in ``bvh`` for scenes of N surfaces or
+    more; the tree is the reference's, array for array.
     """
     if steam_rt_module is None:
         import acoustic_agent.steam_rt as steam_rt_module  # type: ignore[import-not-found]
@@ -253,4 +259,16 @@ def install(steam_rt_module: Any = None, *, route_cuda: bool = False) -> Install
 
         steam_rt_module.simulate_direct = routed_direct
         originals["simulate_direct"] = original_direct
+    original_bvh = getattr(steam_rt_module, "build_bvh", None)
+    if gpu_bvh_min_surfaces is not None and original_bvh is not None:
+        threshold = max(1, int(gpu_bvh_min_surfaces))
+
+        def routed_bvh(bounds_min, bounds_max, *, leaf_size: int = 4):
+            if len(bounds_min) >= threshold:
+                from acoustic_agent_b200 import bvh
+                return bvh.build_bvh(bounds_min, bounds_max, leaf_size=leaf_size)
+            return original_bvh(bounds_min, bounds_max, leaf_size=leaf_size)
+
+        steam_rt_module.build_bvh = routed_bvh
+        originals["build_bvh"] = original_bvh
     return Installation(steam_rt_module, originals)

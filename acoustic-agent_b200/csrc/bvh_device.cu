@@ -74,7 +74,7 @@ struct SegState {
     unsigned long long pw[4];                                    // digits of the median's key found so far
     long long kk;                                                // its rank among keys with that prefix
     int32_t chain, resolved, rw, rs;                             // axis order; last word and shift resolved
-    int32_t left_fill, right_fill, pad0, pad1;
+    int32_t left_fill, right_fill, first_pass, pad1;   // first_pass: digits shared by the node's min and max key
 };
 
 struct TopArgs {
@@ -290,10 +290,16 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
             }
             const uint32_t parent_chain =
                 seg.parent >= 0 ? static_cast<uint32_t>(__ldcg(&A.state[seg.parent].chain)) : kNoChain;
-            st->chain = static_cast<int32_t>(push_axis(parent_chain, widest_axis(cmax, cmin_c)));
+            const int axis = widest_axis(cmax, cmin_c);
+            st->chain = static_cast<int32_t>(push_axis(parent_chain, axis));
             st->kk = seg.count / 2;
             st->resolved = 0;
-            for (int j = 0; j < 4; ++j) st->pw[j] = 0ull;
+            for (int j = 1; j < 4; ++j) st->pw[j] = 0ull;
+            // every key of the node lies in [min, max]: the bytes they share are the median's too
+            const unsigned long long kmin = ~cmin_c[axis], diff = kmin ^ cmax[axis];
+            const int shared = diff == 0ull ? 8 : __clzll(static_cast<long long>(diff)) / 8;
+            st->pw[0] = shared == 0 ? 0ull : shared == 8 ? kmin : (kmin & (~0ull << (64 - 8 * shared)));
+            st->first_pass = shared;
             const int64_t node = seg.node;
             for (int a = 0; a < 3; ++a) {
                 A.out_min[3 * node + a] = key_value(~__ldcg(&st->lmin_c[a]));
@@ -313,23 +319,37 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
                 if (__ldcg(&st->resolved)) continue;   // block-uniform
                 const uint32_t chain = static_cast<uint32_t>(__ldcg(&st->chain));
                 const int nwc = chain_words(chain);
-                const PassDigit d = pass_digit(nwc, p);
+                const PassDigit d = pass_digit(nwc, p + __ldcg(&st->first_pass));
                 if (d.sh < 0) continue;   // past the key's last digit: the select step flags it
                 unsigned long long pw[4];
                 for (int j = 0; j < 4; ++j) pw[j] = __ldcg(&st->pw[j]);
                 const unsigned long long hm = d.sh >= 56 ? 0ull : (~0ull << (d.sh + 8));
+                const int before = d.w == 3 ? nwc : d.w;
                 hist_s[tid] = 0u;
                 __syncthreads();
-                for (int q = ch.begin + tid; q < ch.end; q += kTopThreads) {
-                    const int32_t i = __ldcg(src + q);
-                    if (bad_index(i, A.S, A.status)) continue;
-                    bool match = true;
-                    const int before = d.w == 3 ? nwc : d.w;
-                    for (int j = 0; j < before && match; ++j) match = key_word(A.ckey, A.S, chain, j, i) == pw[j];
-                    if (!match) continue;
-                    const unsigned long long W = key_word(A.ckey, A.S, chain, d.w, i);
-                    if ((W & hm) != (pw[d.w] & hm)) continue;
-                    atomicAdd(&hist_s[(W >> d.sh) & 255u], 1u);
+                for (int q0 = ch.begin + tid; q0 < ch.end; q0 += 4 * kTopThreads) {
+                    int32_t ii[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {   // four independent index loads in flight
+                        const int q = q0 + u * kTopThreads;
+                        ii[u] = q < ch.end ? __ldcg(src + q) : -1;
+                        if (ii[u] >= 0 && bad_index(ii[u], A.S, A.status)) ii[u] = -1;
+                    }
+                    unsigned long long W[4];
+                    bool match[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        match[u] = ii[u] >= 0;
+                        W[u] = match[u] ? key_word(A.ckey, A.S, chain, d.w, ii[u]) : 0ull;
+                    }
+                    for (int j = 0; j < before; ++j) {
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (match[u]) match[u] = key_word(A.ckey, A.S, chain, j, ii[u]) == pw[j];
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (match[u] && (W[u] & hm) == (pw[d.w] & hm)) atomicAdd(&hist_s[(W[u] >> d.sh) & 255u], 1u);
                 }
                 __syncthreads();
                 const unsigned h = hist_s[tid];
@@ -356,7 +376,8 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
                 incl += base;
                 const unsigned excl = incl - h;
                 const long long kk = __ldcg(&st->kk);
-                const PassDigit d = pass_digit(chain_words(static_cast<uint32_t>(__ldcg(&st->chain))), p);
+                const PassDigit d = pass_digit(chain_words(static_cast<uint32_t>(__ldcg(&st->chain))),
+                                               p + __ldcg(&st->first_pass));
                 if (d.sh >= 0 && h > 0 && static_cast<long long>(excl) <= kk && kk < static_cast<long long>(incl)) {
                     st->pw[d.w] = __ldcg(&st->pw[d.w]) | (static_cast<unsigned long long>(tid) << d.sh);
                     const long long left = kk - static_cast<long long>(excl);
@@ -595,10 +616,16 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
             }
             __syncthreads();
         }
-        // 2. bitonic sort of all positions by (segment, key in the segment's axis order, surface index)
+        // 2. bitonic sort of all positions by (segment, key in the segment's axis order, surface index).
+        // Warp w owns pairs [w*ppw, (w+1)*ppw), i.e. positions [2*w*ppw, 2*(w+1)*ppw) while the stride j is at
+        // most ppw: such stages need only the warp's own barrier.
+        const int pairs = p2 >> 1;
+        const int ppw = max(1, pairs / kWarps);
         for (int k = 2; k <= p2; k <<= 1) {
             for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = tid; i < p2 / 2; i += kSmallThreads) {
+                for (int r = lane; r < ppw; r += 32) {
+                    const int i = warp * ppw + r;
+                    if (i >= pairs) break;
                     const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
                     const int hi = lo | j;
                     const int a = m.lp[lo], b = m.lp[hi];
@@ -608,7 +635,10 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
                         m.lp[hi] = static_cast<uint16_t>(a);
                     }
                 }
-                __syncthreads();
+                const int next_j = j > 1 ? j >> 1 : k;
+                const bool last = k == p2 && j == 1;
+                if (!last && j <= ppw && next_j <= ppw) __syncwarp();
+                else __syncthreads();
             }
         }
         // 3. the right halves of the split segments become segments of their own

@@ -349,7 +349,7 @@ def main() -> int:
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--workload", default="u_room_20_boxes",
                         choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving", "late_reverb",
-                                 "direct"))
+                                 "direct", "bvh_build"))
     parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
     parser.add_argument("--no-pipeline", action="store_true",
                         help="run each step's synthesis after its own trace instead of beside the next trace")
@@ -409,6 +409,24 @@ def main() -> int:
                     "e2e": {"value": ref["value"], "unit": "paths/s", "h2d_bytes_per_step": 0,
                             "d2h_bytes_per_step": 0}}), flush=True)
         return 0
+    if args.impl == "reference" and args.workload == "bvh_build":
+        world, rank, _ = _dist_setup()
+        if rank == 0:
+            ref = reference_bvh(max(3, args.steps))
+            if "unavailable" in ref:
+                print(json.dumps({"impl": "reference", "unavailable": ref["unavailable"]}), flush=True)
+            else:
+                print(json.dumps({
+                    "impl": "reference", "metric": "BVH surfaces/s", "value": ref["value"], "unit": "surfaces/s",
+                    "n_gpus": world, "steps": max(3, args.steps), "warmup": args.warmup,
+                    "ms_per_step": ref["seconds"] * 1000.0, "higher_is_better": True, "scaling": "weak",
+                    "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded warehouse AABBs)",
+                    "config": {"workload": f"bvh_build: {BVH_SAMPLE} of the {BVH_SURFACES} warehouse surfaces"},
+                    "cpu_baseline": {"value": ref["value"], "unit": "surfaces/s", "cores": 1, "kind": "reference",
+                                     "sample": ref["sample"]},
+                    "e2e": {"value": ref["value"], "unit": "surfaces/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
     if args.impl == "reference":
         if args.workload in ("mixed_batch", "serving"):
             parser.error("--impl reference times the reference's per-RIR path on a single-scene workload")
@@ -422,6 +440,8 @@ def main() -> int:
         return run_late_reverb(args)
     if args.workload == "direct":
         return run_direct(args)
+    if args.workload == "bvh_build":
+        return run_bvh_build(args)
 
     import torch
     from acoustic_agent_b200 import batching, runtime, scene as scene_mod
@@ -1121,6 +1141,134 @@ def run_direct(args) -> int:
     }
     print(json.dumps(line), flush=True)
     device_scene.close()
+    return 0
+
+
+BVH_SURFACES = 1 << 20
+BVH_SAMPLE = 1 << 16
+
+
+def bvh_build_inputs(n: int, seed: int = 2024) -> tuple[np.ndarray, np.ndarray]:
+    """Padded surface AABBs of a seeded 400 x 400 m warehouse floor (steam_rt.py:234-262 pads by 2e-6).
+
+    Seven in eight surfaces are rotated boxes (side 0.3-2 m, height up to 3 m, the
+    reference's cabinet proxies); the rest are wall pieces on a 2 m grid, whose
+    shared grid coordinates give the sorts many exact ties.
+    """
+    rng = np.random.default_rng(seed)
+    boxes = n - n // 8
+    centre = rng.uniform(0.0, 400.0, (boxes, 2))
+    half = rng.uniform(0.15, 1.0, (boxes, 2))
+    angle = rng.uniform(0.0, np.pi / 2, boxes)
+    c, s = np.abs(np.cos(angle)), np.abs(np.sin(angle))
+    ext = np.stack([half[:, 0] * c + half[:, 1] * s, half[:, 0] * s + half[:, 1] * c], axis=1)
+    z1 = rng.uniform(0.4, 3.0, boxes)
+    lo_b = np.column_stack([centre - ext, np.zeros(boxes)])
+    hi_b = np.column_stack([centre + ext, z1])
+    walls = n - boxes
+    a = rng.integers(0, 200, (walls, 2)).astype(np.float64) * 2.0
+    horizontal = rng.random(walls) < 0.5
+    b = a + np.where(horizontal[:, None], [2.0, 0.0], [0.0, 2.0])
+    lo_w = np.column_stack([np.minimum(a, b), np.zeros(walls)])
+    hi_w = np.column_stack([np.maximum(a, b), np.full(walls, 3.0)])
+    lo = np.concatenate([lo_b, lo_w]) - 2e-6
+    hi = np.concatenate([hi_b, hi_w]) + 2e-6
+    order = rng.permutation(n)
+    return np.ascontiguousarray(lo[order]), np.ascontiguousarray(hi[order])
+
+
+def reference_bvh(steps: int) -> dict:
+    """The reference's build_bvh (bvh.py:8-77, baseline/_ref) on the first BVH_SAMPLE surfaces, one host thread."""
+    ref, why = import_reference_package()
+    if ref is None:
+        return {"unavailable": why}
+    from acoustic_agent.bvh import build_bvh  # the reference package put on sys.path above
+    lo, hi = bvh_build_inputs(BVH_SURFACES)
+    lo, hi = lo[:BVH_SAMPLE], hi[:BVH_SAMPLE]
+    build_bvh(lo[:4096], hi[:4096])
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        build_bvh(lo, hi)
+        times.append(time.perf_counter() - t0)
+    per = float(np.median(times))
+    return {"value": BVH_SAMPLE / per, "seconds": per, "cores": 1, "kind": "reference",
+            "sample": f"the first {BVH_SAMPLE} of the {BVH_SURFACES} warehouse surfaces, acoustic_agent.bvh.build_bvh "
+                      f"(baseline/_ref), one host thread, median of {steps}"}
+
+
+def run_bvh_build(args) -> int:
+    """The reference's BVH over 2^20 warehouse surfaces, built on the GPU (ac_bvh_build_device).
+
+    value: surfaces/s of one build from resident device bounds to the device
+    tree (keys kernel, cooperative large-node kernel, subtree kernel), device
+    time, L2 flushed between steps.  e2e: the drop-in bvh.build_bvh from numpy
+    bounds to the numpy dict (bounds up, tree down).  The oracle (the numpy
+    restatement of the same recursion) and the host C++ builder run beside it.
+    """
+    import torch
+    from acoustic_agent_b200 import _lib, bvh
+    from oracle import oracle
+    world, rank, local = _dist_setup()
+    if world > 1:
+        raise SystemExit("the bvh_build workload runs on one GPU")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    lo, hi = bvh_build_inputs(BVH_SURFACES)
+    b = bvh.builder(local)
+    dlo, dhi = torch.from_numpy(lo).to(device), torch.from_numpy(hi).to(device)
+    tree = b.build(dlo, dhi)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    for _ in range(args.warmup):
+        b.build(dlo, dhi, check=False)
+    sampler = ClockSampler(local)
+    with sampler:
+        times = _device_timed(lambda: b.build(dlo, dhi, check=False), args.steps, device, flush)
+    if int(b.status.item()) != 0:
+        raise SystemExit(f"device BVH build failed (status {int(b.status.item())})")
+    step_ms = float(np.median(times))
+    e2e = []
+    for _ in range(max(3, args.steps)):
+        t0 = time.perf_counter()
+        bvh.build_bvh(lo, hi)
+        e2e.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e))
+    t0 = time.perf_counter()
+    host = _lib.build_bvh(lo, hi, 4)
+    host_s = time.perf_counter() - t0
+    assert host["node_count"] == tree.node_count
+    nodes = tree.node_count
+    # algorithmic bytes of one build: bounds in (48 B/surface), tree out (72 B/node + 8 B/surface)
+    algo_bytes = 48 * BVH_SURFACES + 72 * nodes + 8 * BVH_SURFACES
+    peaks = _peaks()
+    achieved = algo_bytes / (step_ms * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        oracle.build_bvh(lo[:BVH_SAMPLE], hi[:BVH_SAMPLE])
+        port_s = time.perf_counter() - t0
+        cpu = {"value": BVH_SAMPLE / port_s, "unit": "surfaces/s", "cores": 1, "kind": "port",
+               "sample": f"the first {BVH_SAMPLE} surfaces, oracle.build_bvh (numpy restatement), one host thread, "
+                         f"one run"}
+    line = {
+        "metric": "BVH surfaces/s", "value": BVH_SURFACES / (step_ms * 1e-3), "unit": "surfaces/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded warehouse AABBs)",
+        "config": {"workload": f"bvh_build: the reference's BVH (leaf 4) over {BVH_SURFACES} warehouse surfaces, "
+                               f"{nodes} nodes, depth {tree.max_depth}",
+                   "l2": "flushed between timed steps (256 MiB write)"},
+        "e2e": {"value": BVH_SURFACES / e2e_s, "unit": "surfaces/s", "h2d_bytes_per_step": 48 * BVH_SURFACES,
+                "d2h_bytes_per_step": 72 * nodes + 8 * BVH_SURFACES,
+                "note": "bvh.build_bvh from numpy bounds to the numpy dict"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                     "kernel": "the whole build (3 launches)", "algorithmic_bytes": algo_bytes},
+        "cpu_baseline": cpu,
+        "host_builder": {"seconds": host_s, "value": BVH_SURFACES / host_s, "unit": "surfaces/s",
+                         "note": "ac_bvh_build, the C++ restatement, one host thread, full size"},
+        "gpu_launches": 3 * args.steps, "clocks": sampler.summary(),
+    }
+    print(json.dumps(line), flush=True)
     return 0
 
 

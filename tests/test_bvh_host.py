@@ -63,3 +63,29 @@ def test_device_plan_rejects_bad_sizes():
         _lib.device_bvh_plan(10, 0)
     with pytest.raises(_lib.BackendError):
         _lib.device_bvh_plan(1 << 30, 4)
+
+
+def test_install_routes_build_bvh_only_when_asked_and_above_the_threshold(monkeypatch):
+    """install(gpu_bvh_min_surfaces=N) swaps steam_rt.build_bvh (called at steam_rt.py:881); smaller scenes keep
+    the reference's function, uninstall restores it."""
+    import types
+    from acoustic_agent_b200 import backend, bvh
+    calls = []
+
+    def reference_build(lo, hi, *, leaf_size=4):
+        calls.append(("reference", len(lo), leaf_size))
+        return "reference"
+
+    fake = types.SimpleNamespace(trace_energy_field=lambda *a, **k: None,
+                                 _normalize_rt_accelerator=lambda v: str(v), build_bvh=reference_build)
+    handle = backend.install(fake)
+    assert fake.build_bvh is reference_build          # not asked: untouched
+    handle.uninstall()
+    monkeypatch.setattr(bvh, "build_bvh", lambda lo, hi, *, leaf_size=4: calls.append(("gpu", len(lo), leaf_size)) or "gpu")
+    handle = backend.install(fake, gpu_bvh_min_surfaces=100)
+    lo = np.zeros((99, 3))
+    assert fake.build_bvh(lo, lo) == "reference"
+    assert fake.build_bvh(np.zeros((100, 3)), np.zeros((100, 3)), leaf_size=2) == "gpu"
+    assert calls == [("reference", 99, 4), ("gpu", 100, 2)]
+    handle.uninstall()
+    assert fake.build_bvh is reference_build

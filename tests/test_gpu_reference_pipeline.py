@@ -112,3 +112,24 @@ def test_direct_path_routes_to_the_gpu(reference):
     finally:
         handle.uninstall()
     np.testing.assert_array_equal(gpu.rir, cpu.rir)
+
+
+def test_scene_bvh_build_routes_to_the_gpu(reference):
+    """install(gpu_bvh_min_surfaces=1) routes the reference's build_bvh (called by _scene_kernel_arrays at
+    steam_rt.py:881) to the GPU build; the scene's BVH arrays equal the reference's own, array for array."""
+    bench, (steam_rt, models) = reference
+    from acoustic_agent_b200 import backend, workloads
+    w = workloads.u_furnished(1729)
+    scene = bench.reference_scene(steam_rt, models, w.spec)
+    steam_rt._SCENE_ARRAY_CACHE.clear()
+    ref = steam_rt._scene_kernel_arrays(scene)
+    handle = backend.install(steam_rt, gpu_bvh_min_surfaces=1)
+    try:
+        steam_rt._SCENE_ARRAY_CACHE.clear()
+        gpu = steam_rt._scene_kernel_arrays(scene)
+    finally:
+        handle.uninstall()
+        steam_rt._SCENE_ARRAY_CACHE.clear()
+    for k in ("bvh_bounds_min", "bvh_bounds_max", "bvh_start", "bvh_count", "bvh_escape", "bvh_primitives",
+              "bvh_node_count", "bvh_leaf_count", "bvh_max_depth", "bvh_leaf_size"):
+        np.testing.assert_array_equal(np.asarray(gpu[k]), np.asarray(ref[k]), err_msg=k)
