@@ -19,13 +19,16 @@
 //    keys", and the order inside a child never matters (leaves sort by index).
 //
 // Large nodes (more than kSmallMax surfaces) are split level by level by one
-// cooperative kernel: per level a reduction gives each node's bounds and
-// centroid extents, a radix select over the 8-bit digits of the composite key
+// cooperative kernel: per level a reduction gives each node's centroid
+// extents, a radix select over the 8-bit digits of the composite key
 // finds the node's median (k = n/2) and surfaces are scattered to the two
 // halves.  Steps are separated by a grid barrier whose waits are bounded.
 // Each remaining subtree of at most kSmallMax surfaces is built by one CTA in
 // shared memory: per level, a bitonic sort of all its surfaces by (segment,
-// composite key) and a split of every internal segment at its half.
+// composite key) and a split of every internal segment at its half.  Surface
+// bounds are read once, at the leaves; every inner node's bounds are the union
+// of its children's, filled deepest level first (min and max do not depend on
+// the order they are taken in).
 //
 // Centroid keys map -0.0 to +0.0 (numpy compares them equal); bounds keep the
 // sign of zero and take the smaller/larger of -0.0 and +0.0 as -0.0/+0.0.
@@ -44,7 +47,7 @@
 namespace acbvh {
 
 constexpr int kSmallMax = 2048;        // surfaces per shared-memory subtree (a power of two)
-constexpr int kChunk = 4096;           // surfaces per block work item in the large-node levels
+constexpr int kChunk = 1024;           // surfaces per block work item in the large-node levels
 constexpr int kTopThreads = 256;
 constexpr int kSmallThreads = 512;
 constexpr int kMaxPasses = 28;         // 3 centroid words x 8 digits + 4 index digits
@@ -70,7 +73,7 @@ struct LevelTab {   // the (at most two) node counts found at one depth and thei
     int64_t c0, n0, c1, n1;
 };
 struct SegState {
-    unsigned long long cmax[3], cmin_c[3], umax[3], lmin_c[3];   // min kept as max of the complement
+    unsigned long long cmax[3], cmin_c[3];                       // centroid keys; min kept as max of the complement
     unsigned long long pw[4];                                    // digits of the median's key found so far
     long long kk;                                                // its rank among keys with that prefix
     int32_t chain, resolved, rw, rs;                             // axis order; last word and shift resolved
@@ -78,7 +81,6 @@ struct SegState {
 };
 
 struct TopArgs {
-    const double *lo, *hi;
     const unsigned long long *ckey;   // [3][S] centroid sort keys
     int32_t *perm0, *perm1;
     int64_t S;
@@ -91,7 +93,6 @@ struct TopArgs {
     unsigned *hist;                   // [big segments][256]
     unsigned *bar;                    // grid barrier: count, generation
     int32_t *unresolved;              // [levels][kMaxPasses]
-    double *out_min, *out_max;
     int64_t *out_start, *out_count, *out_escape;
     int32_t *status;
 };
@@ -230,7 +231,7 @@ __device__ __forceinline__ unsigned long long key_word(const unsigned long long 
 
 __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
     __shared__ unsigned hist_s[256];
-    __shared__ unsigned long long red[kTopThreads / 32][12];
+    __shared__ unsigned long long red[kTopThreads / 32][6];
     __shared__ unsigned scan_s[kTopThreads / 32];
     __shared__ int ok_flag, found_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -241,12 +242,12 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
         const int32_t *src = (lvl & 1) ? A.perm1 : A.perm0;
         int32_t *dst = (lvl & 1) ? A.perm0 : A.perm1;
 
-        // 1. bounds and centroid extents of every node of the level
+        // 1. centroid extents of every node of the level (bounds come bottom-up at the end)
         for (int c = lv.chunk_begin + blockIdx.x; c < lv.chunk_end; c += gridDim.x) {
             const Chunk ch = A.chunks[c];
-            unsigned long long acc[12];
+            unsigned long long acc[6];
 #pragma unroll
-            for (int j = 0; j < 12; ++j) acc[j] = 0ull;
+            for (int j = 0; j < 6; ++j) acc[j] = 0ull;
             for (int q = ch.begin + tid; q < ch.end; q += kTopThreads) {
                 const int32_t i = __ldcg(src + q);
                 if (bad_index(i, A.S, A.status)) continue;
@@ -255,24 +256,20 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
                     const unsigned long long k = A.ckey[a * A.S + i];
                     acc[a] = max(acc[a], k);
                     acc[3 + a] = max(acc[3 + a], ~k);
-                    acc[6 + a] = max(acc[6 + a], order_key(A.hi[3 * static_cast<int64_t>(i) + a]));
-                    acc[9 + a] = max(acc[9 + a], ~order_key(A.lo[3 * static_cast<int64_t>(i) + a]));
                 }
             }
 #pragma unroll
-            for (int j = 0; j < 12; ++j) {
+            for (int j = 0; j < 6; ++j) {
                 unsigned long long v = acc[j];
                 for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
                 if (lane == 0) red[warp][j] = v;
             }
             __syncthreads();
-            if (tid < 12) {
+            if (tid < 6) {
                 unsigned long long v = red[0][tid];
                 for (int w = 1; w < kTopThreads / 32; ++w) v = max(v, red[w][tid]);
                 SegState *st = A.state + ch.seg;
-                unsigned long long *field = tid < 3 ? &st->cmax[tid] : tid < 6 ? &st->cmin_c[tid - 3]
-                                          : tid < 9 ? &st->umax[tid - 6] : &st->lmin_c[tid - 9];
-                atomicMax(field, v);
+                atomicMax(tid < 3 ? &st->cmax[tid] : &st->cmin_c[tid - 3], v);
             }
             __syncthreads();
         }
@@ -301,10 +298,6 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
             st->pw[0] = shared == 0 ? 0ull : shared == 8 ? kmin : (kmin & (~0ull << (64 - 8 * shared)));
             st->first_pass = shared;
             const int64_t node = seg.node;
-            for (int a = 0; a < 3; ++a) {
-                A.out_min[3 * node + a] = key_value(~__ldcg(&st->lmin_c[a]));
-                A.out_max[3 * node + a] = key_value(__ldcg(&st->umax[a]));
-            }
             A.out_start[node] = -1;
             A.out_count[node] = 0;
             A.out_escape[node] = node + subtree_nodes(A.tab, seg.depth, seg.count);
@@ -460,6 +453,8 @@ struct Entry {
     uint32_t chain;
 };
 
+constexpr int kMaxSubtreeLevels = 32;
+
 struct SmallSmem {
     unsigned long long key[3][kSmallMax];
     int32_t gidx[kSmallMax];
@@ -468,9 +463,10 @@ struct SmallSmem {
     uint16_t cnt_at[kSmallMax];    // segment start -> count
     uint8_t chain_at[kSmallMax];   // segment start -> axis order
     uint8_t split_at[kSmallMax];   // segment start -> depth at which it was split
-    Entry cur[kSmallMax / 2], nxt[kSmallMax / 2];
-    unsigned long long part[kSmallThreads / 32][12];
-    int ncur, nnext;
+    Entry inner[kSmallMax];        // every internal node of the subtree, level after level (at most n - 1)
+    unsigned long long part[kSmallThreads / 32][6];
+    int level_begin[kMaxSubtreeLevels + 2];
+    int nnext;
 };
 
 __device__ __forceinline__ bool slot_less(const SmallSmem &m, int a, int b) {
@@ -516,10 +512,35 @@ __device__ void emit_leaf(SmallSmem &m, const SmallArgs &A, const SmallRoot &r, 
     A.out_escape[node] = node + 1;
 }
 
-// Internal segments of a level number at most n / 2 (each holds two or more surfaces).
+// An inner node's bounds: the union of its two children's (the min and max over its surfaces, in any order).
+__device__ __forceinline__ void union_children(double *out_min, double *out_max, int64_t node, int64_t left,
+                                               int64_t right) {
+    for (int a = 0; a < 3; ++a) {
+        const unsigned long long lmin = min(order_key(out_min[3 * left + a]), order_key(out_min[3 * right + a]));
+        const unsigned long long umax = max(order_key(out_max[3 * left + a]), order_key(out_max[3 * right + a]));
+        out_min[3 * node + a] = key_value(lmin);
+        out_max[3 * node + a] = key_value(umax);
+    }
+}
+
+// Axis and key order of an internal node from its centroid key extents, and its record (bounds come later).
+__device__ __forceinline__ void finish_inner(SmallSmem &m, const SmallArgs &A, Entry &en, int depth,
+                                             const unsigned long long cmax[3], const unsigned long long cmin_c[3]) {
+    const uint32_t chain = push_axis(en.chain, widest_axis(cmax, cmin_c));
+    en.chain = chain;
+    m.chain_at[en.start] = static_cast<uint8_t>(chain);
+    m.cnt_at[en.start] = en.count;
+    m.split_at[en.start] = static_cast<uint8_t>(depth);
+    const int64_t node = en.node;
+    A.out_start[node] = -1;
+    A.out_count[node] = 0;
+    A.out_escape[node] = node + subtree_nodes(A.tab, depth, en.count);
+}
+
+// Internal nodes of a level number at most n / 2 (each holds two or more surfaces); all of them at most n - 1.
 __device__ __forceinline__ void push_entry(SmallSmem &m, int32_t *status, const Entry &e) {
     const int at = atomicAdd(&m.nnext, 1);
-    if (at < kSmallMax / 2) m.nxt[at] = e;
+    if (at < kSmallMax) m.inner[at] = e;
     else atomicOr(status, AC_BVH_STATUS_INTERNAL);
 }
 
@@ -553,69 +574,65 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
     __syncthreads();
     if (tid == 0) {
         const uint32_t parent_chain = r.parent >= 0 ? static_cast<uint32_t>(A.state[r.parent].chain) : kNoChain;
-        m.cur[0] = Entry{0, static_cast<uint16_t>(n), r.node, parent_chain};
-        m.ncur = n > A.leaf ? 1 : 0;
-        m.nnext = 0;
+        m.inner[0] = Entry{0, static_cast<uint16_t>(n), r.node, parent_chain};
+        m.level_begin[0] = 0;
+        m.level_begin[1] = n > A.leaf ? 1 : 0;
         if (n <= A.leaf) emit_leaf(m, A, r, 0, n, r.node);
     }
     __syncthreads();
-    int depth = r.depth;
-    while (m.ncur > 0) {
-        const int ncur = m.ncur;
-        // 1. bounds and extents of every internal segment: g warps per segment
-        const int g = max(1, kWarps / ncur);
-        const int per_round = kWarps / g;
-        for (int round = 0; round < ncur; round += per_round) {
-            const int e = round + warp / g;
-            unsigned long long acc[12];
-#pragma unroll
-            for (int j = 0; j < 12; ++j) acc[j] = 0ull;
-            if (warp / g < per_round && e < ncur) {
-                const Entry en = m.cur[e];
+    int lev = 0;
+    for (; lev < kMaxSubtreeLevels; ++lev) {
+        const int b = m.level_begin[lev], e = m.level_begin[lev + 1], ncur = e - b;
+        if (ncur <= 0) break;
+        const int depth = r.depth + lev;
+        // 1. centroid extents of every internal node: a thread per node, or warps per node while they are few
+        if (ncur >= kWarps) {
+            for (int x = b + tid; x < e; x += kSmallThreads) {
+                Entry &en = m.inner[x];
+                unsigned long long cmax[3] = {0ull, 0ull, 0ull}, cmin_c[3] = {0ull, 0ull, 0ull};
+                for (int q = en.start; q < en.start + en.count; ++q) {
+                    const int slot = m.lp[q];
+                    for (int a = 0; a < 3; ++a) {
+                        const unsigned long long k = m.key[a][slot];
+                        cmax[a] = max(cmax[a], k);
+                        cmin_c[a] = max(cmin_c[a], ~k);
+                    }
+                }
+                finish_inner(m, A, en, depth, cmax, cmin_c);
+            }
+        } else {
+            const int g = kWarps / ncur;
+            unsigned long long acc[6] = {0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+            if (warp / g < ncur) {
+                const Entry en = m.inner[b + warp / g];
                 for (int q = en.start + (warp % g) * 32 + lane; q < en.start + en.count; q += g * 32) {
                     const int slot = m.lp[q];
-                    const int64_t gi = m.gidx[slot];
 #pragma unroll
                     for (int a = 0; a < 3; ++a) {
                         const unsigned long long k = m.key[a][slot];
                         acc[a] = max(acc[a], k);
                         acc[3 + a] = max(acc[3 + a], ~k);
-                        acc[6 + a] = max(acc[6 + a], order_key(A.hi[3 * gi + a]));
-                        acc[9 + a] = max(acc[9 + a], ~order_key(A.lo[3 * gi + a]));
                     }
                 }
             }
 #pragma unroll
-            for (int j = 0; j < 12; ++j) {
+            for (int j = 0; j < 6; ++j) {
                 unsigned long long v = acc[j];
                 for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
                 if (lane == 0) m.part[warp][j] = v;
             }
             __syncthreads();
-            if (tid < per_round && round + tid < ncur) {
-                const int ee = round + tid;
-                unsigned long long v[12];
-                for (int j = 0; j < 12; ++j) {
+            if (tid < ncur) {
+                unsigned long long v[6];
+                for (int j = 0; j < 6; ++j) {
                     v[j] = m.part[tid * g][j];
                     for (int w = 1; w < g; ++w) v[j] = max(v[j], m.part[tid * g + w][j]);
                 }
-                Entry &en = m.cur[ee];
-                const uint32_t chain = push_axis(en.chain, widest_axis(v, v + 3));
-                en.chain = chain;
-                m.chain_at[en.start] = static_cast<uint8_t>(chain);
-                m.cnt_at[en.start] = en.count;
-                m.split_at[en.start] = static_cast<uint8_t>(depth);
-                const int64_t node = en.node;
-                for (int a = 0; a < 3; ++a) {
-                    A.out_min[3 * node + a] = key_value(~v[9 + a]);
-                    A.out_max[3 * node + a] = key_value(v[6 + a]);
-                }
-                A.out_start[node] = -1;
-                A.out_count[node] = 0;
-                A.out_escape[node] = node + subtree_nodes(A.tab, depth, en.count);
+                finish_inner(m, A, m.inner[b + tid], depth, v, v + 3);
             }
-            __syncthreads();
         }
+        if (tid == 0) m.nnext = e;
+        __syncthreads();
         // 2. bitonic sort of all positions by (segment, key in the segment's axis order, surface index).
         // Warp w owns pairs [w*ppw, (w+1)*ppw), i.e. positions [2*w*ppw, 2*(w+1)*ppw) while the stride j is at
         // most ppw: such stages need only the warp's own barrier.
@@ -623,15 +640,15 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
         const int ppw = max(1, pairs / kWarps);
         for (int k = 2; k <= p2; k <<= 1) {
             for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int r = lane; r < ppw; r += 32) {
-                    const int i = warp * ppw + r;
+                for (int rr = lane; rr < ppw; rr += 32) {
+                    const int i = warp * ppw + rr;
                     if (i >= pairs) break;
                     const int lo = ((i & ~(j - 1)) << 1) | (i & (j - 1));
                     const int hi = lo | j;
-                    const int a = m.lp[lo], b = m.lp[hi];
+                    const int a = m.lp[lo], bb = m.lp[hi];
                     const bool up = (lo & k) == 0;
-                    if (slot_less(m, b, a) == up) {
-                        m.lp[lo] = static_cast<uint16_t>(b);
+                    if (slot_less(m, bb, a) == up) {
+                        m.lp[lo] = static_cast<uint16_t>(bb);
                         m.lp[hi] = static_cast<uint16_t>(a);
                     }
                 }
@@ -644,16 +661,16 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
         // 3. the right halves of the split segments become segments of their own
         for (int q = tid; q < n; q += kSmallThreads) {
             const int slot = m.lp[q];
-            const unsigned s = m.segslot[slot];
-            if (m.split_at[s] == static_cast<uint8_t>(depth)) {
-                const unsigned half = s + m.cnt_at[s] / 2u;
+            const unsigned s0 = m.segslot[slot];
+            if (m.split_at[s0] == static_cast<uint8_t>(depth)) {
+                const unsigned half = s0 + m.cnt_at[s0] / 2u;
                 if (static_cast<unsigned>(q) >= half) m.segslot[slot] = static_cast<uint16_t>(half);
             }
         }
         __syncthreads();
         // 4. children: leaves are written now, internal ones form the next level
-        for (int e = tid; e < ncur; e += kSmallThreads) {
-            const Entry en = m.cur[e];
+        for (int x = b + tid; x < e; x += kSmallThreads) {
+            const Entry en = m.inner[x];
             const int lc = en.count / 2, rc = en.count - lc;
             const int64_t lnode = en.node + 1;
             const int64_t rnode = lnode + subtree_nodes(A.tab, depth + 1, lc);
@@ -664,15 +681,35 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
                                                static_cast<int32_t>(rnode), en.chain});
         }
         __syncthreads();
-        const int nn = min(m.nnext, kSmallMax / 2);
-        for (int e = tid; e < nn; e += kSmallThreads) m.cur[e] = m.nxt[e];
+        if (tid == 0) m.level_begin[lev + 2] = min(m.nnext, kSmallMax);
         __syncthreads();
-        if (tid == 0) {
-            m.ncur = nn;
-            m.nnext = 0;
+    }
+    if (lev == kMaxSubtreeLevels && tid == 0) atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
+    // 5. bounds of the internal nodes, deepest level first, from their children's
+    for (int l = lev - 1; l >= 0; --l) {
+        const int depth = r.depth + l;
+        for (int x = m.level_begin[l] + tid; x < m.level_begin[l + 1]; x += kSmallThreads) {
+            const Entry en = m.inner[x];
+            const int64_t left = static_cast<int64_t>(en.node) + 1;
+            union_children(A.out_min, A.out_max, en.node, left, left + subtree_nodes(A.tab, depth + 1, en.count / 2));
         }
         __syncthreads();
-        ++depth;
+    }
+}
+
+// Bounds of the large nodes, deepest level first, once every subtree below them has its own.
+__global__ void __launch_bounds__(512) bvh_big_bounds_kernel(const LevelPlan *levels, int32_t num_levels,
+                                                             const BigSeg *bigs, const LevelTab *tab, double *out_min,
+                                                             double *out_max, const int32_t *status) {
+    if (ld_status(status) != 0) return;
+    for (int l = num_levels - 1; l >= 0; --l) {
+        const LevelPlan lv = levels[l];
+        for (int g = lv.seg_begin + threadIdx.x; g < lv.seg_end; g += blockDim.x) {
+            const BigSeg seg = bigs[g];
+            const int64_t left = static_cast<int64_t>(seg.node) + 1;
+            union_children(out_min, out_max, seg.node, left, left + subtree_nodes(tab, seg.depth + 1, seg.count / 2));
+        }
+        __syncthreads();
     }
 }
 
@@ -902,8 +939,6 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
         if (occ < 1) return ac::fail(AC_ERR_UNSUPPORTED, "ac_bvh_build_device: the top-level kernel does not fit an SM");
         const int grid = static_cast<int>(std::min<size_t>(p.max_items, static_cast<size_t>(occ) * sms));
         TopArgs ta{};
-        ta.lo = bounds_min;
-        ta.hi = bounds_max;
         ta.ckey = ckey;
         ta.perm0 = perm0;
         ta.perm1 = perm1;
@@ -917,8 +952,6 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
         ta.hist = reinterpret_cast<unsigned *>(ws + L.hist);
         ta.bar = reinterpret_cast<unsigned *>(ws + L.bar);
         ta.unresolved = reinterpret_cast<int32_t *>(ws + L.unresolved);
-        ta.out_min = out->bounds_min;
-        ta.out_max = out->bounds_max;
         ta.out_start = out->start;
         ta.out_count = out->count;
         ta.out_escape = out->escape;
@@ -950,6 +983,13 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
         sa.out_prims = out->primitives;
         sa.status = status;
         bvh_small_kernel<<<static_cast<unsigned>(p.smalls.size()), kSmallThreads, sizeof(SmallSmem), stream>>>(sa);
+        AC_CUDA_TRY(cudaGetLastError());
+    }
+    if (!p.levels.empty()) {
+        bvh_big_bounds_kernel<<<1, 512, 0, stream>>>(reinterpret_cast<const LevelPlan *>(ws + L.plan + L.levels),
+                                                     static_cast<int32_t>(p.levels.size()),
+                                                     reinterpret_cast<const BigSeg *>(ws + L.plan + L.bigs), tab,
+                                                     out->bounds_min, out->bounds_max, status);
         AC_CUDA_TRY(cudaGetLastError());
     }
     out->node_count = p.root.nodes;
