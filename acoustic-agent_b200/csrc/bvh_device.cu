@@ -72,12 +72,18 @@ struct SmallRoot {
 struct LevelTab {   // the (at most two) node counts found at one depth and their subtree sizes
     int64_t c0, n0, c1, n1;
 };
+// The median search of one node after some passes: the digits of the median's key found so far and its rank
+// among the keys that share them.  Resolved once that rank is 0: the keys below the prefix are the left half.
+struct Select {
+    unsigned long long pw[4];
+    long long kk;
+    int32_t resolved, rw, rs, pad;
+};
 struct SegState {
-    unsigned long long cmax[3], cmin_c[3];                       // centroid keys; min kept as max of the complement
-    unsigned long long pw[4];                                    // digits of the median's key found so far
-    long long kk;                                                // its rank among keys with that prefix
-    int32_t chain, resolved, rw, rs;                             // axis order; last word and shift resolved
-    int32_t left_fill, right_fill, first_pass, pad1;   // first_pass: digits shared by the node's min and max key
+    unsigned long long cmax[3], cmin_c[3];   // centroid keys; min kept as max of the complement
+    int32_t chain, first_pass;               // axis order; digits shared by the node's min and max key
+    int32_t left_fill, right_fill;
+    Select sel[2];                           // the median search after an even / odd number of passes
 };
 
 struct TopArgs {
@@ -90,9 +96,10 @@ struct TopArgs {
     const Chunk *chunks;
     const LevelTab *tab;
     SegState *state;
-    unsigned *hist;                   // [big segments][256]
+    unsigned *hist;                   // [3][big segments][256], one per pass modulo 3
+    int64_t num_bigs;
     unsigned *bar;                    // grid barrier: count, generation
-    int32_t *unresolved;              // [levels][kMaxPasses]
+    int32_t *unresolved;              // [levels][kMaxPasses + 1]
     int64_t *out_start, *out_count, *out_escape;
     int32_t *status;
 };
@@ -229,10 +236,49 @@ __device__ __forceinline__ unsigned long long key_word(const unsigned long long 
     return ckey[axis * S + i];
 }
 
+// One pass's digit choice from the node's histogram: every block of the node computes it from the same counts.
+__device__ Select select_digit(const Select &prev, const unsigned *hist, PassDigit d, unsigned *scan_s,
+                               Select *sel_s, int *found_s, int32_t *status) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned h = __ldcg(hist + tid);
+    unsigned incl = h;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) scan_s[warp] = incl;
+    if (tid == 0) *found_s = 0;
+    __syncthreads();
+    unsigned base = 0;
+    for (int w = 0; w < warp; ++w) base += scan_s[w];
+    incl += base;
+    const unsigned excl = incl - h;
+    if (d.sh >= 0 && h > 0 && static_cast<long long>(excl) <= prev.kk && prev.kk < static_cast<long long>(incl)) {
+        Select s = prev;
+        s.pw[d.w] |= static_cast<unsigned long long>(tid) << d.sh;
+        s.kk = prev.kk - static_cast<long long>(excl);
+        s.rw = d.w;
+        s.rs = d.sh;
+        s.resolved = s.kk == 0 ? 1 : 0;
+        *sel_s = s;
+        *found_s = 1;
+    }
+    __syncthreads();
+    Select out = *sel_s;
+    if (!*found_s) {   // cannot happen with unique keys; stop this node's search
+        out = prev;
+        out.resolved = 1;
+        if (tid == 0) atomicOr(status, AC_BVH_STATUS_INTERNAL);
+    }
+    __syncthreads();
+    return out;
+}
+
 __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
     __shared__ unsigned hist_s[256];
     __shared__ unsigned long long red[kTopThreads / 32][6];
     __shared__ unsigned scan_s[kTopThreads / 32];
+    __shared__ Select sel_s;
     __shared__ int ok_flag, found_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (ld_status(A.status) & (AC_BVH_STATUS_NONFINITE | AC_BVH_STATUS_ORDER)) return;   // uniform: set before launch
@@ -275,47 +321,74 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
         }
         if (!grid_barrier(A.bar, A.status, &ok_flag)) return;
 
-        // 2. axis, key order and the node's record
-        for (int g = lv.seg_begin + blockIdx.x; g < lv.seg_end; g += gridDim.x) {
-            if (tid != 0) continue;
-            SegState *st = A.state + g;
-            const BigSeg seg = A.bigs[g];
-            unsigned long long cmax[3], cmin_c[3];
-            for (int a = 0; a < 3; ++a) {
-                cmax[a] = __ldcg(&st->cmax[a]);
-                cmin_c[a] = __ldcg(&st->cmin_c[a]);
-            }
-            const uint32_t parent_chain =
-                seg.parent >= 0 ? static_cast<uint32_t>(__ldcg(&A.state[seg.parent].chain)) : kNoChain;
-            const int axis = widest_axis(cmax, cmin_c);
-            st->chain = static_cast<int32_t>(push_axis(parent_chain, axis));
-            st->kk = seg.count / 2;
-            st->resolved = 0;
-            for (int j = 1; j < 4; ++j) st->pw[j] = 0ull;
-            // every key of the node lies in [min, max]: the bytes they share are the median's too
-            const unsigned long long kmin = ~cmin_c[axis], diff = kmin ^ cmax[axis];
-            const int shared = diff == 0ull ? 8 : __clzll(static_cast<long long>(diff)) / 8;
-            st->pw[0] = shared == 0 ? 0ull : shared == 8 ? kmin : (kmin & (~0ull << (64 - 8 * shared)));
-            st->first_pass = shared;
-            const int64_t node = seg.node;
-            A.out_start[node] = -1;
-            A.out_count[node] = 0;
-            A.out_escape[node] = node + subtree_nodes(A.tab, seg.depth, seg.count);
-        }
-        if (!grid_barrier(A.bar, A.status, &ok_flag)) return;
-
-        // 3. radix select of each node's median, one 8-bit digit per pass
-        for (int p = 0; p < kMaxPasses; ++p) {
+        // 2. radix select of each node's median over 8-bit digits.  Pass p applies the digit choice of pass
+        // p - 1 (every block of a node from the same histogram; the node's first block keeps the result in
+        // sel[(p - 1) & 1]) and counts the digits of pass p, so one grid barrier ends a pass.  Pass 0 chooses
+        // the node's axis and starts after the bytes its smallest and largest keys share.
+        int final_pass = -1;
+        for (int p = 0; p <= kMaxPasses; ++p) {
             for (int c = lv.chunk_begin + blockIdx.x; c < lv.chunk_end; c += gridDim.x) {
                 const Chunk ch = A.chunks[c];
-                const SegState *st = A.state + ch.seg;
-                if (__ldcg(&st->resolved)) continue;   // block-uniform
-                const uint32_t chain = static_cast<uint32_t>(__ldcg(&st->chain));
+                const BigSeg seg = A.bigs[ch.seg];
+                SegState *st = A.state + ch.seg;
+                const bool first = ch.begin == seg.start;
+                uint32_t chain;
+                int first_pass;
+                Select cur;
+                if (p == 0) {
+                    unsigned long long cmax[3], cmin_c[3];
+                    for (int a = 0; a < 3; ++a) {
+                        cmax[a] = __ldcg(&st->cmax[a]);
+                        cmin_c[a] = __ldcg(&st->cmin_c[a]);
+                    }
+                    const uint32_t parent_chain =
+                        seg.parent >= 0 ? static_cast<uint32_t>(__ldcg(&A.state[seg.parent].chain)) : kNoChain;
+                    const int axis = widest_axis(cmax, cmin_c);
+                    chain = push_axis(parent_chain, axis);
+                    // every key of the node lies in [min, max]: the bytes they share are the median's too
+                    const unsigned long long kmin = ~cmin_c[axis], diff = kmin ^ cmax[axis];
+                    first_pass = diff == 0ull ? 8 : __clzll(static_cast<long long>(diff)) / 8;
+                    cur.pw[0] = first_pass == 0 ? 0ull : first_pass == 8 ? kmin
+                                                                          : (kmin & (~0ull << (64 - 8 * first_pass)));
+                    cur.pw[1] = cur.pw[2] = cur.pw[3] = 0ull;
+                    cur.kk = seg.count / 2;
+                    cur.resolved = 0;
+                    cur.rw = cur.rs = cur.pad = 0;
+                    if (first && tid == 0) {
+                        st->chain = static_cast<int32_t>(chain);
+                        st->first_pass = first_pass;
+                        st->sel[1] = cur;
+                        A.out_start[seg.node] = -1;
+                        A.out_count[seg.node] = 0;
+                        A.out_escape[seg.node] = seg.node + subtree_nodes(A.tab, seg.depth, seg.count);
+                    }
+                } else {
+                    chain = static_cast<uint32_t>(__ldcg(&st->chain));
+                    first_pass = __ldcg(&st->first_pass);
+                    const Select *prevp = &st->sel[(p - 2) & 1];
+                    Select prev;
+                    for (int j = 0; j < 4; ++j) prev.pw[j] = __ldcg(&prevp->pw[j]);
+                    prev.kk = __ldcg(&prevp->kk);
+                    prev.resolved = __ldcg(&prevp->resolved);
+                    prev.rw = __ldcg(&prevp->rw);
+                    prev.rs = __ldcg(&prevp->rs);
+                    prev.pad = 0;
+                    cur = prev;
+                    if (!prev.resolved) {   // block-uniform
+                        const PassDigit d = pass_digit(chain_words(chain), p - 1 + first_pass);
+                        cur = select_digit(prev, A.hist + (static_cast<int64_t>((p - 1) % 3) * A.num_bigs + ch.seg) * 256,
+                                           d, scan_s, &sel_s, &found_flag, A.status);
+                    }
+                    if (first && tid == 0) {
+                        st->sel[(p - 1) & 1] = cur;
+                        if (!cur.resolved) atomicAdd(&A.unresolved[lvl * (kMaxPasses + 1) + p - 1], 1);
+                    }
+                    if (first) A.hist[(static_cast<int64_t>((p + 1) % 3) * A.num_bigs + ch.seg) * 256 + tid] = 0u;
+                }
+                if (cur.resolved || p == kMaxPasses) continue;   // block-uniform
                 const int nwc = chain_words(chain);
-                const PassDigit d = pass_digit(nwc, p + __ldcg(&st->first_pass));
-                if (d.sh < 0) continue;   // past the key's last digit: the select step flags it
-                unsigned long long pw[4];
-                for (int j = 0; j < 4; ++j) pw[j] = __ldcg(&st->pw[j]);
+                const PassDigit d = pass_digit(nwc, p + first_pass);
+                if (d.sh < 0) continue;   // past the key's last digit: the next choice flags it
                 const unsigned long long hm = d.sh >= 56 ? 0ull : (~0ull << (d.sh + 8));
                 const int before = d.w == 3 ? nwc : d.w;
                 hist_s[tid] = 0u;
@@ -338,71 +411,38 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
                     for (int j = 0; j < before; ++j) {
 #pragma unroll
                         for (int u = 0; u < 4; ++u)
-                            if (match[u]) match[u] = key_word(A.ckey, A.S, chain, j, ii[u]) == pw[j];
+                            if (match[u]) match[u] = key_word(A.ckey, A.S, chain, j, ii[u]) == cur.pw[j];
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u)
-                        if (match[u] && (W[u] & hm) == (pw[d.w] & hm)) atomicAdd(&hist_s[(W[u] >> d.sh) & 255u], 1u);
+                        if (match[u] && (W[u] & hm) == (cur.pw[d.w] & hm))
+                            atomicAdd(&hist_s[(W[u] >> d.sh) & 255u], 1u);
                 }
                 __syncthreads();
                 const unsigned h = hist_s[tid];
-                if (h) atomicAdd(&A.hist[static_cast<int64_t>(ch.seg) * 256 + tid], h);
+                if (h) atomicAdd(&A.hist[(static_cast<int64_t>(p % 3) * A.num_bigs + ch.seg) * 256 + tid], h);
                 __syncthreads();
             }
             if (!grid_barrier(A.bar, A.status, &ok_flag)) return;
-
-            for (int g = lv.seg_begin + blockIdx.x; g < lv.seg_end; g += gridDim.x) {
-                SegState *st = A.state + g;
-                if (__ldcg(&st->resolved)) continue;   // block-uniform
-                unsigned *hg = A.hist + static_cast<int64_t>(g) * 256;
-                const unsigned h = __ldcg(hg + tid);
-                unsigned incl = h;
-                for (int o = 1; o < 32; o <<= 1) {
-                    const unsigned v = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += v;
-                }
-                if (lane == 31) scan_s[warp] = incl;
-                if (tid == 0) found_flag = 0;
-                __syncthreads();
-                unsigned base = 0;
-                for (int w = 0; w < warp; ++w) base += scan_s[w];
-                incl += base;
-                const unsigned excl = incl - h;
-                const long long kk = __ldcg(&st->kk);
-                const PassDigit d = pass_digit(chain_words(static_cast<uint32_t>(__ldcg(&st->chain))),
-                                               p + __ldcg(&st->first_pass));
-                if (d.sh >= 0 && h > 0 && static_cast<long long>(excl) <= kk && kk < static_cast<long long>(incl)) {
-                    st->pw[d.w] = __ldcg(&st->pw[d.w]) | (static_cast<unsigned long long>(tid) << d.sh);
-                    const long long left = kk - static_cast<long long>(excl);
-                    st->kk = left;
-                    st->rw = d.w;
-                    st->rs = d.sh;
-                    st->resolved = left == 0 ? 1 : 0;
-                    found_flag = 1;
-                    if (left != 0) atomicAdd(&A.unresolved[lvl * kMaxPasses + p], 1);
-                }
-                hg[tid] = 0u;
-                __syncthreads();
-                if (tid == 0 && !found_flag) {   // cannot happen with unique keys; stop this node's search
-                    atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
-                    st->resolved = 1;
-                }
-                __syncthreads();
+            // grid-uniform: every count of pass p - 1 landed before the barrier
+            if (p >= 1 && (__ldcg(&A.unresolved[lvl * (kMaxPasses + 1) + p - 1]) == 0 || p == kMaxPasses)) {
+                final_pass = p - 1;
+                break;
             }
-            if (!grid_barrier(A.bar, A.status, &ok_flag)) return;
-            if (__ldcg(&A.unresolved[lvl * kMaxPasses + p]) == 0) break;   // grid-uniform after the barrier
         }
 
-        // 4. scatter: keys below the median's to the left half, the rest to the right half
+        // 3. scatter: keys below the median's to the left half, the rest to the right half
         for (int c = lv.chunk_begin + blockIdx.x; c < lv.chunk_end; c += gridDim.x) {
             const Chunk ch = A.chunks[c];
             SegState *st = A.state + ch.seg;
             const BigSeg seg = A.bigs[ch.seg];
             const uint32_t chain = static_cast<uint32_t>(__ldcg(&st->chain));
             const int nwc = chain_words(chain);
-            const int rw = __ldcg(&st->rw), rs = __ldcg(&st->rs);
+            const Select *fin = &st->sel[final_pass & 1];
+            if (!__ldcg(&fin->resolved) && tid == 0) atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
+            const int rw = __ldcg(&fin->rw), rs = __ldcg(&fin->rs);
             unsigned long long pw[4];
-            for (int j = 0; j < 4; ++j) pw[j] = __ldcg(&st->pw[j]);
+            for (int j = 0; j < 4; ++j) pw[j] = __ldcg(&fin->pw[j]);
             const int64_t half = seg.count / 2;
             for (int base = ch.begin + warp * 32; base < ch.end; base += kTopThreads) {
                 const int q = base + lane;
@@ -829,9 +869,9 @@ Layout layout(const Plan &p, int64_t S) {
     L.perm1 = take(static_cast<size_t>(S) * sizeof(int32_t));
     const size_t zero_begin = off;
     L.state = take(std::max<size_t>(1, p.bigs.size()) * sizeof(SegState));
-    L.hist = take(std::max<size_t>(1, p.bigs.size()) * 256 * sizeof(unsigned));
+    L.hist = take(3 * std::max<size_t>(1, p.bigs.size()) * 256 * sizeof(unsigned));
     L.bar = take(2 * sizeof(unsigned));
-    L.unresolved = take(std::max<size_t>(1, p.levels.size()) * kMaxPasses * sizeof(int32_t));
+    L.unresolved = take(std::max<size_t>(1, p.levels.size()) * (kMaxPasses + 1) * sizeof(int32_t));
     (void)zero_begin;
     // the plan, copied from the host in one piece
     size_t po = 0;
@@ -950,6 +990,7 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
         ta.tab = tab;
         ta.state = state;
         ta.hist = reinterpret_cast<unsigned *>(ws + L.hist);
+        ta.num_bigs = static_cast<int64_t>(p.bigs.size());
         ta.bar = reinterpret_cast<unsigned *>(ws + L.bar);
         ta.unresolved = reinterpret_cast<int32_t *>(ws + L.unresolved);
         ta.out_start = out->start;
