@@ -191,6 +191,8 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_bvh_build": (ctypes.c_int, [c_double_p, c_double_p, ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ACBvh)]),
     "ac_bvh_device_workspace_size": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.POINTER(ctypes.c_size_t),
                                                     ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int64)]),
+    "ac_bvh_barrier_probe": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_void_p]),
     "ac_bvh_build_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32,
                                            ctypes.POINTER(ACBvh), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
                                            ctypes.c_void_p, ctypes.c_void_p]),

@@ -185,23 +185,26 @@ __device__ __forceinline__ bool bad_index(int32_t i, int64_t S, int32_t *status)
     return true;
 }
 
-// Grid-wide barrier of a cooperative launch.  A wait gives up after kSpinLimit
-// polls, flags AC_BVH_STATUS_TIMEOUT and every block then leaves the kernel.
-__device__ bool grid_barrier(unsigned *bar, int32_t *status, int *ok_flag) {
+// Grid-wide barrier of a cooperative launch over `blocks` arrivals.  A wait
+// gives up after `poll_limit` polls, flags AC_BVH_STATUS_TIMEOUT and every
+// block then leaves the kernel.
+__device__ bool grid_barrier(unsigned *bar, int32_t *status, int *ok_flag, unsigned blocks = 0,
+                             long long poll_limit = kSpinLimit) {
+    if (blocks == 0) blocks = gridDim.x;
     __syncthreads();
     if (threadIdx.x == 0) {
         int ok = 1;
         volatile unsigned *gen = bar + 1;
         const unsigned g = *gen;
         __threadfence();
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+        if (atomicAdd(bar, 1u) == blocks - 1) {
             atomicExch(bar, 0u);
             __threadfence();
             atomicAdd(bar + 1, 1u);
         } else {
             long long polls = 0;
             while (*gen == g) {
-                if (++polls > kSpinLimit || (ld_status(status) & AC_BVH_STATUS_TIMEOUT)) {
+                if (++polls > poll_limit || (ld_status(status) & AC_BVH_STATUS_TIMEOUT)) {
                     atomicOr(status, AC_BVH_STATUS_TIMEOUT);
                     ok = 0;
                     break;
@@ -215,6 +218,12 @@ __device__ bool grid_barrier(unsigned *bar, int32_t *status, int *ok_flag) {
     }
     __syncthreads();
     return *reinterpret_cast<volatile int *>(ok_flag) != 0;
+}
+
+// The barrier alone, for tests of its bounded wait: `expected` arrivals awaited by the launch's blocks.
+__global__ void bvh_barrier_probe_kernel(unsigned *bar, int32_t *status, unsigned expected, long long poll_limit) {
+    __shared__ int ok_flag;
+    grid_barrier(bar, status, &ok_flag, expected, poll_limit);
 }
 
 struct PassDigit {
@@ -1036,5 +1045,20 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
     out->node_count = p.root.nodes;
     out->leaf_count = p.root.leaves;
     out->max_depth = p.root.height;
+    return AC_OK;
+}
+
+extern "C" int ac_bvh_barrier_probe(int32_t blocks, int32_t expected_blocks, int64_t poll_limit, void *workspace,
+                                    int32_t *status, void *stream_ptr) {
+    using namespace acbvh;
+    if (!workspace || !status) return ac::fail(AC_ERR_INVALID, "ac_bvh_barrier_probe: null pointer");
+    if (blocks < 1 || blocks > 64 || expected_blocks < 1 || poll_limit < 1 || poll_limit > (int64_t{1} << 26))
+        return ac::fail(AC_ERR_INVALID, "ac_bvh_barrier_probe: blocks 1..64, expected >= 1, poll limit 1..2^26");
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    AC_CUDA_TRY(cudaMemsetAsync(workspace, 0, 2 * sizeof(unsigned), stream));
+    AC_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int32_t), stream));
+    bvh_barrier_probe_kernel<<<blocks, 32, 0, stream>>>(static_cast<unsigned *>(workspace), status,
+                                                        static_cast<unsigned>(expected_blocks), poll_limit);
+    AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
 }

@@ -502,6 +502,15 @@ int ac_read_bandwidth_probe(const void *buffer, size_t bytes, int32_t repeats, u
  * the FDN's roofline is reported against.  `sink` is one device word. */
 int ac_fp64_rate_probe(int32_t iterations, unsigned long long *sink, int64_t *ops, void *stream);
 
+/* Test: the device BVH build's grid barrier alone.  `blocks` blocks (1..64)
+ * wait for `expected_blocks` arrivals, each giving up after `poll_limit` polls
+ * (1..2^26): with expected_blocks > blocks no wait can end, so *status (one
+ * device int32, zeroed by the call) reads AC_BVH_STATUS_TIMEOUT once the
+ * stream reaches the end, and the kernel has returned.  `workspace`: 8 bytes
+ * of device memory, zeroed by the call. */
+int ac_bvh_barrier_probe(int32_t blocks, int32_t expected_blocks, int64_t poll_limit, void *workspace,
+                         int32_t *status, void *stream);
+
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */
 int ac_philox_workspace(uint64_t seed, uint64_t stream_key, int64_t num_rays, int32_t num_bounces,

@@ -116,3 +116,31 @@ def test_invalid_bounds_raise_the_reference_errors(bvh):
     # the builder stays usable after a rejected build
     tree = bvh.build_bvh(lo, hi)
     assert tree["node_count"] == 2047 and sorted(tree["primitives"].tolist()) == list(range(3000))
+
+
+def test_grid_barrier_wait_is_bounded(bvh):
+    """The build's grid barrier gives up after its poll limit with AC_BVH_STATUS_TIMEOUT instead of waiting for
+    ever: two blocks wait for a third arrival that never comes; the kernel returns, the status says so, and the
+    context stays usable for a build."""
+    import ctypes
+    import time
+    from acoustic_agent_b200 import _lib
+    lib = _lib.load()
+    ws = torch.zeros(2, dtype=torch.int32, device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def probe(blocks, expected):
+        _lib.check(lib.ac_bvh_barrier_probe(blocks, expected, 1 << 16, ctypes.c_void_p(ws.data_ptr()),
+                                            ctypes.c_void_p(status.data_ptr()), ctypes.c_void_p(stream.cuda_stream)),
+                   "ac_bvh_barrier_probe")
+        torch.cuda.synchronize()
+        return int(status.item())
+
+    assert probe(2, 2) == 0
+    t0 = time.perf_counter()
+    assert probe(2, 3) & _lib.AC_BVH_STATUS_TIMEOUT
+    assert time.perf_counter() - t0 < 5.0
+    from acoustic_agent_b200 import _lib as lib_module
+    lo, hi = _inputs("random", 5000, 1)
+    assert_same_tree(bvh.build_bvh(lo, hi), lib_module.build_bvh(lo, hi, 4), "after a timed-out barrier")
