@@ -208,6 +208,12 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
                                                ctypes.POINTER(ctypes.c_size_t)]),
     "ac_trace_batch": (ctypes.c_int, [ctypes.POINTER(ACJob), ctypes.c_int32, ctypes.POINTER(ACBatchConfig),
                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_batch_submit": (ctypes.c_int, [ctypes.POINTER(ACJob), ctypes.c_int32, ctypes.POINTER(ACBatchConfig),
+                                       ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.POINTER(ctypes.c_void_p)]),
+    "ac_batch_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32)]),
+    "ac_batch_wait": (ctypes.c_int, [ctypes.c_void_p]),
+    "ac_batch_release": (ctypes.c_int, [ctypes.c_void_p]),
     "ac_synth_workspace_size": (ctypes.c_int, [ctypes.POINTER(ACSynthParams), ctypes.POINTER(ctypes.c_size_t)]),
     "ac_synthesize": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACSynthParams), ctypes.c_void_p,
                                      ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]),

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -252,6 +253,62 @@ int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *
         if (rc != AC_OK) return rc;
         offset += bytes;
     }
+    return AC_OK;
+}
+
+// A submitted batch: the event recorded on the caller's stream after its launches.
+struct ac_batch_ticket_s {
+    cudaEvent_t done;
+};
+
+int ac_batch_submit(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
+                    size_t workspace_bytes, void *host_staging, void *stream, ac_batch_ticket_t *ticket) {
+    ac::NvtxRange nvtx_range("ac_batch_submit");
+    if (!ticket) return ac::fail(AC_ERR_INVALID, "ac_batch_submit: null ticket");
+    *ticket = nullptr;
+    const int rc = ac_trace_batch(jobs, num_jobs, config, workspace, workspace_bytes, host_staging, stream);
+    if (rc != AC_OK) return rc;
+    ac_batch_ticket_s *t = new (std::nothrow) ac_batch_ticket_s();
+    if (!t) return ac::fail(AC_ERR_NOMEM, "out of host memory");
+    cudaError_t err = cudaEventCreateWithFlags(&t->done, cudaEventDisableTiming);
+    if (err == cudaSuccess) {
+        err = cudaEventRecord(t->done, static_cast<cudaStream_t>(stream));
+        if (err != cudaSuccess) cudaEventDestroy(t->done);
+    }
+    if (err != cudaSuccess) {
+        delete t;
+        return ac::fail(AC_ERR_CUDA, "ac_batch_submit: event: %s", cudaGetErrorString(err));
+    }
+    *ticket = t;
+    return AC_OK;
+}
+
+int ac_batch_poll(ac_batch_ticket_t ticket, int32_t *done) {
+    if (!ticket || !done) return ac::fail(AC_ERR_INVALID, "ac_batch_poll: null argument");
+    const cudaError_t err = cudaEventQuery(ticket->done);
+    if (err == cudaSuccess) {
+        *done = 1;
+        return AC_OK;
+    }
+    if (err == cudaErrorNotReady) {
+        cudaGetLastError();   // not-ready is an answer, not a failure: leave no error behind
+        *done = 0;
+        return AC_OK;
+    }
+    return ac::fail(AC_ERR_CUDA, "ac_batch_poll: %s", cudaGetErrorString(err));
+}
+
+int ac_batch_wait(ac_batch_ticket_t ticket) {
+    if (!ticket) return ac::fail(AC_ERR_INVALID, "ac_batch_wait: null ticket");
+    AC_CUDA_TRY(cudaEventSynchronize(ticket->done));
+    return AC_OK;
+}
+
+int ac_batch_release(ac_batch_ticket_t ticket) {
+    if (!ticket) return AC_OK;
+    const cudaError_t err = cudaEventDestroy(ticket->done);
+    delete ticket;
+    if (err != cudaSuccess) return ac::fail(AC_ERR_CUDA, "ac_batch_release: %s", cudaGetErrorString(err));
     return AC_OK;
 }
 

@@ -420,6 +420,57 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
     workspace._keepalive = keep  # type: ignore[attr-defined]
 
 
+class BatchTicket:
+    """Completion ticket of ac_batch_submit: ``done()`` polls, ``wait()`` blocks, ``release()`` frees it."""
+
+    def __init__(self, handle: ctypes.c_void_p, keep: list[Any]) -> None:
+        self.handle = handle
+        self._keep = keep   # the job table's parameter tables stay alive until the batch is done
+
+    def done(self) -> bool:
+        flag = ctypes.c_int32()
+        _lib.check(_lib.load().ac_batch_poll(self.handle, ctypes.byref(flag)), "ac_batch_poll")
+        return bool(flag.value)
+
+    def wait(self) -> None:
+        _lib.check(_lib.load().ac_batch_wait(self.handle), "ac_batch_wait")
+
+    def release(self) -> None:
+        if self.handle:
+            _lib.check(_lib.load().ac_batch_release(self.handle), "ac_batch_release")
+            self.handle = ctypes.c_void_p()
+            self._keep = []
+
+    def __del__(self) -> None:
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def submit_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
+                 block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0,
+                 stream: torch.cuda.Stream | None = None) -> BatchTicket:
+    """trace_batch through the queue entry points: the launch plus a ticket to poll (ac_batch_submit)."""
+    if not jobs:
+        raise ValueError("submit_batch needs at least one job")
+    device = require_cuda(jobs[0][0].device)
+    arr = (_lib.ACJob * len(jobs))()
+    keep: list[Any] = []
+    for k, (scene, spec, buffers) in enumerate(jobs):
+        arr[k].scene = scene.handle.value
+        arr[k].params = params_struct(spec, device, keep)
+        arr[k].outputs = buffers.outputs_struct()
+    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), 0)
+    ws, ws_bytes, host = workspace.ensure(arr, len(jobs), cfg)
+    handle = ctypes.c_void_p()
+    _lib.check(_lib.load().ac_batch_submit(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
+                                           ctypes.c_void_p(host), _stream_ptr(stream), ctypes.byref(handle)),
+               "ac_batch_submit")
+    workspace.launched(stream)
+    return BatchTicket(handle, keep)
+
+
 def fixed_to_float64(fixed: torch.Tensor, scale: float) -> np.ndarray:
     """Fixed-point word pairs [..., 2] -> float64 values: (word1 * 2^32 + word0) / scale."""
     words = fixed.cpu().numpy()

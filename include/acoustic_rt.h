@@ -21,7 +21,8 @@
  *   ac_trace            acoustic_agent/steam_rt.py:1757-1804         trace_energy_field
  *                       (kernels: steam_rt.py:4708-4850, steam_rt_cuda.py:491-710)
  *   ac_trace_batch      acoustic_agent/api.py:477-639, batch.py:139-185, engine.py:64-73
- *                       (the per-job loops, run as one persistent launch)
+ *                       (the per-job loops, run as one persistent launch;
+ *                       ac_batch_submit / _poll / _wait / _release queue it)
  *   ac_synthesize       acoustic_agent/steam_rt.py:2205-2232         reconstruct_band_irs
  *                       + steam_rt.py:3070-3083                      bandlimit_band_signals
  *   ac_synthesize_batch the same per RIR, over the per-job loops of engine.py:64-73 and
@@ -299,6 +300,19 @@ int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch
  * same size, or NULL to use a pageable copy). */
 int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
                    size_t workspace_bytes, void *host_staging, void *stream);
+
+/* The persistent queue for hosts without the CUDA runtime: ac_batch_submit is
+ * ac_trace_batch plus a completion ticket recorded on `stream` after the
+ * launches; ac_batch_poll answers *done = 1 once the batch's outputs are
+ * written (0 before, never blocking), ac_batch_wait blocks until then, and
+ * ac_batch_release frees the ticket (NULL is accepted).  The workspace and
+ * outputs must stay alive until the ticket reports done. */
+typedef struct ac_batch_ticket_s *ac_batch_ticket_t;
+int ac_batch_submit(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, void *workspace,
+                    size_t workspace_bytes, void *host_staging, void *stream, ac_batch_ticket_t *ticket);
+int ac_batch_poll(ac_batch_ticket_t ticket, int32_t *done);
+int ac_batch_wait(ac_batch_ticket_t ticket);
+int ac_batch_release(ac_batch_ticket_t ticket);
 
 /* Device workspace needed by ac_synthesize. */
 int ac_synth_workspace_size(const ac_synth_params *params, size_t *bytes);

@@ -238,6 +238,33 @@ def test_batched_launch_equals_single_launches(rt):
         s.close()
 
 
+def test_queued_batch_equals_the_direct_launch(rt):
+    """ac_batch_submit runs the same launches as ac_trace_batch; its ticket polls not-done/done and waits."""
+    import time
+    cases = [load_case(n) for n in ("shoebox_linear", "u_furnished_bvh")]
+    scenes = [rt.DeviceScene(c["arrays"]) for c in cases]
+    specs = [spec_for(rt, c, "float32", rng="philox", stream_key=k) for k, c in enumerate(cases)]
+
+    def jobs():
+        return [(s, sp, rt.TraceBuffers.allocate(s.num_surfaces, sp.num_bins, torch.device("cuda"),
+                                                 ambisonics=sp.render_ambisonics)) for s, sp in zip(scenes, specs)]
+    direct_jobs, queued_jobs = jobs(), jobs()
+    rt.trace_batch(direct_jobs, rt.BatchWorkspace(torch.device("cuda")))
+    torch.cuda.synchronize()
+    ticket = rt.submit_batch(queued_jobs, rt.BatchWorkspace(torch.device("cuda")))
+    deadline = time.monotonic() + 60.0
+    while not ticket.done():
+        assert time.monotonic() < deadline
+        time.sleep(0.001)
+    ticket.wait()
+    ticket.release()
+    ticket.release()   # a second release is a no-op
+    for (_, _, a), (_, _, b) in zip(direct_jobs, queued_jobs):
+        assert torch.equal(a.echogram_fx, b.echogram_fx) and torch.equal(a.counters[:4], b.counters[:4])
+    for s in scenes:
+        s.close()
+
+
 @pytest.mark.parametrize("label", ["shoebox_f64", "shoebox_f32", "furnished_f32"])
 def test_gpu_synthesis_is_bit_exact(rt, label):
     from acoustic_agent_b200 import bands

@@ -162,3 +162,15 @@ def test_empty_batches_are_accepted():
     scfg.sample_rates[0] = 16000
     assert lib.ac_synth_batch_workspace_size(None, 0, ctypes.byref(scfg), ctypes.byref(size)) == _lib.AC_OK
     assert lib.ac_synthesize_batch(None, 0, ctypes.byref(scfg), None, 0, None, None) == _lib.AC_OK
+
+
+def test_batch_queue_rejects_null_arguments_without_a_device():
+    """The queue entry points validate their pointers before any CUDA call (usable on a CPU-only host)."""
+    import ctypes
+    from acoustic_agent_b200 import _lib
+    lib = _lib.load()
+    done = ctypes.c_int32(7)
+    assert lib.ac_batch_poll(None, ctypes.byref(done)) == _lib.AC_ERR_INVALID and done.value == 7
+    assert lib.ac_batch_wait(None) == _lib.AC_ERR_INVALID
+    assert lib.ac_batch_release(None) == _lib.AC_OK
+    assert lib.ac_batch_submit(None, 0, None, None, 0, None, None, None) == _lib.AC_ERR_INVALID
