@@ -49,6 +49,7 @@ namespace acbvh {
 constexpr int kSmallMax = 2048;        // surfaces per shared-memory subtree (a power of two)
 constexpr int kChunk = 1024;           // surfaces per block work item in the large-node levels
 constexpr int kTopThreads = 256;
+constexpr int kItems = kChunk / kTopThreads;   // surfaces per thread in a chunk's scatter
 constexpr int kSmallThreads = 512;
 constexpr int kMaxPasses = 28;         // 3 centroid words x 8 digits + 4 index digits
 constexpr long long kSpinLimit = 1ll << 23;
@@ -288,6 +289,7 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
     __shared__ unsigned long long red[kTopThreads / 32][6];
     __shared__ unsigned scan_s[kTopThreads / 32];
     __shared__ Select sel_s;
+    __shared__ unsigned wsum_s[kTopThreads / 32][2], base_s[2];
     __shared__ int ok_flag, found_flag;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (ld_status(A.status) & (AC_BVH_STATUS_NONFINITE | AC_BVH_STATUS_ORDER)) return;   // uniform: set before launch
@@ -440,7 +442,8 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
             }
         }
 
-        // 3. scatter: keys below the median's to the left half, the rest to the right half
+        // 3. scatter: keys below the median's to the left half, the rest to the right half.  A block places a
+        // whole chunk with one pair of atomics: each thread holds its kItems surfaces, the block scans the counts.
         for (int c = lv.chunk_begin + blockIdx.x; c < lv.chunk_end; c += gridDim.x) {
             const Chunk ch = A.chunks[c];
             SegState *st = A.state + ch.seg;
@@ -453,42 +456,69 @@ __global__ void __launch_bounds__(kTopThreads) bvh_top_kernel(TopArgs A) {
             unsigned long long pw[4];
             for (int j = 0; j < 4; ++j) pw[j] = __ldcg(&fin->pw[j]);
             const int64_t half = seg.count / 2;
-            for (int base = ch.begin + warp * 32; base < ch.end; base += kTopThreads) {
-                const int q = base + lane;
-                int32_t i = q < ch.end ? __ldcg(src + q) : 0;
-                const bool valid = q < ch.end && !bad_index(i, A.S, A.status);
-                bool left = false;
-                if (valid) {
+            int32_t ii[kItems];
+            bool valid[kItems], left[kItems];
+            unsigned nl = 0, nr = 0;
+#pragma unroll
+            for (int u = 0; u < kItems; ++u) {
+                const int q = ch.begin + u * kTopThreads + tid;
+                ii[u] = q < ch.end ? __ldcg(src + q) : 0;
+                valid[u] = q < ch.end && !bad_index(ii[u], A.S, A.status);
+                left[u] = false;
+                if (valid[u]) {
                     const int words = rw == 3 ? nwc + 1 : rw + 1;
                     for (int j = 0; j < words; ++j) {
                         const int w = j < nwc ? j : 3;
-                        const unsigned long long W = key_word(A.ckey, A.S, chain, w, i);
+                        const unsigned long long W = key_word(A.ckey, A.S, chain, w, ii[u]);
                         if (w == rw) {
-                            left = (W & (~0ull << rs)) < pw[w];
+                            left[u] = (W & (~0ull << rs)) < pw[w];
                             break;
                         }
                         if (W != pw[w]) {
-                            left = W < pw[w];
+                            left[u] = W < pw[w];
                             break;
                         }
                     }
-                }
-                const unsigned lmask = __ballot_sync(0xffffffffu, valid && left);
-                const unsigned rmask = __ballot_sync(0xffffffffu, valid && !left);
-                int lbase = 0, rbase = 0;
-                if (lane == 0) {
-                    if (lmask) lbase = atomicAdd(&st->left_fill, __popc(lmask));
-                    if (rmask) rbase = atomicAdd(&st->right_fill, __popc(rmask));
-                }
-                lbase = __shfl_sync(0xffffffffu, lbase, 0);
-                rbase = __shfl_sync(0xffffffffu, rbase, 0);
-                if (valid) {
-                    const unsigned below = (1u << lane) - 1u;
-                    const int64_t pos = left ? lbase + __popc(lmask & below) : half + rbase + __popc(rmask & below);
-                    if (left ? pos < half : pos < seg.count) dst[seg.start + pos] = i;
-                    else atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
+                    nl += left[u] ? 1u : 0u;
+                    nr += left[u] ? 0u : 1u;
                 }
             }
+            unsigned il = nl, ir = nr;   // inclusive scans within the warp
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned vl = __shfl_up_sync(0xffffffffu, il, o), vr = __shfl_up_sync(0xffffffffu, ir, o);
+                if (lane >= o) {
+                    il += vl;
+                    ir += vr;
+                }
+            }
+            if (lane == 31) {
+                wsum_s[warp][0] = il;
+                wsum_s[warp][1] = ir;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                unsigned tl = 0, tr = 0;
+                for (int w = 0; w < kTopThreads / 32; ++w) {
+                    const unsigned a = wsum_s[w][0], b = wsum_s[w][1];
+                    wsum_s[w][0] = tl;
+                    wsum_s[w][1] = tr;
+                    tl += a;
+                    tr += b;
+                }
+                base_s[0] = tl ? static_cast<unsigned>(atomicAdd(&st->left_fill, static_cast<int>(tl))) : 0u;
+                base_s[1] = tr ? static_cast<unsigned>(atomicAdd(&st->right_fill, static_cast<int>(tr))) : 0u;
+            }
+            __syncthreads();
+            int64_t pl = static_cast<int64_t>(base_s[0]) + wsum_s[warp][0] + (il - nl);
+            int64_t pr = half + static_cast<int64_t>(base_s[1]) + wsum_s[warp][1] + (ir - nr);
+#pragma unroll
+            for (int u = 0; u < kItems; ++u) {
+                if (!valid[u]) continue;
+                const int64_t pos = left[u] ? pl++ : pr++;
+                if (left[u] ? pos < half : pos < seg.count) dst[seg.start + pos] = ii[u];
+                else atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
+            }
+            __syncthreads();   // wsum_s and base_s are reused by the next chunk
         }
         if (!grid_barrier(A.bar, A.status, &ok_flag)) return;
     }
