@@ -14,6 +14,7 @@ There is no CPU fallback: without a CUDA device both raise.
 from __future__ import annotations
 
 import ctypes
+import threading
 from dataclasses import dataclass
 from typing import Any
 
@@ -37,6 +38,7 @@ class DeviceBvh:
     leaf_count: int
     max_depth: int
     leaf_size: int
+    inputs: tuple = ()         # the bounds the build reads, kept alive until it has run
 
     def to_numpy(self) -> dict[str, Any]:
         return {
@@ -68,7 +70,10 @@ def _raise_status(status: int) -> None:
 
 
 class DeviceBvhBuilder:
-    """Workspace, pinned plan staging and status word of ac_bvh_build_device, reused across builds."""
+    """Workspace, pinned plan staging and status word of ac_bvh_build_device, reused across builds.
+
+    Builds through one builder are serialised: a build waits until the previous one has finished on the device
+    before it reuses the workspace, and the status word describes the latest build only."""
 
     def __init__(self, device: torch.device | int = 0) -> None:
         self.device = runtime.require_cuda(device.index if isinstance(device, torch.device) else int(device))
@@ -76,6 +81,7 @@ class DeviceBvhBuilder:
         self.staging: torch.Tensor | None = None
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         self._copied: torch.cuda.Event | None = None
+        self._lock = threading.Lock()
 
     def _buffers(self, ws_bytes: int, staging_bytes: int) -> None:
         if self._copied is not None:
@@ -95,7 +101,11 @@ class DeviceBvhBuilder:
             raise ValueError("device BVH bounds must be float64 tensors")
         if lower.device != self.device or upper.device != self.device:
             raise ValueError(f"device BVH bounds must live on {self.device}")
-        lower, upper = lower.contiguous(), upper.contiguous()
+        with self._lock:
+            return self._build(lower.contiguous(), upper.contiguous(), n, leaf_size, stream, check)
+
+    def _build(self, lower: torch.Tensor, upper: torch.Tensor, n: int, leaf_size: int,
+               stream: torch.cuda.Stream | None, check: bool) -> DeviceBvh:
         ws_bytes, staging_bytes, nodes = _lib.device_bvh_plan(n, leaf_size)
         self._buffers(ws_bytes, staging_bytes)
         assert self.workspace is not None and self.staging is not None
@@ -120,6 +130,7 @@ class DeviceBvhBuilder:
             ev.record(s)
             self._copied = ev
         out.node_count, out.leaf_count, out.max_depth = int(desc.node_count), int(desc.leaf_count), int(desc.max_depth)
+        out.inputs = (lower, upper)
         if check:
             ev.synchronize()
             _raise_status(int(self.status.item()))
@@ -127,12 +138,15 @@ class DeviceBvhBuilder:
 
 
 _BUILDERS: dict[int, DeviceBvhBuilder] = {}
+_BUILDERS_LOCK = threading.Lock()
 
 
 def builder(device: int = 0) -> DeviceBvhBuilder:
-    if device not in _BUILDERS:
-        _BUILDERS[device] = DeviceBvhBuilder(device)
-    return _BUILDERS[device]
+    """The process's shared builder for one device."""
+    with _BUILDERS_LOCK:
+        if device not in _BUILDERS:
+            _BUILDERS[device] = DeviceBvhBuilder(device)
+        return _BUILDERS[device]
 
 
 def build_bvh(bounds_min: np.ndarray, bounds_max: np.ndarray, *, leaf_size: int = 4, device: int = 0) -> dict[str, Any]:

@@ -144,3 +144,14 @@ def test_grid_barrier_wait_is_bounded(bvh):
     from acoustic_agent_b200 import _lib as lib_module
     lo, hi = _inputs("random", 5000, 1)
     assert_same_tree(bvh.build_bvh(lo, hi), lib_module.build_bvh(lo, hi, 4), "after a timed-out barrier")
+
+
+def test_concurrent_builds_through_one_builder(bvh):
+    """Threads sharing the process's builder get their own trees (builds through one builder are serialised)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from acoustic_agent_b200 import _lib
+    inputs = [_inputs("random", 9000 + 1000 * k, k) for k in range(4)]
+    with ThreadPoolExecutor(4) as pool:
+        trees = list(pool.map(lambda io: bvh.build_bvh(*io), inputs))
+    for (lo, hi), tree in zip(inputs, trees):
+        assert_same_tree(tree, _lib.build_bvh(lo, hi, 4), "concurrent")
