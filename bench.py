@@ -1261,15 +1261,32 @@ def run_bvh_build(args) -> int:
                 "d2h_bytes_per_step": 72 * nodes + 8 * BVH_SURFACES,
                 "note": "bvh.build_bvh from numpy bounds to the numpy dict"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
-                     "kernel": "the whole build (3 launches)", "algorithmic_bytes": algo_bytes},
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": _profiled_value("bvh_build_warehouse_1m",
+                                                                                    "traffic_bytes_per_build_1m"),
+                     "traffic_note": "DRAM bytes of the four kernels at 2^18 surfaces (ncu), times 4",
+                     "peak_source": peaks["source"], "kernel": "the whole build (4 launches)",
+                     "algorithmic_bytes": algo_bytes},
         "cpu_baseline": cpu,
         "host_builder": {"seconds": host_s, "value": BVH_SURFACES / host_s, "unit": "surfaces/s",
                          "note": "ac_bvh_build, the C++ restatement, one host thread, full size"},
-        "gpu_launches": 3 * args.steps, "clocks": sampler.summary(),
+        "gpu_launches": 4 * args.steps, "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def _profiled_value(summary: str, key: str):
+    """A `key: number` line of a committed profile summary (profiles/<summary>.md), or None."""
+    path = REPO / "profiles" / f"{summary}.md"
+    if not path.exists():
+        return None
+    for text in path.read_text().splitlines():
+        if text.strip().lower().startswith(key + ":"):
+            try:
+                return float(text.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
 
 
 def _cpu_baseline(port, ref_cpu):

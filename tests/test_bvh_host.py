@@ -89,3 +89,14 @@ def test_install_routes_build_bvh_only_when_asked_and_above_the_threshold(monkey
     assert calls == [("reference", 99, 4), ("gpu", 100, 2)]
     handle.uninstall()
     assert fake.build_bvh is reference_build
+
+
+def test_bench_bvh_inputs_and_profiled_traffic():
+    """The bvh_build workload's seeded warehouse bounds are valid input for build_bvh, and the bench finds the
+    committed per-build DRAM traffic."""
+    import bench
+    lo, hi = bench.bvh_build_inputs(4096, seed=5)
+    assert lo.shape == hi.shape == (4096, 3) and np.isfinite(lo).all() and (hi >= lo).all()
+    assert np.array_equal(lo, bench.bvh_build_inputs(4096, seed=5)[0])          # seeded
+    traffic = bench._profiled_value("bvh_build_warehouse_1m", "traffic_bytes_per_build_1m")
+    assert traffic is not None and traffic > 96_468_920   # above the algorithmic bytes of a 2^20 build
