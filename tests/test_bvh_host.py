@@ -100,3 +100,13 @@ def test_bench_bvh_inputs_and_profiled_traffic():
     assert np.array_equal(lo, bench.bvh_build_inputs(4096, seed=5)[0])          # seeded
     traffic = bench._profiled_value("bvh_build_warehouse_1m", "traffic_bytes_per_build_1m")
     assert traffic is not None and traffic > 96_468_920   # above the algorithmic bytes of a 2^20 build
+
+
+def test_bench_reference_arm_runs_the_references_build_bvh():
+    """bench.py --impl reference --workload bvh_build times the reference's own build_bvh (baseline/_ref)."""
+    import bench
+    ref = bench.reference_bvh(1)
+    if "unavailable" in ref:
+        pytest.skip(ref["unavailable"])
+    assert ref["kind"] == "reference" and ref["cores"] == 1 and ref["value"] > 0
+    assert str(bench.BVH_SAMPLE) in ref["sample"]
