@@ -110,3 +110,28 @@ def test_bench_reference_arm_runs_the_references_build_bvh():
         pytest.skip(ref["unavailable"])
     assert ref["kind"] == "reference" and ref["cores"] == 1 and ref["value"] > 0
     assert str(bench.BVH_SAMPLE) in ref["sample"]
+
+
+def test_host_builder_equals_the_oracle_on_random_tied_scenes():
+    """Property: for any bounds drawn from a handful of values (ties on every axis, signed zeros, zero-size
+    boxes) and any leaf size, the C++ restatement builds the oracle's tree array for array."""
+    from hypothesis import given, settings, strategies as st
+    from acoustic_agent_b200 import _lib
+    from oracle import oracle
+    values = st.sampled_from([-2.0, -0.5, -0.0, 0.0, 0.25, 0.5, 1.0, 3.0])
+
+    @settings(max_examples=60, deadline=None, derandomize=True)
+    @given(st.integers(1, 160).flatmap(lambda n: st.tuples(
+        st.lists(st.tuples(values, values, values), min_size=n, max_size=n),
+        st.lists(st.tuples(values, values, values), min_size=n, max_size=n))), st.integers(1, 8))
+    def check(pairs, leaf):
+        a = np.asarray(pairs[0], dtype=np.float64)
+        b = np.asarray(pairs[1], dtype=np.float64)
+        lo, hi = np.minimum(a, b), np.maximum(a, b)
+        ours, ref = _lib.build_bvh(lo, hi, leaf), oracle.build_bvh(lo, hi, leaf)
+        for k in KEYS:
+            np.testing.assert_array_equal(np.asarray(ours[k]), np.asarray(ref[k]), err_msg=k)
+        assert (ours["node_count"], ours["leaf_count"], ours["max_depth"]) == (
+            ref["node_count"], ref["leaf_count"], ref["max_depth"])
+
+    check()
