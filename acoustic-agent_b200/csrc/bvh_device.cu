@@ -18,12 +18,12 @@
 //    unique key.  Which surfaces form the left child is then "the n/2 smallest
 //    keys", and the order inside a child never matters (leaves sort by index).
 //
-// Large nodes (more than kSmallMax surfaces) are split level by level by one
+// Large nodes (more than 1,024 or 2,048 surfaces) are split level by level by one
 // cooperative kernel: per level a reduction gives each node's centroid
 // extents, a radix select over the 8-bit digits of the composite key
 // finds the node's median (k = n/2) and surfaces are scattered to the two
 // halves.  Steps are separated by a grid barrier whose waits are bounded.
-// Each remaining subtree of at most kSmallMax surfaces is built by one CTA in
+// Each remaining subtree of at most 1,024 or 2,048 surfaces is built by one CTA in
 // shared memory: per level, a bitonic sort of all its surfaces by (segment,
 // composite key) and a split of every internal segment at its half.  Surface
 // bounds are read once, at the leaves; every inner node's bounds are the union
@@ -46,7 +46,11 @@
 
 namespace acbvh {
 
-constexpr int kSmallMax = 2048;        // surfaces per shared-memory subtree (a power of two)
+// Surfaces per shared-memory subtree: 1024 (four CTAs per SM) for scenes of 2,049 to 2^18 - 1 surfaces, where the
+// extra cooperative level costs less than the larger subtrees' sorts; 2048 (two CTAs per SM) otherwise.
+constexpr int kSmallMax = 2048;
+constexpr int kSmallMid = 1024;
+constexpr int64_t kSmallMidBelow = int64_t{1} << 18;
 constexpr int kChunk = 1024;           // surfaces per block work item in the large-node levels
 constexpr int kTopThreads = 256;
 constexpr int kItems = kChunk / kTopThreads;   // surfaces per thread in a chunk's scatter
@@ -534,21 +538,25 @@ struct Entry {
 
 constexpr int kMaxSubtreeLevels = 32;
 
+// Shared-memory state of one subtree of at most N surfaces (N a power of two, at most 4096).
+template <int N>
 struct SmallSmem {
-    unsigned long long key[3][kSmallMax];
-    int32_t gidx[kSmallMax];
-    uint16_t lp[kSmallMax];        // position -> slot, sorted every level
-    uint16_t segslot[kSmallMax];   // slot -> start of its segment (0xFFFF: padding)
-    uint16_t cnt_at[kSmallMax];    // segment start -> count
-    uint8_t chain_at[kSmallMax];   // segment start -> axis order
-    uint8_t split_at[kSmallMax];   // segment start -> depth at which it was split
-    Entry inner[kSmallMax];        // every internal node of the subtree, level after level (at most n - 1)
+    static constexpr int kCapacity = N;
+    unsigned long long key[3][N];
+    int32_t gidx[N];
+    uint16_t lp[N];        // position -> slot, sorted every level
+    uint16_t segslot[N];   // slot -> start of its segment (0xFFFF: padding)
+    uint16_t cnt_at[N];    // segment start -> count
+    uint8_t chain_at[N];   // segment start -> axis order
+    uint8_t split_at[N];   // segment start -> depth at which it was split
+    Entry inner[N];        // every internal node of the subtree, level after level (at most n - 1)
     unsigned long long part[kSmallThreads / 32][6];
     int level_begin[kMaxSubtreeLevels + 2];
     int nnext;
 };
 
-__device__ __forceinline__ bool slot_less(const SmallSmem &m, int a, int b) {
+template <class M>
+__device__ __forceinline__ bool slot_less(const M &m, int a, int b) {
     const unsigned sa = m.segslot[a], sb = m.segslot[b];
     if (sa != sb) return sa < sb;
     if (sa == 0xFFFFu) return a < b;
@@ -563,7 +571,8 @@ __device__ __forceinline__ bool slot_less(const SmallSmem &m, int a, int b) {
 }
 
 // A leaf of the positions [s, s + c): its surfaces in ascending index order (bvh.py:48) and its bounds.
-__device__ void emit_leaf(SmallSmem &m, const SmallArgs &A, const SmallRoot &r, int s, int c, int64_t node) {
+template <class M>
+__device__ void emit_leaf(M &m, const SmallArgs &A, const SmallRoot &r, int s, int c, int64_t node) {
     for (int x = s + 1; x < s + c; ++x) {   // insertion sort of the leaf's slots by surface index
         const uint16_t v = m.lp[x];
         int y = x - 1;
@@ -603,7 +612,8 @@ __device__ __forceinline__ void union_children(double *out_min, double *out_max,
 }
 
 // Axis and key order of an internal node from its centroid key extents, and its record (bounds come later).
-__device__ __forceinline__ void finish_inner(SmallSmem &m, const SmallArgs &A, Entry &en, int depth,
+template <class M>
+__device__ __forceinline__ void finish_inner(M &m, const SmallArgs &A, Entry &en, int depth,
                                              const unsigned long long cmax[3], const unsigned long long cmin_c[3]) {
     const uint32_t chain = push_axis(en.chain, widest_axis(cmax, cmin_c));
     en.chain = chain;
@@ -617,15 +627,17 @@ __device__ __forceinline__ void finish_inner(SmallSmem &m, const SmallArgs &A, E
 }
 
 // Internal nodes of a level number at most n / 2 (each holds two or more surfaces); all of them at most n - 1.
-__device__ __forceinline__ void push_entry(SmallSmem &m, int32_t *status, const Entry &e) {
+template <class M>
+__device__ __forceinline__ void push_entry(M &m, int32_t *status, const Entry &e) {
     const int at = atomicAdd(&m.nnext, 1);
-    if (at < kSmallMax) m.inner[at] = e;
+    if (at < M::kCapacity) m.inner[at] = e;
     else atomicOr(status, AC_BVH_STATUS_INTERNAL);
 }
 
+template <int N>
 __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SmallSmem &m = *reinterpret_cast<SmallSmem *>(smem_raw);
+    SmallSmem<N> &m = *reinterpret_cast<SmallSmem<N> *>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int kWarps = kSmallThreads / 32;
     if (ld_status(A.status) != 0) return;
@@ -634,7 +646,7 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
     int p2 = 1;
     while (p2 < n) p2 <<= 1;
     const int32_t *src = r.buf ? A.perm1 : A.perm0;
-    for (int q = tid; q < kSmallMax; q += kSmallThreads) {
+    for (int q = tid; q < N; q += kSmallThreads) {
         m.chain_at[q] = static_cast<uint8_t>(kNoChain);
         m.split_at[q] = 0xFF;
         if (q < p2) {
@@ -760,7 +772,7 @@ __global__ void __launch_bounds__(kSmallThreads) bvh_small_kernel(SmallArgs A) {
                                                static_cast<int32_t>(rnode), en.chain});
         }
         __syncthreads();
-        if (tid == 0) m.level_begin[lev + 2] = min(m.nnext, kSmallMax);
+        if (tid == 0) m.level_begin[lev + 2] = min(m.nnext, N);
         __syncthreads();
     }
     if (lev == kMaxSubtreeLevels && tid == 0) atomicOr(A.status, AC_BVH_STATUS_INTERNAL);
@@ -809,6 +821,7 @@ struct Plan {
 
     std::map<int64_t, Info> memo;
     int64_t leaf = 4;
+    int64_t small_max = kSmallMax;   // surfaces per shared-memory subtree for this scene
 
     Info info(int64_t c) {
         auto it = memo.find(c);
@@ -824,7 +837,7 @@ struct Plan {
 
     void walk(int64_t start, int64_t count, int64_t node, int depth, int parent, int buf,
               std::vector<std::vector<BigSeg>> &by_level, std::vector<std::vector<int>> &parent_level_index) {
-        if (count > kSmallMax) {
+        if (count > small_max) {
             const int lvl = depth - 1;
             if (static_cast<int>(by_level.size()) <= lvl) {
                 by_level.resize(lvl + 1);
@@ -843,6 +856,7 @@ struct Plan {
 
     void build(int64_t S, int64_t leaf_size) {
         leaf = leaf_size;
+        small_max = (S > kSmallMax && S < kSmallMidBelow) ? kSmallMid : kSmallMax;
         root = info(S);
         // level table: the counts at each depth (at most two, consecutive)
         tab.assign(static_cast<size_t>(root.height) + 2, LevelTab{-1, 0, -1, 0});
@@ -1041,9 +1055,11 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
                                                 dim3(kTopThreads), args, 0, stream));
     }
     {
-        static_assert(sizeof(SmallSmem) <= 227 * 1024, "subtree state must fit shared memory");
-        AC_CUDA_TRY(cudaFuncSetAttribute(bvh_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(sizeof(SmallSmem))));
+        static_assert(sizeof(SmallSmem<kSmallMax>) <= 227 * 1024, "subtree state must fit shared memory");
+        const bool mid = p.small_max == kSmallMid;
+        const size_t smem = mid ? sizeof(SmallSmem<kSmallMid>) : sizeof(SmallSmem<kSmallMax>);
+        AC_CUDA_TRY(cudaFuncSetAttribute(mid ? bvh_small_kernel<kSmallMid> : bvh_small_kernel<kSmallMax>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         SmallArgs sa{};
         sa.lo = bounds_min;
         sa.hi = bounds_max;
@@ -1062,7 +1078,10 @@ extern "C" int ac_bvh_build_device(const double *bounds_min, const double *bound
         sa.out_escape = out->escape;
         sa.out_prims = out->primitives;
         sa.status = status;
-        bvh_small_kernel<<<static_cast<unsigned>(p.smalls.size()), kSmallThreads, sizeof(SmallSmem), stream>>>(sa);
+        if (mid)
+            bvh_small_kernel<kSmallMid><<<static_cast<unsigned>(p.smalls.size()), kSmallThreads, smem, stream>>>(sa);
+        else
+            bvh_small_kernel<kSmallMax><<<static_cast<unsigned>(p.smalls.size()), kSmallThreads, smem, stream>>>(sa);
         AC_CUDA_TRY(cudaGetLastError());
     }
     if (!p.levels.empty()) {
