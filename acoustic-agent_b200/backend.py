@@ -63,28 +63,61 @@ def resolve_intersection_backend(value: str, surface_count: int, min_surfaces: i
 
 
 class _SceneCache:
-    """Resident device scenes keyed by the identity of their array dict (cf. steam_rt_cuda.py:229-261)."""
+    """Resident device scenes keyed by the identity of their array dict (cf. steam_rt_cuda.py:229-261).
+
+    ``acquire`` hands out a scene with a user count; ``release`` returns it.
+    Only scenes without users are evicted (least recently used first), so a
+    thread tracing a scene never sees it destroyed under it; while every entry
+    is in use the cache holds more than ``limit`` scenes until they are
+    released.  Work already enqueued on a stream is ordered before the memory
+    is freed by ac_scene_destroy itself.
+    """
 
     def __init__(self, limit: int = 32) -> None:
         self.limit = limit
-        self.entries: OrderedDict[tuple[int, int], tuple[Any, runtime.DeviceScene]] = OrderedDict()
+        # key -> [array dict (kept alive so its id is not reused), scene, users]
+        self.entries: OrderedDict[tuple[int, int], list[Any]] = OrderedDict()
         self.lock = Lock()
 
-    def get(self, arrays: Mapping[str, Any] | SceneArrays, device: int) -> tuple[runtime.DeviceScene, bool]:
+    def acquire(self, arrays: Mapping[str, Any] | SceneArrays, device: int) -> tuple[runtime.DeviceScene, bool]:
         key = (id(arrays), int(device))
         with self.lock:
             hit = self.entries.get(key)
             if hit is not None and hit[0] is arrays:
+                hit[2] += 1
                 self.entries.move_to_end(key)
                 return hit[1], True
         scene = runtime.DeviceScene(arrays, device=device)
+        evicted: list[runtime.DeviceScene] = []
         with self.lock:
-            self.entries[key] = (arrays, scene)
-            self.entries.move_to_end(key)
-            while len(self.entries) > self.limit:
-                _, (_, old) = self.entries.popitem(last=False)
-                old.close()
-        return scene, False
+            hit = self.entries.get(key)
+            if hit is not None and hit[0] is arrays:
+                # another thread uploaded the same arrays meanwhile: use its scene, drop ours
+                hit[2] += 1
+                self.entries.move_to_end(key)
+                evicted.append(scene)
+                scene, found = hit[1], True
+            else:
+                if hit is not None:
+                    if hit[2] == 0:
+                        evicted.append(hit[1])
+                    del self.entries[key]
+                self.entries[key] = [arrays, scene, 1]
+                found = False
+            for k in [k for k, e in self.entries.items() if e[2] == 0]:
+                if len(self.entries) <= self.limit:
+                    break
+                evicted.append(self.entries.pop(k)[1])
+        for old in evicted:
+            old.close()
+        return scene, found
+
+    def release(self, scene: runtime.DeviceScene) -> None:
+        with self.lock:
+            for entry in self.entries.values():
+                if entry[1] is scene:
+                    entry[2] -= 1
+                    return
 
 
 SCENES = _SceneCache()
@@ -141,20 +174,24 @@ def trace_energy_field(scene: Any, source: np.ndarray, listener: np.ndarray, con
     )
     transfer_started = time.perf_counter()
     hits_before, misses_before = runtime.STREAMS.hits, runtime.STREAMS.misses
-    device_scene, scene_hit = SCENES.get(arrays, device_id)
-    stream = torch.cuda.current_stream(device)
-    buffers = runtime.TraceBuffers.allocate(device_scene.num_surfaces, num_bins, device,
-                                            ambisonics=bool(render_ambisonics),
-                                            visual=(visual_limit, num_bounces, spec.dtype) if visual_limit else None)
-    if mode == "reference":
-        runtime.reference_stream(spec, device)
-    runtime.diffuse_bank(spec.dtype, device)
-    stream.synchronize()
-    upload_time = time.perf_counter() - transfer_started
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    runtime.trace(device_scene, spec, buffers, stream=stream)
-    stop.record(stream)
+    device_scene, scene_hit = SCENES.acquire(arrays, device_id)
+    try:
+        stream = torch.cuda.current_stream(device)
+        buffers = runtime.TraceBuffers.allocate(device_scene.num_surfaces, num_bins, device,
+                                                ambisonics=bool(render_ambisonics),
+                                                visual=(visual_limit, num_bounces, spec.dtype) if visual_limit
+                                                else None)
+        if mode == "reference":
+            runtime.reference_stream(spec, device)
+        runtime.diffuse_bank(spec.dtype, device)
+        stream.synchronize()
+        upload_time = time.perf_counter() - transfer_started
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        runtime.trace(device_scene, spec, buffers, stream=stream)
+        stop.record(stream)
+    finally:
+        SCENES.release(device_scene)
     stop.synchronize()
     kernel_time = start.elapsed_time(stop) / 1000.0
     download_started = time.perf_counter()

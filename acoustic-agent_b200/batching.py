@@ -56,11 +56,16 @@ class Plan:
     workspace: runtime.BatchWorkspace
     synth_workspace: runtime.SynthBatchWorkspace
     graph: torch.cuda.CUDAGraph | None = None
+    # capture(split=True): `graph` holds the trace alone and `synth_graph` the synthesis, replayed back to
+    # back on one stream, so that events recorded between the two replays time the trace live
+    synth_graph: torch.cuda.CUDAGraph | None = None
     keepalive: list[Any] = field(default_factory=list)
     # pipelined steps (launch_pipelined): a copy of the previous step's echograms and its synthesis jobs
     echo_prev: torch.Tensor | None = None
     synth_jobs_prev: Any = None
     pipe_graph: torch.cuda.CUDAGraph | None = None
+    # recorded after every replay of either graph; the plan's scenes wait for it before they are destroyed
+    replayed: torch.cuda.Event | None = None
 
     @property
     def num_rirs(self) -> int:
@@ -143,22 +148,49 @@ class RIRRenderer:
         return Plan(list(jobs), device_scenes, buffers, echo_store, ir_store, irs, synth_jobs, config,
                     self._trace_ws, self._synth_ws)
 
-    def launch(self, plan: Plan, stream: torch.cuda.Stream | None = None) -> None:
-        """Enqueue trace + synthesis of every job (asynchronous)."""
+    def launch(self, plan: Plan, stream: torch.cuda.Stream | None = None,
+               trace_events: tuple[torch.cuda.Event, torch.cuda.Event] | None = None) -> None:
+        """Enqueue trace + synthesis of every job (asynchronous).
+
+        `trace_events` (a pair of timing events) are recorded around the trace
+        alone; with a captured plan that needs ``capture(plan, split=True)``.
+        """
         if plan.graph is not None:
+            current = torch.cuda.current_stream(self.device)
+            if trace_events is not None and plan.synth_graph is None:
+                raise ValueError("timing the trace of a captured plan needs capture(plan, split=True)")
+            if trace_events is not None:
+                trace_events[0].record(current)
             plan.graph.replay()
+            if trace_events is not None:
+                trace_events[1].record(current)
+            if plan.synth_graph is not None:
+                plan.synth_graph.replay()
+            plan.replayed.record(current)
             return
-        self._enqueue(plan, stream)
+        self._enqueue(plan, stream, trace_events)
 
-    def _enqueue(self, plan: Plan, stream: torch.cuda.Stream | None) -> None:
-        runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
-                            plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
-                            chunk_rays=self.chunk_rays, stream=stream)
-        runtime.synthesize_batch((plan.synth_jobs, len(plan.jobs), plan.synth_config), plan.synth_workspace,
-                                 stream=stream)
+    def _enqueue(self, plan: Plan, stream: torch.cuda.Stream | None,
+                 trace_events: tuple[torch.cuda.Event, torch.cuda.Event] | None = None, *,
+                 trace: bool = True, synth: bool = True) -> None:
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        if trace:
+            if trace_events is not None:
+                trace_events[0].record(s)
+            runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
+                                plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
+                                chunk_rays=self.chunk_rays, stream=stream)
+            if trace_events is not None:
+                trace_events[1].record(s)
+        if synth:
+            runtime.synthesize_batch((plan.synth_jobs, len(plan.jobs), plan.synth_config), plan.synth_workspace,
+                                     stream=stream)
 
-    def capture(self, plan: Plan) -> None:
-        """Record the launch sequence once as a CUDA graph (the job table is staged in pinned memory)."""
+    def capture(self, plan: Plan, *, split: bool = False) -> None:
+        """Record the launch sequence once as a CUDA graph (the job table is staged in pinned memory).
+
+        With `split`, the trace and the synthesis are two graphs replayed back to back.
+        """
         plan.workspace = runtime.BatchWorkspace(self.device)
         plan.synth_workspace = runtime.SynthBatchWorkspace(self.device)
         side = torch.cuda.Stream(self.device)
@@ -168,9 +200,16 @@ class RIRRenderer:
         side.synchronize()
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph, stream=side):
-            self._enqueue(plan, side)
+            self._enqueue(plan, side, synth=not split)
+        synth_graph = None
+        if split:
+            synth_graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(synth_graph, stream=side):
+                self._enqueue(plan, side, trace=False)
         torch.cuda.current_stream(self.device).wait_stream(side)
         plan.graph = graph
+        plan.synth_graph = synth_graph
+        _guard_scenes(plan)
 
     # ---- pipelined steps: the trace of step k runs beside the synthesis of step k-1
     def _pipe_setup(self, plan: Plan) -> None:
@@ -222,6 +261,7 @@ class RIRRenderer:
         self._pipe_setup(plan)
         if plan.pipe_graph is not None:
             plan.pipe_graph.replay()
+            plan.replayed.record(torch.cuda.current_stream(self.device))
             return
         self._enqueue_pipelined(plan, torch.cuda.current_stream(self.device))
 
@@ -238,6 +278,7 @@ class RIRRenderer:
             self._enqueue_pipelined(plan, main)
         torch.cuda.current_stream(self.device).wait_stream(main)
         plan.pipe_graph = graph
+        _guard_scenes(plan)
 
     def late_tails(self, plan: Plan, *, transition_s: float = 1.0, overlap_fraction: float = 0.25,
                    stream: torch.cuda.Stream | None = None):
@@ -256,6 +297,15 @@ class RIRRenderer:
             out.append(host[off:off + t.numel()].reshape(t.shape))
             off += t.numel()
         return out
+
+
+def _guard_scenes(plan: Plan) -> None:
+    """Make each of the plan's scenes wait, before it is destroyed, for the plan's last graph replay."""
+    if plan.replayed is None:
+        plan.replayed = torch.cuda.Event()
+    for scene in plan.scenes:
+        if not any(g is plan.replayed for g in scene.graph_guards):
+            scene.graph_guards.append(plan.replayed)
 
 
 def plan_late_tails(renderer: "RIRRenderer", plan: Plan, *, transition_s: float = 1.0,

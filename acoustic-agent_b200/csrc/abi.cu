@@ -213,8 +213,10 @@ int ac_trace(ac_scene_t scene, const ac_trace_params *params, const ac_trace_out
     if (rc != AC_OK) return rc;
     const double scale = params->energy_scale > 0.0 ? params->energy_scale : ac::choose_energy_scale(scene, params);
     if (outputs->scale_out) *outputs->scale_out = scale;
-    if (params->precision == AC_PRECISION_FP64) return ac::launch_trace_f64(scene, params, outputs, scale, stream);
-    return ac::launch_trace_f32(scene, params, outputs, scale, stream);
+    rc = params->precision == AC_PRECISION_FP64 ? ac::launch_trace_f64(scene, params, outputs, scale, stream)
+                                                : ac::launch_trace_f32(scene, params, outputs, scale, stream);
+    if (rc != AC_OK) return rc;
+    return ac::note_scene_use(scene, stream);
 }
 
 int ac_batch_workspace_size(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *config, size_t *bytes) {
@@ -252,6 +254,12 @@ int ac_trace_batch(const ac_job *jobs, int32_t num_jobs, const ac_batch_config *
                                  : ac::launch_batch_f32(jobs, part.indices.data(), n, config, ws, bytes, host, stream);
         if (rc != AC_OK) return rc;
         offset += bytes;
+    }
+    // jobs of one scene are usually adjacent: note each run of them once
+    for (int32_t j = 0; j < num_jobs; ++j) {
+        if (j > 0 && jobs[j].scene == jobs[j - 1].scene) continue;
+        const int rc = ac::note_scene_use(jobs[j].scene, stream);
+        if (rc != AC_OK) return rc;
     }
     return AC_OK;
 }

@@ -267,5 +267,5 @@ extern "C" int ac_direct(ac_scene_t scene, const ac_direct_query *queries, int32
     ac::direct_kernel<<<blocks, 128, 0, stream>>>(static_cast<const ac_direct_query *>(workspace), num_queries,
                                                   scene->f64, t, results);
     AC_CUDA_TRY(cudaGetLastError());
-    return AC_OK;
+    return ac::note_scene_use(scene, stream_ptr);
 }

@@ -484,11 +484,43 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
     return AC_OK;
 }
 
+namespace ac {
+
+int note_scene_use(ac_scene_s *scene, void *stream_ptr) {
+    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    AC_CUDA_TRY(cudaStreamIsCapturing(stream, &capture));
+    if (capture != cudaStreamCaptureStatusNone) return AC_OK;
+    std::lock_guard<std::mutex> guard(scene->use_lock);
+    cudaEvent_t event = nullptr;
+    for (const auto &use : scene->uses)
+        if (use.first == stream) event = use.second;
+    if (!event) {
+        AC_CUDA_TRY(cudaEventCreateWithFlags(&event, cudaEventDisableTiming));
+        scene->uses.emplace_back(stream, event);
+    }
+    AC_CUDA_TRY(cudaEventRecord(event, stream));
+    return AC_OK;
+}
+
+}  // namespace ac
+
 extern "C" int ac_scene_destroy(ac_scene_t s) {
     ac::NvtxRange nvtx_range("ac_scene_destroy");
     if (!s) return AC_OK;
     cudaSetDevice(s->device);
-    // the caller destroys a scene only after the work that reads it has finished
+    // The frees go on the legacy stream after every recorded last use, so work
+    // still queued on other streams reads the scene before its memory returns
+    // to the pool.  Work captured into a CUDA graph is the graph owner's to
+    // finish before destroying the scene.
+    {
+        std::lock_guard<std::mutex> guard(s->use_lock);
+        for (const auto &use : s->uses) {
+            cudaStreamWaitEvent(cudaStreamLegacy, use.second, 0);
+            cudaEventDestroy(use.second);   // released once its last record completes
+        }
+        s->uses.clear();
+    }
     if (s->storage_f32) cudaFreeAsync(s->storage_f32, cudaStreamLegacy);
     if (s->storage_f64) cudaFreeAsync(s->storage_f64, cudaStreamLegacy);
     delete s;

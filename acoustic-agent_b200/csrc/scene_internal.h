@@ -4,7 +4,11 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <mutex>
+#include <utility>
 #include <vector>
+
+#include <cuda_runtime.h>
 
 #include "acoustic_rt.h"
 #include "trace_fast.cuh"
@@ -31,6 +35,12 @@ struct ac_scene_s {
     double max_reflection = 0.0;   // bound used when choosing the fixed-point scale
     double max_scattering = 0.0;
     double min_scattering = 0.0;
+    // Last use of the scene on each stream that launched work reading it: an
+    // event recorded after that work.  ac_scene_destroy orders the frees after
+    // all of them, so a scene may be destroyed while kernels that read it are
+    // still queued on streams that do not synchronise with the legacy stream.
+    std::mutex use_lock;
+    std::vector<std::pair<cudaStream_t, cudaEvent_t>> uses;
 };
 
 namespace ac {
@@ -50,6 +60,12 @@ double choose_energy_scale(const ac_scene_s *scene, const ac_trace_params *p);
 int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o);
 
 int device_sm_count(int device);
+
+// Records, after the work just enqueued on `stream`, that `scene` is in use
+// there (see ac_scene_s::uses).  Work enqueued while the stream is being
+// captured into a CUDA graph is not recorded: the graph's owner keeps the
+// scene alive while the graph can still run.
+int note_scene_use(ac_scene_s *scene, void *stream);
 
 // Per-precision launchers (trace_f32.cu / trace_f64.cu).
 int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o, double scale,

@@ -260,21 +260,27 @@ extern "C" int ac_synth_workspace_size(const ac_synth_params *p, size_t *bytes) 
     return AC_OK;
 }
 
-extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, float *band_irs, void *workspace,
-                             size_t workspace_bytes, void *stream_ptr) {
-    ac::NvtxRange nvtx_range("ac_synthesize");
-    if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize: null argument");
+namespace ac {
+namespace {
+
+// Argument checks shared by ac_synthesize and ac_synthesize_static.
+int check_synth(const char *name, const float *echograms, const ac_synth_params *p, const float *band_irs) {
+    if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "%s: null argument", name);
     if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
         return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
     const int64_t N = static_cast<int64_t>(p->num_bins) * p->samples_per_bin;
     if (N + 3 > 0x7FFFFFFF) return ac::fail(AC_ERR_CAPACITY, "signal of %lld samples is too long", (long long)N);
     if (p->rng_mode == AC_RNG_REFERENCE && !p->white) return ac::fail(AC_ERR_INVALID, "reference mode needs white noise");
     if (!p->air && !p->direct_delays) return ac::fail(AC_ERR_INVALID, "need an air table or the direct delays");
-    if (p->num_rirs == 0) return AC_OK;
-    const ac::SynthLayout l = ac::synth_layout(p);
-    if (!workspace || workspace_bytes < l.total)
-        return ac::fail(AC_ERR_CAPACITY, "synthesis workspace too small: %zu < %zu", workspace_bytes, l.total);
-    ac::SynthArgs a;
+    return AC_OK;
+}
+
+// The three launches of one single-shape synthesis, over a workspace laid out
+// by synth_layout(p) (caller-owned or the static scratch; at least l.total bytes).
+int enqueue_synthesis(const float *echograms, const ac_synth_params *p, float *band_irs, unsigned char *ws,
+                      const SynthLayout &l, cudaStream_t stream) {
+    const int64_t N = static_cast<int64_t>(p->num_bins) * p->samples_per_bin;
+    SynthArgs a;
     std::memcpy(a.crossover, p->crossover, sizeof(a.crossover));
     std::memcpy(a.air_coefficients, p->air_coefficients, sizeof(a.air_coefficients));
     a.speed_of_sound = p->speed_of_sound;
@@ -282,16 +288,14 @@ extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, f
     a.num_bins = p->num_bins;
     a.spb = p->samples_per_bin;
     a.sample_rate = p->sample_rate;
-    unsigned char *ws = static_cast<unsigned char *>(workspace);
     double *amps = reinterpret_cast<double *>(ws + l.amps);
     double *air = p->air ? nullptr : reinterpret_cast<double *>(ws + l.air);
     double *wtab = reinterpret_cast<double *>(ws + l.wtab);
     double *white = p->rng_mode == AC_RNG_PHILOX ? reinterpret_cast<double *>(ws + l.white) : nullptr;
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
     const size_t cells = static_cast<size_t>(p->num_rirs) * 6 * p->num_bins;
     const size_t work = std::max<size_t>(cells, static_cast<size_t>(white ? N : p->samples_per_bin));
     const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, 8192));
-    ac::synth_prepare_kernel<<<grid, 256, 0, stream>>>(echograms, p->direct_delays, a, amps, air, wtab, white, p->seed);
+    synth_prepare_kernel<<<grid, 256, 0, stream>>>(echograms, p->direct_delays, a, amps, air, wtab, white, p->seed);
     AC_CUDA_TRY(cudaGetLastError());
     const double *air_table = p->air ? p->air : air;
     const double *noise = white ? white : p->white;
@@ -299,14 +303,30 @@ extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, f
     double *raw = reinterpret_cast<double *>(ws + l.raw);
     const size_t samples = static_cast<size_t>(p->num_rirs) * 6 * static_cast<size_t>(N);
     const int raw_grid = static_cast<int>(std::min<size_t>((samples + 255) / 256, 65536));
-    ac::synth_raw_kernel<<<raw_grid, 256, 0, stream>>>(amps, air_table, wtab, noise, stride, a, raw);
+    synth_raw_kernel<<<raw_grid, 256, 0, stream>>>(amps, air_table, wtab, noise, stride, a, raw);
     AC_CUDA_TRY(cudaGetLastError());
     const int units = p->num_rirs * 6;
     const int warps = (units + 3) / 4;
     const int threads = 32;  // one warp per block: spread the sequential chains over all SMs
-    ac::synth_filter_kernel<<<warps, threads, 0, stream>>>(raw, a, band_irs);
+    synth_filter_kernel<<<warps, threads, 0, stream>>>(raw, a, band_irs);
     AC_CUDA_TRY(cudaGetLastError());
     return AC_OK;
+}
+
+}  // namespace
+}  // namespace ac
+
+extern "C" int ac_synthesize(const float *echograms, const ac_synth_params *p, float *band_irs, void *workspace,
+                             size_t workspace_bytes, void *stream_ptr) {
+    ac::NvtxRange nvtx_range("ac_synthesize");
+    const int rc = ac::check_synth("ac_synthesize", echograms, p, band_irs);
+    if (rc != AC_OK) return rc;
+    if (p->num_rirs == 0) return AC_OK;
+    const ac::SynthLayout l = ac::synth_layout(p);
+    if (!workspace || workspace_bytes < l.total)
+        return ac::fail(AC_ERR_CAPACITY, "synthesis workspace too small: %zu < %zu", workspace_bytes, l.total);
+    return ac::enqueue_synthesis(echograms, p, band_irs, static_cast<unsigned char *>(workspace), l,
+                                 static_cast<cudaStream_t>(stream_ptr));
 }
 
 // ---------------------------------------------------------------------------
@@ -533,13 +553,9 @@ int static_scratch(void **out) {
 extern "C" int ac_synthesize_static(const float *echograms, const ac_synth_params *p, float *band_irs,
                                     void *stream_ptr) {
     ac::NvtxRange nvtx_range("ac_synthesize_static");
-    if (!p || !echograms || !band_irs) return ac::fail(AC_ERR_INVALID, "ac_synthesize_static: null argument");
-    if (p->num_rirs < 0 || p->num_bins < 1 || p->samples_per_bin < 1 || p->sample_rate < 1)
-        return ac::fail(AC_ERR_INVALID, "synthesis sizes must be positive");
+    int rc = ac::check_synth("ac_synthesize_static", echograms, p, band_irs);
+    if (rc != AC_OK) return rc;
     const int64_t N = static_cast<int64_t>(p->num_bins) * p->samples_per_bin;
-    if (N + 3 > 0x7FFFFFFF) return ac::fail(AC_ERR_CAPACITY, "signal of %lld samples is too long", (long long)N);
-    if (p->rng_mode == AC_RNG_REFERENCE && !p->white) return ac::fail(AC_ERR_INVALID, "reference mode needs white noise");
-    if (!p->air && !p->direct_delays) return ac::fail(AC_ERR_INVALID, "need an air table or the direct delays");
     const ac::SynthLayout l = ac::synth_layout(p);
     if (l.total > static_cast<size_t>(AC_SYNTH_STATIC_BYTES))
         return ac::fail(AC_ERR_CAPACITY,
@@ -548,37 +564,8 @@ extern "C" int ac_synthesize_static(const float *echograms, const ac_synth_param
                         p->num_rirs, (long long)N, l.total, static_cast<size_t>(AC_SYNTH_STATIC_BYTES));
     if (p->num_rirs == 0) return AC_OK;
     void *scratch = nullptr;
-    const int rc = static_scratch(&scratch);
+    rc = static_scratch(&scratch);
     if (rc != AC_OK) return rc;
-    ac::SynthArgs a;
-    std::memcpy(a.crossover, p->crossover, sizeof(a.crossover));
-    std::memcpy(a.air_coefficients, p->air_coefficients, sizeof(a.air_coefficients));
-    a.speed_of_sound = p->speed_of_sound;
-    a.num_rirs = p->num_rirs;
-    a.num_bins = p->num_bins;
-    a.spb = p->samples_per_bin;
-    a.sample_rate = p->sample_rate;
-    unsigned char *ws = static_cast<unsigned char *>(scratch);
-    double *amps = reinterpret_cast<double *>(ws + l.amps);
-    double *air = p->air ? nullptr : reinterpret_cast<double *>(ws + l.air);
-    double *wtab = reinterpret_cast<double *>(ws + l.wtab);
-    double *white = p->rng_mode == AC_RNG_PHILOX ? reinterpret_cast<double *>(ws + l.white) : nullptr;
-    double *raw = reinterpret_cast<double *>(ws + l.raw);
-    cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
-    const size_t cells = static_cast<size_t>(p->num_rirs) * 6 * p->num_bins;
-    const size_t work = std::max<size_t>(cells, static_cast<size_t>(white ? N : p->samples_per_bin));
-    const int grid = static_cast<int>(std::min<size_t>((work + 255) / 256, 8192));
-    ac::synth_prepare_kernel<<<grid, 256, 0, stream>>>(echograms, p->direct_delays, a, amps, air, wtab, white, p->seed);
-    AC_CUDA_TRY(cudaGetLastError());
-    const double *air_table = p->air ? p->air : air;
-    const double *noise = white ? white : p->white;
-    const size_t stride = (white || p->white_shared) ? 0 : static_cast<size_t>(N);
-    const size_t samples = static_cast<size_t>(p->num_rirs) * 6 * static_cast<size_t>(N);
-    const int raw_grid = static_cast<int>(std::min<size_t>((samples + 255) / 256, 65536));
-    ac::synth_raw_kernel<<<raw_grid, 256, 0, stream>>>(amps, air_table, wtab, noise, stride, a, raw);
-    AC_CUDA_TRY(cudaGetLastError());
-    const int warps = (p->num_rirs * 6 + 3) / 4;
-    ac::synth_filter_kernel<<<warps, 32, 0, stream>>>(raw, a, band_irs);
-    AC_CUDA_TRY(cudaGetLastError());
-    return AC_OK;
+    return ac::enqueue_synthesis(echograms, p, band_irs, static_cast<unsigned char *>(scratch), l,
+                                 static_cast<cudaStream_t>(stream_ptr));
 }

@@ -127,7 +127,7 @@ def scene_surfaces(scene: Any) -> tuple[list[str], np.ndarray]:
 def _device_scene_and_tables(scene: Any, device_id: int) -> tuple[runtime.DeviceScene, DirectTables]:
     from acoustic_agent_b200 import backend
     arrays = backend._scene_arrays(scene)
-    device_scene, _ = backend.SCENES.get(arrays, device_id)
+    device_scene, _ = backend.SCENES.acquire(arrays, device_id)
     key = (id(scene), device_id)
     with _TABLES_LOCK:
         hit = _TABLES.get(key)
@@ -147,9 +147,13 @@ def simulate_direct_batch(scene: Any, pairs: Sequence[tuple[Sequence[float], Seq
     """simulate_direct for many (source, listener) pairs of one scene, with one GPU launch for all of them."""
     device_id = int(getattr(config, "rt_cuda_device", 0))
     runtime.require_cuda(device_id)
+    from acoustic_agent_b200 import backend
     with torch.cuda.device(device_id):
         device_scene, tables = _device_scene_and_tables(scene, device_id)
-        return direct_results(device_scene, tables, pairs, config, source_model)
+        try:
+            return direct_results(device_scene, tables, pairs, config, source_model)
+        finally:
+            backend.SCENES.release(device_scene)
 
 
 def direct_results(device_scene: runtime.DeviceScene, tables: DirectTables,

@@ -113,9 +113,14 @@ class DeviceScene:
         self.bvh_depth = int(info.bvh_depth)
         self.bvh_nodes = int(info.bvh_nodes)
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
+        # events recorded after CUDA-graph replays that read this scene (the library tracks eager launches
+        # itself, not work captured into a graph); close() waits for them
+        self.graph_guards: list[torch.cuda.Event] = []
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:
+            for event in getattr(self, "graph_guards", ()):
+                event.synchronize()
             _lib.load().ac_scene_destroy(self.handle)
             self.handle = ctypes.c_void_p()
 
@@ -206,13 +211,20 @@ def reference_stream(spec: TraceSpec, device: torch.device) -> tuple[torch.Tenso
     key = ("stream", int(spec.num_rays), int(spec.num_bounces), NUM_BANK, int(spec.seed), spec.dtype, device.index)
 
     def build():
-        directions = rng.sphere_samples(spec.num_rays, spec.seed)
-        random_values, indices = rng.diffuse_random_sequence(spec.num_rays, spec.num_bounces, NUM_BANK, spec.seed)
-        # numpy may hand out read-only views; torch wants writable host memory to copy from
-        host = [np.array(a, copy=True) for a in (directions, random_values, indices)]
-        return (torch.as_tensor(host[0], dtype=spec.dtype, device=device),
-                torch.as_tensor(host[1], dtype=spec.dtype, device=device),
-                torch.as_tensor(host[2], dtype=torch.int32, device=device))
+        # directions (cos/sin of the host's libm, 24 bytes per ray) are drawn on the host; the per-bounce
+        # uniforms and bank indices (12 bytes per ray-bounce) on the device, the same draws bit for bit
+        directions = torch.as_tensor(np.array(rng.sphere_samples(spec.num_rays, spec.seed), copy=True),
+                                     dtype=spec.dtype, device=device)
+        drawn = rng.device_diffuse_random_sequence(spec.num_rays, spec.num_bounces, NUM_BANK, spec.seed,
+                                                   dtype=spec.dtype, device=device)
+        if drawn is None:
+            random_values, indices = rng.diffuse_random_sequence(spec.num_rays, spec.num_bounces, NUM_BANK,
+                                                                 spec.seed)
+            drawn = (torch.as_tensor(np.array(random_values, copy=True), dtype=spec.dtype, device=device),
+                     torch.as_tensor(np.array(indices, copy=True), dtype=torch.int32, device=device))
+        # the cached tensors may be read from any stream next: finish drawing them first
+        torch.cuda.current_stream(device).synchronize()
+        return (directions, *drawn)
 
     return STREAMS.get(key, build)
 
@@ -286,8 +298,11 @@ class TraceBuffers:
         return o
 
 
-def params_struct(spec: TraceSpec, device: torch.device,
-                  keepalive: list[Any] | None = None) -> _lib.ACTraceParams:
+def params_struct(spec: TraceSpec, device: torch.device, keepalive: list[Any] | None = None,
+                  workspace: tuple[torch.Tensor, torch.Tensor, torch.Tensor] | None = None) -> _lib.ACTraceParams:
+    """ac_trace_params for `spec`.  In reference-stream mode the random workspace is the reference's own
+    (generated from the seed and cached), or `workspace` = (directions [R,3], uniforms [B,R], bank indices
+    [B,R]) already on the device in the trace's precision (int32 indices)."""
     p = _lib.ACTraceParams()
     p.source[:] = [float(v) for v in spec.source]
     p.listener[:] = [float(v) for v in spec.listener]
@@ -319,7 +334,17 @@ def params_struct(spec: TraceSpec, device: torch.device,
     p.diffuse_bank = bank.data_ptr()
     p.num_bank = NUM_BANK
     if spec.rng == "reference":
-        directions, random_values, indices = reference_stream(spec, device)
+        if workspace is not None:
+            directions, random_values, indices = workspace
+            R, B = int(spec.num_rays), int(spec.num_bounces)
+            if (tuple(directions.shape) != (R, 3) or tuple(random_values.shape) != (B, R)
+                    or tuple(indices.shape) != (B, R) or directions.dtype != spec.dtype
+                    or random_values.dtype != spec.dtype or indices.dtype != torch.int32
+                    or not all(t.is_cuda and t.is_contiguous() for t in workspace)):
+                raise ValueError("workspace must be contiguous device tensors: directions [R,3] and uniforms "
+                                 "[B,R] in the trace's precision, bank indices [B,R] int32")
+        else:
+            directions, random_values, indices = reference_stream(spec, device)
         p.directions = directions.data_ptr()
         p.diffuse_random = random_values.data_ptr()
         p.diffuse_indices = indices.data_ptr()
@@ -336,15 +361,17 @@ def params_struct(spec: TraceSpec, device: torch.device,
 
 
 def trace(scene: DeviceScene, spec: TraceSpec, buffers: TraceBuffers | None = None, *,
-          stream: torch.cuda.Stream | None = None, record_rays: bool = False) -> TraceBuffers:
-    """Launch one trace asynchronously on `stream` and return its device buffers."""
+          stream: torch.cuda.Stream | None = None, record_rays: bool = False,
+          workspace: tuple[torch.Tensor, torch.Tensor, torch.Tensor] | None = None) -> TraceBuffers:
+    """Launch one trace asynchronously on `stream` and return its device buffers (`workspace`: see
+    params_struct)."""
     device = require_cuda(scene.device)
     if buffers is None:
         buffers = TraceBuffers.allocate(scene.num_surfaces, int(spec.num_bins), device,
                                         ambisonics=spec.render_ambisonics,
                                         record_rays=(int(spec.num_rays), int(spec.num_bounces)) if record_rays else None)
     keep: list[Any] = []
-    params = params_struct(spec, device, keep)
+    params = params_struct(spec, device, keep, workspace)
     outputs = buffers.outputs_struct()
     _lib.check(_lib.load().ac_trace(scene.handle, ctypes.byref(params), ctypes.byref(outputs), _stream_ptr(stream)),
                "ac_trace")

@@ -156,8 +156,10 @@ class SceneCache:
         self.entries: OrderedDict[str, runtime.DeviceScene] = OrderedDict()
         self.refs: dict[str, int] = {}
         # compiled arrays by the identity of the workload's spec dict; the spec is kept with its
-        # entry, so an id reused by a later object can never alias an earlier scene
-        self.arrays: dict[int, tuple[Any, str, SceneArrays]] = {}
+        # entry, so an id reused by a later object can never alias an earlier scene.  Entries go
+        # when their scene is evicted, and the map keeps at most `max_arrays` (least recent out).
+        self.arrays: OrderedDict[int, tuple[Any, str, SceneArrays]] = OrderedDict()
+        self.max_arrays = 1024
         self.hits = self.misses = self.evictions = 0
 
     def resident_bytes(self) -> int:
@@ -169,6 +171,10 @@ class SceneCache:
             arrays = compile_scene(w.spec)
             entry = (w.spec, autotune.fingerprint(arrays), arrays)
             self.arrays[id(w.spec)] = entry
+            while len(self.arrays) > self.max_arrays:
+                self.arrays.popitem(last=False)
+        else:
+            self.arrays.move_to_end(id(w.spec))
         return entry[1], entry[2]
 
     def is_resident(self, w: Workload) -> bool:
@@ -206,6 +212,8 @@ class SceneCache:
             freed += scene.device_bytes
             scene.close()
             self.evictions += 1
+            for spec_id in [i for i, e in self.arrays.items() if e[1] == key]:
+                del self.arrays[spec_id]
         return freed
 
     def close(self) -> None:

@@ -280,7 +280,13 @@ int ac_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_majo
 /* The scene's device memory comes from the device's stream-ordered pool, so
  * creating or destroying a scene does not wait for work that other streams
  * have in flight; ac_scene_create returns once the upload is complete.
- * Destroy a scene only after the work that reads it has finished. */
+ * ac_trace, ac_trace_batch and ac_direct record an event after the work they
+ * enqueue on their stream, and ac_scene_destroy frees the scene's memory only
+ * after the last such event of every stream: a scene may be destroyed while
+ * that work is still queued.  Work enqueued while a stream is being captured
+ * into a CUDA graph is not tracked: destroy the scene only after the graph's
+ * last replay has finished.  Destroy each scene once, from one thread, after
+ * every call that uses it has returned. */
 int ac_scene_create(const ac_scene_desc *desc, ac_scene_t *out);
 int ac_scene_destroy(ac_scene_t scene);
 int ac_scene_get_info(ac_scene_t scene, ac_scene_info *info);
@@ -524,6 +530,24 @@ int ac_fp64_rate_probe(int32_t iterations, unsigned long long *sink, int64_t *op
  * of device memory, zeroed by the call. */
 int ac_bvh_barrier_probe(int32_t blocks, int32_t expected_blocks, int64_t poll_limit, void *workspace,
                          int32_t *status, void *stream);
+
+/* The reference's per-bounce random workspace drawn on the device, bit for
+ * bit: replaces the host loop of steam_rt.py:4009-4044
+ * (`_diffuse_random_sequence`: for each bounce, `rng.random(R)` then
+ * `rng.integers(0, num_bank, R, dtype=int32)` from `rng = default_rng(seed + 1)`)
+ * and the upload of its 12 bytes per ray-bounce.  (state, inc) are that
+ * generator's 128-bit PCG64 state and increment before its first draw, split
+ * into 64-bit halves (numpy's `bit_generator.state`).  Writes `random`
+ * [num_bounces, num_rays] (double for AC_PRECISION_FP64, else float, rounded
+ * from the double draw) and `indices` [num_bounces, num_rays] int32, device
+ * memory, asynchronously on `stream`.  num_bank must be a power of two
+ * (AC_ERR_UNSUPPORTED otherwise: numpy's bounded draw can then consume an
+ * extra word at an unpredictable place; draw such workspaces on the host);
+ * the default bank of 128 qualifies.  The directions of the same workspace
+ * (steam_rt.py:3959-3968) use the host's cos/sin and stay on the host. */
+int ac_reference_stream(uint64_t state_hi, uint64_t state_lo, uint64_t inc_hi, uint64_t inc_lo, int64_t num_rays,
+                        int32_t num_bounces, int32_t num_bank, int32_t precision, void *random, int32_t *indices,
+                        void *stream);
 
 /* Debug/test: fill the Philox reference-equivalent workspace the kernels
  * generate internally (directions [R,3], random [B,R], indices [B,R]). */

@@ -119,3 +119,34 @@ def test_capacity_and_sizes_are_checked_before_launch(backend):
         runtime.trace(dev, runtime.TraceSpec(num_rays=0, num_bounces=3, **base), buffers)
     torch.cuda.synchronize()
     dev.close()
+
+
+def test_scene_destroyed_while_its_trace_is_queued_keeps_its_result(backend):
+    """A scene may be destroyed right after a trace that reads it is enqueued on a non-blocking stream: its
+    memory returns to the pool only after that trace, so a scene uploaded next (which may get the same block)
+    cannot overwrite it under the running trace.  Repeated a few times to give the pool the chance to reuse."""
+    from acoustic_agent_b200 import runtime, scene, workloads
+    w = workloads.u_furnished(7, rays=100_000, bounces=100, channels=1)
+    other = workloads.u_furnished(8, rays=1000, bounces=10, channels=1)
+    arrays, other_arrays = scene.compile_scene(w.spec), scene.compile_scene(other.spec)
+    cfg = w.config
+    src, lst = np.asarray(w.sources[0]), np.asarray(w.listeners[0])
+    spec = runtime.TraceSpec(source=src, listener=lst, num_rays=cfg.rt_num_rays, num_bounces=cfg.rt_num_bounces,
+                             num_bins=cfg.num_bins, bin_duration=cfg.rt_bin_duration_s, speed_of_sound=cfg.c,
+                             max_path_length=cfg.max_path_length, direct_delay=float(np.linalg.norm(src - lst)) / cfg.c,
+                             precision="float32", rng="philox", seed=cfg.seed, stream_key=5, use_bvh=True)
+    alone = runtime.DeviceScene(arrays, device=0)
+    want = runtime.trace(alone, spec)
+    torch.cuda.synchronize()
+    want_bins = want.echogram_fx.cpu().numpy()
+    alone.close()
+    side = torch.cuda.Stream()
+    for _ in range(3):
+        with torch.cuda.stream(side):
+            doomed = runtime.DeviceScene(arrays, device=0)
+            got = runtime.trace(doomed, spec, stream=side)
+            doomed.close()
+            replacement = runtime.DeviceScene(other_arrays, device=0)
+        side.synchronize()
+        np.testing.assert_array_equal(got.echogram_fx.cpu().numpy(), want_bins)
+        replacement.close()

@@ -86,3 +86,44 @@ def test_static_entry_point_matches_workspace_entry_point_twice():
         torch.cuda.synchronize(dev)
         # the synthesis tests' bar: bit-identical output
         np.testing.assert_array_equal(out.cpu().numpy(), reference)
+
+
+@pytest.mark.gpu
+def test_static_entry_point_with_philox_noise_and_delay_derived_air():
+    """The scratch regions the reference-noise case leaves unused: Philox noise drawn into the scratch and the
+    air-absorption table built there from each RIR's direct delay (no caller table), two calls in a row."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    s = np.load(GOLDEN / "synthesis.npz")
+    fs, bin_dur, delay, seed = s["furnished_f32_meta"]
+    fs = int(fs)
+    echogram = s["furnished_f32_input"]
+    nb = echogram.shape[1]
+    n = nb * bands.samples_per_bin(float(bin_dur), fs)
+    dev = torch.device("cuda", 0)
+    echo = torch.as_tensor(np.stack([echogram, echogram * 0.5]).astype(np.float32), device=dev)
+    delays = torch.tensor([float(delay), 0.5 * float(delay)], dtype=torch.float64, device=dev)
+    p = _params(2, nb, float(bin_dur), fs, None, None)
+    p.rng_mode = _lib.AC_RNG_PHILOX
+    p.seed = int(seed) + 7
+    p.direct_delays = delays.data_ptr()
+    lib = _lib.load()
+    size = ctypes.c_size_t()
+    _lib.check(lib.ac_synth_workspace_size(ctypes.byref(p), ctypes.byref(size)), "ac_synth_workspace_size")
+    assert size.value <= _lib.AC_SYNTH_STATIC_BYTES
+    workspace = torch.empty(size.value, dtype=torch.uint8, device=dev)
+    expected = torch.empty(2, 6, n, dtype=torch.float32, device=dev)
+    stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    _lib.check(lib.ac_synthesize(ctypes.c_void_p(echo.data_ptr()), ctypes.byref(p),
+                                 ctypes.c_void_p(expected.data_ptr()), ctypes.c_void_p(workspace.data_ptr()),
+                                 size.value, stream), "ac_synthesize")
+    torch.cuda.synchronize(dev)
+    reference = expected.cpu().numpy()
+    assert np.isfinite(reference).all() and np.abs(reference).max() > 0.0
+    for _ in range(2):
+        out = torch.full((2, 6, n), float("nan"), dtype=torch.float32, device=dev)
+        _lib.check(lib.ac_synthesize_static(ctypes.c_void_p(echo.data_ptr()), ctypes.byref(p),
+                                            ctypes.c_void_p(out.data_ptr()), stream), "ac_synthesize_static")
+        torch.cuda.synchronize(dev)
+        np.testing.assert_array_equal(out.cpu().numpy(), reference)
