@@ -86,6 +86,42 @@ def diffuse_random_sequence(num_rays: int, num_bounces: int, sample_count: int, 
     return random_values, sample_indices
 
 
+def pcg64_state(seed: int) -> tuple[int, int]:
+    """(state, increment) of numpy's ``default_rng(seed)`` PCG64 before its first draw, as 128-bit integers."""
+    st = np.random.default_rng(int(seed)).bit_generator.state
+    if st["bit_generator"] != "PCG64" or st["has_uint32"]:
+        raise RuntimeError("numpy's default generator is not a fresh PCG64")
+    return int(st["state"]["state"]), int(st["state"]["inc"])
+
+
+def device_diffuse_random_sequence(num_rays: int, num_bounces: int, sample_count: int, seed: int, *, dtype, device,
+                                   stream=None):
+    """`diffuse_random_sequence` drawn on the device (ac_reference_stream), bit for bit the same draws.
+
+    Returns (uniforms [B, R] in `dtype`, bank indices [B, R] int32) as device tensors, or None when the bank
+    size is not a power of two (numpy can then redraw a word, which only the host sequence reproduces).
+    """
+    import ctypes
+
+    import torch
+
+    from acoustic_agent_b200 import _lib
+    if sample_count < 1 or sample_count & (sample_count - 1):
+        return None
+    state, inc = pcg64_state(int(seed) + 1)
+    mask = (1 << 64) - 1
+    random_values = torch.empty(int(num_bounces), int(num_rays), dtype=dtype, device=device)
+    indices = torch.empty(int(num_bounces), int(num_rays), dtype=torch.int32, device=device)
+    s = stream if stream is not None else torch.cuda.current_stream(device)
+    precision = _lib.AC_PRECISION_FP64 if dtype == torch.float64 else _lib.AC_PRECISION_FP32
+    _lib.check(_lib.load().ac_reference_stream(state >> 64, state & mask, inc >> 64, inc & mask, int(num_rays),
+                                               int(num_bounces), int(sample_count), precision,
+                                               ctypes.c_void_p(random_values.data_ptr()),
+                                               ctypes.c_void_p(indices.data_ptr()), ctypes.c_void_p(s.cuda_stream)),
+               "ac_reference_stream")
+    return random_values, indices
+
+
 def reference_white_noise(num_samples: int, seed: int) -> np.ndarray:
     """Coherent band noise of reconstruct_band_irs: default_rng(seed + 7).uniform(-1, 1) (steam_rt.py:2209-2210)."""
     rng = np.random.default_rng(int(seed) + 7)

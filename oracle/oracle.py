@@ -67,7 +67,7 @@ class _Outputs(ctypes.Structure):
                 ("surface_energy", _d), ("actual_bounces", ctypes.c_int64), ("active_count", ctypes.c_int64),
                 ("ray_surfaces", _i32), ("ray_bounces", _i32), ("closest_queries", ctypes.c_int64),
                 ("shadow_queries", ctypes.c_int64), ("nodes_visited", ctypes.c_int64),
-                ("prims_tested", ctypes.c_int64 * 3), ("polygon_edges", ctypes.c_int64)]
+                ("prims_tested", ctypes.c_int64 * 3), ("polygon_edges", ctypes.c_int64), ("ray_states", _d)]
 
 
 def build(force: bool = False) -> Path:
@@ -95,6 +95,9 @@ def _lib() -> ctypes.CDLL:
         lib.oracle_trace.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Params), ctypes.POINTER(_Outputs)]
         lib.oracle_closest_hit.restype = ctypes.c_int
         lib.oracle_closest_hit.argtypes = [ctypes.POINTER(_Scene), _d, _d, _d, _d]
+        lib.oracle_bounce_outcome.restype = ctypes.c_int64
+        lib.oracle_bounce_outcome.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Params), _d, _d,
+                                              ctypes.c_double, ctypes.c_int64, _d]
         lib.oracle_synthesize.restype = ctypes.c_int
         lib.oracle_synthesize.argtypes = [_d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _d, _d, _d, _f32]
         lib.oracle_bandlimit.restype = ctypes.c_int
@@ -145,8 +148,12 @@ def trace(arrays: Mapping[str, Any], *, source, listener, directions, diffuse_ba
           listener_radius: float = 0.1, source_radius: float = 0.1, irradiance_min_distance: float = 1.0,
           specular_exponent: float = 100.0, source_forward=(1.0, 0.0, 0.0), dipole_weight: float = 0.0,
           dipole_power: float = 1.0, use_bvh: bool = False, render_ambisonics: bool = False, threads: int = 0,
-          record_rays: bool = False) -> dict[str, Any]:
-    """float64 trace of steam_rt.py:4708-4850 (plus per-ray hit sequences and traversal counts)."""
+          record_rays: bool = False, record_states: bool = False) -> dict[str, Any]:
+    """float64 trace of steam_rt.py:4708-4850 (plus per-ray hit sequences and traversal counts).
+
+    `record_states` adds ``ray_states`` [R, B, 7]: each ray's origin, direction and path length before
+    every closest-hit query (NaN after it ends).
+    """
     scene = Scene(arrays, use_bvh)
     dirs = np.ascontiguousarray(directions, dtype=np.float64)
     bank = np.ascontiguousarray(diffuse_bank, dtype=np.float64)
@@ -181,6 +188,8 @@ def trace(arrays: Mapping[str, Any], *, source, listener, directions, diffuse_ba
     out.hit_counts, out.contrib_counts, out.surface_energy = _p(hits, _i64), _p(contrib, _i64), _p(energy, _d)
     out.ray_surfaces = _p(ray_surfaces, _i32) if record_rays else None
     out.ray_bounces = _p(ray_bounces, _i32) if record_rays else None
+    ray_states = np.zeros((R, B, 7)) if record_states else None
+    out.ray_states = _p(ray_states, _d) if record_states else None
     rc = _lib().oracle_trace(ctypes.byref(scene.struct), ctypes.byref(params), ctypes.byref(out))
     if rc != 0:
         raise RuntimeError(f"oracle_trace failed ({rc})")
@@ -194,7 +203,99 @@ def trace(arrays: Mapping[str, Any], *, source, listener, directions, diffuse_ba
     if record_rays:
         result["ray_surfaces"] = ray_surfaces
         result["ray_bounces"] = ray_bounces
+    if record_states:
+        result["ray_states"] = ray_states
     return result
+
+
+def first_divergence(a: np.ndarray, b: np.ndarray) -> np.ndarray:
+    """Per ray, the first bounce where two [R, B] hit-surface sequences differ (-1: identical)."""
+    diff = np.asarray(a) != np.asarray(b)
+    first = np.argmax(diff, axis=1)
+    return np.where(diff.any(axis=1), first, -1)
+
+
+def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfaces: np.ndarray,
+                      ref_surfaces: np.ndarray, directions, diffuse_bank, diffuse_random, diffuse_indices,
+                      trials: int = 48, origin_eps: float = 4e-6, direction_eps: float = 4e-7, seed: int = 0,
+                      **trace_kwargs) -> dict[str, Any]:
+    """Why a float32 trace left the float64 one on each of `rays` (rays whose hit sequences differ).
+
+    At the first differing bounce the float64 state (origin, direction, path length) is taken from this
+    oracle.  The divergence is a precision tie when the float64 decision at that bounce is not robust to
+    perturbations of float32 size: moving the origin by up to origin_eps x (bounce + 1) metres and turning
+    the direction by up to direction_eps x (bounce + 1) radians, in `trials` seeded random ways, gives the
+    float32 trace's outcome at least once (a grazing hit, an edge or corner, two surfaces at the same
+    distance, a sphere or path-length threshold).  It is a diffuse-threshold tie when, at a bounce up to
+    that one, the ray's uniform draw lies within float32 rounding of the surface's scattering, so the two
+    traces chose different reflection kinds on the same surface.  Anything else is counted as unexplained.
+    """
+    rays = np.asarray(rays, dtype=np.int64)
+    dirs = np.ascontiguousarray(np.asarray(directions, dtype=np.float64)[rays])
+    rnd = np.ascontiguousarray(np.asarray(diffuse_random, dtype=np.float64)[:, rays])
+    idx = np.ascontiguousarray(np.asarray(diffuse_indices, dtype=np.int32)[:, rays])
+    sub = trace(arrays, directions=dirs, diffuse_bank=diffuse_bank, diffuse_random=rnd, diffuse_indices=idx,
+                record_rays=True, record_states=True, threads=1, **trace_kwargs)
+    scene = Scene(arrays, bool(trace_kwargs.get("use_bvh", False)))
+    params = _Params()
+    params.source[:] = [float(v) for v in trace_kwargs["source"]]
+    params.listener[:] = [float(v) for v in trace_kwargs["listener"]]
+    params.max_path_len = float(trace_kwargs["max_path_len"])
+    params.listener_radius = float(trace_kwargs.get("listener_radius", 0.1))
+    params.source_radius = float(trace_kwargs.get("source_radius", 0.1))
+    scattering = np.asarray(arrays["scattering"], dtype=np.float64)
+    rng = np.random.default_rng(seed)
+    causes = {"precision_tie": 0, "diffuse_threshold_tie": 0, "path_length_tie": 0, "unexplained": 0}
+    unexplained: list[int] = []
+    t = np.zeros(1)
+    for k, ray in enumerate(rays):
+        ref_seq = np.asarray(ref_surfaces[ray])
+        if not np.array_equal(sub["ray_surfaces"][k], ref_seq):
+            raise AssertionError("the oracle traced a ray differently alone")
+        b = int(first_divergence(np.asarray(gpu_surfaces[ray])[None], ref_seq[None])[0])
+        want = int(gpu_surfaces[ray][b])
+        # reflection kind chosen on a float32 rounding edge at an earlier bounce (or at this one)
+        threshold = False
+        for j in range(b):   # the reflection kind chosen after bounce j sets the direction of bounce j + 1
+            s = int(ref_seq[j])
+            if abs(float(rnd[j, k]) - float(scattering[s])) <= 2.0 ** -22 * max(1.0, abs(scattering[s])):
+                threshold = True
+        if threshold:
+            causes["diffuse_threshold_tie"] += 1
+            continue
+        state = sub["ray_states"][k, b]
+        if not np.isfinite(state).all():
+            # the float64 ray ended after bounce b - 1 because its path grew past the limit
+            prev = sub["ray_states"][k, b - 1]
+            _lib().oracle_bounce_outcome(ctypes.byref(scene.struct), ctypes.byref(params),
+                                         _p(np.ascontiguousarray(prev[:3]), _d), _p(np.ascontiguousarray(prev[3:6]), _d),
+                                         float(prev[6]), b - 1, _p(t, _d))
+            end = float(prev[6]) + float(t[0])
+            if abs(end - params.max_path_len) <= 1e-5 * params.max_path_len * b:
+                causes["path_length_tie"] += 1
+            else:
+                causes["unexplained"] += 1
+                unexplained.append(int(ray))
+            continue
+        o, d, dist = state[:3], state[3:6], float(state[6])
+        tie = False
+        for _ in range(trials):
+            u = rng.normal(size=3)
+            v = rng.normal(size=3)
+            o2 = np.ascontiguousarray(o + origin_eps * (b + 1) * rng.uniform() * u / np.linalg.norm(u))
+            d2 = d + direction_eps * (b + 1) * rng.uniform() * v / np.linalg.norm(v)
+            d2 = np.ascontiguousarray(d2 / np.linalg.norm(d2))
+            got = _lib().oracle_bounce_outcome(ctypes.byref(scene.struct), ctypes.byref(params), _p(o2, _d),
+                                               _p(d2, _d), dist, b, _p(t, _d))
+            if int(got) == want:
+                tie = True
+                break
+        if tie:
+            causes["precision_tie"] += 1
+        else:
+            causes["unexplained"] += 1
+            unexplained.append(int(ray))
+    return {"rays": int(rays.size), **causes, "unexplained_rays": unexplained}
 
 
 def synthesize(echogram: np.ndarray, *, fs: int, bin_dur: float, direct_delay: float, c: float,
@@ -614,3 +715,54 @@ def late_reverb(traced: np.ndarray, bin_duration_s: float, rt60_bands: Mapping[s
     out += comp
     return out.astype(np.float32), comp.astype(np.float32), {"scales": scales, "powers": powers,
                                                              "starts": starts, "ends": ends}
+
+
+# ---------------------------------------------------------------------------
+# numpy's PCG64 (O'Neill 2014), restated with Python integers: pins the draw positions the device
+# fill of the reference's random workspace uses (steam_rt.py:4009-4044 `_diffuse_random_sequence`).
+
+PCG64_MULTIPLIER = 0x2360ED051FC65DA44385DF649FCCF645
+
+
+def pcg64_outputs(state: int, inc: int, first: int, count: int) -> list[int]:
+    """Outputs `first` .. `first + count - 1` of the generator with the given 128-bit state and increment
+    (each output: one LCG step, then XSL-RR of the new state), reached by Brown's arbitrary-stride jump."""
+    mask = (1 << 128) - 1
+    am, ap, m, c, steps = 1, 0, PCG64_MULTIPLIER, inc, first + 1
+    while steps:
+        if steps & 1:
+            am, ap = (am * m) & mask, (ap * m + c) & mask
+        c, m, steps = ((m + 1) * c) & mask, (m * m) & mask, steps >> 1
+    s = (am * state + ap) & mask
+    out = []
+    for _ in range(count):
+        rot = s >> 122
+        x = ((s >> 64) ^ s) & ((1 << 64) - 1)
+        out.append(((x >> rot) | (x << ((64 - rot) & 63))) & ((1 << 64) - 1))
+        s = (s * PCG64_MULTIPLIER + inc) & mask
+    return out
+
+
+def pcg64_reference_stream(num_rays: int, num_bounces: int, seed: int, bank_size: int = 128):
+    """The uniforms [B, R] and bank indices [B, R] of `_diffuse_random_sequence`, each draw taken from its
+    position in the PCG64 output sequence (power-of-two banks: numpy's Lemire map never redraws)."""
+    if bank_size & (bank_size - 1):
+        raise ValueError("positions are fixed only for power-of-two banks")
+    st = np.random.default_rng(int(seed) + 1).bit_generator.state["state"]
+    state, inc = int(st["state"]), int(st["inc"])
+    R, B = int(num_rays), int(num_bounces)
+    u = 1 if bank_size > 1 else 0
+    shift = bank_size.bit_length() - 1
+    rnd = np.empty((B, R))
+    idx = np.zeros((B, R), np.int32)
+    for b in range(B):
+        first = b * R + (b * R * u + 1) // 2
+        rnd[b] = [(x >> 11) * 2.0 ** -53 for x in pcg64_outputs(state, inc, first, R)]
+        if u:
+            for r in range(R):
+                k = b * R + r
+                p = k >> 1
+                x = pcg64_outputs(state, inc, (2 * p // R + 1) * R + p, 1)[0]
+                word = (x >> 32) if k & 1 else (x & 0xFFFFFFFF)
+                idx[b, r] = (word << shift) >> 32
+    return rnd, idx

@@ -111,6 +111,9 @@ typedef struct {
     int64_t nodes_visited;
     int64_t prims_tested[3];
     int64_t polygon_edges;
+    /* [R,B,7] or NULL: the ray's state before each closest-hit query (origin xyz, direction xyz, path
+     * length so far), NaN once the ray has ended; for locating where a float32 trace parts from this one */
+    double *ray_states;
 } oracle_outputs;
 
 typedef struct {
@@ -373,8 +376,15 @@ int oracle_trace(const oracle_scene *sc, const oracle_params *p, oracle_outputs 
         int32_t queries = 0;
         if (out->ray_surfaces)
             for (int64_t b = 0; b < B; ++b) out->ray_surfaces[ri * B + b] = -1;
+        if (out->ray_states)
+            for (int64_t k = 0; k < B * 7; ++k) out->ray_states[ri * B * 7 + k] = NAN;
         for (int64_t bounce = 0; bounce < B; ++bounce) {
             if (bounce + 1 > l_bounces[tid]) l_bounces[tid] = bounce + 1;
+            if (out->ray_states) {
+                double *rs = out->ray_states + (ri * B + bounce) * 7;
+                rs[0] = origin[0]; rs[1] = origin[1]; rs[2] = origin[2];
+                rs[3] = dir[0]; rs[4] = dir[1]; rs[5] = dir[2]; rs[6] = accum_distance;
+            }
             double t, n[3];
             int64_t surf = closest_hit(sc, origin, dir, &t, n, st);
             l_closest[tid] += 1;
@@ -490,6 +500,29 @@ int oracle_trace(const oracle_scene *sc, const oracle_params *p, oracle_outputs 
     free(l_echo); free(l_amb); free(l_hits); free(l_contrib); free(l_energy); free(l_active);
     free(l_bounces); free(l_stats); free(l_closest); free(l_shadow);
     return 0;
+}
+
+/* The decision at the top of one bounce of oracle_trace (steam_rt.py:4743-4760) from a given ray state:
+ * the closest surface, or -1 when the ray ends there (no hit, t within the listener radius, path too
+ * long, or, after the first bounce, the listener or source sphere in front of the hit). */
+int64_t oracle_bounce_outcome(const oracle_scene *sc, const oracle_params *p, const double *origin,
+                              const double *dir, double accum_distance, int64_t bounce, double *t_out)
+{
+    visit_stats st = {0, {0, 0, 0}, 0};
+    double t, n[3];
+    const double *src = p->source, *lst = p->listener;
+    int64_t surf = closest_hit(sc, origin, dir, &t, n, &st);
+    *t_out = t;
+    if (surf < 0 || t <= p->listener_radius || accum_distance > p->max_path_len) return -1;
+    if (bounce > 0) {
+        if (sphere_before(origin, dir, lst[0], lst[1], lst[2], p->listener_radius, t)) return -1;
+        double dx = lst[0] - src[0], dy = lst[1] - src[1], dz = lst[2] - src[2];
+        double source_distance = sqrt(dx * dx + dy * dy + dz * dz);
+        if (source_distance > p->source_radius && sphere_before(origin, dir, src[0], src[1], src[2],
+                                                                p->source_radius, t))
+            return -1;
+    }
+    return surf;
 }
 
 /* steam_rt.py:4131-4146: one biquad section; state in double, output rounded to float32. */

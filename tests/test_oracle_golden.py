@@ -125,3 +125,26 @@ def test_reference_rt60_fit_restatement_on_a_known_decay():
     energy = 10.0 ** (-6.0 * t / rt60)          # -60 dB per rt60 seconds
     assert abs(metrics.schroeder_rt60(energy, bin_dur) - rt60) < 1e-3
     assert metrics.schroeder_rt60(np.zeros(10), bin_dur) == 0.0
+
+
+@pytest.mark.parametrize("rays,bounces,seed,bank", [(7, 5, 1729, 128), (64, 3, 3, 128), (33, 4, 99, 64),
+                                                     (10, 3, 5, 1), (1, 6, 8, 2)])
+def test_pcg64_draw_positions_equal_numpy(rays, bounces, seed, bank):
+    """Each uniform and bank index of the reference's workspace sits at a fixed position of the PCG64 output
+    sequence (odd ray counts carry a buffered half word across bounces; a one-entry bank draws no words)."""
+    from oracle import oracle
+    rnd, idx = oracle.pcg64_reference_stream(rays, bounces, seed, bank)
+    g = np.random.default_rng(seed + 1)
+    for b in range(bounces):
+        np.testing.assert_array_equal(rnd[b], g.random(rays))
+        np.testing.assert_array_equal(idx[b], g.integers(0, bank, size=rays, dtype=np.int32))
+
+
+def test_pcg64_draw_positions_equal_golden_workspace():
+    """The reference's own workspace (1,000 rays x 5 bounces, seed 1729, written by its
+    `_diffuse_random_sequence`) from the position restatement."""
+    from oracle import oracle
+    g = np.load(GOLDEN / "workspace.npz")
+    rnd, idx = oracle.pcg64_reference_stream(1000, 5, 1729, 128)
+    np.testing.assert_array_equal(rnd, g["random"])
+    np.testing.assert_array_equal(idx, g["indices"])
