@@ -39,19 +39,25 @@ int fast_grid(FastKernel kernel, int device, int block, int64_t total_rays, int 
 }
 
 // Workspace layout for a float32 batch (each part 256-aligned):
-//   [0] chunk counter | ray prefix int64[J+1] | Job<float>[J] | FinalizeTargets[J] | FastGroup[G] | FastChunk[NC]
+//   [0] chunk counter | group queue counters u64[G] | ray prefix int64[J+1] | Job<float>[J] |
+//   FinalizeTargets[J] | FastGroup[G] | FastChunk[NC] | group chunk prefix int64[G+1] | group ray prefix int64[G+1]
+// Everything from the ray prefix on is staged on the host and copied in one transfer; the counters are zeroed
+// on the device.
 struct F32Layout {
-    size_t prefix, jobs, targets, groups, chunks, total;
+    size_t queues, prefix, jobs, targets, groups, chunks, group_chunks, group_rays, total;
 };
 
 F32Layout f32_layout(int32_t jobs, int64_t groups, int64_t chunks) {
     F32Layout l{};
     size_t off = 256;
-    l.prefix = off;  off = align256(off + sizeof(int64_t) * (static_cast<size_t>(jobs) + 1));
-    l.jobs = off;    off = align256(off + sizeof(Job<float>) * static_cast<size_t>(jobs));
-    l.targets = off; off = align256(off + sizeof(FinalizeTargets) * static_cast<size_t>(jobs));
-    l.groups = off;  off = align256(off + sizeof(FastGroup) * static_cast<size_t>(groups));
-    l.chunks = off;  off = align256(off + sizeof(FastChunk) * static_cast<size_t>(chunks));
+    l.queues = off;       off = align256(off + sizeof(unsigned long long) * static_cast<size_t>(groups));
+    l.prefix = off;       off = align256(off + sizeof(int64_t) * (static_cast<size_t>(jobs) + 1));
+    l.jobs = off;         off = align256(off + sizeof(Job<float>) * static_cast<size_t>(jobs));
+    l.targets = off;      off = align256(off + sizeof(FinalizeTargets) * static_cast<size_t>(jobs));
+    l.groups = off;       off = align256(off + sizeof(FastGroup) * static_cast<size_t>(groups));
+    l.chunks = off;       off = align256(off + sizeof(FastChunk) * static_cast<size_t>(chunks));
+    l.group_chunks = off; off = align256(off + sizeof(int64_t) * (static_cast<size_t>(groups) + 1));
+    l.group_rays = off;   off = align256(off + sizeof(int64_t) * (static_cast<size_t>(groups) + 1));
     l.total = off;
     return l;
 }
@@ -146,11 +152,15 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
     FinalizeTargets *targets = reinterpret_cast<FinalizeTargets *>(host + l.targets);
     FastGroup *groups = reinterpret_cast<FastGroup *>(host + l.groups);
     FastChunk *chunks = reinterpret_cast<FastChunk *>(host + l.chunks);
+    int64_t *group_chunks = reinterpret_cast<int64_t *>(host + l.group_chunks);
+    int64_t *group_rays = reinterpret_cast<int64_t *>(host + l.group_rays);
     int device = -1;
     int64_t total = 0, g = -1, c = 0;
     const ac_scene_s *current = nullptr;
     int64_t group_begin = 0;
     auto close_group = [&](int64_t group_end) {
+        group_chunks[g] = c;
+        group_rays[g] = group_begin;
         for (int64_t b = group_begin; b < group_end; b += chunk_rays)
             chunks[c++] = FastChunk{b, std::min(b + chunk_rays, group_end), static_cast<int32_t>(g), 0};
     };
@@ -182,10 +192,13 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
     }
     if (g >= 0) close_group(total);
     prefix[count] = total;
+    group_chunks[num_groups] = c;
+    group_rays[num_groups] = total;
     AC_CUDA_TRY(cudaSetDevice(device));
     unsigned char *ws = static_cast<unsigned char *>(workspace);
     AC_CUDA_TRY(cudaMemcpyAsync(ws + l.prefix, host + l.prefix, l.total - l.prefix, cudaMemcpyHostToDevice, stream));
     if (!host_staging) AC_CUDA_TRY(cudaStreamSynchronize(stream));
+    AC_CUDA_TRY(cudaMemsetAsync(ws + l.queues, 0, sizeof(unsigned long long) * static_cast<size_t>(num_groups), stream));
     const Job<float> *d_jobs = reinterpret_cast<const Job<float> *>(ws + l.jobs);
     unsigned long long *counter = reinterpret_cast<unsigned long long *>(ws);
     {
@@ -205,6 +218,10 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         table.num_jobs = count;
         table.chunk_rays = static_cast<int32_t>(chunk_rays);
         table.chunk_counter = counter;
+        table.group_next = reinterpret_cast<unsigned long long *>(ws + l.queues);
+        table.group_chunk_begin = reinterpret_cast<const int64_t *>(ws + l.group_chunks);
+        table.group_ray_begin = reinterpret_cast<const int64_t *>(ws + l.group_rays);
+        table.num_groups = static_cast<int32_t>(num_groups);
         Job<float> unused;
         std::memset(&unused, 0, sizeof(unused));
         FastScene none{};

@@ -84,11 +84,21 @@ struct FastTable {
     const Job<float> *jobs;
     const int64_t *ray_begin;      // [num_jobs + 1]
     const FastGroup *groups;
-    const FastChunk *chunks;
+    const FastChunk *chunks;       // group by group
     int64_t num_chunks;
     int32_t num_jobs;
     int32_t chunk_rays;            // single-job launches: rays per chunk
-    unsigned long long *chunk_counter;
+    unsigned long long *chunk_counter;   // single-job launches: next chunk
+    // Batched launches: one chunk queue per scene group.  A warp starts on the
+    // group that holds its share of the rays and stays on it until the group's
+    // chunks run out, then takes the following groups' (wrapping), so a warp
+    // drains its lanes for a change of scene about once per group it visits,
+    // not at every group boundary of one shared queue.
+    unsigned long long *group_next;      // [num_groups] chunks taken from each group
+    const int64_t *group_chunk_begin;    // [num_groups + 1] first chunk of each group
+    const int64_t *group_ray_begin;      // [num_groups + 1] first ray (over all jobs) of each group
+    int32_t num_groups;
+    int32_t reserved;
 };
 
 struct FRay {
@@ -452,6 +462,20 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     int64_t pending = -1;           // chunk of another scene, taken but not started
     bool exhausted = false;
     const int64_t num_chunks = kSingle ? (single.num_rays + table.chunk_rays - 1) / table.chunk_rays : table.num_chunks;
+    int queue = 0;                  // batched launches: the group queue this warp takes chunks from
+    if (!kSingle) {
+        const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+        const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        const int64_t total = __ldg(table.group_ray_begin + table.num_groups);
+        const int64_t at = static_cast<int64_t>((static_cast<double>(warp) + 0.5) / static_cast<double>(warps) *
+                                                static_cast<double>(total));
+        int lo = 0, hi = table.num_groups - 1;
+        while (lo < hi) {   // last group whose first ray is at or before `at`
+            const int mid = (lo + hi + 1) >> 1;
+            if (__ldg(table.group_ray_begin + mid) <= at) lo = mid; else hi = mid - 1;
+        }
+        queue = lo;
+    }
 
     FastLane s;
     bool has = false;
@@ -463,9 +487,31 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         while (need && pending < 0 && !exhausted) {
             if (next >= end) {
                 long long c = 0;
-                if (lane_id == 0) c = static_cast<long long>(atomicAdd(table.chunk_counter, 1ull));
-                c = __shfl_sync(full, c, 0);
-                if (c >= num_chunks) { exhausted = true; break; }
+                if (kSingle) {
+                    if (lane_id == 0) c = static_cast<long long>(atomicAdd(table.chunk_counter, 1ull));
+                    c = __shfl_sync(full, c, 0);
+                    if (c >= num_chunks) { exhausted = true; break; }
+                } else {
+                    // this warp's group queue, then the following groups' until one has chunks left
+                    int probes = 0;
+                    while (true) {
+                        if (lane_id == 0) {
+                            c = -1;
+                            const int64_t first = __ldg(table.group_chunk_begin + queue);
+                            const int64_t count = __ldg(table.group_chunk_begin + queue + 1) - first;
+                            const unsigned long long taken =
+                                *reinterpret_cast<volatile unsigned long long *>(table.group_next + queue);
+                            if (static_cast<int64_t>(taken) < count) {
+                                const int64_t k = static_cast<int64_t>(atomicAdd(table.group_next + queue, 1ull));
+                                if (k < count) c = first + k;
+                            }
+                        }
+                        c = __shfl_sync(full, c, 0);
+                        if (c >= 0 || ++probes >= table.num_groups) break;
+                        queue = queue + 1 == table.num_groups ? 0 : queue + 1;
+                    }
+                    if (c < 0) { exhausted = true; break; }
+                }
                 int64_t cb, ce;
                 int cg;
                 if (kSingle) {

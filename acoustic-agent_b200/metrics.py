@@ -83,3 +83,39 @@ def c50(echogram: np.ndarray, bin_dur: float) -> np.ndarray:
     late = np.sum(e[:, k:], axis=1)
     with np.errstate(divide="ignore"):
         return 10.0 * np.log10(np.where(late > 0, early / np.where(late > 0, late, 1.0), np.inf))
+
+
+def parity(ours: np.ndarray, ref: np.ndarray, bin_dur: float) -> dict:
+    """Worst band of each decay statistic of `ours` against `ref` ([bands, bins] echograms):
+
+    * ``edc_err_db_max``: max |EDC difference| over the first 30 dB of the reference's decay;
+    * ``t30_rel``, ``edt_rel``: max relative difference of T30 and EDT;
+    * ``c50_rel``: max relative difference of the early-to-late energy ratio (the linear C50),
+      ``c50_db``: the same difference in dB;
+    * ``band_energy_rel``: max relative difference of a band's total energy.
+
+    Bands whose reference energy is zero are skipped.
+    """
+    a = np.asarray(ours, dtype=np.float64)
+    b = np.asarray(ref, dtype=np.float64)
+    live = np.sum(b, axis=1) > 0.0
+    if not np.any(live):
+        return {"edc_err_db_max": 0.0, "t30_rel": 0.0, "edt_rel": 0.0, "c50_rel": 0.0, "c50_db": 0.0,
+                "band_energy_rel": 0.0}
+    a, b = a[live], b[live]
+
+    def rel(x, y):
+        x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            r = np.where(y != 0.0, np.abs(x - y) / np.abs(y), np.where(x == y, 0.0, np.inf))
+        return float(np.max(r))
+
+    ca, cb = c50(a, bin_dur), c50(b, bin_dur)
+    return {
+        "edc_err_db_max": float(np.max(edc_error_db(a, b))),
+        "t30_rel": rel(t30(a, bin_dur), t30(b, bin_dur)),
+        "edt_rel": rel(edt(a, bin_dur), edt(b, bin_dur)),
+        "c50_rel": rel(10.0 ** (ca / 10.0), 10.0 ** (cb / 10.0)),
+        "c50_db": float(np.max(np.abs(ca - cb))),
+        "band_energy_rel": rel(np.sum(a, axis=1), np.sum(b, axis=1)),
+    }

@@ -1,21 +1,25 @@
 """Benchmark: RIRs/s (and ray-bounces/s) of the B200 reflection backend.
 
-Default workload (one step = one pass over one batch): the furnished U-shaped
-room of the second benchmark configuration -- 6 x 10 x 2.8 m, 20 seeded boxes
-(30 surfaces), cardioid source, 8-channel circular array, 200,000 rays x 100
-bounces per channel, fs 48 kHz, 2 s, 1 ms bins -- traced in float32 with the
-on-device Philox stream and turned into six band IRs per channel: 8 RIRs per
-step, all in one persistent trace launch plus one synthesis launch, replayed
-as a CUDA graph.  Inputs (the scene) are resident in HBM; L2 is flushed
-between timed steps.
+Default workload (one step = one pass over one batch): the batching
+configuration -- 256 seeded scenes whose sizes run from a single furnished
+room to an 8-room apartment, 1-4 sources x 1-8 receiver channels each, ray
+budgets log-uniform in 1e4-1e6, 50-200 bounces, fs 16 kHz, 1-2 s, per-scene
+six-band materials (2,863 RIRs per step).  A step is one graph-captured
+persistent trace launch over every job followed by one ragged band synthesis
+of every job; scenes are resident in HBM and L2 is flushed between timed
+steps.  Beside it the line reports the plain per-job loop over the same jobs,
+the drop-in ``trace_energy_field`` per job inside the reference, the
+reference's own Numba-CUDA float32 backend per job on this GPU, the
+reference's float64 Numba path (``cpu_baseline``), the parity of the GPU
+echograms against that float64 path, and the single-scene U-room figures
+(``config1_u_room``; ``--workload u_room_20_boxes`` gives that workload a
+line of its own).
 
 ``--impl reference`` times the reference's own CPU implementation of the path
 instead: the unmodified reference package installed under baseline/_ref,
 ``steam_rt.trace_energy_field`` on its float64 Numba path over all host
-threads plus ``reconstruct_band_irs``, one RIR of the same workload per step
-(the float64 C restatement when the package is absent).  The default arm also
-reports the reference's Numba-CUDA float32 backend on the same GPU
-(``reference_cuda``).  Under torchrun each rank runs an independent replica
+threads plus ``reconstruct_band_irs``, one uniformly drawn job of the same
+batch per step.  Under torchrun each rank runs an independent replica
 (replicas only: jobs are independent, no collective on the data path); rank 0
 prints one JSON line.
 """
@@ -341,13 +345,46 @@ def run_reference_arm(args, workload_name: str) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_reference_mixed(args) -> None:
+    """The reference's own CPU path on the headline mix: one job of the 256-scene batch per step.
+
+    Jobs are drawn uniformly (seeded) from the same batch as the default arm, so the mean time per step
+    estimates the reference's mean time per RIR over the batch; each step runs the unmodified reference's
+    ``trace_energy_field`` on its float64 Numba path over all host threads plus ``reconstruct_band_irs``.
+    Under torchrun only rank 0 runs.
+    """
+    world, rank, _ = _dist_setup()
+    if rank != 0:
+        return
+    from acoustic_agent_b200 import batching, workloads
+    population = workloads.mixed_batch(1729, args.scenes)
+    _, jobs = batching.workload_jobs(population)
+    picks = uniform_jobs(jobs, args.warmup + args.steps, seed=11)
+    ref = reference_job_loop(population, jobs, picks, accelerator="numba", precision="float64", untimed=args.warmup)
+    config = {"workload": f"mixed_batch: {args.scenes} scenes of 1-8 rooms, 1-4 sources x 1-8 channels, "
+                          "1e4-1e6 rays, 50-200 bounces, fs 16 kHz, 1-2 s, 10 ms bins",
+              "rirs_per_step": 1, "note": "one uniformly drawn job of the batch per step"}
+    if "unavailable" in ref:
+        print(json.dumps({"impl": "reference", "unavailable": ref["unavailable"]}), flush=True)
+        return
+    value = ref["rirs_per_s"]
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": world,
+        "steps": ref["jobs_timed"], "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded scene generator)",
+        "config": config,
+        "cpu_baseline": {"value": value, "unit": "RIRs/s", "cores": ref["threads"], "kind": "reference",
+                         "sample": ref["sample"]},
+        "e2e": {"value": value, "unit": "RIRs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
 def main() -> int:
     parser = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=10)
     parser.add_argument("--warmup", type=int, default=3)
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    parser.add_argument("--workload", default="u_room_20_boxes",
+    parser.add_argument("--workload", default="mixed_batch",
                         choices=("u_room_20_boxes", "shoebox", "apartment", "mixed_batch", "serving", "late_reverb",
                                  "direct", "bvh_build"))
     parser.add_argument("--no-graph", action="store_true", help="launch eagerly instead of replaying a CUDA graph")
@@ -361,6 +398,12 @@ def main() -> int:
                         help="mixed_batch: jobs of the reference's plain per-scene CUDA path to time")
     parser.add_argument("--plain-jobs", type=int, default=0,
                         help="mixed_batch: jobs of the plain per-job loop to time (0: all)")
+    parser.add_argument("--parity-jobs", type=int, default=3,
+                        help="mixed_batch: uniformly drawn jobs traced by the reference's float64 path for the "
+                             "parity block and the CPU baseline")
+    parser.add_argument("--e2e-steps", type=int, default=2, help="mixed_batch: end-to-end steps to time")
+    parser.add_argument("--no-config1", dest="with_config1", action="store_false",
+                        help="mixed_batch: skip the single-scene U-room figures added to the line")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
     parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     parser.add_argument("--policy", default="small_first", choices=("small_first", "fifo"),
@@ -428,9 +471,12 @@ def main() -> int:
                             "d2h_bytes_per_step": 0}}), flush=True)
         return 0
     if args.impl == "reference":
-        if args.workload in ("mixed_batch", "serving"):
-            parser.error("--impl reference times the reference's per-RIR path on a single-scene workload")
-        run_reference_arm(args, args.workload)
+        if args.workload == "serving":
+            parser.error("--impl reference has no serving arm: the reference has no request loop")
+        if args.workload == "mixed_batch":
+            run_reference_mixed(args)
+        else:
+            run_reference_arm(args, args.workload)
         return 0
     if args.workload == "mixed_batch":
         return run_mixed_batch(args)
@@ -443,6 +489,16 @@ def main() -> int:
     if args.workload == "bvh_build":
         return run_bvh_build(args)
 
+    return run_single_scene(args, args.workload)
+
+
+def run_single_scene(args, workload_name: str, *, extras_only: bool = False):
+    """One scene (the U room of the second configuration by default): every channel per step in one
+    persistent trace launch beside the band synthesis of the previous step (pipelined, graph-replayed).
+
+    With `extras_only` it returns the resident throughput and trace launch time as a dict (no end-to-end
+    run, no baselines) for the headline line instead of printing a line of its own.
+    """
     import torch
     from acoustic_agent_b200 import batching, runtime, scene as scene_mod
 
@@ -450,11 +506,11 @@ def main() -> int:
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
     dist = None
-    if world > 1:
+    if world > 1 and not extras_only:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=device)
 
-    workloads_ = _workload(args.workload)
+    workloads_ = _workload(workload_name)
     specs, jobs = batching.workload_jobs(workloads_, precision="float32", rng_mode="philox")
     renderer = batching.RIRRenderer(local, block_size=args.block)
     arrays = [scene_mod.compile_scene(s) for s in specs]
@@ -511,6 +567,12 @@ def main() -> int:
         e.synchronize()
         trace_ms.append(s.elapsed_time(e))
     trace_launch_ms = float(np.median(trace_ms))
+    if extras_only:
+        return {"workload": f"{workloads_[0].name}: {rirs_per_step} channels x {workloads_[0].config.rt_num_rays} "
+                            f"rays x {workloads_[0].config.rt_num_bounces} bounces, fs {workloads_[0].config.fs}",
+                "rirs_per_s": value, "ms_per_step": ms_per_step, "trace_launch_ms": trace_launch_ms,
+                "ray_bounces_per_s": ray_bounces_per_step / (ms_per_step / 1000.0), "steps": args.steps,
+                "step": "pipelined trace + synthesis, graph-replayed, L2 flushed between steps"}
 
     # End to end through the public API: every step uploads the scene from host arrays
     # (ac_scene_create), lays out the jobs' outputs, traces and synthesises, and copies the band IRs
@@ -565,15 +627,13 @@ def main() -> int:
             ref_cpu = reference_rirs(workloads_[0], 1, 1, accelerator="numba", precision="float64")
             ref_cuda = reference_rirs(workloads_[0], 3, 1, accelerator="cuda", precision="float32")
         bytes_per_rb = cpu["bytes_per_ray_bounce"] if cpu else None
-        l2_gbs = l2_read_gbs(device)
         achieved = (bytes_per_rb * ray_bounces_per_step / (trace_launch_ms / 1000.0) / 1e9) if bytes_per_rb else None
-        traffic = _profiled_traffic(args.workload)
         result = {
             "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
             "config": {"workload": f"{workloads_[0].name}: U room 6x10x2.8 m, 20 boxes, 8-mic circular array"
-                       if args.workload == "u_room_20_boxes" else workloads_[0].name,
+                       if workload_name == "u_room_20_boxes" else workloads_[0].name,
                        "rirs_per_step": rirs_per_step, "rays_per_rir": workloads_[0].config.rt_num_rays,
                        "max_bounces": workloads_[0].config.rt_num_bounces, "fs": workloads_[0].config.fs,
                        "bins": workloads_[0].config.num_bins, "rng": "philox", "graph": not args.no_graph,
@@ -590,13 +650,8 @@ def main() -> int:
                     "step": "upload the scene, plan, trace + synthesise, band IRs to pinned host memory; "
                             f"{len(slots)} steps in flight on {len(slots)} streams"},
             "gpu_launches": LAUNCHES_PER_STEP * args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": (achieved / peaks["hbm_gbs"]) if achieved else None, "traffic": traffic,
-                         "peak_source": peaks["source"],
-                         "l2_peak": l2_gbs, "frac_of_l2": (achieved / l2_gbs) if achieved else None,
-                         "l2_peak_source": "measured in this run: L2-cached 16-byte loads over a 32 MiB buffer",
-                         "kernel": "trace_kernel (ac_trace_batch)",
-                         "bytes_per_ray_bounce": bytes_per_rb},
+            "roofline": roofline_line(achieved, bytes_per_rb, workload_name, device, ray_bounces_per_step)
+            if achieved else None,
             "cpu_baseline": _cpu_baseline(cpu, ref_cpu),
             "reference_cuda": _reference_cuda_line(ref_cuda),
             "clocks": sampler.summary(),
@@ -623,75 +678,148 @@ def _device_timed(fn, steps: int, device, flush) -> list[float]:
     return out
 
 
-def reference_plain_sample(population, jobs, count: int, seed: int = 0) -> dict:
-    """The reference's own plain per-scene GPU path on a random sample of the batch's jobs.
+def sim_config(models, w, *, accelerator: str, precision: str, rays: int | None = None):
+    """The reference's SimConfig for one workload of the mix (the settings its job loops pass per call)."""
+    cfg = w.config
+    return models.SimConfig(fs=cfg.fs, c=cfg.c, duration_s=cfg.duration_s, rt_duration_s=cfg.rt_duration_s,
+                            rt_num_rays=int(rays or cfg.rt_num_rays), rt_num_bounces=cfg.rt_num_bounces,
+                            rt_bin_duration_s=cfg.rt_bin_duration_s, rt_specular_exponent=cfg.rt_specular_exponent,
+                            rt_irradiance_min_distance=cfg.rt_irradiance_min_distance,
+                            rt_source_radius=cfg.rt_source_radius, rt_listener_radius=cfg.rt_listener_radius,
+                            intersection_backend=cfg.intersection_backend, seed=cfg.seed, rt_accelerator=accelerator,
+                            rt_precision=precision, collect_visual_paths=False, render_ambisonics=False)
 
-    One call per job, as the reference's job loops make them (engine.py:64-73,
-    batch.py:139-185): ``trace_energy_field`` with its Numba-CUDA float32
-    kernel (``rt_accelerator="cuda"``) and ``reconstruct_band_irs`` on the
-    host.  The jobs are drawn uniformly, so their mean time estimates the mean
-    over the whole batch; the first call (kernel compilation) is not timed.
+
+def uniform_jobs(jobs, count: int, seed: int) -> list[int]:
+    """`count` job indices drawn uniformly without replacement (seeded), so their mean cost estimates the batch's."""
+    rng = np.random.default_rng(seed)
+    return [int(k) for k in rng.choice(len(jobs), size=min(count, len(jobs)), replace=False)]
+
+
+def reference_job_loop(population, jobs, picks, *, accelerator: str, precision: str, warm: bool = True,
+                       time_limit_s: float | None = None, untimed: int = 0) -> dict:
+    """The reference's own per-job call on jobs of the mix, as its job loops make them (engine.py:64-73,
+    batch.py:139-185): ``steam_rt.trace_energy_field`` + ``reconstruct_band_irs`` per (scene, source, channel).
+
+    accelerator "numba" = its float64 Numba path over all host threads, "cuda" = its Numba-CUDA float32 kernel
+    on this GPU, "b200" = this repository's drop-in installed into the reference.  The first call (kernel
+    compilation) runs on the batch's smallest job and is not timed.  Returns RIRs/s over the timed jobs and,
+    per job, its float echogram.
     """
     ref, reason = import_reference_package()
     if ref is None:
         return {"unavailable": reason}
     steam_rt, models = ref
-    try:
-        from acoustic_agent.steam_rt_cuda import cuda_available
-        if not cuda_available(0):
-            return {"unavailable": "the reference's Numba-CUDA backend reports no usable CUDA device"}
-    except Exception as exc:  # pragma: no cover - depends on the box
-        return {"unavailable": f"reference CUDA backend import failed: {type(exc).__name__}: {exc}"}
-    rng = np.random.default_rng(seed)
-    pick = [int(k) for k in rng.choice(len(jobs), size=min(count, len(jobs)), replace=False)]
+    installation = None
+    if accelerator == "cuda":
+        try:
+            from acoustic_agent.steam_rt_cuda import cuda_available
+            if not cuda_available(0):
+                return {"unavailable": "the reference's Numba-CUDA backend reports no usable CUDA device"}
+        except Exception as exc:  # pragma: no cover - depends on the box
+            return {"unavailable": f"reference CUDA backend import failed: {type(exc).__name__}: {exc}"}
+    if accelerator == "b200":
+        from acoustic_agent_b200 import backend
+        installation = backend.install(steam_rt)
     scenes: dict[int, object] = {}
 
     def run(k):
         j = jobs[k]
         w = population[j.workload]
-        cfg = w.config
         if j.workload not in scenes:
             scenes[j.workload] = reference_scene(steam_rt, models, w.spec)
-        sim = models.SimConfig(fs=cfg.fs, c=cfg.c, duration_s=cfg.duration_s, rt_duration_s=cfg.rt_duration_s,
-                               rt_num_rays=cfg.rt_num_rays, rt_num_bounces=cfg.rt_num_bounces,
-                               rt_bin_duration_s=cfg.rt_bin_duration_s, rt_specular_exponent=cfg.rt_specular_exponent,
-                               rt_irradiance_min_distance=cfg.rt_irradiance_min_distance,
-                               rt_source_radius=cfg.rt_source_radius, rt_listener_radius=cfg.rt_listener_radius,
-                               intersection_backend=cfg.intersection_backend, seed=cfg.seed, rt_accelerator="cuda",
-                               rt_precision="float32", collect_visual_paths=False, render_ambisonics=False)
+        sim = sim_config(models, w, accelerator=accelerator, precision=precision)
         field = steam_rt.trace_energy_field(scenes[j.workload], np.asarray(w.sources[j.source], dtype=float),
                                             np.asarray(w.listeners[j.channel], dtype=float), sim, w.source_model,
                                             render_ambisonics=False)
         steam_rt.reconstruct_band_irs(field, sim)
+        return np.asarray(field["echogram"], dtype=np.float64)
 
-    smallest = min(range(len(jobs)), key=lambda k: jobs[k].spec.num_rays)
-    run(smallest)   # compiles the reference's kernels
-    t0 = time.perf_counter()
-    for k in pick:
-        run(k)
-    seconds = time.perf_counter() - t0
-    return {"rirs_per_s": len(pick) / seconds, "jobs_timed": len(pick), "seconds": seconds,
-            "rays_timed": int(sum(jobs[k].spec.num_rays for k in pick)),
-            "note": "the reference's trace_energy_field (Numba-CUDA float32, this GPU) + reconstruct_band_irs "
-                    "(host) per job, on uniformly drawn jobs of this batch"}
+    try:
+        if warm:
+            run(min(range(len(jobs)), key=lambda k: jobs[k].spec.num_rays))
+        for k in picks[:untimed]:
+            run(k)
+        echograms, seconds, timed = {}, 0.0, []
+        for k in picks[untimed:]:
+            t0 = time.perf_counter()
+            echograms[k] = run(k)
+            seconds += time.perf_counter() - t0
+            timed.append(k)
+            if time_limit_s is not None and seconds > time_limit_s:
+                break
+    finally:
+        if installation is not None:
+            installation.uninstall()
+    threads = None
+    if accelerator == "numba":
+        import numba
+        threads = int(numba.get_num_threads())
+    rays = [jobs[k].spec.num_rays for k in timed]
+    return {"rirs_per_s": len(timed) / seconds, "jobs_timed": len(timed), "seconds": seconds,
+            "ray_mean": float(np.mean(rays)), "threads": threads, "echograms": echograms,
+            "sample": (f"{len(timed)} jobs drawn uniformly from the batch (mean {np.mean(rays):,.0f} rays against "
+                       f"{np.mean([j.spec.num_rays for j in jobs]):,.0f} over the batch): trace_energy_field("
+                       f"rt_accelerator={accelerator!r}, rt_precision={precision!r}) + reconstruct_band_irs per job, "
+                       "after one untimed call")}
+
+
+def mix_bytes_per_ray_bounce(arrays, jobs, ray_bounces_per_job, sample_rays: int = 512) -> float:
+    """Algorithmic bytes per ray-bounce over the mix (roofline numerator, per-unit figure).
+
+    For each scene, the float64 C restatement traces the first `sample_rays` rays of its first job on the same
+    Philox stream as the GPU and counts the reference traversal's fetches (nodes 32 B, walls 32 B, polygons
+    16 B + 8 B per edge, boxes 48 B, one 32 B material row per closest-hit query); scenes are weighted by the
+    ray-bounces the GPU executed for their jobs.
+    """
+    from oracle import oracle
+    from acoustic_agent_b200.directivity import source_directivity, source_forward
+    _, bank, _, _ = oracle.workspace(1, 0, 0)
+    first: dict[int, int] = {}
+    weight: dict[int, float] = {}
+    for k, j in enumerate(jobs):
+        first.setdefault(j.scene_index, k)
+        weight[j.scene_index] = weight.get(j.scene_index, 0.0) + float(ray_bounces_per_job[k])
+    total_bytes = total_rb = 0.0
+    for si, k in first.items():
+        spec = jobs[k].spec
+        R = min(int(spec.num_rays), sample_rays)
+        dirs, rnd, idx = oracle.philox_workspace(R, int(spec.num_bounces), int(spec.seed), int(spec.stream_key))
+        emitter = {"dipole_weight": spec.dipole_weight, "dipole_power": spec.dipole_power}
+        res = oracle.trace(arrays[si], source=np.asarray(spec.source), listener=np.asarray(spec.listener),
+                           directions=dirs, diffuse_bank=bank, diffuse_random=rnd, diffuse_indices=idx,
+                           num_bins=int(spec.num_bins), bin_dur=spec.bin_duration, c=spec.speed_of_sound,
+                           max_path_len=spec.max_path_length, direct_delay=spec.direct_delay,
+                           source_forward=np.asarray(spec.source_forward, dtype=float),
+                           dipole_weight=float(emitter["dipole_weight"]), dipole_power=float(emitter["dipole_power"]),
+                           use_bvh=bool(spec.use_bvh), threads=1)
+        q = res["closest_queries"]
+        walls, polys, boxes = res["prims_tested"]
+        per = (res["nodes_visited"] * 32 + walls * 32 + polys * 16 + res["polygon_edges"] * 8 + boxes * 48 + q * 32)
+        total_bytes += weight[si] * per / max(q, 1)
+        total_rb += weight[si]
+    return total_bytes / max(total_rb, 1.0)
 
 
 def run_mixed_batch(args) -> int:
-    """Batched mixed-size workload: many scenes, sources and channels in one persistent launch.
+    """Batched mixed-size workload (the headline): many scenes, sources and channels in one persistent launch.
 
-    256 seeded scenes log-uniform between a single room and an 8-room
-    apartment, 1-4 sources and 1-8 channels each, 1e4-1e6 rays, fs 16 kHz,
-    1-2 s: the graph-captured tracer + ragged synthesis (autotuned traversal
-    per scene and launch shape) against looping the plain per-job drop-in call
-    (one ac_trace + one ac_synthesize + a host copy per RIR).
+    256 seeded scenes log-uniform between a single room and an 8-room apartment, 1-4 sources and 1-8 channels
+    each, 1e4-1e6 rays, fs 16 kHz, 1-2 s.  One step = the graph-captured tracer over every job + the ragged
+    band synthesis of every job (autotuned traversal per scene and launch shape).  Beside it: the plain
+    per-job loop over the same jobs (resident ac_trace + ac_synthesize + host copy per RIR), the drop-in
+    ``trace_energy_field`` per job inside the reference, the reference's own Numba-CUDA float32 backend per
+    job, the reference's float64 Numba path (CPU baseline) and the parity of the GPU echograms against it.
     """
     import torch
-    from acoustic_agent_b200 import autotune, batching, runtime, scene as scene_mod, workloads
+    from acoustic_agent_b200 import autotune, batching, metrics, runtime, scene as scene_mod, workloads
     world, rank, local = _dist_setup()
-    if world > 1:
-        raise SystemExit("mixed_batch runs on one GPU")
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=device)
     t0 = time.perf_counter()
     population = workloads.mixed_batch(1729, args.scenes)
     specs, jobs = batching.workload_jobs(population)
@@ -710,24 +838,49 @@ def run_mixed_batch(args) -> int:
     renderer.block_size, renderer.chunk_rays = launch.block_size, launch.chunk_rays
     t_tune = time.perf_counter() - t0
     if not args.no_graph:
-        renderer.capture(plan)
+        renderer.capture(plan, split=True)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
     for _ in range(args.warmup):
         renderer.launch(plan)
     torch.cuda.synchronize(device)
-    rb = renderer.ray_bounces(plan)
+    per_job_rb = [int(b.counters[2].item()) for b in plan.buffers]
+    rb = int(sum(per_job_rb))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier(device_ids=[local])
+
+    marks = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize(device)
     with sampler:
-        step_ms = _device_timed(lambda: renderer.launch(plan), args.steps, device, flush)
+        for k in range(args.steps):
+            flush.fill_(float(k))   # evict L2 (256 MiB > 126 MB) outside the timed events
+            start, t_start, t_stop, stop = marks[k]
+            start.record(stream)
+            renderer.launch(plan, trace_events=(t_start, t_stop))
+            stop.record(stream)
+        torch.cuda.synchronize(device)
+    barrier()
+    step_ms = [m[0].elapsed_time(m[3]) for m in marks]
+    trace_ms = float(np.mean([m[1].elapsed_time(m[2]) for m in marks]))
     ms = float(np.mean(step_ms))
-    # plain drop-in loop: one trace launch + one synthesis + one host copy per job, scenes resident
+    ms, value = replica_throughput(ms, len(jobs), dist, device)
+    if rank != 0:
+        barrier()
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+
+    # plain per-job loop over the same jobs: one ac_trace + one ac_synthesize + a host copy per RIR, scenes resident
     order = list(range(len(jobs)))
     if args.plain_jobs > 0:
-        order = list(np.random.default_rng(0).permutation(len(jobs))[:args.plain_jobs])
+        order = uniform_jobs(jobs, args.plain_jobs, seed=0)
     ws = runtime.SynthWorkspace(device)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
-    plain_rays = 0
     for k in order:
         j = jobs[k]
         b = runtime.trace(plan.scenes[j.scene_index], j.spec)
@@ -735,64 +888,112 @@ def run_mixed_batch(args) -> int:
         p = runtime.synth_params(1, j.spec.num_bins, j.spec.bin_duration, j.fs, j.spec.speed_of_sound,
                                  rng_mode="philox", seed=int(j.spec.seed) + 7, direct_delays=d)
         runtime.synthesize(b.echogram[None].contiguous(), p, ws).cpu()
-        plain_rays += j.spec.num_rays
     plain_s = time.perf_counter() - t0
     plain_rirs_per_s = len(order) / plain_s
-    # end to end: host scene arrays in, host band IRs out
+
+    # end to end through the public API, host buffers: every step uploads the 256 scenes from host arrays,
+    # lays out the jobs, traces + synthesises them (one launch each) and copies the band IRs to pinned host memory
+    host_out = torch.empty(plan.ir_store.shape, dtype=plan.ir_store.dtype, pin_memory=True)
+    e2e_renderer = batching.RIRRenderer(local, block_size=launch.block_size, chunk_rays=launch.chunk_rays)
+
+    def e2e_step():
+        scenes_k = [runtime.DeviceScene(a, device=local, **o) for a, o in zip(arrays, options)]
+        plan_k = e2e_renderer.plan(scenes_k, jobs)
+        e2e_renderer.launch(plan_k)
+        host_out.copy_(plan_k.ir_store, non_blocking=True)
+        torch.cuda.current_stream(device).synchronize()
+        for sc in scenes_k:
+            sc.close()
+        return scenes_k, plan_k
+
+    e2e_step()   # warm-up (staging buffers, allocator)
+    e2e_steps = max(2, args.e2e_steps)
     t0 = time.perf_counter()
-    plan_e = renderer.plan(arrays, jobs, scene_options=options)
-    renderer.launch(plan_e)
-    host = plan_e.ir_store.cpu()
+    for _ in range(e2e_steps):
+        scenes_k, plan_k = e2e_step()
     e2e_s = time.perf_counter() - t0
-    h2d = sum(s.device_bytes for s in plan_e.scenes)
-    d2h = host.numel() * 4
-    for s in plan_e.scenes:
-        s.close()
-    value = len(jobs) / (ms / 1000.0)
-    # hybrid FDN late tails of every job of the batch (RT60 from each echogram, batched designs, one FDN
-    # launch and one tail launch), after a warm-up call
-    renderer.launch(plan)
-    renderer.late_tails(plan)
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    tails = renderer.late_tails(plan)
-    torch.cuda.synchronize(device)
-    tails_s = time.perf_counter() - t0
-    late = {"tails": len(jobs), "seconds": tails_s, "host_seconds": tails.host_seconds,
-            "tails_per_s": len(jobs) / tails_s,
-            "note": "RIRRenderer.late_tails after a step: RT60 estimates and FDN designs on the host, "
-                    "ac_fdn_impulse + ac_late_tail over all jobs"}
-    del tails
-    ref_plain = None if args.no_cpu_baseline else reference_plain_sample(population, jobs, args.reference_jobs)
-    if ref_plain and "rirs_per_s" in ref_plain:
-        # the sample's rays differ from the batch's: also extrapolate its time in proportion to rays
-        total_rays = sum(j.spec.num_rays for j in jobs)
-        ref_plain["rays_weighted_rirs_per_s"] = len(jobs) / (ref_plain["seconds"] * total_rays /
-                                                           max(ref_plain["rays_timed"], 1))
+    h2d = sum(sc.device_bytes for sc in scenes_k) + plan_k.workspace.device_buffer.numel()
+    d2h = plan_k.ir_store.numel() * plan_k.ir_store.element_size()
+    del plan_k, scenes_k
+
     line = {
-        "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded scene generator)",
-        "config": {"workload": f"mixed_batch: {args.scenes} scenes, 1-8 rooms, 1-4 sources x 1-8 channels, "
-                               "1e4-1e6 rays, fs 16 kHz, 1-2 s",
+        "metric": METRIC, "value": value, "unit": "RIRs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded scene generator: 256 scenes of 1-8 rooms, random-init materials)",
+        "config": {"workload": f"mixed_batch: {args.scenes} scenes of 1-8 rooms, 1-4 sources x 1-8 channels, "
+                               "1e4-1e6 rays, 50-200 bounces, fs 16 kHz, 1-2 s, 10 ms bins",
                    "rirs_per_step": len(jobs), "rays_per_step": int(sum(j.spec.num_rays for j in jobs)),
-                   "graph": not args.no_graph, "l2": "flushed between timed steps (256 MiB write)",
-                   "traversal": {m: sum(1 for s in plan.scenes if s.traversal == m) for m in ("scan", "bvh")},
+                   "step": "one graph-captured persistent trace launch over every job, then one ragged band "
+                           "synthesis of every job (second graph)",
+                   "graph": not args.no_graph, "rng": "philox", "parallelism": f"replicas x{world}",
+                   "l2": "flushed between timed steps (256 MiB write)",
+                   "traversal": {m: sum(1 for s in plan.scenes if s.traversal == m) for m in ("scan", "bvh", "hybrid")},
                    "launch": {"block_size": launch.block_size, "chunk_rays": launch.chunk_rays}},
-        "ray_bounces_per_step": rb, "ray_bounces_per_s": rb / (ms / 1000.0),
+        "ray_bounces_per_step": rb, "ray_bounces_per_s": world * rb / (ms / 1000.0),
+        "trace_launch_ms": trace_ms, "synthesis_ms": ms - trace_ms,
         "plain": {"rirs_per_s": plain_rirs_per_s, "jobs_timed": len(order), "seconds": plain_s,
-                  "note": "per job: ac_trace + ac_synthesize + copy to host, scenes resident"},
+                  "note": "per job: ac_trace + ac_synthesize + copy to host, scenes resident, same jobs"},
         "batched_vs_plain": value / plain_rirs_per_s,
-        "reference_plain": ref_plain,
-        "late_tails": late,
-        "batched_vs_reference_plain": (value / ref_plain["rirs_per_s"]) if ref_plain and "rirs_per_s" in ref_plain
-        else None,
-        "e2e": {"value": len(jobs) / e2e_s, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h), "note": "scene upload + plan + launch + host copy, one pass"},
-        "setup_s": {"compile": t_compile, "tune": t_tune}, "gpu_launches": 6 * args.steps,
+        "e2e": {"value": len(jobs) * e2e_steps / e2e_s, "unit": "RIRs/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h), "steps": e2e_steps,
+                "step": "upload 256 scenes from host arrays, plan, trace + synthesise, band IRs to pinned host"},
+        "gpu_launches": 6 * args.steps,
+        "setup_s": {"compile": t_compile, "tune": t_tune},
         "clocks": sampler.summary(),
     }
+
+    # roofline of the trace launch: algorithmic bytes over the mix / its live CUDA-event duration
+    if not args.no_cpu_baseline:
+        bpr = mix_bytes_per_ray_bounce(arrays, jobs, per_job_rb)
+        achieved = bpr * rb / (trace_ms / 1000.0) / 1e9
+        line["roofline"] = roofline_line(achieved, bpr, "mixed_batch", device)
+
+    if not args.no_cpu_baseline and world == 1:
+        picks = uniform_jobs(jobs, args.reference_jobs, seed=3)
+        ref64 = reference_job_loop(population, jobs, picks[:args.parity_jobs], accelerator="numba",
+                                   precision="float64")
+        if "unavailable" not in ref64:
+            drop = reference_job_loop(population, jobs, picks[:max(args.parity_jobs, 4)], accelerator="b200",
+                                      precision="float32", time_limit_s=30.0)
+            echo_host = plan.echo_store.cpu().numpy()
+            offsets = np.cumsum([0] + [6 * int(j.spec.num_bins) for j in jobs])
+            same, philox = [], []
+            for k, ref_echo in ref64["echograms"].items():
+                bd = jobs[k].spec.bin_duration
+                ours_philox = echo_host[offsets[k]:offsets[k + 1]].reshape(6, -1)
+                philox.append(metrics.parity(ours_philox, ref_echo, bd))
+                if k in drop.get("echograms", {}):
+                    same.append(metrics.parity(drop["echograms"][k], ref_echo, bd))
+
+            def worst(rows):
+                return {key: max(r[key] for r in rows) for key in rows[0]} if rows else None
+
+            line["parity"] = {
+                "jobs": len(ref64["echograms"]),
+                "same_stream": worst(same),
+                "philox_stream": worst(philox),
+                "note": ("GPU float32 echograms against the reference's float64 Numba echogram of the same job "
+                         "(trace_energy_field, rt_precision='float64'); same_stream: the drop-in on the reference's "
+                         "own random stream (identical rays); philox_stream: the batch's own echogram (Philox rays, "
+                         "Monte-Carlo difference); worst band and job"),
+            }
+            line["cpu_baseline"] = {"value": ref64["rirs_per_s"], "unit": "RIRs/s", "cores": ref64["threads"],
+                                    "kind": "reference", "sample": ref64["sample"]}
+            line["drop_in_plain"] = {k: v for k, v in drop.items() if k != "echograms"}
+            if "rirs_per_s" in drop:
+                line["batched_vs_drop_in_plain"] = value / drop["rirs_per_s"]
+        else:
+            line["cpu_baseline"] = {"unavailable": ref64["unavailable"]}
+        ref_cuda = reference_job_loop(population, jobs, picks, accelerator="cuda", precision="float32")
+        line["reference_cuda_plain"] = {k: v for k, v in ref_cuda.items() if k != "echograms"}
+        if "rirs_per_s" in ref_cuda:
+            line["batched_vs_reference_cuda_plain"] = value / ref_cuda["rirs_per_s"]
+    if args.with_config1:
+        line["config1_u_room"] = run_single_scene(args, "u_room_20_boxes", extras_only=True)
     print(json.dumps(line), flush=True)
+    barrier()
+    if dist is not None:
+        dist.destroy_process_group()
     return 0
 
 
@@ -1321,18 +1522,39 @@ def l2_read_gbs(device) -> float:
     return runtime.read_bandwidth_gbs(device, 32 << 20)
 
 
-def _profiled_traffic(workload: str):
-    """DRAM bytes per trace launch from the committed ncu summary, if one exists for this workload."""
-    path = REPO / "profiles" / f"trace_kernel_{workload}.md"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        if line.lower().startswith("traffic_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+# Figures of the trace launch read from one ncu capture of the same kernel code, per workload (constants,
+# recorded with the summary that gives them and the commit of the kernel it measured): issue-active fraction,
+# SIMT efficiency (thread instructions per warp instruction / 32) and DRAM bytes per ray-bounce
+# (dram__bytes_read.sum + dram__bytes_write.sum of the captured launch over its ray-bounces).
+PROFILED = {
+    "u_room_20_boxes": {"issue_active": 0.69, "simt_efficiency": 13.99 / 32.0,
+                        "dram_bytes_per_ray_bounce": 4753408 / 52028160,
+                        "profile": "profiles/trace_kernel_u_room_20_boxes.md", "kernel_commit": "e64c19a"},
+}
+
+
+def roofline_line(achieved: float, bytes_per_rb: float, workload: str, device, ray_bounces: int) -> dict:
+    """The trace launch's roofline.
+
+    `achieved` = algorithmic bytes of one launch (the reference traversal's node, surface and material fetches
+    per ray-bounce x the launch's ray-bounces) over its CUDA-event duration.  Scenes are kilobytes, so those
+    bytes are served from L1/L2 and the memory roof is the L2 read rate measured in this run; the HBM copy
+    peak is given beside it.  The launch is issue-bound (divergent per-lane traversal), which the ncu figures
+    of the same kernel show: `bound` says so and `frac` is taken against the L2 roof.
+    """
+    peaks = _peaks()
+    l2 = l2_read_gbs(device)
+    prof = PROFILED.get(workload)
+    out = {"bound": "issue", "achieved": achieved, "peak": l2, "unit": "GB/s", "frac": achieved / l2,
+           "traffic": prof["dram_bytes_per_ray_bounce"] * ray_bounces if prof else None,
+           "peak_source": "measured in this run: L2-cached 16-byte loads over a 32 MiB buffer (ac_read_bandwidth_probe)",
+           "hbm_peak": peaks["hbm_gbs"], "hbm_peak_source": peaks["source"], "frac_of_hbm": achieved / peaks["hbm_gbs"],
+           "kernel": "trace_fast_kernel (ac_trace_batch)", "bytes_per_ray_bounce": bytes_per_rb}
+    if prof:
+        out.update({"issue_active": prof["issue_active"], "simt_efficiency": prof["simt_efficiency"],
+                    "ncu_profile": prof["profile"], "ncu_kernel_commit": prof["kernel_commit"],
+                    "traffic_basis": "DRAM bytes per ray-bounce of the profiled launch x this launch's ray-bounces"})
+    return out
 
 
 if __name__ == "__main__":
