@@ -109,6 +109,17 @@ class ACBatchConfig(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+class ACServiceConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("capacity", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("block_size", ctypes.c_int32), ("chunk_rays", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("idle_timeout_ns", ctypes.c_int64)]
+
+
+class ACServiceStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("in_flight", ctypes.c_int64), ("launches", ctypes.c_int64),
+                ("running_launches", ctypes.c_int32), ("grid_blocks", ctypes.c_int32), ("capacity", ctypes.c_int64)]
+
+
 class ACSynthParams(ctypes.Structure):
     _fields_ = [
         ("num_rirs", ctypes.c_int32), ("num_bins", ctypes.c_int32), ("samples_per_bin", ctypes.c_int32),
@@ -252,6 +263,13 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
     "ac_philox_workspace": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int64, ctypes.c_int32,
                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "ac_service_create": (ctypes.c_int, [ctypes.POINTER(ACServiceConfig), ctypes.POINTER(ctypes.c_void_p)]),
+    "ac_service_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACJob), ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_int64)]),
+    "ac_service_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32,
+                                       ctypes.POINTER(ctypes.c_int32)]),
+    "ac_service_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACServiceStats)]),
+    "ac_service_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "ac_reference_stream": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                            ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),

@@ -29,7 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 # Units whose float64 arithmetic must not be contracted into FMAs.
 NO_FMA = {"trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu", "bvh_device.cu"}
 SOURCES = ["abi.cu", "scene.cu", "trace_f32.cu", "trace_f64.cu", "synth.cu", "late_reverb.cu", "direct.cu",
-           "bvh_device.cu", "refstream.cu", "bvh_build.cpp", "fast_bvh.cpp"]
+           "bvh_device.cu", "refstream.cu", "service.cu", "bvh_build.cpp", "fast_bvh.cpp"]
 
 
 def nvcc() -> str:

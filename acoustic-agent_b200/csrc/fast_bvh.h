@@ -24,7 +24,10 @@
 namespace ac {
 
 constexpr int kBvhMaxLeaf = 8;
-constexpr int kBvhStack = 32;   // traversal stack entries; the builder keeps the depth below this
+#ifndef AC_BVH_STACK
+#define AC_BVH_STACK 32
+#endif
+constexpr int kBvhStack = AC_BVH_STACK;   // traversal stack entries; the builder keeps the depth below this
 
 struct TraversalBvh {
     std::vector<float> nodes;      // [num_nodes][16]

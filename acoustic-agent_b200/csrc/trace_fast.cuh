@@ -80,6 +80,34 @@ struct FastChunk {
     int32_t pad;
 };
 
+// Continuous batching (ac_service_*): a ring of job slots in device memory that
+// the host appends to while a persistent launch runs.  A slot is written once
+// per job before the job is published and not rewritten while a launch that
+// may hold it in L1 runs (each launch takes at most half a ring of sequence
+// numbers); the slot stride keeps slots on separate cache lines.
+struct alignas(256) ServiceSlot {
+    Job<float> job;
+    FastScene fast;
+    float *echogram;             // float32 outputs the finishing warp converts the fixed-point sums into
+    float *surface_energy;
+    int64_t seq;                 // the job's sequence number
+    int64_t num_chunks;
+    uint64_t scene_id;           // jobs with equal ids share a scene (no lane drain between them)
+    int64_t chunk_rays;
+};
+
+struct ServiceSlotState {        // device, zeroed by the host before the slot is published
+    unsigned long long chunks_taken;
+    unsigned long long rays_finished;
+};
+
+// Host-mapped control block.
+struct ServiceControl {
+    long long published;         // host: jobs below this sequence number are in the ring
+    long long pad[15];
+    long long done[1];           // [capacity] device: done[slot] = seq once that job's outputs are final
+};
+
 struct FastTable {
     const Job<float> *jobs;
     const int64_t *ray_begin;      // [num_jobs + 1]
@@ -99,12 +127,115 @@ struct FastTable {
     const int64_t *group_ray_begin;      // [num_groups + 1] first ray (over all jobs) of each group
     int32_t num_groups;
     int32_t reserved;
+    // Service launches (continuous batching): the ring, its per-slot state and the control block.
+    const ServiceSlot *slots;
+    ServiceSlotState *slot_state;
+    ServiceControl *control;             // host-mapped
+    unsigned long long *low_water;       // device: jobs below it have no chunks left
+    int64_t window_first;                // this launch takes jobs from this sequence number
+    int64_t window_end;                  // to below this one only
+    int64_t idle_ns;                     // and ends once its warps found no work for this long
+    int64_t mask;                        // ring capacity - 1
 };
+
+// Service launches, lane 0 of a warp: the next chunk (seq, chunk index) from job `queue` onward, or false
+// when the launch should end -- its warps found no published job with chunks left for `idle_ns`, or its
+// window of sequence numbers is used up.  Every wait is bounded: the idle deadline, and a poll cap.
+__device__ __forceinline__ bool service_take(const FastTable &t, int64_t &queue, int64_t &published,
+                                             int64_t *seq_out, int64_t *chunk_out) {
+    unsigned long long idle_from = 0;
+    unsigned sleep_ns = 256;
+    bool rescanned = false;
+#pragma unroll 1
+    for (int polls = 0; polls < (1 << 22); ++polls) {
+        if (queue < published && queue < t.window_end) {
+            const ServiceSlot &sl = t.slots[queue & t.mask];
+            ServiceSlotState *st = t.slot_state + (queue & t.mask);
+            const int64_t chunks = sl.num_chunks;
+            if (static_cast<int64_t>(*reinterpret_cast<volatile unsigned long long *>(&st->chunks_taken)) < chunks) {
+                const int64_t k = static_cast<int64_t>(atomicAdd(&st->chunks_taken, 1ull));
+                if (k < chunks) {
+                    *seq_out = queue;
+                    *chunk_out = k;
+                    return true;
+                }
+            }
+            // no chunks left here: raise the low-water mark past it if it points here, then move on
+            atomicCAS(t.low_water, static_cast<unsigned long long>(queue), static_cast<unsigned long long>(queue + 1));
+            ++queue;
+            idle_from = 0;
+            continue;
+        }
+        // caught up with the published jobs (or this launch's window): older jobs may still hold chunks
+        // (other warps' jobs), so rescan them once from the low-water mark
+        if (!rescanned) {
+            rescanned = true;
+            const int64_t low = max(static_cast<int64_t>(*reinterpret_cast<volatile unsigned long long *>(t.low_water)),
+                                    t.window_first);
+            if (low < queue) {
+                queue = low;
+                continue;
+            }
+        }
+        if (queue >= t.window_end) return false;
+        // wait for the host to publish more, within the idle limit
+        unsigned long long now;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+        if (idle_from == 0) idle_from = now;
+        if (now - idle_from > static_cast<unsigned long long>(t.idle_ns)) return false;
+        __nanosleep(sleep_ns);
+        if (sleep_ns < 32768) sleep_ns <<= 1;
+        long long pub;
+        asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(pub) : "l"(&t.control->published) : "memory");
+        if (pub > published) {
+            published = pub;
+            rescanned = false;
+        }
+    }
+    return false;
+}
+
+// Service launches: the job in `slot` has finished its last ray; every lane of the warp converts its
+// fixed-point sums to the float32 outputs, then lane 0 flags it done to the host.  The sums were added at L2
+// by atomics of all warps before they counted their rays finished (each lane fenced first); they are read
+// around L1 here.
+__device__ __forceinline__ void service_finish(const FastTable &t, int slot, int lane_id) {
+    __threadfence();
+    const ServiceSlot &sl = t.slots[slot];
+    const Job<float> &job = sl.job;
+    const double inv = 1.0 / job.energy_scale;
+    const int64_t nb = static_cast<int64_t>(kBands) * job.num_bins;
+    for (int64_t i = lane_id; i < nb; i += 32) {
+        const double v = ldexp(static_cast<double>(static_cast<long long>(__ldcg(job.echogram_fx + 2 * i + 1))), 32) +
+                         static_cast<double>(__ldcg(job.echogram_fx + 2 * i));
+        sl.echogram[i] = static_cast<float>(v * inv);
+    }
+    if (sl.surface_energy) {
+        for (int64_t i = lane_id; i < job.scene.num_surfaces; i += 32) {
+            const double v =
+                ldexp(static_cast<double>(static_cast<long long>(__ldcg(job.surface_energy_fx + 2 * i + 1))), 32) +
+                static_cast<double>(__ldcg(job.surface_energy_fx + 2 * i));
+            sl.surface_energy[i] = static_cast<float>(v * inv);
+        }
+    }
+    __syncwarp();
+    if (lane_id == 0) {
+        __threadfence_system();
+        asm volatile("st.release.sys.global.s64 [%0], %1;" ::"l"(&t.control->done[slot]), "l"(sl.seq) : "memory");
+    }
+}
+
+#ifndef AC_FMA_SLAB
+#define AC_FMA_SLAB 0
+#endif
 
 struct FRay {
     float o[3];
     float d[3];
     float inv[3];
+#if AC_FMA_SLAB
+    float oi[3];   // o * inv: a slab plane's t is then one fused multiply-add
+#endif
 };
 
 // Approximate reciprocal (MUFU, ~1 ulp): the float32 path needs no correctly rounded division.
@@ -125,7 +256,19 @@ __device__ __forceinline__ void make_ray(FRay &r, const float *o, const float *d
         r.o[a] = o[a];
         r.d[a] = d[a];
         r.inv[a] = safe_inv(d[a]);
+#if AC_FMA_SLAB
+        r.oi[a] = o[a] * r.inv[a];
+#endif
     }
+}
+
+// t of the plane x_a = v along the ray (conservative box culling only: node boxes are padded)
+__device__ __forceinline__ float slab_t(const FRay &r, int a, float v) {
+#if AC_FMA_SLAB
+    return fmaf(v, r.inv[a], -r.oi[a]);
+#else
+    return (v - r.o[a]) * r.inv[a];
+#endif
 }
 
 // Conservative slab test: could any point of the box be hit before max_t?
@@ -213,13 +356,14 @@ __device__ __forceinline__ void take(float t, int si, float &best_t, int &best) 
     }
 }
 
-// Warp-uniform scene query; every lane of the warp must call it.
+// Scene query of the warp's lanes; every lane of the warp must call it.
 //
 // Closest-hit mode (best_t starts at 1e30): the minimum t over all surfaces,
 // ties to the lower surface index.  Any-hit mode (best_t starts at the shadow
 // ray's length): a lane stops as soon as it finds any surface closer than
 // that.  Both modes use the same update rule, so the code exists once:
-// `best` is the surface found (-1: none) and best_t its t.
+// `best` is the surface found (-1: none) and best_t its t.  The mode is a
+// lane's own: lanes of one warp may run closest-hit and shadow queries together.
 __device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, bool active, bool any_hit,
                                            float &best_t, int &best) {
     const unsigned full = 0xFFFFFFFFu;
@@ -228,7 +372,7 @@ __device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, b
 #pragma unroll 1
     for (int c = 0; c < fs.num_wall_clusters; ++c) {
         const bool searching = active && !(any_hit && best >= 0);
-        if (any_hit && !__any_sync(full, searching)) return;
+        if (!__any_sync(full, searching)) return;
         const float *cp = fs.wall_clusters + kClusterStride * c;
         const Quad<float> lo = ldq(cp), hi = ldq(cp + 4);
         const bool pass = searching && cluster_overlaps(r, lo, hi, best_t);
@@ -258,7 +402,7 @@ __device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, b
 #pragma unroll 1
     for (int c = 0; c < fs.num_box_clusters; ++c) {
         const bool searching = active && !(any_hit && best >= 0);
-        if (any_hit && !__any_sync(full, searching)) return;
+        if (!__any_sync(full, searching)) return;
         const float *cp = fs.box_clusters + kClusterStride * c;
         const Quad<float> lo = ldq(cp), hi = ldq(cp + 4);
         const bool pass = searching && cluster_overlaps(r, lo, hi, best_t);
@@ -285,9 +429,9 @@ __device__ __forceinline__ void scene_scan(const FastScene &fs, const FRay &r, b
 // Slab test of one child box of a traversal-BVH node, with the scan's margin on max_t.
 __device__ __forceinline__ bool child_box(const FRay &r, float lx, float hx, float ly, float hy, float lz, float hz,
                                           float max_t, float &enter) {
-    const float x0 = (lx - r.o[0]) * r.inv[0], x1 = (hx - r.o[0]) * r.inv[0];
-    const float y0 = (ly - r.o[1]) * r.inv[1], y1 = (hy - r.o[1]) * r.inv[1];
-    const float z0 = (lz - r.o[2]) * r.inv[2], z1 = (hz - r.o[2]) * r.inv[2];
+    const float x0 = slab_t(r, 0, lx), x1 = slab_t(r, 0, hx);
+    const float y0 = slab_t(r, 1, ly), y1 = slab_t(r, 1, hy);
+    const float z0 = slab_t(r, 2, lz), z1 = slab_t(r, 2, hz);
     enter = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
     const float exit_ = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), max_t));
     return enter <= exit_;
@@ -426,6 +570,10 @@ __device__ __forceinline__ void diffuse_direction_f(float s0, float s1, float s2
     normalize3f(s0 * t[0] + s1 * bx + s2 * nx, s0 * t[1] + s1 * by + s2 * ny, s0 * t[2] + s1 * bz + s2 * nz, out);
 }
 
+#ifndef AC_SPLIT_QUERIES
+#define AC_SPLIT_QUERIES 0
+#endif
+
 struct FastLane {
     float o[3];
     float d[3];
@@ -438,6 +586,13 @@ struct FastLane {
     int queries;
     int shadows;
     int vslot;    // visual-candidate slot, -1 for none
+#if AC_SPLIT_QUERIES
+    // between a bounce's closest hit and its shadow query (o is then the offset hit point)
+    float hit_t;
+    float n[3];
+    int surf;
+    bool shadow_next;
+#endif
 };
 
 __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int hi, int64_t g) {
@@ -448,7 +603,7 @@ __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int
     return lo;
 }
 
-template <bool kSingle, bool kPhilox, bool kAmb, bool kVisual>
+template <bool kSingle, bool kPhilox, bool kAmb, bool kVisual, bool kService = false>
 __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(const __grid_constant__ Job<float> single,
                                                          const __grid_constant__ FastScene single_fast,
                                                          const __grid_constant__ FastTable table) {
@@ -463,7 +618,21 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     bool exhausted = false;
     const int64_t num_chunks = kSingle ? (single.num_rays + table.chunk_rays - 1) / table.chunk_rays : table.num_chunks;
     int queue = 0;                  // batched launches: the group queue this warp takes chunks from
-    if (!kSingle) {
+    int64_t svc_queue = 0, svc_published = 0;   // service launches: next job to take chunks from, jobs seen
+    int cur_slot = 0;                            // service launches: the job of the chunk being handed out
+    int64_t pending_begin = 0, pending_end = 0;
+    if (kService) {
+        long long pub = 0;
+        if (lane_id == 0)
+            asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(pub) : "l"(&table.control->published) : "memory");
+        pub = __shfl_sync(full, pub, 0);
+        const long long low = max(static_cast<long long>(*reinterpret_cast<volatile unsigned long long *>(table.low_water)),
+                                  static_cast<long long>(table.window_first));
+        const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
+        const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
+        svc_published = pub;
+        svc_queue = pub > low ? low + (warp * (pub - low)) / warps : low;   // spread the warps over the jobs
+    } else if (!kSingle) {
         const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
         const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
         const int64_t total = __ldg(table.group_ray_begin + table.num_groups);
@@ -487,7 +656,33 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         while (need && pending < 0 && !exhausted) {
             if (next >= end) {
                 long long c = 0;
-                if (kSingle) {
+                if (kService) {
+                    long long seq = -1, chunk = 0;
+                    if (lane_id == 0) {
+                        int64_t sq = 0, ck = 0;
+                        if (service_take(table, svc_queue, svc_published, &sq, &ck)) { seq = sq; chunk = ck; }
+                    }
+                    seq = __shfl_sync(full, seq, 0);
+                    chunk = __shfl_sync(full, chunk, 0);
+                    svc_queue = __shfl_sync(full, static_cast<long long>(svc_queue), 0);
+                    svc_published = __shfl_sync(full, static_cast<long long>(svc_published), 0);
+                    if (seq < 0) { exhausted = true; break; }
+                    const int slot = static_cast<int>(seq & table.mask);
+                    const ServiceSlot &sl = table.slots[slot];
+                    const int64_t cb = chunk * sl.chunk_rays;
+                    const int64_t ce = min(cb + sl.chunk_rays, sl.job.num_rays);
+                    if (group >= 0 && sl.scene_id != table.slots[group].scene_id) {
+                        if (!__any_sync(full, has)) {
+                            group = slot; cur_slot = slot; next = cb; end = ce;   // idle warp: switch scenes now
+                        } else {
+                            pending = slot; pending_begin = cb; pending_end = ce;
+                            break;
+                        }
+                    } else {
+                        if (group < 0) group = slot;
+                        cur_slot = slot; next = cb; end = ce;
+                    }
+                } else if (kSingle) {
                     if (lane_id == 0) c = static_cast<long long>(atomicAdd(table.chunk_counter, 1ull));
                     c = __shfl_sync(full, c, 0);
                     if (c >= num_chunks) { exhausted = true; break; }
@@ -512,25 +707,27 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     }
                     if (c < 0) { exhausted = true; break; }
                 }
-                int64_t cb, ce;
-                int cg;
-                if (kSingle) {
-                    cb = c * table.chunk_rays;
-                    ce = min(cb + static_cast<int64_t>(table.chunk_rays), single.num_rays);
-                    cg = 0;
-                } else {
-                    const FastChunk ch = table.chunks[c];
-                    cb = ch.begin; ce = ch.end; cg = ch.group;
-                }
-                if (group >= 0 && cg != group) {
-                    if (!__any_sync(full, has)) {
-                        group = cg; next = cb; end = ce;  // idle warp: switch scenes now
+                if constexpr (!kService) {
+                    int64_t cb, ce;
+                    int cg;
+                    if (kSingle) {
+                        cb = c * table.chunk_rays;
+                        ce = min(cb + static_cast<int64_t>(table.chunk_rays), single.num_rays);
+                        cg = 0;
                     } else {
-                        pending = c;
-                        break;
+                        const FastChunk ch = table.chunks[c];
+                        cb = ch.begin; ce = ch.end; cg = ch.group;
                     }
-                } else {
-                    group = cg; next = cb; end = ce;
+                    if (group >= 0 && cg != group) {
+                        if (!__any_sync(full, has)) {
+                            group = cg; next = cb; end = ce;  // idle warp: switch scenes now
+                        } else {
+                            pending = c;
+                            break;
+                        }
+                    } else {
+                        group = cg; next = cb; end = ce;
+                    }
                 }
             }
             const int take = static_cast<int>(min(static_cast<int64_t>(__popc(need)), end - next));
@@ -540,15 +737,21 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 const int64_t g = next + rank;
                 int j = 0;
                 int64_t ri = g;
-                if (!kSingle) {
+                if (kService) {
+                    j = cur_slot;
+                } else if (!kSingle) {
                     const FastGroup &grp = table.groups[group];
                     j = find_job_range(table.ray_begin, grp.first_job, grp.first_job + grp.num_jobs - 1, g);
                     ri = g - __ldg(table.ray_begin + j);
                 }
-                const Job<float> &job = kSingle ? single : table.jobs[j];
+                const Job<float> &job = kSingle ? single : (kService ? table.slots[j].job : table.jobs[j]);
                 s.job = j;
                 s.ray = ri;
                 s.bounce = 0;
+#if AC_SPLIT_QUERIES
+                s.shadow_next = false;
+                s.surf = 0;
+#endif
                 s.queries = 0;
                 s.shadows = 0;
                 s.path = 0.0;
@@ -568,7 +771,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
 #pragma unroll
                 for (int b = 0; b < kBands; ++b) s.acc[b] = 1.0f;
                 has = true;
-                if (job.num_bounces <= 0) {
+                if (job.num_bounces <= 0) {   // the host refuses such jobs in service launches
                     atomicAdd(job.counters + 1, 1ull);
                     has = false;
                 }
@@ -578,8 +781,12 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         }
         if (!__any_sync(full, has)) {
             if (pending >= 0) {
-                const FastChunk ch = table.chunks[pending];
-                group = ch.group; next = ch.begin; end = ch.end;
+                if (kService) {
+                    group = static_cast<int>(pending); cur_slot = group; next = pending_begin; end = pending_end;
+                } else {
+                    const FastChunk ch = table.chunks[pending];
+                    group = ch.group; next = ch.begin; end = ch.end;
+                }
                 pending = -1;
                 continue;
             }
@@ -589,9 +796,193 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             }
         }
 
-        const FastScene &fs = kSingle ? single_fast : table.groups[group].fast;
-        const Job<float> &job = kSingle ? single : table.jobs[s.job];
+        const FastScene &fs = kSingle ? single_fast : (kService ? table.slots[group].fast : table.groups[group].fast);
+        const Job<float> &job = kSingle ? single : (kService ? table.slots[s.job].job : table.jobs[s.job]);
 
+#if AC_SPLIT_QUERIES
+        // ---- one query per lane per iteration: a lane runs the closest hit of its next bounce or the
+        // shadow ray of its last hit, whichever it needs, in the same traversal as the other lanes'.
+        bool finished = false, alive_at_end = false, count_hit = false;
+        const bool shadow_turn = has && s.shadow_next;
+        {
+            FRay query;
+            float found_t = 1e30f;
+            if (shadow_turn) {
+                const float tsx = job.src[0] - s.o[0], tsy = job.src[1] - s.o[1], tsz = job.src[2] - s.o[2];
+                const float d2 = tsx * tsx + tsy * tsy + tsz * tsz;
+                const float inv = rsqrtf(fmaxf(d2, 1e-30f));
+                const float sd[3] = {tsx * inv, tsy * inv, tsz * inv};
+                make_ray(query, s.o, sd);
+                found_t = d2 * inv - 1e-6f;
+            } else {
+                make_ray(query, s.o, s.d);
+            }
+            int found = -1;
+            scene_query(fs, query, has, shadow_turn, found_t, found);
+            bool bounce_done = false, deposit = false;
+            if (has && !shadow_turn) {
+                float t = found_t;
+                int surf = found;
+                bool from_walk = false;
+                if (surf < 0 && job.use_bvh) {
+                    // Missed everything: the reference's BVH walk reports the lowest visited surface.
+                    const int2 fb = fallback_walk(job.scene, s.o[0], s.o[1], s.o[2], s.d[0], s.d[1], s.d[2]);
+                    surf = fb.x;
+                    t = __int_as_float(fb.y);
+                    from_walk = true;
+                }
+                s.queries += 1;
+                bool dead = surf < 0 || t <= job.listener_radius || s.path > job.max_path_length;
+                if (!dead && s.bounce > 0) {
+                    if (sphere_before(s.o, s.d, job.lst, job.listener_radius, t)) dead = true;
+                    else if (job.source_distance > job.source_radius &&
+                             sphere_before(s.o, s.d, job.src, job.source_radius, t))
+                        dead = true;
+                }
+                if (dead) {
+                    finished = true;
+                } else {
+                    count_hit = true;
+                    float n[3];
+                    if (!from_walk) {
+                        winner_normal(job.scene, surf, query, t, n);
+                    } else {
+                        n[0] = __ldg(job.scene.normals + 3 * surf);
+                        n[1] = __ldg(job.scene.normals + 3 * surf + 1);
+                        n[2] = __ldg(job.scene.normals + 3 * surf + 2);
+                        if (n[0] * s.d[0] + n[1] * s.d[1] + n[2] * s.d[2] > 0.0f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
+                    }
+                    if (job.ray_surfaces) job.ray_surfaces[s.ray * job.num_bounces + s.bounce] = surf;
+                    const float hx = s.o[0] + t * s.d[0] + 1e-2f * n[0];
+                    const float hy = s.o[1] + t * s.d[1] + 1e-2f * n[1];
+                    const float hz = s.o[2] + t * s.d[2] + 1e-2f * n[2];
+                    if (kVisual && s.vslot >= 0) visual_hit(job, s.vslot, s.bounce, hx, hy, hz, surf);
+                    s.o[0] = hx; s.o[1] = hy; s.o[2] = hz;
+                    s.hit_t = t;
+                    s.surf = surf;
+                    s.n[0] = n[0]; s.n[1] = n[1]; s.n[2] = n[2];
+                    const float tsx = job.src[0] - hx, tsy = job.src[1] - hy, tsz = job.src[2] - hz;
+                    const float d2 = tsx * tsx + tsy * tsy + tsz * tsz;
+                    const float inv = rsqrtf(fmaxf(d2, 1e-30f));
+                    const float dist = d2 * inv;
+                    const bool need_shadow = dist > job.irradiance_min_distance &&
+                                             n[0] * tsx * inv + n[1] * tsy * inv + n[2] * tsz * inv > 0.0f;
+                    if (need_shadow) s.shadow_next = true;
+                    else bounce_done = true;
+                }
+            }
+            // per-surface hit counters: one atomic per distinct (job, surface) in the warp.  The
+            // lanes of a warp trace jobs of one scene group of at most 1024 consecutive jobs
+            // (surfaces < 2^22), so (job mod 1024, surface) is a 32-bit key -- cheaper to match
+            // than a 64-bit one.
+            const unsigned counting = __ballot_sync(full, count_hit);
+            if (count_hit) {
+                const unsigned key = ((static_cast<unsigned>(s.job) & 1023u) << 22) | static_cast<unsigned>(s.surf);
+                const unsigned same = __match_any_sync(counting, key);
+                if (lane_id == __ffs(same) - 1)
+                    atomicAdd(job.hit_counts + s.surf, static_cast<unsigned long long>(__popc(same)));
+            }
+            if (shadow_turn) {
+                s.shadow_next = false;
+                s.shadows += 1;
+                deposit = found < 0;
+                bounce_done = true;
+            }
+            if (bounce_done) {
+                const int surf = s.surf;
+                const float t = s.hit_t;
+                const float *n = s.n;
+                const Quad<float> m0 = ldq(job.scene.mats + static_cast<size_t>(surf) * kMatStride);
+                const Quad<float> m1 = ldq(job.scene.mats + static_cast<size_t>(surf) * kMatStride + 4);
+                const float refl[kBands] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y};
+                const float scat = m1.z;
+                if (deposit) {
+                    const float tsx = job.src[0] - s.o[0], tsy = job.src[1] - s.o[1], tsz = job.src[2] - s.o[2];
+                    const float d2 = tsx * tsx + tsy * tsy + tsz * tsz;
+                    const float inv_dist = rsqrtf(fmaxf(d2, 1e-30f));
+                    const float dist = d2 * inv_dist;
+                    const float sd[3] = {tsx * inv_dist, tsy * inv_dist, tsz * inv_dist};
+                    const float facing = n[0] * sd[0] + n[1] * sd[1] + n[2] * sd[2];
+                    const float diffuse = static_cast<float>(1.0 / kPi) * scat * facing;
+                    float half[3];
+                    normalize3f(sd[0] - s.d[0], sd[1] - s.d[1], sd[2] - s.d[2], half);
+                    float cos_half = half[0] * n[0] + half[1] * n[1] + half[2] * n[2];
+                    cos_half = cos_half > 0.0f ? cos_half : 0.0f;
+                    const float specular = ((job.specular_exponent + 2.0f) * static_cast<float>(1.0 / (8.0 * kPi))) *
+                                           (1.0f - scat) * __powf(cos_half, job.specular_exponent);
+                    // dist > irradiance_min_distance here, so max(dist, min) = dist
+                    const float distance_term = static_cast<float>(1.0 / (4.0 * kPi)) * (inv_dist * inv_dist);
+                    const float source_cosine = -(job.fwd[0] * sd[0] + job.fwd[1] * sd[1] + job.fwd[2] * sd[2]);
+                    const float gain_base = fabsf((1.0f - job.dipole_weight) + job.dipole_weight * source_cosine);
+                    const float source_gain = job.dipole_power == 1.0f ? gain_base : __powf(gain_base, job.dipole_power);
+                    const double rel_delay =
+                        (s.path + static_cast<double>(t) + static_cast<double>(dist)) * job.inv_speed_of_sound -
+                        job.direct_delay;
+                    const double q = floor(rel_delay * job.inv_bin_duration);
+                    if (q >= 0.0 && q < static_cast<double>(job.num_bins)) {
+                        const int bin = static_cast<int>(q);
+                        const float common = job.ray_scale * source_gain * distance_term * (diffuse + specular);
+                        long long esum = 0;
+                        float energy_sum = 0.0f;
+#pragma unroll
+                        for (int b = 0; b < kBands; ++b) {
+                            const float e = common * refl[b] * s.acc[b];
+                            if (kVisual) energy_sum += e;
+                            const long long qe = quantize(e, job.energy_scale);
+                            add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
+                            if (kAmb) {
+                                const float *d0 = s.d0;
+                                unsigned long long *a =
+                                    job.ambisonic_fx + 2 * (static_cast<size_t>(b) * 4 * job.num_bins + bin);
+                                const size_t stride = 2 * static_cast<size_t>(job.num_bins);
+                                add_fixed(a, qe);
+                                add_fixed(a + stride, quantize(e * d0[0], job.energy_scale));
+                                add_fixed(a + 2 * stride, quantize(e * d0[1], job.energy_scale));
+                                add_fixed(a + 3 * stride, quantize(e * d0[2], job.energy_scale));
+                            }
+                            esum += qe;
+                        }
+                        atomicAdd(job.contrib_counts + surf, 1ull);
+                        add_fixed(job.surface_energy_fx + 2 * static_cast<size_t>(surf), esum);
+                        if (kVisual && s.vslot >= 0)
+                            visual_contribution(job, s.vslot, s.bounce, energy_sum,
+                                                static_cast<float>(s.path + static_cast<double>(t) +
+                                                                   static_cast<double>(dist)));
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < kBands; ++b) s.acc[b] *= refl[b];
+                s.path += static_cast<double>(t);
+                bool use_diffuse;
+                int sample;
+                if (!kPhilox) {
+                    const size_t k = static_cast<size_t>(s.bounce) * job.num_rays + s.ray;
+                    use_diffuse = job.diffuse_random[k] < scat;
+                    sample = use_diffuse ? job.diffuse_indices[k] : 0;
+                } else {
+                    const u32x4 rr = trace_draw(job.seed, job.stream_key, static_cast<uint32_t>(s.ray),
+                                                static_cast<uint32_t>(s.bounce) + 1u);
+                    use_diffuse = u01_53(rr.x, rr.y) < static_cast<double>(scat);
+                    sample = static_cast<int>(below(rr.z, static_cast<uint32_t>(job.num_bank)));
+                }
+                if (use_diffuse) {
+                    const float *bs = job.diffuse_bank + 3 * sample;
+                    diffuse_direction_f(__ldg(bs), __ldg(bs + 1), __ldg(bs + 2), n[0], n[1], n[2], s.d);
+                } else {
+                    const float dot = s.d[0] * n[0] + s.d[1] * n[1] + s.d[2] * n[2];
+                    normalize3f(s.d[0] - 2.0f * dot * n[0], s.d[1] - 2.0f * dot * n[1], s.d[2] - 2.0f * dot * n[2],
+                                s.d);
+                }
+                s.bounce += 1;
+                if (s.path > job.max_path_length) {
+                    finished = true;
+                } else if (s.bounce >= job.num_bounces) {
+                    finished = true;
+                    alive_at_end = true;
+                }
+            }
+        }
+#else
         // ---- two queries per bounce through one copy of the scan: phase 0 finds the
         // closest hit, phase 1 casts the shadow ray toward the source.
         FRay ray;
@@ -769,9 +1160,13 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             }
         }
 
+#endif
+
         // ---- ray completion statistics, one atomic per distinct job in the warp
         const unsigned ending = __ballot_sync(full, finished);
+        bool last_ray = false;   // service launches: this lane's job has now finished every ray
         if (finished) {
+            if (kService) __threadfence();   // this ray's sums land before its job counts it finished
             const unsigned grp = __match_any_sync(ending, static_cast<unsigned>(s.job));
             const unsigned q_sum = __reduce_add_sync(grp, static_cast<unsigned>(s.queries));
             const unsigned q_max = __reduce_max_sync(grp, static_cast<unsigned>(s.queries));
@@ -782,10 +1177,23 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 if (alive_sum) atomicAdd(job.counters + 1, static_cast<unsigned long long>(alive_sum));
                 atomicAdd(job.counters + 2, static_cast<unsigned long long>(q_sum));
                 if (sh_sum) atomicAdd(job.counters + 3, static_cast<unsigned long long>(sh_sum));
+                if (kService) {
+                    const unsigned long long n = static_cast<unsigned long long>(__popc(grp));
+                    const unsigned long long before = atomicAdd(&table.slot_state[s.job].rays_finished, n);
+                    last_ray = before + n == static_cast<unsigned long long>(job.num_rays);
+                }
             }
             if (job.ray_surfaces)
                 for (int b = s.bounce; b < job.num_bounces; ++b) job.ray_surfaces[s.ray * job.num_bounces + b] = -1;
             has = false;
+        }
+        if (kService) {
+            unsigned finishing = __ballot_sync(full, last_ray);
+            while (finishing) {
+                const int src = __ffs(finishing) - 1;
+                finishing &= finishing - 1u;
+                service_finish(table, __shfl_sync(full, s.job, src), lane_id);
+            }
         }
     }
 }

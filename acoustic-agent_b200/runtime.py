@@ -447,6 +447,78 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
     workspace._keepalive = keep  # type: ignore[attr-defined]
 
 
+class TraceService:
+    """Continuous batching on one GPU (ac_service_*): one persistent trace launch fed while it runs.
+
+    ``submit`` appends (scene, spec, buffers) jobs -- float32, Philox stream -- and returns their sequence
+    numbers; ``poll`` returns the sequence numbers whose outputs are complete (never blocks).  Jobs submitted
+    while others are on the GPU join the running launch.  The service keeps each job's parameter tables and
+    buffers alive until it is reported done.
+    """
+
+    def __init__(self, device: int = 0, *, capacity: int = 4096, blocks_per_sm: int = 2, block_size: int = 0,
+                 chunk_rays: int = 0, idle_timeout_s: float = 0.02) -> None:
+        self.device = require_cuda(device)
+        cfg = _lib.ACServiceConfig(int(device), int(capacity), int(blocks_per_sm), int(block_size), int(chunk_rays),
+                                   0, int(idle_timeout_s * 1e9))
+        handle = ctypes.c_void_p()
+        _lib.check(_lib.load().ac_service_create(ctypes.byref(cfg), ctypes.byref(handle)), "ac_service_create")
+        self.handle = handle
+        self._keep: dict[int, Any] = {}
+        self._done = (ctypes.c_int64 * 4096)()
+
+    def submit(self, jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]]) -> list[int]:
+        """Append jobs; raises BackendError(AC_ERR_CAPACITY) when the ring cannot take them yet."""
+        if not jobs:
+            return []
+        arr = (_lib.ACJob * len(jobs))()
+        keep: list[Any] = []
+        for k, (scene, spec, buffers) in enumerate(jobs):
+            if spec.rng != "philox" or spec.precision != "float32":
+                raise ValueError("the trace service runs float32 jobs on the Philox stream")
+            arr[k].scene = scene.handle.value
+            arr[k].params = params_struct(spec, self.device, keep)
+            arr[k].outputs = buffers.outputs_struct()
+            keep.append((scene, buffers))
+        first = ctypes.c_int64()
+        _lib.check(_lib.load().ac_service_submit(self.handle, arr, len(jobs), ctypes.byref(first)),
+                   "ac_service_submit")
+        seqs = list(range(first.value, first.value + len(jobs)))
+        for seq in seqs:
+            self._keep[seq] = keep
+        return seqs
+
+    def poll(self) -> list[int]:
+        out: list[int] = []
+        while True:
+            n = ctypes.c_int32()
+            _lib.check(_lib.load().ac_service_poll(self.handle, self._done, len(self._done), ctypes.byref(n)),
+                       "ac_service_poll")
+            out.extend(self._done[k] for k in range(n.value))
+            if n.value < len(self._done):
+                break
+        for seq in out:
+            self._keep.pop(seq, None)
+        return out
+
+    def info(self) -> dict[str, int]:
+        st = _lib.ACServiceStats()
+        _lib.check(_lib.load().ac_service_info(self.handle, ctypes.byref(st)), "ac_service_info")
+        return {k: int(getattr(st, k)) for k, _ in st._fields_}
+
+    def close(self) -> None:
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            _lib.check(_lib.load().ac_service_destroy(self.handle), "ac_service_destroy")
+            self.handle = ctypes.c_void_p()
+            self._keep.clear()
+
+    def __del__(self) -> None:  # pragma: no cover - interpreter teardown order varies
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BatchTicket:
     """Completion ticket of ac_batch_submit: ``done()`` polls, ``wait()`` blocks, ``release()`` frees it."""
 

@@ -40,7 +40,7 @@ from typing import Any, Sequence
 import numpy as np
 import torch
 
-from acoustic_agent_b200 import autotune, bands, rng, runtime
+from acoustic_agent_b200 import _lib, autotune, bands, rng, runtime
 from acoustic_agent_b200.batching import NUM_BANDS
 from acoustic_agent_b200.directivity import source_directivity, source_forward
 from acoustic_agent_b200.scene import SceneArrays, compile_scene
@@ -473,6 +473,216 @@ class Server:
                       evictions=self.scenes.evictions, peak_bytes=peak)
 
     def close(self) -> None:
+        self.scenes.close()
+
+
+@dataclass
+class _Live:
+    """An admitted request of the continuous server: its jobs on the trace service, then its synthesis."""
+
+    request: Request
+    specs: list[runtime.TraceSpec]
+    scene: runtime.DeviceScene
+    buffers: list[runtime.TraceBuffers]
+    seqs: list[int]
+    remaining: set[int]
+    bytes: int
+    admitted_s: float
+    est_ray_bounces: float
+    irs: list[torch.Tensor] = field(default_factory=list)
+    host: torch.Tensor | None = None
+    done: torch.cuda.Event | None = None
+
+
+class ContinuousServer:
+    """Continuous batching at kernel level on one GPU.
+
+    One persistent trace launch (runtime.TraceService, ac_service_*) runs while requests arrive: an admitted
+    request's jobs are appended to the launch's job ring at once, and its warps pick them up as they run out
+    of older work, so a request never waits for a batch to form or for another batch's launch to end.  When a
+    request's last job is done, its band synthesis (one ragged launch for every request that completed in the
+    same poll) and the copy to pinned host memory run on a second stream beside the persistent launch, whose
+    grid leaves room for them (two blocks per SM by default).
+
+    Admission: a request is admitted when its device footprint fits the HBM budget (resident scenes plus the
+    outputs of requests in flight); one that could never fit is rejected.  With `slo_s`, a request is also
+    rejected at arrival when the work already admitted plus its own, at the throughput measured so far
+    (`capacity_rb_per_s` until a first measurement), would not finish within `slo_s` of its arrival: overload
+    is shed instead of queueing without bound.  Requests that wait for memory are admitted in arrival order.
+    Each result is the same as the request rendered alone (rays keyed by request identity, exact fixed-point
+    sums, synthesis noise keyed by the job's seed).
+    """
+
+    def __init__(self, device: int = 0, *, hbm_budget: int | None = None, tune: bool = True,
+                 slo_s: float | None = None, capacity_rb_per_s: float = 4.0e9, blocks_per_sm: int = 2,
+                 capacity: int = 4096, idle_timeout_s: float = 0.02, chunk_rays: int = 0) -> None:
+        self.dev = runtime.require_cuda(device)
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.dev)
+            hbm_budget = int(free * 0.8)
+        self.budget = int(hbm_budget)
+        self.scenes = SceneCache(self.dev.index, tune=tune)
+        self.service = runtime.TraceService(self.dev.index, capacity=capacity, blocks_per_sm=blocks_per_sm,
+                                            chunk_rays=chunk_rays, idle_timeout_s=idle_timeout_s)
+        self.synth_stream = torch.cuda.Stream(self.dev)
+        self.synth_ws = runtime.SynthBatchWorkspace(self.dev)
+        self.slo_s = slo_s
+        self.capacity_rb_per_s = float(capacity_rb_per_s)
+        self.in_use = 0
+        self.bounces_per_ray = 40.0      # running estimate of ray-bounces per ray, from finished jobs
+        self._sizer = Server.__new__(Server)   # footprint arithmetic shared with the batch server
+        self._sizer.scenes, self._sizer.late_tail = self.scenes, False
+
+    def footprint(self, req: Request, specs: Sequence[runtime.TraceSpec]) -> int:
+        return Server.footprint(self._sizer, req, specs)
+
+    def _fits(self, need: int) -> bool:
+        if self.scenes.resident_bytes() + self.in_use + need <= self.budget:
+            return True
+        if self.service.info()["running_launches"] == 0:
+            # a running launch may still hold an evicted scene's lines in L1: evict only between launches
+            self.scenes.evict_idle(self.scenes.resident_bytes() + self.in_use + need - self.budget)
+        return self.scenes.resident_bytes() + self.in_use + need <= self.budget
+
+    def _est_rb(self, specs: Sequence[runtime.TraceSpec]) -> float:
+        return sum(min(float(s.num_bounces), self.bounces_per_ray) * s.num_rays for s in specs)
+
+    def _admit(self, req: Request, specs: list[runtime.TraceSpec], need: int, now: float) -> _Live:
+        scene = self.scenes.acquire(req.workload, specs[0])
+        try:
+            buffers = [runtime.TraceBuffers.allocate(scene.num_surfaces, s.num_bins, self.dev) for s in specs]
+            seqs = self.service.submit([(scene, s, b) for s, b in zip(specs, buffers)])
+        except Exception:
+            self.scenes.release(req.workload)
+            raise
+        self.in_use += need
+        return _Live(req, specs, scene, buffers, seqs, set(seqs), need, now, self._est_rb(specs))
+
+    def _synthesize(self, lives: list[_Live]) -> None:
+        """Band IRs of requests whose traces are done: one ragged synthesis and one host copy per request."""
+        synth = []
+        with torch.cuda.stream(self.synth_stream):
+            for live in lives:
+                fs = live.request.workload.config.fs
+                lengths = [s.num_bins * bands.samples_per_bin(s.bin_duration, fs) for s in live.specs]
+                store = torch.empty(NUM_BANDS * sum(lengths), dtype=torch.float32, device=self.dev)
+                off = 0
+                for s, b, n in zip(live.specs, live.buffers, lengths):
+                    out = store[off:off + NUM_BANDS * n].view(NUM_BANDS, n)
+                    off += NUM_BANDS * n
+                    live.irs.append(out)
+                    synth.append(runtime.SynthJob(b.echogram, out, fs, s.bin_duration, seed=int(s.seed) + 7,
+                                                  direct_delay=max(0.0, float(s.direct_delay)),
+                                                  speed_of_sound=s.speed_of_sound))
+                live.host = torch.empty(store.shape, dtype=torch.float32, pin_memory=True)
+                live.keep = store    # type: ignore[attr-defined]
+            runtime.synthesize_batch(synth, self.synth_ws, stream=self.synth_stream)
+            for live in lives:
+                live.host.copy_(live.keep, non_blocking=True)   # type: ignore[attr-defined]
+                live.done = torch.cuda.Event()
+                live.done.record(self.synth_stream)
+
+    def serve(self, requests: Sequence[Request], *, realtime: bool = True, idle_sleep_s: float = 2e-4) -> Report:
+        """Run every request to completion (or rejection); arrivals follow `arrival_s` when `realtime`."""
+        pending = deque(sorted(requests, key=lambda r: r.arrival_s))
+        waiting: deque[tuple[Request, list[runtime.TraceSpec], int]] = deque()
+        tracing: dict[int, _Live] = {}      # sequence number -> its request
+        synthesizing: list[_Live] = []
+        results: list[Result] = []
+        outstanding_rb = 0.0               # estimated ray-bounces admitted and not yet traced
+        done_rb = 0
+        busy_s = 0.0                       # time with jobs on the trace service
+        peak = 0
+        t0 = time.perf_counter()
+        tick = t0
+        clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
+        live_count = 0
+        while pending or waiting or tracing or synthesizing:
+            now = clock()
+            was_busy = bool(tracing)
+            # arrivals: reject what can never fit, or what the admitted work would make miss its SLO
+            while pending and pending[0].arrival_s <= now:
+                req = pending.popleft()
+                specs = request_jobs(req)
+                need = self.footprint(req, specs)
+                t = time.perf_counter() - t0
+                if need > self.budget:   # could not fit even on an idle device
+                    results.append(Result(req, [], 0, t, t, error=f"needs {need} bytes of device memory; "
+                                                                   f"the budget is {self.budget}"))
+                    continue
+                if self.slo_s is not None:
+                    rate = (done_rb / busy_s) if busy_s > 0.5 and done_rb > 0 else self.capacity_rb_per_s
+                    wait = (outstanding_rb + sum(self._est_rb(w[1]) for w in waiting) + self._est_rb(specs)) / rate
+                    if wait > self.slo_s:
+                        results.append(Result(req, [], 0, t, t, error=f"overloaded: about {wait:.2f} s of traced work "
+                                                                       f"ahead exceeds the {self.slo_s:g} s limit"))
+                        continue
+                waiting.append((req, specs, need))
+            # admission in arrival order while memory allows; the ring may ask us to come back later
+            while waiting:
+                req, specs, need = waiting[0]
+                if not self._fits(need):
+                    break
+                try:
+                    live = self._admit(req, specs, need, time.perf_counter() - t0)
+                except _lib.BackendError as exc:
+                    if exc.code != _lib.AC_ERR_CAPACITY:
+                        raise
+                    break   # the job ring is full: admit it after the next completions
+                waiting.popleft()
+                for seq in live.seqs:
+                    tracing[seq] = live
+                outstanding_rb += live.est_ray_bounces
+                live_count += 1
+                peak = max(peak, self.in_use + self.scenes.resident_bytes())
+            # traces that finished: their requests go to synthesis once all their jobs are done
+            finished = []
+            for seq in self.service.poll():
+                live = tracing.pop(seq)
+                live.remaining.discard(seq)
+                if not live.remaining:
+                    finished.append(live)
+            if finished:
+                for live in finished:
+                    rb = sum(int(b.counters[2].item()) for b in live.buffers)
+                    rays = sum(s.num_rays for s in live.specs)
+                    self.bounces_per_ray = 0.8 * self.bounces_per_ray + 0.2 * rb / max(rays, 1)
+                    done_rb += rb
+                    outstanding_rb -= live.est_ray_bounces
+                    live.ray_bounces = rb     # type: ignore[attr-defined]
+                self._synthesize(finished)
+                synthesizing.extend(finished)
+            for live in list(synthesizing):
+                if live.done is not None and live.done.query():
+                    synthesizing.remove(live)
+                    host = live.host.numpy()
+                    irs, off = [], 0
+                    for ir in live.irs:
+                        irs.append(host[off:off + ir.numel()].reshape(ir.shape).copy())
+                        off += ir.numel()
+                    results.append(Result(live.request, irs, live.ray_bounces,   # type: ignore[attr-defined]
+                                          live.admitted_s, time.perf_counter() - t0))
+                    self.scenes.release(live.request.workload)
+                    self.in_use -= live.bytes
+            nowp = time.perf_counter()
+            if was_busy:
+                busy_s += nowp - tick
+            tick = nowp
+            if not realtime and not tracing and not waiting and not synthesizing and pending:
+                continue
+            if tracing or synthesizing or (pending and realtime):
+                time.sleep(idle_sleep_s)
+        served = [r for r in results if r.error is None]
+        makespan = max((r.done_s for r in served), default=0.0) - min((r.request.arrival_s for r in served),
+                                                                      default=0.0)
+        info = self.service.info()
+        return Report(results=sorted(results, key=lambda r: r.request.id), makespan_s=makespan,
+                      rirs=sum(r.request.num_rirs for r in served), ray_bounces=sum(r.ray_bounces for r in served),
+                      batches=int(info["launches"]), max_inflight_seen=live_count, scene_hits=self.scenes.hits,
+                      scene_misses=self.scenes.misses, evictions=self.scenes.evictions, peak_bytes=peak)
+
+    def close(self) -> None:
+        self.service.close()
         self.scenes.close()
 
 

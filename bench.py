@@ -405,6 +405,14 @@ def main() -> int:
     parser.add_argument("--no-config1", dest="with_config1", action="store_false",
                         help="mixed_batch: skip the single-scene U-room figures added to the line")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
+    parser.add_argument("--rates", default="", help="serving: comma-separated arrival rates (overrides --rate)")
+    parser.add_argument("--runs", type=int, default=1, help="serving: runs per rate")
+    parser.add_argument("--server", default="continuous", choices=("continuous", "batched"),
+                        help="serving: kernel-level continuous batching or batch-level server")
+    parser.add_argument("--slo", type=float, default=2.0,
+                        help="serving (continuous): shed requests whose admitted work ahead exceeds this, seconds")
+    parser.add_argument("--capacity-rb", type=float, default=4.0e9,
+                        help="serving (continuous): ray-bounces/s assumed until the first measurement")
     parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     parser.add_argument("--policy", default="small_first", choices=("small_first", "fifo"),
                         help="serving: order in which waiting requests join a batch")
@@ -764,6 +772,47 @@ def reference_job_loop(population, jobs, picks, *, accelerator: str, precision: 
                        "after one untimed call")}
 
 
+def facade_rirs(workload, runs: int = 2) -> dict:
+    """The reference's public facade on one workload, its reflection trace routed to this backend:
+    ``AcousticAgent.create(scene="geometry", room=Room(...), config=SimConfig(rt_accelerator="b200"),
+    receiver_model=<the workload's circular array>).run()`` (api.py:172-245, :405-475; the channel loop of
+    engine.py:64-73), after one untimed call.  Everything but the reflection trace is the reference's own code
+    on the host (direct sound, diffraction, band synthesis, decay fits); late tail off, as in the reference's
+    accelerator benchmark."""
+    ref, reason = import_reference_package()
+    if ref is None:
+        return {"unavailable": reason}
+    steam_rt, models = ref
+    from acoustic_agent import api
+    from acoustic_agent_b200 import backend
+    cfg = workload.config
+    room = reference_scene(steam_rt, models, workload.spec).room
+    sim = models.SimConfig(fs=cfg.fs, duration_s=cfg.duration_s, rt_duration_s=cfg.rt_duration_s,
+                           rt_num_rays=cfg.rt_num_rays, rt_num_bounces=cfg.rt_num_bounces,
+                           rt_bin_duration_s=cfg.rt_bin_duration_s, intersection_backend=cfg.intersection_backend,
+                           late_tail=False, adaptive_geometry_bounces=False, rt_accelerator="b200",
+                           rt_precision="float32", seed=cfg.seed)
+    center = np.mean(np.asarray(workload.listeners, dtype=float), axis=0)
+    array = {"type": "circular", "count": len(workload.listeners), "radius_m": 0.05}
+    handle = backend.install(steam_rt)
+    try:
+        agent = api.AcousticAgent.create(scene="geometry", room=room, config=sim, receiver_model=array,
+                                         source_model=workload.source_model, source=workload.sources[0],
+                                         receiver=tuple(center))
+        agent.run()
+        t0 = time.perf_counter()
+        for _ in range(runs):
+            result = agent.run()
+        seconds = (time.perf_counter() - t0) / runs
+    finally:
+        handle.uninstall()
+    refl = result.metadata["steam_audio"]["reflections"]
+    channels = int(result.rir.shape[0])
+    return {"rirs_per_s": channels / seconds, "seconds_per_run": seconds, "channels": channels,
+            "trace_kernel_s_channel0": refl.get("kernel_time_s"), "accelerator": refl.get("accelerator"),
+            "sample": f"AcousticAgent.create(...).run() over {channels} channels, mean of {runs} after 1 warm-up"}
+
+
 def mix_bytes_per_ray_bounce(arrays, jobs, ray_bounces_per_job, sample_rays: int = 512) -> float:
     """Algorithmic bytes per ray-bounce over the mix (roofline numerator, per-unit figure).
 
@@ -990,6 +1039,8 @@ def run_mixed_batch(args) -> int:
             line["batched_vs_reference_cuda_plain"] = value / ref_cuda["rirs_per_s"]
     if args.with_config1:
         line["config1_u_room"] = run_single_scene(args, "u_room_20_boxes", extras_only=True)
+        if not args.no_cpu_baseline and world == 1:
+            line["config1_u_room"]["facade"] = facade_rirs(workloads.u_furnished(1729))
     print(json.dumps(line), flush=True)
     barrier()
     if dist is not None:
@@ -998,12 +1049,14 @@ def run_mixed_batch(args) -> int:
 
 
 def run_serving(args) -> int:
-    """Continuous-batching server on a Poisson request stream over the mixed-size population.
+    """Serving: Poisson request streams over the mixed-size population, one line with every rate.
 
-    Requests arrive at `--rate` per second for `--duration` seconds; 20 % move
-    their source along a seeded 3 m path with 8 keyframes.  Scenes are uploaded
-    and tuned before the stream starts (a warm, resident scene cache).
-    Latency = arrival to band IRs in host memory.
+    Requests arrive at each rate of `--rates` (req/s) for `--duration` seconds; 20 % move their source along a
+    seeded 3 m path with 8 keyframes.  Scenes are uploaded and tuned before the streams start (a warm,
+    resident scene cache).  Latency = arrival to band IRs in host memory.  `--server continuous` (default)
+    is the kernel-level continuous batcher (one persistent trace launch fed while it runs, overload shed at
+    arrival when the admitted work would miss `--slo` seconds); `--server batched` the batch-level server.
+    Each rate runs `--runs` times on fresh arrival seeds.
     """
     import torch
     from acoustic_agent_b200 import serving, workloads
@@ -1013,38 +1066,58 @@ def run_serving(args) -> int:
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
     population = workloads.mixed_batch(1730, 64)
-    stream = workloads.request_stream(1729, rate_hz=args.rate, duration_s=args.duration, population=population)
-    requests = serving.requests_from_stream(stream)
-    server = serving.Server(local, max_inflight=args.max_inflight, policy=args.policy,
-                            max_batch_rays=args.max_batch_rays, late_tail=args.late_tail,
-                            trace_blocks_per_sm=args.trace_blocks_per_sm)
+    rates = [float(r) for r in str(args.rates).split(",")] if args.rates else [args.rate]
+    if args.server == "continuous":
+        server = serving.ContinuousServer(local, slo_s=args.slo, capacity_rb_per_s=args.capacity_rb)
+    else:
+        server = serving.Server(local, max_inflight=args.max_inflight, policy=args.policy,
+                                max_batch_rays=args.max_batch_rays, late_tail=args.late_tail,
+                                trace_blocks_per_sm=args.trace_blocks_per_sm)
     t0 = time.perf_counter()
     for w in population:   # warm the resident scene cache (upload + tune) before the clock starts
         req = serving.Request(-1, w, [w.sources[0]])
         server.scenes.acquire(w, serving.request_jobs(req)[0])
         server.scenes.release(w)
     warm_s = time.perf_counter() - t0
-    # warm-up: a short burst of the same mix (kernels, allocator, pinned pool)
-    server.serve(requests[: min(len(requests), 8)], realtime=False)
+    warm = serving.requests_from_stream(workloads.request_stream(1, rate_hz=20.0, duration_s=0.4,
+                                                                 population=population))
+    server.serve(warm, realtime=False)   # kernels, allocator, pinned pool
+    table = []
     sampler = ClockSampler(local)
     with sampler:
-        report = server.serve(requests, realtime=True)
-    server.close()
-    s = report.summary()
+        for rate in rates:
+            for run in range(args.runs):
+                stream = workloads.request_stream(1729 + 97 * run, rate_hz=rate, duration_s=args.duration,
+                                                  population=population)
+                requests = serving.requests_from_stream(stream)
+                report = server.serve(requests, realtime=True)
+                s = report.summary()
+                served = [r for r in report.results if r.error is None]
+                table.append({
+                    "rate_req_s": rate, "run": run, "requests": len(requests), "admitted": len(served),
+                    "rejected": s["rejected"], "offered_rirs_per_s": sum(r.num_rirs for r in requests) / args.duration,
+                    "rirs_per_s": s["rirs_per_s"], "ray_bounces_per_s": s["ray_bounces_per_s"],
+                    "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
+                    "max_admitted_at_once": s["max_inflight"], "launches_or_batches": s["batches"]})
+    if hasattr(server, "close"):
+        server.close()
+    by_rate = {}
+    for rate in rates:
+        rows = [r for r in table if r["rate_req_s"] == rate]
+        by_rate[f"{rate:g}"] = {k: float(np.mean([r[k] for r in rows])) for k in
+                                ("rirs_per_s", "p50_ms", "p99_ms", "admitted", "rejected", "offered_rirs_per_s")}
+    head = by_rate[f"{rates[0]:g}"]
     line = {
-        "metric": METRIC, "value": s["rirs_per_s"], "unit": "RIRs/s", "n_gpus": 1, "steps": len(requests),
-        "warmup": min(len(requests), 8), "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator, Poisson arrivals)",
-        "config": {"workload": f"serving: Poisson {args.rate:g} req/s for {args.duration:g} s over 64 mixed scenes, "
-                               "20% moving sources x 8 keyframes", "requests": len(requests), "policy": args.policy,
-                   "max_batch_rays": args.max_batch_rays, "late_tail": args.late_tail,
-                   "trace_blocks_per_sm": args.trace_blocks_per_sm,
-                   "moving": sum(r.moving for r in requests), "max_inflight": server.max_inflight},
-        "latency_ms": {"p50": s["p50_ms"], "p99": s["p99_ms"]},
-        "ray_bounces_per_s": s["ray_bounces_per_s"], "rirs": s["rirs"], "makespan_s": s["makespan_s"],
-        "batches": s["batches"], "max_inflight_seen": s["max_inflight"], "scene_cache": s["scene_cache"],
-        "offered_rirs_per_s": s["rirs"] / args.duration, "warm_cache_s": warm_s,
-        "e2e": {"value": s["rirs_per_s"], "unit": "RIRs/s", "note": "arrival to host band IRs"},
+        "metric": METRIC, "value": head["rirs_per_s"], "unit": "RIRs/s", "n_gpus": 1, "steps": len(table),
+        "warmup": len(warm), "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded scene generator, Poisson arrivals)",
+        "config": {"workload": f"serving: Poisson arrivals at {', '.join(f'{r:g}' for r in rates)} req/s for "
+                               f"{args.duration:g} s each over 64 mixed scenes, 20% moving sources x 8 keyframes",
+                   "server": args.server, "slo_s": args.slo if args.server == "continuous" else None,
+                   "runs_per_rate": args.runs},
+        "latency_ms": {"p50": head["p50_ms"], "p99": head["p99_ms"]},
+        "by_rate": by_rate, "runs": table, "warm_cache_s": warm_s,
+        "e2e": {"value": head["rirs_per_s"], "unit": "RIRs/s", "note": "arrival to host band IRs"},
         "clocks": sampler.summary(),
     }
     print(json.dumps(line), flush=True)

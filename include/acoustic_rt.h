@@ -320,6 +320,57 @@ int ac_batch_poll(ac_batch_ticket_t ticket, int32_t *done);
 int ac_batch_wait(ac_batch_ticket_t ticket);
 int ac_batch_release(ac_batch_ticket_t ticket);
 
+/* Continuous batching: one persistent float32 trace launch fed while it
+ * runs.  Replaces the reference's request loops, which trace one job to
+ * completion before the next starts (api.py:583-639 `run_many`,
+ * batch.py:139-185, engine.py:64-73), as the batched launch above does, but
+ * jobs submitted while others are on the GPU join the running launch: its
+ * warps take chunks of rays job by job from a ring of job slots in device
+ * memory, so a new job starts as soon as warps run out of older work.
+ *
+ * ac_service_submit appends jobs (the ac_job of ac_trace_batch; float32,
+ * Philox stream, no ambisonics, visual candidates or recorded rays, at least
+ * one bounce) and returns their sequence numbers first_seq ..
+ * first_seq + num_jobs - 1; it returns once their descriptors are in device
+ * memory, and starts a launch if none is running.  It zeroes the jobs'
+ * outputs itself.  When the ring cannot take the jobs yet it fails with
+ * AC_ERR_CAPACITY: poll and submit again.  ac_service_poll writes the
+ * sequence numbers of jobs whose outputs (fixed-point sums, counters, float32
+ * echogram and surface energy) are complete since the last poll; it never
+ * blocks.  A job's outputs, and its scene, must stay alive until it is
+ * reported done.  Keep polling while jobs are in flight: a launch whose
+ * warps find no work for idle_timeout_ns ends on its own (every wait in the
+ * kernel is bounded), and a poll or submit starts the next one when needed.
+ * Results are the same as ac_trace / ac_trace_batch on the same job: rays are
+ * keyed by (seed, stream key, ray) and the sums are exact fixed point.
+ * Scenes whose memory is freed and reused for another scene while a launch
+ * runs could be read stale from L1: destroy scenes only when
+ * ac_service_info reports no running launch.  ac_service_destroy waits for
+ * the running launches to end. */
+typedef struct ac_service_s *ac_service_t;
+typedef struct {
+    int32_t device;
+    int32_t capacity;            /* job slots in the ring, a power of two (0: 4096); at most half in flight */
+    int32_t blocks_per_sm;       /* persistent grid (0: 2, which leaves room for synthesis blocks beside it) */
+    int32_t block_size;          /* 0: 256 */
+    int32_t chunk_rays;          /* rays a warp takes at a time (0: 64) */
+    int32_t reserved;
+    int64_t idle_timeout_ns;     /* 0: 20 ms */
+} ac_service_config;
+typedef struct {
+    int64_t submitted;           /* jobs submitted so far (next sequence number) */
+    int64_t in_flight;           /* submitted and not yet reported done */
+    int64_t launches;            /* persistent launches started so far */
+    int32_t running_launches;
+    int32_t grid_blocks;
+    int64_t capacity;
+} ac_service_stats;
+int ac_service_create(const ac_service_config *config, ac_service_t *out);
+int ac_service_submit(ac_service_t service, const ac_job *jobs, int32_t num_jobs, int64_t *first_seq);
+int ac_service_poll(ac_service_t service, int64_t *done_seqs, int32_t max_done, int32_t *num_done);
+int ac_service_info(ac_service_t service, ac_service_stats *stats);
+int ac_service_destroy(ac_service_t service);
+
 /* Device workspace needed by ac_synthesize. */
 int ac_synth_workspace_size(const ac_synth_params *params, size_t *bytes);
 

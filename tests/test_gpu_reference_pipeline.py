@@ -133,3 +133,44 @@ def test_scene_bvh_build_routes_to_the_gpu(reference):
     for k in ("bvh_bounds_min", "bvh_bounds_max", "bvh_start", "bvh_count", "bvh_escape", "bvh_primitives",
               "bvh_node_count", "bvh_leaf_count", "bvh_max_depth", "bvh_leaf_size"):
         np.testing.assert_array_equal(np.asarray(gpu[k]), np.asarray(ref[k]), err_msg=k)
+
+
+def test_acoustic_agent_facade_runs_through_the_b200_backend(reference):
+    """The reference's public facade, unchanged: AcousticAgent.create(scene="geometry", room=Room(...),
+    config=SimConfig(rt_accelerator="b200"), receiver_model=<8-mic circular array>).run() traces every channel
+    of its channel loop (engine.py:64-73) on the GPU.  With rt_precision="float64" the B200 kernel follows the
+    reference's rays, so the 8-channel RIR equals the one the reference's own float64 Numba path renders."""
+    bench, (steam_rt, models) = reference
+    from acoustic_agent import api
+    from acoustic_agent_b200 import backend, workloads
+    w = workloads.u_furnished(1729)
+    room = bench.reference_scene(steam_rt, models, w.spec).room
+    array = {"type": "circular", "count": 8, "radius_m": 0.05}
+
+    def run(accelerator, precision, rays=3000):
+        cfg = models.SimConfig(fs=16000, duration_s=1.0, rt_duration_s=1.0, rt_num_rays=rays, rt_num_bounces=60,
+                               rt_bin_duration_s=0.001, intersection_backend="bvh", late_tail=False,
+                               adaptive_geometry_bounces=False, rt_accelerator=accelerator, rt_precision=precision,
+                               seed=1729)
+        agent = api.AcousticAgent.create(scene="geometry", room=room, config=cfg, receiver_model=array,
+                                         source_model="cardioid", source=w.sources[0], receiver=(1.079, 6.252, 1.348))
+        return agent.run()
+
+    handle = backend.install(steam_rt)
+    try:
+        gpu64 = run("b200", "float64")
+        gpu32 = run("b200", "float32")
+    finally:
+        handle.uninstall()
+    cpu64 = run("numba", "float64")
+    assert gpu64.rir.shape == (8, 16000) and gpu64.metadata["array_channel_count"] == 8
+    refl = gpu64.metadata["steam_audio"]["reflections"]
+    assert refl["accelerator"] == "b200" and refl["precision"] == "float64"
+    assert gpu32.metadata["steam_audio"]["reflections"]["precision"] == "float32"
+    scale = float(np.abs(cpu64.rir).max())
+    np.testing.assert_allclose(gpu64.rir, cpu64.rir, rtol=1e-5, atol=1e-6 * scale)
+    # the traced field's decay (rounded to 0.1 ms by the reference) is the same field
+    assert gpu64.rt60["traced_rt60_bands"] == cpu64.rt60["traced_rt60_bands"]
+    t32 = np.array(list(gpu32.rt60["traced_rt60_bands"].values()))
+    t64 = np.array(list(cpu64.rt60["traced_rt60_bands"].values()))
+    np.testing.assert_allclose(t32, t64, rtol=0.02)
