@@ -58,6 +58,8 @@ int validate_trace(const ac_scene_s *scene, const ac_trace_params *p, const ac_t
     if (p->num_rays < 1 || p->num_rays > 0x7FFFFFFF) return fail(AC_ERR_INVALID, "num_rays must be in [1, 2^31)");
     if (p->num_bounces < 0 || p->num_bounces > 0xFFFFFE) return fail(AC_ERR_INVALID, "num_bounces must be in [0, 2^24-1)");
     if (p->num_bins < 1) return fail(AC_ERR_INVALID, "num_bins must be positive");
+    if (p->num_bins >= (1 << 21))   // (job, bin) fits the 32-bit keys the kernels may match lanes on
+        return fail(AC_ERR_CAPACITY, "num_bins %d is too many (at most 2^21 - 1)", p->num_bins);
     if (!(p->bin_duration > 0.0) || !(p->speed_of_sound > 0.0))
         return fail(AC_ERR_INVALID, "bin duration and speed of sound must be positive");
     const double values[] = {p->source[0], p->source[1], p->source[2], p->listener[0], p->listener[1], p->listener[2],

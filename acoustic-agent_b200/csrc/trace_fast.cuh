@@ -877,8 +877,12 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             // than a 64-bit one.
             const unsigned counting = __ballot_sync(full, count_hit);
             if (count_hit) {
-                const unsigned key = ((static_cast<unsigned>(s.job) & 1023u) << 22) | static_cast<unsigned>(s.surf);
-                const unsigned same = __match_any_sync(counting, key);
+                // service launches: lanes may hold jobs of any ring slots, so the key is the full slot
+                const unsigned same =
+                    kService ? __match_any_sync(counting, (static_cast<unsigned long long>(s.job) << 32) |
+                                                              static_cast<unsigned>(s.surf))
+                             : __match_any_sync(counting, ((static_cast<unsigned>(s.job) & 1023u) << 22) |
+                                                              static_cast<unsigned>(s.surf));
                 if (lane_id == __ffs(same) - 1)
                     atomicAdd(job.hit_counts + s.surf, static_cast<unsigned long long>(__popc(same)));
             }
@@ -1060,8 +1064,12 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             // than a 64-bit one.
             const unsigned counting = __ballot_sync(full, count_hit);
             if (count_hit) {
-                const unsigned key = ((static_cast<unsigned>(s.job) & 1023u) << 22) | static_cast<unsigned>(surf);
-                const unsigned same = __match_any_sync(counting, key);
+                // service launches: lanes may hold jobs of any ring slots, so the key is the full slot
+                const unsigned same =
+                    kService ? __match_any_sync(counting, (static_cast<unsigned long long>(s.job) << 32) |
+                                                              static_cast<unsigned>(surf))
+                             : __match_any_sync(counting, ((static_cast<unsigned>(s.job) & 1023u) << 22) |
+                                                              static_cast<unsigned>(surf));
                 if (lane_id == __ffs(same) - 1)
                     atomicAdd(job.hit_counts + surf, static_cast<unsigned long long>(__popc(same)));
             }
