@@ -57,7 +57,8 @@ class ACSceneDesc(ctypes.Structure):
         ("bvh_node_count", ctypes.c_int64), ("bvh_bounds_min", c_double_p), ("bvh_bounds_max", c_double_p),
         ("bvh_start", c_int64_p), ("bvh_count", c_int64_p), ("bvh_escape", c_int64_p),
         ("bvh_primitives", c_int64_p), ("device", ctypes.c_int32), ("cluster_size", ctypes.c_int32),
-        ("traversal", ctypes.c_int32), ("bvh_leaf", ctypes.c_int32),
+        ("traversal", ctypes.c_int32), ("bvh_leaf", ctypes.c_int32), ("bvh_width", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
@@ -66,7 +67,8 @@ class ACSceneInfo(ctypes.Structure):
         ("num_surfaces", ctypes.c_int64), ("num_corners", ctypes.c_int64), ("node_count", ctypes.c_int64),
         ("leaf_count", ctypes.c_int64), ("device_bytes", ctypes.c_int64), ("device", ctypes.c_int32),
         ("max_leaf", ctypes.c_int32), ("num_clusters", ctypes.c_int64), ("traversal", ctypes.c_int32),
-        ("bvh_depth", ctypes.c_int32), ("bvh_nodes", ctypes.c_int64),
+        ("bvh_depth", ctypes.c_int32), ("bvh_nodes", ctypes.c_int64), ("bvh_width", ctypes.c_int32),
+        ("bvh_stack_need", ctypes.c_int32),
     ]
 
 

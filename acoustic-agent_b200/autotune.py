@@ -39,11 +39,14 @@ from acoustic_agent_b200 import runtime
 from acoustic_agent_b200.scene import SceneArrays
 
 SCENE_CANDIDATES: tuple[dict[str, Any], ...] = (
-    {"traversal": "scan", "bvh_leaf": 0},
-    {"traversal": "bvh", "bvh_leaf": 1},
-    {"traversal": "bvh", "bvh_leaf": 2},
-    {"traversal": "bvh", "bvh_leaf": 4},
-    {"traversal": "hybrid", "bvh_leaf": 1},
+    {"traversal": "scan", "bvh_leaf": 0, "bvh_width": 0},
+    {"traversal": "bvh", "bvh_leaf": 1, "bvh_width": 2},
+    {"traversal": "bvh", "bvh_leaf": 2, "bvh_width": 2},
+    {"traversal": "bvh", "bvh_leaf": 4, "bvh_width": 2},
+    {"traversal": "hybrid", "bvh_leaf": 1, "bvh_width": 2},
+    {"traversal": "bvh", "bvh_leaf": 1, "bvh_width": 4},
+    {"traversal": "bvh", "bvh_leaf": 2, "bvh_width": 4},
+    {"traversal": "hybrid", "bvh_leaf": 1, "bvh_width": 4},
 )
 LAUNCH_CANDIDATES: tuple[dict[str, int], ...] = tuple(
     {"block_size": b, "chunk_rays": c} for b in (256, 128) for c in (16, 32, 64, 128))
@@ -54,9 +57,10 @@ class SceneChoice:
     traversal: str
     bvh_leaf: int
     ms: float
+    bvh_width: int = 0
 
     def options(self) -> dict[str, Any]:
-        return {"traversal": self.traversal, "bvh_leaf": self.bvh_leaf}
+        return {"traversal": self.traversal, "bvh_leaf": self.bvh_leaf, "bvh_width": self.bvh_width}
 
 
 @dataclass(frozen=True)
@@ -133,12 +137,14 @@ def tune_scene(arrays: SceneArrays, spec: runtime.TraceSpec, *, device: int = 0,
         try:
             if scene.traversal != cand["traversal"]:
                 continue   # nothing for a BVH to hold (no boxes, or only horizontal surfaces)
+            if scene.traversal != "scan" and scene.bvh_width != int(cand.get("bvh_width", 2) or 2):
+                continue   # a four-wide tree that would need too deep a stack stays binary
             buffers = runtime.TraceBuffers.allocate(scene.num_surfaces, int(sample.num_bins), dev)
             ms = _time_ms(lambda: runtime.trace(scene, sample, buffers, stream=stream), reps, stream)
         finally:
             scene.close()
         if best is None or ms < best.ms:
-            best = SceneChoice(cand["traversal"], int(cand.get("bvh_leaf", 0)), ms)
+            best = SceneChoice(cand["traversal"], int(cand.get("bvh_leaf", 0)), ms, int(cand.get("bvh_width", 0)))
     assert best is not None
     if cache is not None:
         cache.put(key, best)

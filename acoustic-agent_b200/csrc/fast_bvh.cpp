@@ -179,10 +179,80 @@ class Builder {
     TraversalBvh *out_;
 };
 
+// Collapse of the binary layout into the four-wide one (fast_bvh.h).
+class Collapser {
+  public:
+    explicit Collapser(const std::vector<float> &bin) : bin_(bin) {}
+
+    struct Child {
+        float box[6];   // lo.x, hi.x, lo.y, hi.y, lo.z, hi.z
+        int32_t ref;
+    };
+
+    // Wide node for binary node `b`; returns its index.  `need`: stack entries a ray can need from here down.
+    int32_t collapse(int32_t b, std::vector<float> &wide, int32_t *need) {
+        std::vector<Child> kids = {child(b, 0), child(b, 1)};
+        while (kids.size() < 4) {
+            int pick = -1;
+            double area = -1.0;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                if (kids[k].ref < 0) continue;
+                const float *q = kids[k].box;
+                const double dx = q[1] - q[0], dy = q[3] - q[2], dz = q[5] - q[4];
+                const double a = dx * dy + dy * dz + dz * dx;
+                if (a > area) { area = a; pick = static_cast<int>(k); }
+            }
+            if (pick < 0) break;
+            const int32_t inner = kids[pick].ref;
+            kids[pick] = child(inner, 0);
+            kids.insert(kids.begin() + pick + 1, child(inner, 1));
+        }
+        const int32_t node = static_cast<int32_t>(wide.size() / kBvh4Floats);
+        wide.resize(wide.size() + kBvh4Floats, 0.0f);
+        int32_t refs[4];
+        int32_t below = 0;
+        for (size_t k = 0; k < 4; ++k) {
+            if (k >= kids.size()) { refs[k] = ~0; continue; }
+            if (kids[k].ref >= 0) {
+                int32_t sub = 0;
+                refs[k] = collapse(kids[k].ref, wide, &sub);
+                below = std::max(below, sub);
+            } else {
+                refs[k] = kids[k].ref;
+            }
+        }
+        float *q = wide.data() + static_cast<size_t>(node) * kBvh4Floats;
+        for (int k = 0; k < 4; ++k) {
+            for (int f = 0; f < 6; ++f)
+                q[4 * f + k] = k < static_cast<int>(kids.size()) ? kids[k].box[f] : kBvh4Empty;
+            std::memcpy(q + 24 + k, &refs[k], 4);
+        }
+        const int32_t count = static_cast<int32_t>(kids.size());
+        std::memcpy(q + 28, &count, 4);
+        // a visit pushes at most (children - 1) entries before descending into one child
+        *need = count - 1 + below;
+        return node;
+    }
+
+  private:
+    Child child(int32_t b, int side) const {
+        const float *q = bin_.data() + 16 * static_cast<size_t>(b);
+        Child c;
+        const float *xy = q + 4 * side;
+        c.box[0] = xy[0]; c.box[1] = xy[1]; c.box[2] = xy[2]; c.box[3] = xy[3];
+        c.box[4] = q[8 + 2 * side]; c.box[5] = q[9 + 2 * side];
+        std::memcpy(&c.ref, q + 12 + side, 4);
+        return c;
+    }
+
+    const std::vector<float> &bin_;
+};
+
 }  // namespace
 
 int build_traversal_bvh(const std::vector<int64_t> &surfaces, const double *lo, const double *hi, int leaf_max,
-                        double pad, TraversalBvh *out) {
+                        double pad, TraversalBvh *out, int width) {
+    if (width != 2 && width != 4) return fail(AC_ERR_INVALID, "BVH width %d is not 2 or 4", width);
     *out = TraversalBvh{};
     if (leaf_max < 1 || leaf_max > kBvhMaxLeaf)
         return fail(AC_ERR_INVALID, "BVH leaf size %d is outside 1..%d", leaf_max, kBvhMaxLeaf);
@@ -211,6 +281,17 @@ int build_traversal_bvh(const std::vector<int64_t> &surfaces, const double *lo, 
     if (root < 0) builder.write_root_pair(root, rb);   // everything fits one leaf
     else if (root != 0) return fail(AC_ERR_INVALID, "internal: BVH root is not node 0");
     if (out->depth > kBvhStack - 1) return fail(AC_ERR_CAPACITY, "float32 BVH depth %d exceeds the traversal stack", out->depth);
+    out->stack_need = out->depth;
+    if (width == 4) {
+        std::vector<float> wide;
+        int32_t need = 0;
+        Collapser(out->nodes).collapse(0, wide, &need);
+        if (need <= kBvhStack - 1) {   // else keep the binary layout, whose need is bounded by its depth
+            out->nodes.swap(wide);
+            out->width = 4;
+            out->stack_need = need;
+        }
+    }
     return AC_OK;
 }
 

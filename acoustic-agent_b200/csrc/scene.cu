@@ -45,6 +45,11 @@ constexpr double kBvhPad = 1e-4;
 // Surfaces per BVH leaf unless the caller chooses: one surface per leaf measured
 // fastest on B200 for rooms of 30 to 430 surfaces (deeper tree, fewer tests).
 constexpr int kDefaultBvhLeaf = 1;
+// Children per inner node of the float32 traversal BVH unless the caller chooses.
+#ifndef AC_DEFAULT_BVH_WIDTH
+#define AC_DEFAULT_BVH_WIDTH 2
+#endif
+constexpr int kDefaultBvhWidth = AC_DEFAULT_BVH_WIDTH;
 
 inline size_t round4(size_t v) { return (v + 3) & ~static_cast<size_t>(3); }
 
@@ -104,6 +109,7 @@ Offsets layout(size_t S, size_t P, size_t N, size_t C, const FastLists *f) {
     o.box_bounds = off;    off += round4(f ? f->box_slots.size() * 8 : 0);
     o.boxes = off;         off += round4(f ? f->box_slots.size() * ac::kPrimStride : 0);
     o.edges = off;         off += round4(f ? C * 4 : 0);
+    off = (off + 31) & ~static_cast<size_t>(31);   // BVH nodes start on a 128-byte line
     o.bvh_nodes = off;     off += round4(f && f->use_bvh ? f->bvh.nodes.size() : 0);
     o.bvh_prims = off;     off += round4(f && f->use_bvh ? f->bvh.order.size() * ac::kPrimStride : 0);
     o.total = off;
@@ -318,6 +324,7 @@ int pack_and_upload(const ac_scene_desc *d, const ac_bvh &bvh, const FastLists *
             s->fast.bvh_nodes = reinterpret_cast<const float4 *>(fbase + o.bvh_nodes);
             s->fast.bvh_prims = fbase + o.bvh_prims;
             s->fast.num_bvh_nodes = static_cast<int32_t>(f->bvh.num_nodes());
+            s->fast.bvh_width = f->bvh.width;
             if (!f->hybrid) s->fast.num_wall_clusters = 0;
             s->fast.num_box_clusters = 0;
         }
@@ -462,7 +469,7 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
             if (!lists.use_bvh) lists.hybrid = false;   // no boxes: plain scan
             if (lists.use_bvh)
                 rc = ac::build_traversal_bvh(members, blo, bhi, d->bvh_leaf > 0 ? d->bvh_leaf : kDefaultBvhLeaf, kBvhPad,
-                                             &lists.bvh);
+                                             &lists.bvh, d->bvh_width > 0 ? d->bvh_width : kDefaultBvhWidth);
         }
     }
     if (rc != AC_OK) {
@@ -472,6 +479,8 @@ extern "C" int ac_scene_create(const ac_scene_desc *d, ac_scene_t *out) {
     s->traversal = lists.hybrid ? AC_TRAVERSAL_HYBRID : (lists.use_bvh ? AC_TRAVERSAL_BVH : AC_TRAVERSAL_SCAN);
     s->bvh_depth = lists.use_bvh ? lists.bvh.depth : 0;
     s->bvh_nodes = lists.use_bvh ? lists.bvh.num_nodes() : 0;
+    s->bvh_width = lists.use_bvh ? lists.bvh.width : 0;
+    s->bvh_stack_need = lists.use_bvh ? lists.bvh.stack_need : 0;
     rc = pack_and_upload<float>(d, bvh, &lists, blo, bhi, s, &s->storage_f32, &s->bytes_f32, &s->f32);
     if (rc == AC_OK)
         rc = pack_and_upload<double>(d, bvh, nullptr, blo, bhi, s, &s->storage_f64, &s->bytes_f64, &s->f64);
@@ -540,5 +549,7 @@ extern "C" int ac_scene_get_info(ac_scene_t s, ac_scene_info *info) {
     info->traversal = s->traversal;
     info->bvh_depth = s->bvh_depth;
     info->bvh_nodes = s->bvh_nodes;
+    info->bvh_width = s->bvh_width;
+    info->bvh_stack_need = s->bvh_stack_need;
     return AC_OK;
 }

@@ -32,6 +32,8 @@ struct ac_scene_s {
     int32_t traversal = AC_TRAVERSAL_SCAN;  // what the float32 kernel uses for this scene
     int32_t bvh_depth = 0;
     int64_t bvh_nodes = 0;
+    int32_t bvh_width = 0;
+    int32_t bvh_stack_need = 0;
     double max_reflection = 0.0;   // bound used when choosing the fixed-point scale
     double max_scattering = 0.0;
     double min_scattering = 0.0;

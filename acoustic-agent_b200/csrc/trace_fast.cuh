@@ -59,10 +59,11 @@ struct FastScene {
     int32_t num_polys;
     int32_t num_box_clusters;
     int32_t num_edges;
-    const float4 *bvh_nodes;     // BVH mode: [N][4] traversal BVH over walls and boxes (fast_bvh.h); else null
+    const float4 *bvh_nodes;     // BVH mode: [N][4] (width 2) or [N][8] (width 4) traversal BVH over walls and
+                                 // boxes (fast_bvh.h); else null
     const float *bvh_prims;      // BVH mode: [P][12] surface records in leaf order
     int32_t num_bvh_nodes;       // 0: scan mode
-    int32_t reserved;
+    int32_t bvh_width;           // 2 or 4
 };
 
 // One group = the jobs that share a scene; chunks never straddle groups.
@@ -501,13 +502,89 @@ __device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r,
     }
 }
 
+// Four-wide descent (width 4 layout of fast_bvh.h), organised like bvh_traverse:
+// a node fetch tests all its children; the hit ones are ordered by entry
+// distance, the nearest is taken next and the others pushed farthest first;
+// leaves are parked so that lanes test them together.  The builder keeps the
+// stack a ray can need below kBvhStack.
+__device__ __forceinline__ void cswap(float &ea, int &ra, float &eb, int &rb) {
+    if (eb < ea) {
+        const float e = ea; ea = eb; eb = e;
+        const int r = ra; ra = rb; rb = r;
+    }
+}
+
+__device__ __forceinline__ void bvh4_traverse(const FastScene &fs, const FRay &r, bool any_hit, float &best_t,
+                                              int &best) {
+    int stack[kBvhStack];
+    stack[0] = kBvhDone;
+    int sp = 1;
+    int node = 0;
+    int leaf = 0;
+#pragma unroll 1
+    while (node != kBvhDone || leaf < 0) {
+#pragma unroll 1
+        while (node >= 0) {
+            const float4 *np = fs.bvh_nodes + 8 * static_cast<size_t>(node);
+            const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+            const float4 lz = __ldg(np + 4), hz = __ldg(np + 5), rf = __ldg(np + 6);
+            const float max_t = best_t * 1.000001f + 1e-5f;
+            float e0, e1, e2, e3;
+            const bool h0 = child_box(r, lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, max_t, e0);
+            const bool h1 = child_box(r, lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, max_t, e1);
+            const bool h2 = child_box(r, lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, max_t, e2);
+            const bool h3 = child_box(r, lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, max_t, e3);
+            // misses sort last (+inf); a five-comparator network orders the four by entry distance
+            const float inf = __int_as_float(0x7f800000);
+            float d0 = h0 ? e0 : inf, d1 = h1 ? e1 : inf, d2 = h2 ? e2 : inf, d3 = h3 ? e3 : inf;
+            int r0 = __float_as_int(rf.x), r1 = __float_as_int(rf.y), r2 = __float_as_int(rf.z), r3 = __float_as_int(rf.w);
+            cswap(d0, r0, d1, r1);
+            cswap(d2, r2, d3, r3);
+            cswap(d0, r0, d2, r2);
+            cswap(d1, r1, d3, r3);
+            cswap(d1, r1, d2, r2);
+            const int hits = static_cast<int>(h0) + static_cast<int>(h1) + static_cast<int>(h2) + static_cast<int>(h3);
+            if (hits >= 4) stack[sp++] = r3;
+            if (hits >= 3) stack[sp++] = r2;
+            if (hits >= 2) stack[sp++] = r1;
+            node = hits >= 1 ? r0 : stack[--sp];
+            if (node < 0 && node != kBvhDone && leaf == 0) {   // park the leaf, keep descending
+                leaf = node;
+                node = stack[--sp];
+            }
+            if (!__any_sync(__activemask(), leaf == 0)) break;   // every lane holds a leaf: test them
+        }
+#pragma unroll 1
+        while (leaf < 0) {
+            const int code = ~leaf;
+            const int first = code >> 3, count = (code & 7) + 1;
+#pragma unroll 1
+            for (int i = 0; i < count; ++i) {
+                const float *rec = fs.bvh_prims + static_cast<size_t>(first + i) * kPrimStride;
+                const int tag = __float_as_int(__ldg(rec + 11));
+                const float tt = (tag & 3) == 0 ? wall_t(ldq(rec), ldq(rec + 4), r) : box_t(rec, r);
+                take(tt, tag >> 2, best_t, best);
+            }
+            if (any_hit && best >= 0) return;
+            leaf = 0;
+            if (node < 0 && node != kBvhDone) {   // the next stop is a leaf too
+                leaf = node;
+                node = stack[--sp];
+            }
+        }
+    }
+}
+
 // The closest-hit / any-hit query of one ray: the lockstep scan (walls and
 // boxes in scan mode, horizontal polygons always) and, in BVH mode, the
 // per-lane BVH descent over walls and boxes.  Every lane must call it.
 __device__ __forceinline__ void scene_query(const FastScene &fs, const FRay &r, bool active, bool any_hit,
                                             float &best_t, int &best) {
     scene_scan(fs, r, active, any_hit, best_t, best);
-    if (fs.num_bvh_nodes > 0 && active && !(any_hit && best >= 0)) bvh_traverse(fs, r, any_hit, best_t, best);
+    if (fs.num_bvh_nodes > 0 && active && !(any_hit && best >= 0)) {
+        if (fs.bvh_width == 4) bvh4_traverse(fs, r, any_hit, best_t, best);
+        else bvh_traverse(fs, r, any_hit, best_t, best);
+    }
 }
 
 // Normal of the winning surface, oriented against the ray.

@@ -58,7 +58,7 @@ class DeviceScene:
     TRAVERSALS = {"auto": 0, "scan": 1, "bvh": 2, "hybrid": 3}
 
     def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0,
-                 traversal: str = "auto", bvh_leaf: int = 0) -> None:
+                 traversal: str = "auto", bvh_leaf: int = 0, bvh_width: int = 0) -> None:
         if traversal not in self.TRAVERSALS:
             raise ValueError(f"traversal must be one of {sorted(self.TRAVERSALS)}")
         require_cuda(device)
@@ -94,6 +94,7 @@ class DeviceScene:
         desc.cluster_size = int(cluster_size)
         desc.traversal = self.TRAVERSALS[traversal]
         desc.bvh_leaf = int(bvh_leaf)
+        desc.bvh_width = int(bvh_width)
         if "surface_bounds_min" in a and "surface_bounds_max" in a:
             keep["surface_bounds_min"] = _f64(a["surface_bounds_min"])
             keep["surface_bounds_max"] = _f64(a["surface_bounds_max"])
@@ -112,6 +113,8 @@ class DeviceScene:
         self.traversal = {1: "scan", 2: "bvh", 3: "hybrid"}.get(int(info.traversal), "scan")
         self.bvh_depth = int(info.bvh_depth)
         self.bvh_nodes = int(info.bvh_nodes)
+        self.bvh_width = int(info.bvh_width)
+        self.bvh_stack_need = int(info.bvh_stack_need)
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
         # events recorded after CUDA-graph replays that read this scene (the library tracks eager launches
         # itself, not work captured into a graph); close() waits for them

@@ -108,6 +108,8 @@ typedef struct ac_scene_desc {
     int32_t cluster_size;        /* surfaces per cluster of the float32 scan (0: 32) */
     int32_t traversal;           /* float32 kernel: AC_TRAVERSAL_AUTO / _SCAN / _BVH / _HYBRID */
     int32_t bvh_leaf;            /* float32 BVH: surfaces per leaf, 1..8 (0: 1) */
+    int32_t bvh_width;           /* float32 BVH: children per inner node, 2 or 4 (0: the library's default) */
+    int32_t reserved;
 } ac_scene_desc;
 
 typedef struct ac_scene_info {
@@ -122,6 +124,8 @@ typedef struct ac_scene_info {
     int32_t traversal;           /* what the float32 kernel uses: AC_TRAVERSAL_SCAN, _BVH or _HYBRID */
     int32_t bvh_depth;           /* float32 BVH: inner-node levels (0 in scan mode) */
     int64_t bvh_nodes;           /* float32 BVH: inner nodes (0 in scan mode) */
+    int32_t bvh_width;           /* float32 BVH: children per inner node (0 in scan mode) */
+    int32_t bvh_stack_need;      /* float32 BVH: traversal stack entries a ray can need */
 } ac_scene_info;
 
 /* One trace: rays from the listener, next-event estimation to the source.

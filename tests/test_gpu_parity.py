@@ -370,27 +370,30 @@ def test_fp32_bvh_traversal_equals_scan(rt, name):
     spec = spec_for(rt, case, "float32")
     has_boxes = bool(np.any(np.asarray(case["arrays"]["kinds"]) == 2))
     got = {}
-    for mode in ("scan", "bvh", "hybrid"):
-        scene = rt.DeviceScene(case["arrays"], traversal=mode)
+    for mode, width in (("scan", 0), ("bvh", 2), ("hybrid", 2), ("bvh", 4), ("hybrid", 4)):
+        scene = rt.DeviceScene(case["arrays"], traversal=mode, bvh_width=width)
         assert scene.traversal == (mode if mode != "hybrid" or has_boxes else "scan")
         if scene.traversal != "scan":
             assert 1 <= scene.bvh_depth <= 31 and scene.bvh_nodes >= 1
+            assert scene.bvh_width == width and 1 <= scene.bvh_stack_need <= 31
         buffers = rt.trace(scene, spec, record_rays=True)
         torch.cuda.synchronize()
-        got[mode] = {"rays": buffers.ray_surfaces.cpu().numpy(), "echogram": buffers.echogram_fx.cpu().numpy(),
-                     "hits": buffers.hit_counts.cpu().numpy(), "counters": buffers.counters.cpu().numpy()}
+        got[(mode, width)] = {"rays": buffers.ray_surfaces.cpu().numpy(),
+                              "echogram": buffers.echogram_fx.cpu().numpy(),
+                              "hits": buffers.hit_counts.cpu().numpy(), "counters": buffers.counters.cpu().numpy()}
         scene.close()
-    for mode in ("bvh", "hybrid"):
+    for key_mode in (("bvh", 2), ("hybrid", 2), ("bvh", 4), ("hybrid", 4)):
         for key in ("rays", "echogram", "hits", "counters"):
-            np.testing.assert_array_equal(got[mode][key], got["scan"][key], err_msg=f"{mode} {key}")
+            np.testing.assert_array_equal(got[key_mode][key], got[("scan", 0)][key], err_msg=f"{key_mode} {key}")
 
 
 @pytest.mark.parametrize("leaf", [1, 2, 8])
-def test_fp32_bvh_leaf_sizes_agree(rt, leaf):
+@pytest.mark.parametrize("width", [2, 4])
+def test_fp32_bvh_leaf_sizes_agree(rt, leaf, width):
     case = load_case("apartment3_bvh")
     spec = spec_for(rt, case, "float32", rng="philox", num_rays=4096)
     got = []
-    for kw in ({"traversal": "scan"}, {"traversal": "bvh", "bvh_leaf": leaf}):
+    for kw in ({"traversal": "scan"}, {"traversal": "bvh", "bvh_leaf": leaf, "bvh_width": width}):
         scene = rt.DeviceScene(case["arrays"], **kw)
         buffers = rt.trace(scene, spec)
         torch.cuda.synchronize()
