@@ -402,6 +402,9 @@ def main() -> int:
                         help="mixed_batch: uniformly drawn jobs traced by the reference's float64 path for the "
                              "parity block and the CPU baseline")
     parser.add_argument("--e2e-steps", type=int, default=2, help="mixed_batch: end-to-end steps to time")
+    parser.add_argument("--profile-launch", action="store_true",
+                        help="mixed_batch: after the warm-up, run one trace launch between cudaProfilerStart/Stop "
+                             "and exit (for ncu --profile-from-start off)")
     parser.add_argument("--no-config1", dest="with_config1", action="store_false",
                         help="mixed_batch: skip the single-scene U-room figures added to the line")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
@@ -895,6 +898,16 @@ def run_mixed_batch(args) -> int:
     torch.cuda.synchronize(device)
     per_job_rb = [int(b.counters[2].item()) for b in plan.buffers]
     rb = int(sum(per_job_rb))
+    if args.profile_launch:
+        # one trace launch of the batch between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)
+        job_list = [(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)]
+        ws = runtime.BatchWorkspace(device)
+        torch.cuda.profiler.start()
+        runtime.trace_batch(job_list, ws, block_size=launch.block_size, chunk_rays=launch.chunk_rays)
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled": "trace launch", "jobs": len(jobs), "ray_bounces": rb}), flush=True)
+        return 0
 
     def barrier():
         if dist is not None:
