@@ -403,7 +403,7 @@ def main() -> int:
                              "parity block and the CPU baseline")
     parser.add_argument("--e2e-steps", type=int, default=2, help="mixed_batch: end-to-end steps to time")
     parser.add_argument("--profile-launch", action="store_true",
-                        help="mixed_batch: after the warm-up, run one trace launch between cudaProfilerStart/Stop "
+                        help="mixed_batch: after the warm-up, run one eager step between cudaProfilerStart/Stop "
                              "and exit (for ncu --profile-from-start off)")
     parser.add_argument("--no-config1", dest="with_config1", action="store_false",
                         help="mixed_batch: skip the single-scene U-room figures added to the line")
@@ -899,14 +899,17 @@ def run_mixed_batch(args) -> int:
     per_job_rb = [int(b.counters[2].item()) for b in plan.buffers]
     rb = int(sum(per_job_rb))
     if args.profile_launch:
-        # one trace launch of the batch between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)
+        # one eager step of the batch (trace + synthesis) between cudaProfilerStart/Stop, for
+        # `ncu --profile-from-start off`
         job_list = [(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)]
-        ws = runtime.BatchWorkspace(device)
+        ws, sws = runtime.BatchWorkspace(device), runtime.SynthBatchWorkspace(device)
         torch.cuda.profiler.start()
         runtime.trace_batch(job_list, ws, block_size=launch.block_size, chunk_rays=launch.chunk_rays)
+        runtime.synthesize_batch((plan.synth_jobs, len(plan.jobs), plan.synth_config), sws)
         torch.cuda.synchronize(device)
         torch.cuda.profiler.stop()
-        print(json.dumps({"profiled": "trace launch", "jobs": len(jobs), "ray_bounces": rb}), flush=True)
+        print(json.dumps({"profiled": "one step (trace + synthesis)", "jobs": len(jobs), "ray_bounces": rb}),
+              flush=True)
         return 0
 
     def barrier():
@@ -1004,56 +1007,75 @@ def run_mixed_batch(args) -> int:
         "clocks": sampler.summary(),
     }
 
-    # roofline of the trace launch: algorithmic bytes over the mix / its live CUDA-event duration
-    if not args.no_cpu_baseline:
+    # the extras below each record an error in the line instead of losing it
+    def guarded(key, fn):
+        try:
+            fn()
+        except Exception as exc:   # pragma: no cover - depends on the box
+            line.setdefault("errors", {})[key] = f"{type(exc).__name__}: {exc}"
+
+    def roofline():
+        # algorithmic bytes over the mix / the trace launch's live CUDA-event duration
         bpr = mix_bytes_per_ray_bounce(arrays, jobs, per_job_rb)
         achieved = bpr * rb / (trace_ms / 1000.0) / 1e9
-        line["roofline"] = roofline_line(achieved, bpr, "mixed_batch", device)
+        line["roofline"] = roofline_line(achieved, bpr, "mixed_batch", device, rb)
 
-    if not args.no_cpu_baseline and world == 1:
-        picks = uniform_jobs(jobs, args.reference_jobs, seed=3)
+    picks = uniform_jobs(jobs, args.reference_jobs, seed=3)
+
+    def reference_float64():
         ref64 = reference_job_loop(population, jobs, picks[:args.parity_jobs], accelerator="numba",
                                    precision="float64")
-        if "unavailable" not in ref64:
-            drop = reference_job_loop(population, jobs, picks[:max(args.parity_jobs, 4)], accelerator="b200",
-                                      precision="float32", time_limit_s=30.0)
-            echo_host = plan.echo_store.cpu().numpy()
-            offsets = np.cumsum([0] + [6 * int(j.spec.num_bins) for j in jobs])
-            same, philox = [], []
-            for k, ref_echo in ref64["echograms"].items():
-                bd = jobs[k].spec.bin_duration
-                ours_philox = echo_host[offsets[k]:offsets[k + 1]].reshape(6, -1)
-                philox.append(metrics.parity(ours_philox, ref_echo, bd))
-                if k in drop.get("echograms", {}):
-                    same.append(metrics.parity(drop["echograms"][k], ref_echo, bd))
-
-            def worst(rows):
-                return {key: max(r[key] for r in rows) for key in rows[0]} if rows else None
-
-            line["parity"] = {
-                "jobs": len(ref64["echograms"]),
-                "same_stream": worst(same),
-                "philox_stream": worst(philox),
-                "note": ("GPU float32 echograms against the reference's float64 Numba echogram of the same job "
-                         "(trace_energy_field, rt_precision='float64'); same_stream: the drop-in on the reference's "
-                         "own random stream (identical rays); philox_stream: the batch's own echogram (Philox rays, "
-                         "Monte-Carlo difference); worst band and job"),
-            }
-            line["cpu_baseline"] = {"value": ref64["rirs_per_s"], "unit": "RIRs/s", "cores": ref64["threads"],
-                                    "kind": "reference", "sample": ref64["sample"]}
-            line["drop_in_plain"] = {k: v for k, v in drop.items() if k != "echograms"}
-            if "rirs_per_s" in drop:
-                line["batched_vs_drop_in_plain"] = value / drop["rirs_per_s"]
-        else:
+        if "unavailable" in ref64:
             line["cpu_baseline"] = {"unavailable": ref64["unavailable"]}
+            return
+        line["cpu_baseline"] = {"value": ref64["rirs_per_s"], "unit": "RIRs/s", "cores": ref64["threads"],
+                                "kind": "reference", "sample": ref64["sample"]}
+        drop = reference_job_loop(population, jobs, picks[:max(args.parity_jobs, 4)], accelerator="b200",
+                                  precision="float32", time_limit_s=30.0)
+        line["drop_in_plain"] = {k: v for k, v in drop.items() if k != "echograms"}
+        if "rirs_per_s" in drop:
+            line["batched_vs_drop_in_plain"] = value / drop["rirs_per_s"]
+        echo_host = plan.echo_store.cpu().numpy()
+        offsets = np.cumsum([0] + [6 * int(j.spec.num_bins) for j in jobs])
+        same, philox = [], []
+        for k, ref_echo in ref64["echograms"].items():
+            bd = jobs[k].spec.bin_duration
+            ours_philox = echo_host[offsets[k]:offsets[k + 1]].reshape(6, -1)
+            philox.append(metrics.parity(ours_philox, ref_echo, bd))
+            if k in drop.get("echograms", {}):
+                same.append(metrics.parity(drop["echograms"][k], ref_echo, bd))
+
+        def worst(rows):
+            return {key: max(r[key] for r in rows) for key in rows[0]} if rows else None
+
+        line["parity"] = {
+            "jobs": len(ref64["echograms"]),
+            "same_stream": worst(same),
+            "philox_stream": worst(philox),
+            "note": ("GPU float32 echograms against the reference's float64 Numba echogram of the same job "
+                     "(trace_energy_field, rt_precision='float64'); same_stream: the drop-in on the reference's "
+                     "own random stream (identical rays); philox_stream: the batch's own echogram (Philox rays, "
+                     "Monte-Carlo difference); worst band and job"),
+        }
+
+    def reference_cuda():
         ref_cuda = reference_job_loop(population, jobs, picks, accelerator="cuda", precision="float32")
         line["reference_cuda_plain"] = {k: v for k, v in ref_cuda.items() if k != "echograms"}
         if "rirs_per_s" in ref_cuda:
             line["batched_vs_reference_cuda_plain"] = value / ref_cuda["rirs_per_s"]
-    if args.with_config1:
+
+    def config1():
         line["config1_u_room"] = run_single_scene(args, "u_room_20_boxes", extras_only=True)
         if not args.no_cpu_baseline and world == 1:
             line["config1_u_room"]["facade"] = facade_rirs(workloads.u_furnished(1729))
+
+    if not args.no_cpu_baseline:
+        guarded("roofline", roofline)
+    if not args.no_cpu_baseline and world == 1:
+        guarded("cpu_baseline", reference_float64)
+        guarded("reference_cuda_plain", reference_cuda)
+    if args.with_config1:
+        guarded("config1_u_room", config1)
     print(json.dumps(line), flush=True)
     barrier()
     if dist is not None:
