@@ -230,6 +230,9 @@ __device__ __forceinline__ void service_finish(const FastTable &t, int slot, int
 // each (t = v * inv - o * inv); measured 2-4 % faster than (v - o) * inv on the
 // U room and the 8-room apartment, with identical results (node boxes are
 // padded, so the culling stays conservative under either rounding).
+#ifndef AC_WARP_DEPOSIT
+#define AC_WARP_DEPOSIT 0
+#endif
 #ifndef AC_FMA_SLAB
 #define AC_FMA_SLAB 1
 #endif
@@ -988,12 +991,49 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                         const float common = job.ray_scale * source_gain * distance_term * (diffuse + specular);
                         long long esum = 0;
                         float energy_sum = 0.0f;
+#if AC_WARP_DEPOSIT
+                        // lanes depositing into the same (job, bin) add their quanta in the warp first and one of
+                        // them issues the two atomics of each band (quanta are non-negative and below 2^62, so
+                        // their 16-bit pieces sum exactly in 32 bits)
+                        const unsigned dep_mask = __activemask();
+                        const unsigned dep_same =
+                            kService ? __match_any_sync(dep_mask, (static_cast<unsigned long long>(s.job) << 32) |
+                                                                      static_cast<unsigned>(bin))
+                                     : __match_any_sync(dep_mask, ((static_cast<unsigned>(s.job) & 1023u) << 21) |
+                                                                      static_cast<unsigned>(bin));
+                        const bool dep_alone = kAmb || __popc(dep_same) == 1;
+                        const bool dep_leader = lane_id == __ffs(dep_same) - 1;
+#endif
 #pragma unroll
                         for (int b = 0; b < kBands; ++b) {
                             const float e = common * refl[b] * s.acc[b];
                             if (kVisual) energy_sum += e;
                             const long long qe = quantize(e, job.energy_scale);
+#if AC_WARP_DEPOSIT
+                            if (dep_alone) {
+                                add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
+                            } else {
+                                const unsigned long long uq = static_cast<unsigned long long>(qe);
+                                const unsigned l0 = __reduce_add_sync(dep_same, static_cast<unsigned>(uq & 0xFFFFu));
+                                const unsigned l1 =
+                                    __reduce_add_sync(dep_same, static_cast<unsigned>((uq >> 16) & 0xFFFFu));
+                                const unsigned h0 =
+                                    __reduce_add_sync(dep_same, static_cast<unsigned>((uq >> 32) & 0xFFFFu));
+                                const unsigned h1 = __reduce_add_sync(dep_same, static_cast<unsigned>(uq >> 48));
+                                if (dep_leader) {
+                                    unsigned long long *w =
+                                        job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin);
+                                    const unsigned long long lo = static_cast<unsigned long long>(l0) +
+                                                                  (static_cast<unsigned long long>(l1) << 16);
+                                    const unsigned long long hi = static_cast<unsigned long long>(h0) +
+                                                                  (static_cast<unsigned long long>(h1) << 16);
+                                    if (lo) atomicAdd(w, lo);
+                                    if (hi) atomicAdd(w + 1, hi);
+                                }
+                            }
+#else
                             add_fixed(job.echogram_fx + 2 * (static_cast<size_t>(b) * job.num_bins + bin), qe);
+#endif
                             if (kAmb) {
                                 const float *d0 = s.d0;
                                 unsigned long long *a =

@@ -217,8 +217,8 @@ def first_divergence(a: np.ndarray, b: np.ndarray) -> np.ndarray:
 
 def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfaces: np.ndarray,
                       ref_surfaces: np.ndarray, directions, diffuse_bank, diffuse_random, diffuse_indices,
-                      trials: int = 48, origin_eps: float = 4e-6, direction_eps: float = 4e-7, seed: int = 0,
-                      **trace_kwargs) -> dict[str, Any]:
+                      trials: int = 48, origin_eps: float = 4e-6, direction_eps: float = 4e-7, edge_eps: float = 2e-5,
+                      seed: int = 0, **trace_kwargs) -> dict[str, Any]:
     """Why a float32 trace left the float64 one on each of `rays` (rays whose hit sequences differ).
 
     At the first differing bounce the float64 state (origin, direction, path length) is taken from this
@@ -228,7 +228,11 @@ def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfac
     float32 trace's outcome at least once (a grazing hit, an edge or corner, two surfaces at the same
     distance, a sphere or path-length threshold).  It is a diffuse-threshold tie when, at a bounce up to
     that one, the ray's uniform draw lies within float32 rounding of the surface's scattering, so the two
-    traces chose different reflection kinds on the same surface.  Anything else is counted as unexplained.
+    traces chose different reflection kinds on the same surface.  It is a box-edge tie when, at an earlier
+    bounce, the ray entered a box within edge_eps x (bounce + 1) metres (along the ray) of one of its edges:
+    the reference takes the normal of the face whose slab the ray entered last, and at an edge the float32
+    arithmetic can pick the neighbouring face, so the surfaces part only at the next bounce.  Anything else
+    is counted as unexplained.
     """
     rays = np.asarray(rays, dtype=np.int64)
     dirs = np.ascontiguousarray(np.asarray(directions, dtype=np.float64)[rays])
@@ -245,7 +249,9 @@ def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfac
     params.source_radius = float(trace_kwargs.get("source_radius", 0.1))
     scattering = np.asarray(arrays["scattering"], dtype=np.float64)
     rng = np.random.default_rng(seed)
-    causes = {"precision_tie": 0, "diffuse_threshold_tie": 0, "path_length_tie": 0, "unexplained": 0}
+    causes = {"precision_tie": 0, "diffuse_threshold_tie": 0, "box_edge_tie": 0, "path_length_tie": 0,
+              "unexplained": 0}
+    kinds = np.asarray(arrays["kinds"])
     unexplained: list[int] = []
     t = np.zeros(1)
     for k, ray in enumerate(rays):
@@ -262,6 +268,20 @@ def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfac
                 threshold = True
         if threshold:
             causes["diffuse_threshold_tie"] += 1
+            continue
+        # a box hit near one of its edges at an earlier bounce: the float32 trace may take the other face's
+        # normal there, so the surfaces agree at that bounce and part at the next one
+        edge = False
+        for j in range(b):
+            s = int(ref_seq[j])
+            if kinds[s] != 2:
+                continue
+            st = sub["ray_states"][k, j]
+            if _box_face_gap(arrays, s, st[:3], st[3:6]) <= edge_eps * (j + 1):
+                edge = True
+                break
+        if edge:
+            causes["box_edge_tie"] += 1
             continue
         state = sub["ray_states"][k, b]
         if not np.isfinite(state).all():
@@ -296,6 +316,28 @@ def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfac
             causes["unexplained"] += 1
             unexplained.append(int(ray))
     return {"rays": int(rays.size), **causes, "unexplained_rays": unexplained}
+
+
+def _box_face_gap(arrays: Mapping[str, Any], si: int, origin, direction) -> float:
+    """For a ray entering oriented box `si` (steam_rt.py:4277-4358 frame), the distance along the ray
+    between the last and the second-to-last slab it enters: small near an edge of the entry face."""
+    c = np.asarray(arrays["box_center"][si], dtype=float)
+    u = np.asarray(arrays["box_axis_u"][si], dtype=float)
+    v = np.asarray(arrays["box_axis_v"][si], dtype=float)
+    half = np.asarray(arrays["box_half"][si], dtype=float)
+    z0, z1 = (float(x) for x in arrays["box_z"][si])
+    rel = np.asarray(origin[:2], dtype=float) - c
+    o = [float(rel @ u), float(rel @ v), float(origin[2])]
+    d = [float(np.asarray(direction[:2]) @ u), float(np.asarray(direction[:2]) @ v), float(direction[2])]
+    lo, hi = [-half[0], -half[1], z0], [half[0], half[1], z1]
+    entries = []
+    for a in range(3):
+        if abs(d[a]) > 1e-15:
+            entries.append(min((lo[a] - o[a]) / d[a], (hi[a] - o[a]) / d[a]))
+    if len(entries) < 2:
+        return float("inf")
+    entries.sort()
+    return entries[-1] - entries[-2]
 
 
 def synthesize(echogram: np.ndarray, *, fs: int, bin_dur: float, direct_delay: float, c: float,
