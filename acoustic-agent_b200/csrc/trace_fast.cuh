@@ -455,9 +455,38 @@ __device__ __forceinline__ bool child_box(const FRay &r, float lx, float hx, flo
 // any-hit modes work as there.
 constexpr int kBvhDone = static_cast<int>(0x80000000u);  // below every leaf reference
 
+// The per-lane traversal stack.  In shared memory (AC_SMEM_STACK, the
+// default): entry-major, [kBvhStack][256] words per block, so the lanes of a
+// warp hit 32 different banks whatever their stack depths, and stack traffic
+// stays out of L1, where the scene's nodes and surfaces live.  Otherwise in
+// local memory (a per-thread array).
+#ifndef AC_SMEM_STACK
+#define AC_SMEM_STACK 1
+#endif
+constexpr int kStackStride = 256;   // threads per block at most
+
+struct LaneStack {
+#if AC_SMEM_STACK
+    int *base;
+    __device__ __forceinline__ int &operator[](int i) { return base[i * kStackStride]; }
+#else
+    int entries[kBvhStack];
+    __device__ __forceinline__ int &operator[](int i) { return entries[i]; }
+#endif
+};
+
+__device__ __forceinline__ LaneStack lane_stack() {
+#if AC_SMEM_STACK
+    __shared__ int stack_words[kBvhStack * kStackStride];
+    return LaneStack{stack_words + threadIdx.x};
+#else
+    return LaneStack{};
+#endif
+}
+
 __device__ __forceinline__ void bvh_traverse(const FastScene &fs, const FRay &r, bool any_hit, float &best_t,
                                              int &best) {
-    int stack[kBvhStack];
+    LaneStack stack = lane_stack();
     stack[0] = kBvhDone;
     int sp = 1;
     int node = 0;      // next node to visit (>= 0 inner, < 0 leaf, kBvhDone finished)
@@ -523,7 +552,7 @@ __device__ __forceinline__ void cswap(float &ea, int &ra, float &eb, int &rb) {
 
 __device__ __forceinline__ void bvh4_traverse(const FastScene &fs, const FRay &r, bool any_hit, float &best_t,
                                               int &best) {
-    int stack[kBvhStack];
+    LaneStack stack = lane_stack();
     stack[0] = kBvhDone;
     int sp = 1;
     int node = 0;

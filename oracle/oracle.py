@@ -95,9 +95,6 @@ def _lib() -> ctypes.CDLL:
         lib.oracle_trace.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Params), ctypes.POINTER(_Outputs)]
         lib.oracle_closest_hit.restype = ctypes.c_int
         lib.oracle_closest_hit.argtypes = [ctypes.POINTER(_Scene), _d, _d, _d, _d]
-        lib.oracle_bounce_outcome.restype = ctypes.c_int64
-        lib.oracle_bounce_outcome.argtypes = [ctypes.POINTER(_Scene), ctypes.POINTER(_Params), _d, _d,
-                                              ctypes.c_double, ctypes.c_int64, _d]
         lib.oracle_synthesize.restype = ctypes.c_int
         lib.oracle_synthesize.argtypes = [_d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, _d, _d, _d, _f32]
         lib.oracle_bandlimit.restype = ctypes.c_int
@@ -215,129 +212,42 @@ def first_divergence(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     return np.where(diff.any(axis=1), first, -1)
 
 
-def divergence_causes(arrays: Mapping[str, Any], *, rays: np.ndarray, gpu_surfaces: np.ndarray,
-                      ref_surfaces: np.ndarray, directions, diffuse_bank, diffuse_random, diffuse_indices,
-                      trials: int = 48, origin_eps: float = 4e-6, direction_eps: float = 4e-7, edge_eps: float = 2e-5,
-                      seed: int = 0, **trace_kwargs) -> dict[str, Any]:
-    """Why a float32 trace left the float64 one on each of `rays` (rays whose hit sequences differ).
+def path_sensitivity(arrays: Mapping[str, Any], *, rays: np.ndarray, directions, diffuse_bank, diffuse_random,
+                     diffuse_indices, trials: int = 32, eps: float = 1e-6, seed: int = 0,
+                     target_surfaces: np.ndarray | None = None, **trace_kwargs) -> dict[str, Any]:
+    """How robust each of `rays` is to float32-scale changes: every ray is traced again `trials` times in
+    float64 with its initial direction turned by about `eps` radians (a seeded random offset of norm ~eps,
+    renormalised; float32 rounds a unit vector's components by up to 6e-8).
 
-    At the first differing bounce the float64 state (origin, direction, path length) is taken from this
-    oracle.  The divergence is a precision tie when the float64 decision at that bounce is not robust to
-    perturbations of float32 size: moving the origin by up to origin_eps x (bounce + 1) metres and turning
-    the direction by up to direction_eps x (bounce + 1) radians, in `trials` seeded random ways, gives the
-    float32 trace's outcome at least once (a grazing hit, an edge or corner, two surfaces at the same
-    distance, a sphere or path-length threshold).  It is a diffuse-threshold tie when, at a bounce up to
-    that one, the ray's uniform draw lies within float32 rounding of the surface's scattering, so the two
-    traces chose different reflection kinds on the same surface.  It is a box-edge tie when, at an earlier
-    bounce, the ray entered a box within edge_eps x (bounce + 1) metres (along the ray) of one of its edges:
-    the reference takes the normal of the face whose slab the ray entered last, and at an edge the float32
-    arithmetic can pick the neighbouring face, so the surfaces part only at the next bounce.  Anything else
-    is counted as unexplained.
+    `sensitive`: the fraction of rays whose float64 hit sequence changes under at least one such turn.
+    With `target_surfaces` ([R_total, B] hit sequences of another trace, e.g. a float32 one, indexed by ray):
+    `reproduced`, the fraction of rays for which some turned float64 trace follows the target sequence up
+    to and including the first bounce where the target leaves the unturned float64 path.
     """
     rays = np.asarray(rays, dtype=np.int64)
-    dirs = np.ascontiguousarray(np.asarray(directions, dtype=np.float64)[rays])
-    rnd = np.ascontiguousarray(np.asarray(diffuse_random, dtype=np.float64)[:, rays])
-    idx = np.ascontiguousarray(np.asarray(diffuse_indices, dtype=np.int32)[:, rays])
-    sub = trace(arrays, directions=dirs, diffuse_bank=diffuse_bank, diffuse_random=rnd, diffuse_indices=idx,
-                record_rays=True, record_states=True, threads=1, **trace_kwargs)
-    scene = Scene(arrays, bool(trace_kwargs.get("use_bvh", False)))
-    params = _Params()
-    params.source[:] = [float(v) for v in trace_kwargs["source"]]
-    params.listener[:] = [float(v) for v in trace_kwargs["listener"]]
-    params.max_path_len = float(trace_kwargs["max_path_len"])
-    params.listener_radius = float(trace_kwargs.get("listener_radius", 0.1))
-    params.source_radius = float(trace_kwargs.get("source_radius", 0.1))
-    scattering = np.asarray(arrays["scattering"], dtype=np.float64)
+    dirs = np.asarray(directions, dtype=np.float64)
+    rnd = np.asarray(diffuse_random, dtype=np.float64)
+    idx = np.asarray(diffuse_indices, dtype=np.int32)
+    base = trace(arrays, directions=dirs[rays], diffuse_bank=diffuse_bank, diffuse_random=rnd[:, rays],
+                 diffuse_indices=idx[:, rays], record_rays=True, **trace_kwargs)["ray_surfaces"]
     rng = np.random.default_rng(seed)
-    causes = {"precision_tie": 0, "diffuse_threshold_tie": 0, "box_edge_tie": 0, "path_length_tie": 0,
-              "unexplained": 0}
-    kinds = np.asarray(arrays["kinds"])
-    unexplained: list[int] = []
-    t = np.zeros(1)
-    for k, ray in enumerate(rays):
-        ref_seq = np.asarray(ref_surfaces[ray])
-        if not np.array_equal(sub["ray_surfaces"][k], ref_seq):
-            raise AssertionError("the oracle traced a ray differently alone")
-        b = int(first_divergence(np.asarray(gpu_surfaces[ray])[None], ref_seq[None])[0])
-        want = int(gpu_surfaces[ray][b])
-        # reflection kind chosen on a float32 rounding edge at an earlier bounce (or at this one)
-        threshold = False
-        for j in range(b):   # the reflection kind chosen after bounce j sets the direction of bounce j + 1
-            s = int(ref_seq[j])
-            if abs(float(rnd[j, k]) - float(scattering[s])) <= 2.0 ** -22 * max(1.0, abs(scattering[s])):
-                threshold = True
-        if threshold:
-            causes["diffuse_threshold_tie"] += 1
-            continue
-        # a box hit near one of its edges at an earlier bounce: the float32 trace may take the other face's
-        # normal there, so the surfaces agree at that bounce and part at the next one
-        edge = False
-        for j in range(b):
-            s = int(ref_seq[j])
-            if kinds[s] != 2:
-                continue
-            st = sub["ray_states"][k, j]
-            if _box_face_gap(arrays, s, st[:3], st[3:6]) <= edge_eps * (j + 1):
-                edge = True
-                break
-        if edge:
-            causes["box_edge_tie"] += 1
-            continue
-        state = sub["ray_states"][k, b]
-        if not np.isfinite(state).all():
-            # the float64 ray ended after bounce b - 1 because its path grew past the limit
-            prev = sub["ray_states"][k, b - 1]
-            _lib().oracle_bounce_outcome(ctypes.byref(scene.struct), ctypes.byref(params),
-                                         _p(np.ascontiguousarray(prev[:3]), _d), _p(np.ascontiguousarray(prev[3:6]), _d),
-                                         float(prev[6]), b - 1, _p(t, _d))
-            end = float(prev[6]) + float(t[0])
-            if abs(end - params.max_path_len) <= 1e-5 * params.max_path_len * b:
-                causes["path_length_tie"] += 1
-            else:
-                causes["unexplained"] += 1
-                unexplained.append(int(ray))
-            continue
-        o, d, dist = state[:3], state[3:6], float(state[6])
-        tie = False
-        for _ in range(trials):
-            u = rng.normal(size=3)
-            v = rng.normal(size=3)
-            o2 = np.ascontiguousarray(o + origin_eps * (b + 1) * rng.uniform() * u / np.linalg.norm(u))
-            d2 = d + direction_eps * (b + 1) * rng.uniform() * v / np.linalg.norm(v)
-            d2 = np.ascontiguousarray(d2 / np.linalg.norm(d2))
-            got = _lib().oracle_bounce_outcome(ctypes.byref(scene.struct), ctypes.byref(params), _p(o2, _d),
-                                               _p(d2, _d), dist, b, _p(t, _d))
-            if int(got) == want:
-                tie = True
-                break
-        if tie:
-            causes["precision_tie"] += 1
-        else:
-            causes["unexplained"] += 1
-            unexplained.append(int(ray))
-    return {"rays": int(rays.size), **causes, "unexplained_rays": unexplained}
-
-
-def _box_face_gap(arrays: Mapping[str, Any], si: int, origin, direction) -> float:
-    """For a ray entering oriented box `si` (steam_rt.py:4277-4358 frame), the distance along the ray
-    between the last and the second-to-last slab it enters: small near an edge of the entry face."""
-    c = np.asarray(arrays["box_center"][si], dtype=float)
-    u = np.asarray(arrays["box_axis_u"][si], dtype=float)
-    v = np.asarray(arrays["box_axis_v"][si], dtype=float)
-    half = np.asarray(arrays["box_half"][si], dtype=float)
-    z0, z1 = (float(x) for x in arrays["box_z"][si])
-    rel = np.asarray(origin[:2], dtype=float) - c
-    o = [float(rel @ u), float(rel @ v), float(origin[2])]
-    d = [float(np.asarray(direction[:2]) @ u), float(np.asarray(direction[:2]) @ v), float(direction[2])]
-    lo, hi = [-half[0], -half[1], z0], [half[0], half[1], z1]
-    entries = []
-    for a in range(3):
-        if abs(d[a]) > 1e-15:
-            entries.append(min((lo[a] - o[a]) / d[a], (hi[a] - o[a]) / d[a]))
-    if len(entries) < 2:
-        return float("inf")
-    entries.sort()
-    return entries[-1] - entries[-2]
+    rep = np.repeat(rays, trials)
+    turned = dirs[rep] + eps * rng.normal(size=(rep.size, 3)) / math.sqrt(3.0)
+    turned /= np.linalg.norm(turned, axis=1, keepdims=True)
+    pert = trace(arrays, directions=turned, diffuse_bank=diffuse_bank, diffuse_random=rnd[:, rep],
+                 diffuse_indices=idx[:, rep], record_rays=True, **trace_kwargs)["ray_surfaces"]
+    pert = pert.reshape(rays.size, trials, -1)
+    sensitive = np.array([np.any(pert[k] != base[k][None]) for k in range(rays.size)])
+    out: dict[str, Any] = {"rays": int(rays.size), "sensitive": float(sensitive.mean()) if rays.size else 0.0}
+    if target_surfaces is not None:
+        tgt = np.asarray(target_surfaces)[rays]
+        reproduced = []
+        for k in range(rays.size):
+            diff = np.flatnonzero(tgt[k] != base[k])
+            upto = (int(diff[0]) if diff.size else tgt.shape[1] - 1) + 1
+            reproduced.append(bool(np.any(np.all(pert[k][:, :upto] == tgt[k][None, :upto], axis=1))))
+        out["reproduced"] = float(np.mean(reproduced)) if reproduced else 0.0
+    return out
 
 
 def synthesize(echogram: np.ndarray, *, fs: int, bin_dur: float, direct_delay: float, c: float,

@@ -502,29 +502,6 @@ int oracle_trace(const oracle_scene *sc, const oracle_params *p, oracle_outputs 
     return 0;
 }
 
-/* The decision at the top of one bounce of oracle_trace (steam_rt.py:4743-4760) from a given ray state:
- * the closest surface, or -1 when the ray ends there (no hit, t within the listener radius, path too
- * long, or, after the first bounce, the listener or source sphere in front of the hit). */
-int64_t oracle_bounce_outcome(const oracle_scene *sc, const oracle_params *p, const double *origin,
-                              const double *dir, double accum_distance, int64_t bounce, double *t_out)
-{
-    visit_stats st = {0, {0, 0, 0}, 0};
-    double t, n[3];
-    const double *src = p->source, *lst = p->listener;
-    int64_t surf = closest_hit(sc, origin, dir, &t, n, &st);
-    *t_out = t;
-    if (surf < 0 || t <= p->listener_radius || accum_distance > p->max_path_len) return -1;
-    if (bounce > 0) {
-        if (sphere_before(origin, dir, lst[0], lst[1], lst[2], p->listener_radius, t)) return -1;
-        double dx = lst[0] - src[0], dy = lst[1] - src[1], dz = lst[2] - src[2];
-        double source_distance = sqrt(dx * dx + dy * dy + dz * dz);
-        if (source_distance > p->source_radius && sphere_before(origin, dir, src[0], src[1], src[2],
-                                                                p->source_radius, t))
-            return -1;
-    }
-    return surf;
-}
-
 /* steam_rt.py:4131-4146: one biquad section; state in double, output rounded to float32. */
 static void biquad(const double *x, float *y, int64_t n, const double *co)
 {
