@@ -403,8 +403,8 @@ def main() -> int:
                              "parity block and the CPU baseline")
     parser.add_argument("--e2e-steps", type=int, default=2, help="mixed_batch: end-to-end steps to time")
     parser.add_argument("--profile-launch", action="store_true",
-                        help="mixed_batch: after the warm-up, run one eager step between cudaProfilerStart/Stop "
-                             "and exit (for ncu --profile-from-start off)")
+                        help="after the warm-up, run one eager step (mixed_batch) or trace launch (single-scene "
+                             "workloads) between cudaProfilerStart/Stop and exit (for ncu --profile-from-start off)")
     parser.add_argument("--no-config1", dest="with_config1", action="store_false",
                         help="mixed_batch: skip the single-scene U-room figures added to the line")
     parser.add_argument("--rate", type=float, default=50.0, help="serving: Poisson arrival rate, requests/s")
@@ -543,6 +543,15 @@ def run_single_scene(args, workload_name: str, *, extras_only: bool = False):
         step()
     torch.cuda.synchronize(device)
     ray_bounces_per_step = renderer.ray_bounces(plan)
+    if args.profile_launch and not extras_only:
+        # one trace launch of every channel between cudaProfilerStart/Stop (for `ncu --profile-from-start off`)
+        profiled = [(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)]
+        torch.cuda.profiler.start()
+        runtime.trace_batch(profiled, runtime.BatchWorkspace(device), block_size=args.block)
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled": "trace launch", "ray_bounces": ray_bounces_per_step}), flush=True)
+        return 0
 
     def barrier():
         if dist is not None:
@@ -1638,6 +1647,9 @@ PROFILED = {
     "u_room_20_boxes": {"issue_active": 0.69, "simt_efficiency": 13.99 / 32.0,
                         "dram_bytes_per_ray_bounce": 4753408 / 52028160,
                         "profile": "profiles/trace_kernel_u_room_20_boxes.md", "kernel_commit": "e64c19a"},
+    "mixed_batch": {"issue_active": 0.6255, "simt_efficiency": 13.11 / 32.0,
+                    "dram_bytes_per_ray_bounce": (32922624 + 1248512) / 2209616616,
+                    "profile": "profiles/trace_kernel_mixed_batch_24_scenes.md", "kernel_commit": "2860a90"},
 }
 
 
