@@ -825,6 +825,40 @@ def facade_rirs(workload, runs: int = 2) -> dict:
             "sample": f"AcousticAgent.create(...).run() over {channels} channels, mean of {runs} after 1 warm-up"}
 
 
+def single_rir_latency(workload, repeats: int = 5) -> dict:
+    """Latency of ONE RIR (channel 0) end to end through the drop-in: ``backend.trace_energy_field`` (scene
+    resident after the first call, the reference's random stream drawn on the device, echogram back on the
+    host), then the band synthesis of that echogram on the GPU (``runtime.synthesize``, band IRs back on the
+    host).  Median of `repeats` after one warm-up; the synthesis share is stated."""
+    import torch
+    from acoustic_agent_b200 import backend, runtime, scene as scene_mod
+    cfg = workload.config
+    arrays = scene_mod.compile_scene(workload.spec)
+    src = np.asarray(workload.sources[0], dtype=float)
+    lst = np.asarray(workload.listeners[0], dtype=float)
+    device = torch.device("cuda", 0)
+    ws = runtime.SynthWorkspace(device)
+    trace_ms, synth_ms = [], []
+    for k in range(repeats + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        field = backend.trace_energy_field(arrays, src, lst, cfg, workload.source_model, render_ambisonics=False)
+        t1 = time.perf_counter()
+        echo = torch.as_tensor(field["echogram"][None], device=device)
+        d = torch.tensor([field["direct_delay_s"]], dtype=torch.float64, device=device)
+        params = runtime.synth_params(1, int(field["num_bins"]), cfg.rt_bin_duration_s, cfg.fs, cfg.c,
+                                      rng_mode="philox", seed=int(cfg.seed) + 7, direct_delays=d)
+        runtime.synthesize(echo.contiguous(), params, ws).cpu()
+        t2 = time.perf_counter()
+        if k:
+            trace_ms.append(1e3 * (t1 - t0))
+            synth_ms.append(1e3 * (t2 - t1))
+    tr, sy = float(np.median(trace_ms)), float(np.median(synth_ms))
+    return {"trace_ms": tr, "synthesis_ms": sy, "total_ms": tr + sy, "synthesis_share": sy / (tr + sy),
+            "note": "one channel: drop-in trace_energy_field (reference stream, on the device) + GPU band "
+                    "synthesis, host arrays in and out, median of 5 after 1 warm-up"}
+
+
 def mix_bytes_per_ray_bounce(arrays, jobs, ray_bounces_per_job, sample_rays: int = 512) -> float:
     """Algorithmic bytes per ray-bounce over the mix (roofline numerator, per-unit figure).
 
@@ -1076,6 +1110,7 @@ def run_mixed_batch(args) -> int:
     def config1():
         line["config1_u_room"] = run_single_scene(args, "u_room_20_boxes", extras_only=True)
         if not args.no_cpu_baseline and world == 1:
+            line["config1_u_room"]["single_rir_latency"] = single_rir_latency(workloads.u_furnished(1729))
             line["config1_u_room"]["facade"] = facade_rirs(workloads.u_furnished(1729))
 
     if not args.no_cpu_baseline:
