@@ -1080,13 +1080,27 @@ def run_mixed_batch(args) -> int:
             line["batched_vs_drop_in_plain"] = value / drop["rirs_per_s"]
         echo_host = plan.echo_store.cpu().numpy()
         offsets = np.cumsum([0] + [6 * int(j.spec.num_bins) for j in jobs])
-        same, philox = [], []
+        same, philox, philox_rays = [], [], []
+        from oracle import oracle
+        _, bank, _, _ = oracle.workspace(1, 0, 0)
         for k, ref_echo in ref64["echograms"].items():
-            bd = jobs[k].spec.bin_duration
+            spec = jobs[k].spec
+            bd = spec.bin_duration
             ours_philox = echo_host[offsets[k]:offsets[k + 1]].reshape(6, -1)
             philox.append(metrics.parity(ours_philox, ref_echo, bd))
             if k in drop.get("echograms", {}):
                 same.append(metrics.parity(drop["echograms"][k], ref_echo, bd))
+            # the float64 restatement of the reference's tracer fed the batch's own Philox rays
+            dirs, rnd, idx = oracle.philox_workspace(int(spec.num_rays), int(spec.num_bounces), int(spec.seed),
+                                                     int(spec.stream_key))
+            f64 = oracle.trace(arrays[jobs[k].scene_index], source=np.asarray(spec.source),
+                               listener=np.asarray(spec.listener), directions=dirs, diffuse_bank=bank,
+                               diffuse_random=rnd, diffuse_indices=idx, num_bins=int(spec.num_bins), bin_dur=bd,
+                               c=spec.speed_of_sound, max_path_len=spec.max_path_length, direct_delay=spec.direct_delay,
+                               source_forward=np.asarray(spec.source_forward, dtype=float),
+                               dipole_weight=spec.dipole_weight, dipole_power=spec.dipole_power,
+                               use_bvh=bool(spec.use_bvh))["echogram"]
+            philox_rays.append(metrics.parity(ours_philox, f64, bd))
 
         def worst(rows):
             return {key: max(r[key] for r in rows) for key in rows[0]} if rows else None
@@ -1094,11 +1108,14 @@ def run_mixed_batch(args) -> int:
         line["parity"] = {
             "jobs": len(ref64["echograms"]),
             "same_stream": worst(same),
+            "philox_same_rays": worst(philox_rays),
             "philox_stream": worst(philox),
-            "note": ("GPU float32 echograms against the reference's float64 Numba echogram of the same job "
-                     "(trace_energy_field, rt_precision='float64'); same_stream: the drop-in on the reference's "
-                     "own random stream (identical rays); philox_stream: the batch's own echogram (Philox rays, "
-                     "Monte-Carlo difference); worst band and job"),
+            "note": ("worst band and job.  same_stream: the drop-in (float32) on the reference's own random stream "
+                     "against the reference's float64 Numba echogram of the same job (trace_energy_field, "
+                     "rt_precision='float64'; identical rays).  philox_same_rays: the batch's own float32 echogram "
+                     "against the float64 restatement of the reference's tracer fed the same Philox rays.  "
+                     "philox_stream: the batch's echogram against the reference's float64 echogram on its own "
+                     "stream (different rays: Monte-Carlo difference, large for 1e4-ray jobs)"),
         }
 
     def reference_cuda():
