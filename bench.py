@@ -1090,7 +1090,10 @@ def run_mixed_batch(args) -> int:
             philox.append(metrics.parity(ours_philox, ref_echo, bd))
             if k in drop.get("echograms", {}):
                 same.append(metrics.parity(drop["echograms"][k], ref_echo, bd))
-            # the float64 restatement of the reference's tracer fed the batch's own Philox rays
+            # the float64 restatement of the reference's tracer fed the batch's own Philox rays (its workspace
+            # holds 12 bytes per ray-bounce slot: jobs up to 4e7 slots)
+            if int(spec.num_rays) * int(spec.num_bounces) > 40_000_000:
+                continue
             dirs, rnd, idx = oracle.philox_workspace(int(spec.num_rays), int(spec.num_bounces), int(spec.seed),
                                                      int(spec.stream_key))
             f64 = oracle.trace(arrays[jobs[k].scene_index], source=np.asarray(spec.source),
