@@ -506,15 +506,18 @@ class ContinuousServer:
 
     Admission: a request is admitted when its device footprint fits the HBM budget (resident scenes plus the
     outputs of requests in flight); one that could never fit is rejected.  With `slo_s`, a request is also
-    rejected at arrival when the work already admitted plus its own, at the throughput measured so far
-    (`capacity_rb_per_s` until a first measurement), would not finish within `slo_s` of its arrival: overload
-    is shed instead of queueing without bound.  Requests that wait for memory are admitted in arrival order.
+    rejected at arrival when the traced work already admitted or waiting ahead of it would take longer than
+    `slo_s` at the service's throughput: overload is shed instead of queueing without bound.  The throughput
+    is `capacity_rb_per_s` ray-bounces/s (the persistent launch's rate with two blocks per SM) until the
+    server has run saturated -- at least a quarter second of work ahead -- for a second; from then on, the
+    rate measured while saturated (a rate measured while the device idles between requests would understate
+    it and shed work the device could take).  Requests that wait for memory are admitted in arrival order.
     Each result is the same as the request rendered alone (rays keyed by request identity, exact fixed-point
     sums, synthesis noise keyed by the job's seed).
     """
 
     def __init__(self, device: int = 0, *, hbm_budget: int | None = None, tune: bool = True,
-                 slo_s: float | None = None, capacity_rb_per_s: float = 4.0e9, blocks_per_sm: int = 2,
+                 slo_s: float | None = None, capacity_rb_per_s: float = 2.2e9, blocks_per_sm: int = 2,
                  capacity: int = 4096, idle_timeout_s: float = 0.02, chunk_rays: int = 0) -> None:
         self.dev = runtime.require_cuda(device)
         if hbm_budget is None:
@@ -590,16 +593,16 @@ class ContinuousServer:
         synthesizing: list[_Live] = []
         results: list[Result] = []
         outstanding_rb = 0.0               # estimated ray-bounces admitted and not yet traced
-        done_rb = 0
-        busy_s = 0.0                       # time with jobs on the trace service
+        sat_rb = 0.0                       # ray-bounces finished, and seconds spent, while saturated
+        sat_s = 0.0
         peak = 0
         t0 = time.perf_counter()
         tick = t0
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
-        live_count = 0
+        max_live = 0
         while pending or waiting or tracing or synthesizing:
             now = clock()
-            was_busy = bool(tracing)
+            saturated = outstanding_rb >= 0.25 * self.capacity_rb_per_s
             # arrivals: reject what can never fit, or what the admitted work would make miss its SLO
             while pending and pending[0].arrival_s <= now:
                 req = pending.popleft()
@@ -611,8 +614,8 @@ class ContinuousServer:
                                                                    f"the budget is {self.budget}"))
                     continue
                 if self.slo_s is not None:
-                    rate = (done_rb / busy_s) if busy_s > 0.5 and done_rb > 0 else self.capacity_rb_per_s
-                    wait = (outstanding_rb + sum(self._est_rb(w[1]) for w in waiting) + self._est_rb(specs)) / rate
+                    rate = sat_rb / sat_s if sat_s >= 1.0 and sat_rb > 0 else self.capacity_rb_per_s
+                    wait = (outstanding_rb + sum(self._est_rb(w[1]) for w in waiting)) / rate
                     if wait > self.slo_s:
                         results.append(Result(req, [], 0, t, t, error=f"overloaded: about {wait:.2f} s of traced work "
                                                                        f"ahead exceeds the {self.slo_s:g} s limit"))
@@ -633,7 +636,6 @@ class ContinuousServer:
                 for seq in live.seqs:
                     tracing[seq] = live
                 outstanding_rb += live.est_ray_bounces
-                live_count += 1
                 peak = max(peak, self.in_use + self.scenes.resident_bytes())
             # traces that finished: their requests go to synthesis once all their jobs are done
             finished = []
@@ -647,7 +649,8 @@ class ContinuousServer:
                     rb = sum(int(b.counters[2].item()) for b in live.buffers)
                     rays = sum(s.num_rays for s in live.specs)
                     self.bounces_per_ray = 0.8 * self.bounces_per_ray + 0.2 * rb / max(rays, 1)
-                    done_rb += rb
+                    if saturated:
+                        sat_rb += rb
                     outstanding_rb -= live.est_ray_bounces
                     live.ray_bounces = rb     # type: ignore[attr-defined]
                 self._synthesize(finished)
@@ -664,9 +667,10 @@ class ContinuousServer:
                                           live.admitted_s, time.perf_counter() - t0))
                     self.scenes.release(live.request.workload)
                     self.in_use -= live.bytes
+            max_live = max(max_live, len({id(v) for v in tracing.values()}) + len(synthesizing))
             nowp = time.perf_counter()
-            if was_busy:
-                busy_s += nowp - tick
+            if saturated:
+                sat_s += nowp - tick
             tick = nowp
             if not realtime and not tracing and not waiting and not synthesizing and pending:
                 continue
@@ -678,7 +682,7 @@ class ContinuousServer:
         info = self.service.info()
         return Report(results=sorted(results, key=lambda r: r.request.id), makespan_s=makespan,
                       rirs=sum(r.request.num_rirs for r in served), ray_bounces=sum(r.ray_bounces for r in served),
-                      batches=int(info["launches"]), max_inflight_seen=live_count, scene_hits=self.scenes.hits,
+                      batches=int(info["launches"]), max_inflight_seen=max_live, scene_hits=self.scenes.hits,
                       scene_misses=self.scenes.misses, evictions=self.scenes.evictions, peak_bytes=peak)
 
     def close(self) -> None:

@@ -414,8 +414,8 @@ def main() -> int:
                         help="serving: kernel-level continuous batching or batch-level server")
     parser.add_argument("--slo", type=float, default=2.0,
                         help="serving (continuous): shed requests whose admitted work ahead exceeds this, seconds")
-    parser.add_argument("--capacity-rb", type=float, default=4.0e9,
-                        help="serving (continuous): ray-bounces/s assumed until the first measurement")
+    parser.add_argument("--capacity-rb", type=float, default=2.2e9,
+                        help="serving (continuous): ray-bounces/s assumed until measured while saturated")
     parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     parser.add_argument("--policy", default="small_first", choices=("small_first", "fifo"),
                         help="serving: order in which waiting requests join a batch")
@@ -1197,7 +1197,7 @@ def run_serving(args) -> int:
                     "rejected": s["rejected"], "offered_rirs_per_s": sum(r.num_rirs for r in requests) / args.duration,
                     "rirs_per_s": s["rirs_per_s"], "ray_bounces_per_s": s["ray_bounces_per_s"],
                     "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
-                    "max_admitted_at_once": s["max_inflight"], "launches_or_batches": s["batches"]})
+                    "max_requests_on_gpu": s["max_inflight"], "launches_or_batches": s["batches"]})
     if hasattr(server, "close"):
         server.close()
     by_rate = {}
