@@ -1699,9 +1699,9 @@ def l2_read_gbs(device) -> float:
 # SIMT efficiency (thread instructions per warp instruction / 32) and DRAM bytes per ray-bounce
 # (dram__bytes_read.sum + dram__bytes_write.sum of the captured launch over its ray-bounces).
 PROFILED = {
-    "u_room_20_boxes": {"issue_active": 0.69, "simt_efficiency": 13.99 / 32.0,
-                        "dram_bytes_per_ray_bounce": 4753408 / 52028160,
-                        "profile": "profiles/trace_kernel_u_room_20_boxes.md", "kernel_commit": "e64c19a"},
+    "u_room_20_boxes": {"issue_active": 0.6706, "simt_efficiency": 14.41 / 32.0,
+                        "dram_bytes_per_ray_bounce": (3123456 + 734208) / 52028160,
+                        "profile": "profiles/trace_kernel_u_room_20_boxes.md", "kernel_commit": "2860a90"},
     "mixed_batch": {"issue_active": 0.6255, "simt_efficiency": 13.11 / 32.0,
                     "dram_bytes_per_ray_bounce": (32922624 + 1248512) / 2209616616,
                     "profile": "profiles/trace_kernel_mixed_batch_24_scenes.md", "kernel_commit": "2860a90"},
