@@ -599,7 +599,7 @@ class ContinuousServer:
         t0 = time.perf_counter()
         tick = t0
         clock = (lambda: time.perf_counter() - t0) if realtime else (lambda: float("inf"))
-        max_live = 0
+        max_live = live_now = 0            # requests on the GPU (tracing or synthesizing), most at once
         while pending or waiting or tracing or synthesizing:
             now = clock()
             saturated = outstanding_rb >= 0.25 * self.capacity_rb_per_s
@@ -636,6 +636,7 @@ class ContinuousServer:
                 for seq in live.seqs:
                     tracing[seq] = live
                 outstanding_rb += live.est_ray_bounces
+                live_now += 1
                 peak = max(peak, self.in_use + self.scenes.resident_bytes())
             # traces that finished: their requests go to synthesis once all their jobs are done
             finished = []
@@ -667,7 +668,8 @@ class ContinuousServer:
                                           live.admitted_s, time.perf_counter() - t0))
                     self.scenes.release(live.request.workload)
                     self.in_use -= live.bytes
-            max_live = max(max_live, len({id(v) for v in tracing.values()}) + len(synthesizing))
+                    live_now -= 1
+            max_live = max(max_live, live_now)
             nowp = time.perf_counter()
             if saturated:
                 sat_s += nowp - tick
