@@ -52,7 +52,8 @@ struct ac_service_s {
     int64_t idle_ns = 20000000;
     ac::ServiceSlot *slots = nullptr;              // device ring
     ac::ServiceSlotState *state = nullptr;         // device
-    unsigned long long *low_water = nullptr;       // device
+    unsigned long long *words = nullptr;           // device: low-water mark, published copy, refresh time
+                                                   // (one 128-byte line each)
     ac::ServiceControl *control = nullptr;         // host, mapped
     ac::ServiceControl *control_dev = nullptr;     // its device address
     ac::ServiceSlot *staging = nullptr;            // pinned, one ring's worth
@@ -61,6 +62,7 @@ struct ac_service_s {
     Launch launches[kMaxLaunches];
     int next_launch = 0;
     int64_t next_seq = 0;                          // sequence number of the next submitted job
+    int64_t rays_submitted = 0;                    // rays of all jobs submitted so far
     std::vector<int64_t> inflight;                 // submitted, not yet reported done
     int64_t launches_started = 0;
     std::mutex lock;
@@ -71,7 +73,7 @@ namespace {
 int service_fail_cleanup(ac_service_s *s, int code) {
     if (s->slots) cudaFree(s->slots);
     if (s->state) cudaFree(s->state);
-    if (s->low_water) cudaFree(s->low_water);
+    if (s->words) cudaFree(s->words);
     if (s->control) cudaFreeHost(s->control);
     if (s->staging) cudaFreeHost(s->staging);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
@@ -120,7 +122,9 @@ int ensure_launch(ac_service_s *s) {
     t.slots = s->slots;
     t.slot_state = s->state;
     t.control = s->control_dev;
-    t.low_water = s->low_water;
+    t.low_water = s->words;
+    t.published_copy = s->words + 16;
+    t.refresh_at = s->words + 32;
     t.window_first = slot->first;
     t.window_end = slot->window_end;
     t.idle_ns = s->idle_ns;
@@ -188,7 +192,7 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     const size_t control_bytes = sizeof(ac::ServiceControl) + sizeof(long long) * static_cast<size_t>(capacity);
     if (cudaMalloc(&s->slots, sizeof(ac::ServiceSlot) * capacity) != cudaSuccess ||
         cudaMalloc(&s->state, sizeof(ac::ServiceSlotState) * capacity) != cudaSuccess ||
-        cudaMalloc(&s->low_water, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&s->words, 48 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void **>(&s->control), control_bytes, cudaHostAllocMapped) != cudaSuccess ||
         cudaHostAlloc(reinterpret_cast<void **>(&s->staging), sizeof(ac::ServiceSlot) * capacity,
                       cudaHostAllocDefault) != cudaSuccess) {
@@ -199,7 +203,7 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     std::memset(s->control, 0xFF, control_bytes);   // done flags: -1 (no job)
     s->control->published = 0;
     if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->control_dev), s->control, 0) != cudaSuccess ||
-        cudaMemset(s->low_water, 0, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMemset(s->words, 0, 48 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
@@ -262,6 +266,8 @@ extern "C" int ac_service_submit(ac_service_t s, const ac_job *jobs, int32_t num
         sl.chunk_rays = s->chunk_rays;
         sl.num_chunks = (in.params.num_rays + s->chunk_rays - 1) / s->chunk_rays;
         sl.scene_id = reinterpret_cast<uint64_t>(in.scene);
+        sl.ray_offset = s->rays_submitted;
+        s->rays_submitted += in.params.num_rays;
         s->control->done[seq & (s->capacity - 1)] = -1;
     }
     // copy the slots (one or two runs of the ring), zero the jobs' sums and counters

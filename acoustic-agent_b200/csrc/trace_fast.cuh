@@ -95,6 +95,8 @@ struct alignas(256) ServiceSlot {
     int64_t num_chunks;
     uint64_t scene_id;           // jobs with equal ids share a scene (no lane drain between them)
     int64_t chunk_rays;
+    int64_t ray_offset;          // rays of every job submitted before this one (a launch's warps start on
+                                 // the job that holds their share of the published rays)
 };
 
 struct ServiceSlotState {        // device, zeroed by the host before the slot is published
@@ -133,17 +135,53 @@ struct FastTable {
     ServiceSlotState *slot_state;
     ServiceControl *control;             // host-mapped
     unsigned long long *low_water;       // device: jobs below it have no chunks left
+    unsigned long long *published_copy;  // device: the published count as last read from the host
+    unsigned long long *refresh_at;      // device: %globaltimer time at which the copy is read again
     int64_t window_first;                // this launch takes jobs from this sequence number
     int64_t window_end;                  // to below this one only
     int64_t idle_ns;                     // and ends once its warps found no work for this long
     int64_t mask;                        // ring capacity - 1
 };
 
-// Service launches, lane 0 of a warp: the next chunk (seq, chunk index) from job `queue` onward, or false
-// when the launch should end -- its warps found no published job with chunks left for `idle_ns`, or its
-// window of sequence numbers is used up.  Every wait is bounded: the idle deadline, and a poll cap.
-__device__ __forceinline__ bool service_take(const FastTable &t, int64_t &queue, int64_t &published,
-                                             int64_t *seq_out, int64_t *chunk_out) {
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    return now;
+}
+
+// Service launches: the published job count.  One warp of the whole grid at a time reads the host-mapped
+// word (at most once per `kRefreshNs`) and raises a device copy of it; the others read the copy.  The
+// acquire/release pair carries the host's slot writes to the reading warp through the copy.
+constexpr unsigned long long kServiceRefreshNs = 2000;
+
+__device__ __forceinline__ long long service_published(const FastTable &t) {
+    const unsigned long long now = global_ns();
+    const unsigned long long due = *reinterpret_cast<volatile unsigned long long *>(t.refresh_at);
+    if (now >= due && atomicCAS(t.refresh_at, due, now + kServiceRefreshNs) == due) {
+        long long pub;
+        asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(pub) : "l"(&t.control->published) : "memory");
+        asm volatile("red.release.gpu.global.max.u64 [%0], %1;" ::"l"(t.published_copy),
+                     "l"(static_cast<unsigned long long>(pub)) : "memory");
+        return pub;
+    }
+    unsigned long long pub;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(pub) : "l"(t.published_copy) : "memory");
+    return static_cast<long long>(pub);
+}
+
+enum ServiceTake : int { kTakeChunk = 1, kTakeNone = 0, kTakeEnd = -1 };
+constexpr unsigned long long kServiceRetryNs = 4000;   // a warp with live lanes asks for work this often
+
+// Service launches, lane 0 of a warp: the next chunk (seq, chunk index) from job `queue` onward.
+//  * kTakeChunk: a chunk was taken.
+//  * kTakeNone (only when `may_wait` is false, i.e. some lanes of the warp still trace rays): nothing to
+//    take right now; the warp carries on with its live lanes and asks again later.  A warp never sleeps
+//    while it holds rays.
+//  * kTakeEnd: the launch should end for this warp -- it found no published job with chunks left for
+//    `idle_ns` while it had nothing to trace, or the launch's window of sequence numbers is used up.
+// Every wait is bounded: the idle deadline, and a poll cap.
+__device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, int64_t &queue, int64_t &published,
+                                            int64_t *seq_out, int64_t *chunk_out) {
     unsigned long long idle_from = 0;
     unsigned sleep_ns = 256;
     bool rescanned = false;
@@ -158,7 +196,7 @@ __device__ __forceinline__ bool service_take(const FastTable &t, int64_t &queue,
                 if (k < chunks) {
                     *seq_out = queue;
                     *chunk_out = k;
-                    return true;
+                    return kTakeChunk;
                 }
             }
             // no chunks left here: raise the low-water mark past it if it points here, then move on
@@ -178,28 +216,43 @@ __device__ __forceinline__ bool service_take(const FastTable &t, int64_t &queue,
                 continue;
             }
         }
-        if (queue >= t.window_end) return false;
-        // wait for the host to publish more, within the idle limit
-        unsigned long long now;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-        if (idle_from == 0) idle_from = now;
-        if (now - idle_from > static_cast<unsigned long long>(t.idle_ns)) return false;
-        __nanosleep(sleep_ns);
-        if (sleep_ns < 32768) sleep_ns <<= 1;
-        long long pub;
-        asm volatile("ld.acquire.sys.global.s64 %0, [%1];" : "=l"(pub) : "l"(&t.control->published) : "memory");
+        if (queue >= t.window_end) return kTakeEnd;
+        const long long pub = service_published(t);
         if (pub > published) {
             published = pub;
             rescanned = false;
+            continue;
         }
+        if (!may_wait) return kTakeNone;
+        // nothing to trace: wait for the host to publish more, within the idle limit
+        const unsigned long long now = global_ns();
+        if (idle_from == 0) idle_from = now;
+        if (now - idle_from > static_cast<unsigned long long>(t.idle_ns)) return kTakeEnd;
+        __nanosleep(sleep_ns);
+        if (sleep_ns < 32768) sleep_ns <<= 1;
     }
-    return false;
+    return kTakeEnd;
+}
+
+// Service launches, whole warp: `n` more rays of the job in `slot` have finished in this warp.  Every lane's
+// sums and counters for those rays were added before this call; after the warp barrier lane 0's fence
+// orders them (cumulatively) before the count, so the warp that completes the count sees every ray's sums.
+// Returns true on the warp that counted the job's last ray.
+__device__ __forceinline__ bool service_count(const FastTable &t, int slot, unsigned long long n, int lane_id) {
+    __syncwarp();
+    unsigned long long before = 0;
+    if (lane_id == 0) {
+        __threadfence();
+        before = atomicAdd(&t.slot_state[slot].rays_finished, n);
+    }
+    before = __shfl_sync(0xFFFFFFFFu, before, 0);
+    return before + n == static_cast<unsigned long long>(t.slots[slot].job.num_rays);
 }
 
 // Service launches: the job in `slot` has finished its last ray; every lane of the warp converts its
 // fixed-point sums to the float32 outputs, then lane 0 flags it done to the host.  The sums were added at L2
-// by atomics of all warps before they counted their rays finished (each lane fenced first); they are read
-// around L1 here.
+// by atomics of all warps before they counted their rays finished (service_count fences first); they are
+// read around L1 here.
 __device__ __forceinline__ void service_finish(const FastTable &t, int slot, int lane_id) {
     __threadfence();
     const ServiceSlot &sl = t.slots[slot];
@@ -723,6 +776,9 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     int queue = 0;                  // batched launches: the group queue this warp takes chunks from
     int64_t svc_queue = 0, svc_published = 0;   // service launches: next job to take chunks from, jobs seen
     int cur_slot = 0;                            // service launches: the job of the chunk being handed out
+    unsigned long long retry_at = 0;             // service launches, lane 0: next ask while lanes are live
+    int count_slot = -1;                         // service launches: the job whose finished rays the warp
+    unsigned long long count_n = 0;              //   is counting, and how many it has not added yet
     int64_t pending_begin = 0, pending_end = 0;
     if (kService) {
         long long pub = 0;
@@ -734,7 +790,22 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
         const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
         svc_published = pub;
-        svc_queue = pub > low ? low + (warp * (pub - low)) / warps : low;   // spread the warps over the jobs
+        svc_queue = low;
+        const int64_t last = min(static_cast<int64_t>(pub), table.window_end) - 1;
+        if (last > low) {
+            // start on the job that holds this warp's share of the published rays
+            const ServiceSlot &a = table.slots[low & table.mask];
+            const ServiceSlot &b = table.slots[last & table.mask];
+            const int64_t r0 = a.ray_offset;
+            const int64_t at = r0 + static_cast<int64_t>((static_cast<double>(warp) + 0.5) / static_cast<double>(warps) *
+                                                         static_cast<double>(b.ray_offset + b.job.num_rays - r0));
+            int64_t lo = low, hi = last;
+            while (lo < hi) {   // last job whose first ray is at or before `at`
+                const int64_t mid = (lo + hi + 1) >> 1;
+                if (table.slots[mid & table.mask].ray_offset <= at) lo = mid; else hi = mid - 1;
+            }
+            svc_queue = lo;
+        }
     } else if (!kSingle) {
         const int64_t warps = static_cast<int64_t>(gridDim.x) * (blockDim.x >> 5);
         const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -760,16 +831,22 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             if (next >= end) {
                 long long c = 0;
                 if (kService) {
+                    const bool live = __any_sync(full, has);
                     long long seq = -1, chunk = 0;
-                    if (lane_id == 0) {
+                    int got = kTakeNone;
+                    if (lane_id == 0 && (!live || global_ns() >= retry_at)) {   // live warps ask every few us
                         int64_t sq = 0, ck = 0;
-                        if (service_take(table, svc_queue, svc_published, &sq, &ck)) { seq = sq; chunk = ck; }
+                        got = service_take(table, !live, svc_queue, svc_published, &sq, &ck);
+                        if (got == kTakeChunk) { seq = sq; chunk = ck; }
+                        if (got == kTakeNone) retry_at = global_ns() + kServiceRetryNs;
                     }
+                    got = __shfl_sync(full, got, 0);
                     seq = __shfl_sync(full, seq, 0);
                     chunk = __shfl_sync(full, chunk, 0);
                     svc_queue = __shfl_sync(full, static_cast<long long>(svc_queue), 0);
                     svc_published = __shfl_sync(full, static_cast<long long>(svc_published), 0);
-                    if (seq < 0) { exhausted = true; break; }
+                    if (got == kTakeEnd) { exhausted = true; break; }
+                    if (got == kTakeNone) break;   // nothing now: trace the live lanes, ask again later
                     const int slot = static_cast<int>(seq & table.mask);
                     const ServiceSlot &sl = table.slots[slot];
                     const int64_t cb = chunk * sl.chunk_rays;
@@ -1119,9 +1196,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
 
         // ---- ray completion statistics, one atomic per distinct job in the warp
         const unsigned ending = __ballot_sync(full, finished);
-        bool last_ray = false;   // service launches: this lane's job has now finished every ray
         if (finished) {
-            if (kService) __threadfence();   // this ray's sums land before its job counts it finished
             const unsigned grp = __match_any_sync(ending, static_cast<unsigned>(s.job));
             const unsigned q_sum = __reduce_add_sync(grp, static_cast<unsigned>(s.queries));
             const unsigned q_max = __reduce_max_sync(grp, static_cast<unsigned>(s.queries));
@@ -1132,25 +1207,37 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 if (alive_sum) atomicAdd(job.counters + 1, static_cast<unsigned long long>(alive_sum));
                 atomicAdd(job.counters + 2, static_cast<unsigned long long>(q_sum));
                 if (sh_sum) atomicAdd(job.counters + 3, static_cast<unsigned long long>(sh_sum));
-                if (kService) {
-                    const unsigned long long n = static_cast<unsigned long long>(__popc(grp));
-                    const unsigned long long before = atomicAdd(&table.slot_state[s.job].rays_finished, n);
-                    last_ray = before + n == static_cast<unsigned long long>(job.num_rays);
-                }
             }
             if (job.ray_surfaces)
                 for (int b = s.bounce; b < job.num_bounces; ++b) job.ray_surfaces[s.ray * job.num_bounces + b] = -1;
             has = false;
         }
         if (kService) {
-            unsigned finishing = __ballot_sync(full, last_ray);
-            while (finishing) {
-                const int src = __ffs(finishing) - 1;
-                finishing &= finishing - 1u;
-                service_finish(table, __shfl_sync(full, s.job, src), lane_id);
+            // The warp counts its finished rays per job and adds them to the job's count once it holds no
+            // more of that job's rays (or a ray of another job finishes first): one fence per run of a job
+            // through the warp instead of one per iteration in which a ray ends.
+            unsigned rest = ending;
+            while (rest) {
+                const int j = __shfl_sync(full, s.job, __ffs(rest) - 1);
+                const unsigned grp = __ballot_sync(full, finished && s.job == j);
+                rest &= ~grp;
+                if (j != count_slot) {
+                    if (count_n && service_count(table, count_slot, count_n, lane_id))
+                        service_finish(table, count_slot, lane_id);
+                    count_slot = j;
+                    count_n = 0;
+                }
+                count_n += static_cast<unsigned long long>(__popc(grp));
+            }
+            if (count_n && !__any_sync(full, has && s.job == count_slot) && !(cur_slot == count_slot && next < end)) {
+                if (service_count(table, count_slot, count_n, lane_id)) service_finish(table, count_slot, lane_id);
+                count_slot = -1;
+                count_n = 0;
             }
         }
     }
+    if (kService && count_n && service_count(table, count_slot, count_n, lane_id))
+        service_finish(table, count_slot, lane_id);
 }
 
 }  // namespace ac
