@@ -86,7 +86,7 @@ class ACTraceParams(ctypes.Structure):
         ("directions", ctypes.c_void_p), ("diffuse_random", ctypes.c_void_p), ("diffuse_indices", ctypes.c_void_p),
         ("diffuse_bank", ctypes.c_void_p), ("num_bank", ctypes.c_int32), ("block_size", ctypes.c_int32),
         ("energy_scale", ctypes.c_double), ("grid_blocks", ctypes.c_int32), ("visual_limit", ctypes.c_int32),
-        ("visual_stride", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("visual_stride", ctypes.c_int32), ("stack_entries", ctypes.c_int32),
     ]
 
 
@@ -108,18 +108,24 @@ class ACJob(ctypes.Structure):
 
 class ACBatchConfig(ctypes.Structure):
     _fields_ = [("block_size", ctypes.c_int32), ("chunk_rays", ctypes.c_int32), ("grid_blocks", ctypes.c_int32),
-                ("reserved", ctypes.c_int32)]
+                ("stack_entries", ctypes.c_int32)]
 
 
 class ACServiceConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("capacity", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("block_size", ctypes.c_int32), ("chunk_rays", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("block_size", ctypes.c_int32), ("chunk_rays", ctypes.c_int32), ("stack_entries", ctypes.c_int32),
                 ("idle_timeout_ns", ctypes.c_int64)]
 
 
 class ACServiceStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("in_flight", ctypes.c_int64), ("launches", ctypes.c_int64),
                 ("running_launches", ctypes.c_int32), ("grid_blocks", ctypes.c_int32), ("capacity", ctypes.c_int64)]
+
+
+class ACServiceJobState(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_int64), ("chunks", ctypes.c_int64), ("chunks_taken", ctypes.c_int64),
+                ("rays", ctypes.c_int64), ("rays_finished", ctypes.c_int64), ("done_seq", ctypes.c_int64),
+                ("low_water", ctypes.c_int64), ("in_flight", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class ACSynthParams(ctypes.Structure):
@@ -267,10 +273,11 @@ SIGNATURES: dict[str, tuple[Any, list[Any]]] = {
                                            ctypes.c_void_p, ctypes.c_void_p]),
     "ac_service_create": (ctypes.c_int, [ctypes.POINTER(ACServiceConfig), ctypes.POINTER(ctypes.c_void_p)]),
     "ac_service_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACJob), ctypes.c_int32,
-                                         ctypes.POINTER(ctypes.c_int64)]),
+                                         ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p]),
     "ac_service_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32,
                                        ctypes.POINTER(ctypes.c_int32)]),
     "ac_service_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ACServiceStats)]),
+    "ac_service_inspect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ACServiceJobState)]),
     "ac_service_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "ac_reference_stream": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                            ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

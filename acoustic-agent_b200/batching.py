@@ -105,11 +105,13 @@ def workload_jobs(workloads: Sequence[Workload], *, precision: str = "float32", 
 class RIRRenderer:
     """Batched tracer + synthesis on one GPU."""
 
-    def __init__(self, device: int = 0, *, block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0) -> None:
+    def __init__(self, device: int = 0, *, block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0,
+                 stack_entries: int | None = None) -> None:
         self.device = runtime.require_cuda(device)
         self.block_size = block_size
         self.grid_blocks = grid_blocks
         self.chunk_rays = chunk_rays
+        self.stack_entries = stack_entries   # None: the largest of the plan's scenes' choices
         # eager plans share one pair of staged workspaces; a captured plan gets its own
         self._trace_ws = runtime.BatchWorkspace(self.device)
         self._synth_ws = runtime.SynthBatchWorkspace(self.device)
@@ -179,7 +181,7 @@ class RIRRenderer:
                 trace_events[0].record(s)
             runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
                                 plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
-                                chunk_rays=self.chunk_rays, stream=stream)
+                                chunk_rays=self.chunk_rays, stack_entries=self.stack_entries, stream=stream)
             if trace_events is not None:
                 trace_events[1].record(s)
         if synth:
@@ -245,7 +247,7 @@ class RIRRenderer:
         with torch.cuda.stream(main):
             runtime.trace_batch([(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)],
                                 plan.workspace, block_size=self.block_size, grid_blocks=self.grid_blocks,
-                                chunk_rays=self.chunk_rays, stream=main)
+                                chunk_rays=self.chunk_rays, stack_entries=self.stack_entries, stream=main)
         with torch.cuda.stream(side):
             # the recursion runs as one-warp blocks beside the persistent trace blocks
             runtime.synthesize_batch(synth, plan.synth_workspace, stream=side, phase="filter")

@@ -281,7 +281,7 @@ int build_traversal_bvh(const std::vector<int64_t> &surfaces, const double *lo, 
     if (root < 0) builder.write_root_pair(root, rb);   // everything fits one leaf
     else if (root != 0) return fail(AC_ERR_INVALID, "internal: BVH root is not node 0");
     if (out->depth > kBvhStack - 1) return fail(AC_ERR_CAPACITY, "float32 BVH depth %d exceeds the traversal stack", out->depth);
-    out->stack_need = out->depth;
+    out->stack_need = out->depth + 1;   // one push per inner level on a path, plus the sentinel entry
     if (width == 4) {
         std::vector<float> wide;
         int32_t need = 0;
@@ -289,7 +289,7 @@ int build_traversal_bvh(const std::vector<int64_t> &surfaces, const double *lo, 
         if (need <= kBvhStack - 1) {   // else keep the binary layout, whose need is bounded by its depth
             out->nodes.swap(wide);
             out->width = 4;
-            out->stack_need = need;
+            out->stack_need = need + 1;
         }
     }
     return AC_OK;

@@ -27,7 +27,9 @@ constexpr int kBvhMaxLeaf = 8;
 #ifndef AC_BVH_STACK
 #define AC_BVH_STACK 32
 #endif
-constexpr int kBvhStack = AC_BVH_STACK;   // traversal stack entries; the builder keeps the depth below this
+// Most traversal stack entries per lane; the builder keeps the depth below this.  A launch sizes each lane's
+// stack (shared memory) between the scenes' stack_need and this.
+constexpr int kBvhStack = AC_BVH_STACK;
 
 // Four-wide variant (`width` 4): the binary tree above collapsed so that every
 // inner node holds up to four children -- a node repeatedly replaces its inner
@@ -49,7 +51,7 @@ struct TraversalBvh {
     std::vector<int64_t> order;    // surface index per leaf slot
     int32_t depth = 0;             // inner-node levels of the binary tree on the longest root-to-leaf path
     int32_t width = 2;
-    int32_t stack_need = 0;        // traversal stack entries a ray can need at most
+    int32_t stack_need = 0;        // traversal stack entries a ray can need at most, the sentinel included
     int64_t num_nodes() const { return static_cast<int64_t>(nodes.size() / (width == 4 ? kBvh4Floats : 16)); }
 };
 

@@ -7,8 +7,10 @@
 //
 // Protocol (one service per device; calls on one service are serialised by its lock):
 //  * submit: the job descriptors are staged in pinned memory, copied into their slots and the slots' chunk
-//    and ray counters zeroed on the service's copy stream; once that copy has completed, the count of
-//    published jobs in a host-mapped control word is raised.  A launch is started if none is running.
+//    and ray counters and the jobs' outputs zeroed on the service's copy stream, behind the work the caller
+//    queued on its own stream before the call (which may still be writing those outputs); once that copy
+//    has completed, the count of published jobs in a host-mapped control word is raised.  A launch is
+//    started if none is running.
 //  * the launch's warps take chunks of rays job by job from the ring (per-job chunk counters); the warp that
 //    finishes a job's last ray converts its fixed-point sums into the float32 echogram and writes the job's
 //    sequence number into the job's host-mapped done flag.
@@ -49,6 +51,7 @@ struct ac_service_s {
     int32_t block = 256;
     int32_t grid = 0;
     int32_t chunk_rays = 64;
+    int32_t stack_entries = ac::kBvhStack;         // traversal stack entries per lane
     int64_t idle_ns = 20000000;
     ac::ServiceSlot *slots = nullptr;              // device ring
     ac::ServiceSlotState *state = nullptr;         // device
@@ -59,6 +62,7 @@ struct ac_service_s {
     ac::ServiceSlot *staging = nullptr;            // pinned, one ring's worth
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t copied = nullptr;
+    cudaEvent_t caller_ready = nullptr;            // recorded on the submitting caller's stream
     Launch launches[kMaxLaunches];
     int next_launch = 0;
     int64_t next_seq = 0;                          // sequence number of the next submitted job
@@ -78,6 +82,7 @@ int service_fail_cleanup(ac_service_s *s, int code) {
     if (s->staging) cudaFreeHost(s->staging);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->copied) cudaEventDestroy(s->copied);
+    if (s->caller_ready) cudaEventDestroy(s->caller_ready);
     for (Launch &l : s->launches) {
         if (l.stream) cudaStreamDestroy(l.stream);
         if (l.done) cudaEventDestroy(l.done);
@@ -132,7 +137,8 @@ int ensure_launch(ac_service_s *s) {
     ac::Job<float> unused;
     std::memset(&unused, 0, sizeof(unused));
     ac::FastScene none{};
-    ac::trace_fast_kernel<false, true, false, false, true><<<s->grid, s->block, 0, slot->stream>>>(unused, none, t);
+    ac::trace_fast_kernel<false, true, false, false, true>
+        <<<s->grid, s->block, ac::stack_smem_bytes(s->stack_entries), slot->stream>>>(unused, none, t);
     AC_CUDA_TRY(cudaGetLastError());
     AC_CUDA_TRY(cudaEventRecord(slot->done, slot->stream));
     slot->alive = true;
@@ -173,14 +179,17 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
         return ac::fail(AC_ERR_INVALID, "ac_service_create: capacity must be a power of two in 64..2^20");
     const int block = cfg->block_size > 0 ? cfg->block_size : 256;
     if (block % 32 != 0 || block > 256) return ac::fail(AC_ERR_INVALID, "block_size must be a multiple of 32 up to 256");
-    if (cfg->chunk_rays < 0 || cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 8 || cfg->idle_timeout_ns < 0)
-        return ac::fail(AC_ERR_INVALID, "ac_service_create: bad chunk_rays, blocks_per_sm or idle_timeout_ns");
+    if (cfg->chunk_rays < 0 || cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 8 || cfg->idle_timeout_ns < 0 ||
+        cfg->stack_entries < 0 || cfg->stack_entries > ac::kBvhStack)
+        return ac::fail(AC_ERR_INVALID,
+                        "ac_service_create: bad chunk_rays, blocks_per_sm, stack_entries or idle_timeout_ns");
     ac_service_s *s = new (std::nothrow) ac_service_s();
     if (!s) return ac::fail(AC_ERR_NOMEM, "out of host memory");
     s->device = cfg->device;
     s->capacity = capacity;
     s->block = block;
     s->chunk_rays = cfg->chunk_rays > 0 ? cfg->chunk_rays : 64;
+    s->stack_entries = cfg->stack_entries > 0 ? cfg->stack_entries : ac::kBvhStack;
     s->idle_ns = cfg->idle_timeout_ns > 0 ? cfg->idle_timeout_ns : 20000000;
     cudaError_t err = cudaSetDevice(s->device);
     if (err != cudaSuccess) {
@@ -205,7 +214,8 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     if (cudaHostGetDevicePointer(reinterpret_cast<void **>(&s->control_dev), s->control, 0) != cudaSuccess ||
         cudaMemset(s->words, 0, 48 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&s->copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->caller_ready, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         ac::fail(AC_ERR_CUDA, "ac_service_create: set-up failed");
         return service_fail_cleanup(s, AC_ERR_CUDA);
@@ -222,7 +232,8 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     return AC_OK;
 }
 
-extern "C" int ac_service_submit(ac_service_t s, const ac_job *jobs, int32_t num_jobs, int64_t *first_seq) {
+extern "C" int ac_service_submit(ac_service_t s, const ac_job *jobs, int32_t num_jobs, int64_t *first_seq,
+                                 void *stream) {
     ac::NvtxRange nvtx_range("ac_service_submit");
     if (!s || num_jobs < 0 || (num_jobs > 0 && !jobs) || !first_seq)
         return ac::fail(AC_ERR_INVALID, "ac_service_submit: bad argument");
@@ -236,6 +247,9 @@ extern "C" int ac_service_submit(ac_service_t s, const ac_job *jobs, int32_t num
             return ac::fail(AC_ERR_INVALID, "job %d: the service traces float32 Philox jobs without ambisonics, "
                             "visual candidates or recorded rays", j);
         if (in.params.num_bounces < 1) return ac::fail(AC_ERR_INVALID, "job %d: needs at least one bounce", j);
+        if (in.scene->fast.num_bvh_nodes > 0 && in.scene->bvh_stack_need > s->stack_entries)
+            return ac::fail(AC_ERR_INVALID, "job %d: its scene needs %d traversal stack entries, the service has %d",
+                            j, in.scene->bvh_stack_need, s->stack_entries);
     }
     std::lock_guard<std::mutex> guard(s->lock);
     *first_seq = s->next_seq;
@@ -270,7 +284,11 @@ extern "C" int ac_service_submit(ac_service_t s, const ac_job *jobs, int32_t num
         s->rays_submitted += in.params.num_rays;
         s->control->done[seq & (s->capacity - 1)] = -1;
     }
-    // copy the slots (one or two runs of the ring), zero the jobs' sums and counters
+    // copy the slots (one or two runs of the ring), zero the jobs' sums and counters -- after what the caller
+    // queued on its stream so far (e.g. its own initialisation of the outputs), which could otherwise land
+    // on top of the first rays' sums
+    AC_CUDA_TRY(cudaEventRecord(s->caller_ready, static_cast<cudaStream_t>(stream)));
+    AC_CUDA_TRY(cudaStreamWaitEvent(s->copy_stream, s->caller_ready, 0));
     const int64_t mask = s->capacity - 1;
     int64_t seq = s->next_seq;
     int32_t left = num_jobs;
@@ -334,6 +352,32 @@ extern "C" int ac_service_info(ac_service_t s, ac_service_stats *stats) {
     stats->running_launches = alive;
     stats->capacity = s->capacity;
     stats->grid_blocks = s->grid;
+    return AC_OK;
+}
+
+extern "C" int ac_service_inspect(ac_service_t s, int64_t seq, ac_service_job_state *out) {
+    if (!s || !out) return ac::fail(AC_ERR_INVALID, "ac_service_inspect: null argument");
+    std::lock_guard<std::mutex> guard(s->lock);
+    if (seq < 0 || seq >= s->next_seq || seq < s->next_seq - s->capacity)
+        return ac::fail(AC_ERR_INVALID, "ac_service_inspect: %lld is not one of the last %lld jobs submitted",
+                        (long long)seq, (long long)s->capacity);
+    AC_CUDA_TRY(cudaSetDevice(s->device));
+    const int64_t slot = seq & (s->capacity - 1);
+    ac::ServiceSlotState st{};
+    unsigned long long low = 0;
+    AC_CUDA_TRY(cudaMemcpyAsync(&st, s->state + slot, sizeof(st), cudaMemcpyDeviceToHost, s->copy_stream));
+    AC_CUDA_TRY(cudaMemcpyAsync(&low, s->words, sizeof(low), cudaMemcpyDeviceToHost, s->copy_stream));
+    AC_CUDA_TRY(cudaStreamSynchronize(s->copy_stream));
+    const ac::ServiceSlot &sl = s->staging[slot];   // the descriptor as submitted
+    std::memset(out, 0, sizeof(*out));
+    out->seq = seq;
+    out->chunks = sl.num_chunks;
+    out->chunks_taken = static_cast<int64_t>(st.chunks_taken);
+    out->rays = sl.job.num_rays;
+    out->rays_finished = static_cast<int64_t>(st.rays_finished);
+    out->done_seq = __atomic_load_n(&s->control->done[slot], __ATOMIC_ACQUIRE);
+    out->low_water = static_cast<int64_t>(low);
+    out->in_flight = std::find(s->inflight.begin(), s->inflight.end(), seq) != s->inflight.end() ? 1 : 0;
     return AC_OK;
 }
 

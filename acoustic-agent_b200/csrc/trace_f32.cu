@@ -28,9 +28,9 @@ FastKernel pick_kernel(bool philox, bool amb, bool visual) {
     return visual ? pick_variant<kSingle, true>(philox, amb) : pick_variant<kSingle, false>(philox, amb);
 }
 
-int fast_grid(FastKernel kernel, int device, int block, int64_t total_rays, int requested) {
+int fast_grid(FastKernel kernel, int device, int block, size_t smem, int64_t total_rays, int requested) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, 0) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem) != cudaSuccess || per_sm < 1)
         per_sm = 1;
     int grid = requested > 0 ? requested : per_sm * device_sm_count(device);
     const int64_t needed = (total_rays + block - 1) / block;
@@ -94,6 +94,10 @@ void count_groups_chunks(const ac_job *jobs, const std::vector<int32_t> &order, 
 int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac_trace_outputs *o, double scale,
                      void *stream_ptr) {
     cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
+    int entries = 0;
+    const int rc = launch_stack_entries(p->stack_entries, scene->fast.num_bvh_nodes > 0 ? scene->bvh_stack_need : 0,
+                                        &entries);
+    if (rc != AC_OK) return rc;
     Job<float> job;
     fill_job<float>(scene, p, o, scale, job);
     AC_CUDA_TRY(cudaSetDevice(scene->device));
@@ -118,8 +122,9 @@ int launch_trace_f32(const ac_scene_s *scene, const ac_trace_params *p, const ac
     table.chunk_counter = reinterpret_cast<unsigned long long *>(o->counters) + 4;
     const FastKernel kernel = pick_kernel<true>(p->rng_mode == AC_RNG_PHILOX, p->render_ambisonics != 0,
                                                 p->visual_limit > 0);
-    const int grid = fast_grid(kernel, scene->device, block, p->num_rays, p->grid_blocks);
-    kernel<<<grid, block, 0, stream>>>(job, scene->fast, table);
+    const size_t smem = stack_smem_bytes(entries);
+    const int grid = fast_grid(kernel, scene->device, block, smem, p->num_rays, p->grid_blocks);
+    kernel<<<grid, block, smem, stream>>>(job, scene->fast, table);
     AC_CUDA_TRY(cudaGetLastError());
     return launch_finalize_single<float>(scene, p, o, scale, stream_ptr);
 }
@@ -154,7 +159,7 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
     FastChunk *chunks = reinterpret_cast<FastChunk *>(host + l.chunks);
     int64_t *group_chunks = reinterpret_cast<int64_t *>(host + l.group_chunks);
     int64_t *group_rays = reinterpret_cast<int64_t *>(host + l.group_rays);
-    int device = -1;
+    int device = -1, need = 0;
     int64_t total = 0, g = -1, c = 0;
     const ac_scene_s *current = nullptr;
     int64_t group_begin = 0;
@@ -168,6 +173,7 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         const ac_job &in = jobs_in[order[k]];
         if (device < 0) device = in.scene->device;
         if (in.scene->device != device) return fail(AC_ERR_INVALID, "batch jobs must share one device");
+        if (in.scene->fast.num_bvh_nodes > 0) need = std::max(need, in.scene->bvh_stack_need);
         if (in.scene != current || groups[g].num_jobs >= kMaxGroupJobs) {
             if (g >= 0) close_group(total);
             ++g;
@@ -191,6 +197,9 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
                                      in.outputs.surface_energy};
     }
     if (g >= 0) close_group(total);
+    int entries = 0;
+    const int rc = launch_stack_entries(cfg ? cfg->stack_entries : 0, need, &entries);
+    if (rc != AC_OK) return rc;
     prefix[count] = total;
     group_chunks[num_groups] = c;
     group_rays[num_groups] = total;
@@ -228,8 +237,9 @@ int launch_batch_f32(const ac_job *jobs_in, const int32_t *indices, int32_t coun
         // ac_trace_batch partitions jobs so that one launch has one kernel variant.
         const FastKernel kernel = pick_kernel<false>(jobs[0].rng_mode == AC_RNG_PHILOX, jobs[0].render_ambisonics != 0,
                                                      jobs[0].visual_limit > 0);
-        const int grid = fast_grid(kernel, device, block, total, cfg ? cfg->grid_blocks : 0);
-        kernel<<<grid, block, 0, stream>>>(unused, none, table);
+        const size_t smem = stack_smem_bytes(entries);
+        const int grid = fast_grid(kernel, device, block, smem, total, cfg ? cfg->grid_blocks : 0);
+        kernel<<<grid, block, smem, stream>>>(unused, none, table);
         AC_CUDA_TRY(cudaGetLastError());
     }
     {

@@ -504,15 +504,19 @@ __device__ __forceinline__ bool child_box(const FRay &r, float lx, float hx, flo
 // one on a short stack in local memory -- until it holds a leaf, then keeps
 // descending while other lanes of the warp still look for theirs, so leaves
 // are tested by as many lanes at once as possible.  The builder bounds the
-// depth by kBvhStack - 1.  Same update rule as the scan, so closest-hit and
+// depth by kBvhStack - 1; the stack holds one sentinel plus one entry per
+// inner level.  Same update rule as the scan, so closest-hit and
 // any-hit modes work as there.
 constexpr int kBvhDone = static_cast<int>(0x80000000u);  // below every leaf reference
 
 // The per-lane traversal stack.  In shared memory (AC_SMEM_STACK, the
-// default): entry-major, [kBvhStack][256] words per block, so the lanes of a
-// warp hit 32 different banks whatever their stack depths, and stack traffic
-// stays out of L1, where the scene's nodes and surfaces live.  Otherwise in
-// local memory (a per-thread array).
+// default): entry-major, [entries][256] words per block in the launch's
+// dynamic shared memory, so the lanes of a warp hit 32 different banks
+// whatever their stack depths, and stack traffic stays out of L1, where the
+// scene's nodes and surfaces live.  The launch picks `entries` (a tuned
+// knob: fewer entries leave more of the SM's on-chip memory to L1) no lower
+// than the stack_need of any BVH scene it traces, which bounds every push.
+// Otherwise in local memory (a per-thread array of kBvhStack).
 #ifndef AC_SMEM_STACK
 #define AC_SMEM_STACK 1
 #endif
@@ -528,9 +532,28 @@ struct LaneStack {
 #endif
 };
 
+// Host: the traversal stack entries of a float32 launch, from the requested count (0: kBvhStack) and the
+// largest stack_need among the launch's BVH scenes (0: none has a BVH, the launch needs no stack).
+inline int launch_stack_entries(int requested, int need, int *entries) {
+    *entries = 0;
+    if (requested < 0 || requested > kBvhStack)
+        return fail(AC_ERR_INVALID, "stack_entries %d is outside 0..%d", requested, kBvhStack);
+    if (need <= 0) return AC_OK;
+    const int n = requested > 0 ? requested : kBvhStack;
+    if (n < need)
+        return fail(AC_ERR_INVALID, "stack_entries %d is below the %d a BVH scene of the launch needs", n, need);
+    *entries = n;
+    return AC_OK;
+}
+
+// Host: dynamic shared memory of a float32 launch with `entries` stack entries per lane.
+inline size_t stack_smem_bytes(int entries) {
+    return AC_SMEM_STACK ? static_cast<size_t>(entries) * kStackStride * sizeof(int) : 0;
+}
+
 __device__ __forceinline__ LaneStack lane_stack() {
 #if AC_SMEM_STACK
-    __shared__ int stack_words[kBvhStack * kStackStride];
+    extern __shared__ int stack_words[];
     return LaneStack{stack_words + threadIdx.x};
 #else
     return LaneStack{};

@@ -52,13 +52,16 @@ def _stream_ptr(stream: torch.cuda.Stream | None) -> ctypes.c_void_p:
     return ctypes.c_void_p(s.cuda_stream)
 
 
+MAX_STACK_ENTRIES = 32   # traversal stack entries per lane at most (the library's kBvhStack)
+
+
 class DeviceScene:
     """A scene uploaded with ac_scene_create; owns its device memory."""
 
     TRAVERSALS = {"auto": 0, "scan": 1, "bvh": 2, "hybrid": 3}
 
     def __init__(self, arrays: SceneArrays | Mapping[str, Any], device: int = 0, *, cluster_size: int = 0,
-                 traversal: str = "auto", bvh_leaf: int = 0, bvh_width: int = 0) -> None:
+                 traversal: str = "auto", bvh_leaf: int = 0, bvh_width: int = 0, stack_entries: int = 0) -> None:
         if traversal not in self.TRAVERSALS:
             raise ValueError(f"traversal must be one of {sorted(self.TRAVERSALS)}")
         require_cuda(device)
@@ -115,10 +118,16 @@ class DeviceScene:
         self.bvh_nodes = int(info.bvh_nodes)
         self.bvh_width = int(info.bvh_width)
         self.bvh_stack_need = int(info.bvh_stack_need)
+        # traversal stack entries per lane that launches over this scene use unless told otherwise (a tuned
+        # schedule knob; 0: the library's maximum)
+        self.stack_entries = int(stack_entries) if self.bvh_nodes > 0 else 0
         self.max_reflection = float(np.max(keep["reflection"])) if S else 0.0
         # events recorded after CUDA-graph replays that read this scene (the library tracks eager launches
         # itself, not work captured into a graph); close() waits for them
         self.graph_guards: list[torch.cuda.Event] = []
+        if self.stack_entries and not self.bvh_stack_need <= self.stack_entries <= MAX_STACK_ENTRIES:
+            self.close()
+            raise ValueError(f"stack_entries must lie in {self.bvh_stack_need}..{MAX_STACK_ENTRIES} for this scene")
 
     def close(self) -> None:
         if getattr(self, "handle", None) is not None and self.handle.value:
@@ -163,6 +172,7 @@ class TraceSpec:
     energy_scale: float = 0.0
     block_size: int = 0
     grid_blocks: int = 0
+    stack_entries: int = 0     # traversal stack entries per lane (0: the scene's choice, else the library's)
     visual_limit: int = 0      # visual-path candidate slots (0: none)
     visual_stride: int = 1
 
@@ -358,6 +368,7 @@ def params_struct(spec: TraceSpec, device: torch.device, keepalive: list[Any] | 
     p.energy_scale = float(spec.energy_scale)
     p.block_size = int(spec.block_size)
     p.grid_blocks = int(spec.grid_blocks)
+    p.stack_entries = int(spec.stack_entries)
     p.visual_limit = int(spec.visual_limit)
     p.visual_stride = int(spec.visual_stride)
     return p
@@ -375,6 +386,8 @@ def trace(scene: DeviceScene, spec: TraceSpec, buffers: TraceBuffers | None = No
                                         record_rays=(int(spec.num_rays), int(spec.num_bounces)) if record_rays else None)
     keep: list[Any] = []
     params = params_struct(spec, device, keep, workspace)
+    if not params.stack_entries:
+        params.stack_entries = scene.stack_entries
     outputs = buffers.outputs_struct()
     _lib.check(_lib.load().ac_trace(scene.handle, ctypes.byref(params), ctypes.byref(outputs), _stream_ptr(stream)),
                "ac_trace")
@@ -429,10 +442,17 @@ class BatchWorkspace(_StagedWorkspace):
     SIZE_FN = "ac_batch_workspace_size"
 
 
+def launch_stack_entries(scenes: Sequence[DeviceScene]) -> int:
+    """Stack entries of one launch over `scenes`: the largest of the BVH scenes' choices, or 0 (the library's
+    maximum) when one of them has none."""
+    prefs = [s.stack_entries for s in scenes if s.bvh_nodes > 0]
+    return max(prefs) if prefs and all(prefs) else 0
+
+
 def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
-                block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0,
+                block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0, stack_entries: int | None = None,
                 stream: torch.cuda.Stream | None = None) -> None:
-    """All jobs in one persistent launch (ac_trace_batch)."""
+    """All jobs in one persistent launch (ac_trace_batch); `stack_entries` None: launch_stack_entries."""
     if not jobs:
         return
     device = require_cuda(jobs[0][0].device)
@@ -442,7 +462,9 @@ def trace_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wor
         arr[k].scene = scene.handle.value
         arr[k].params = params_struct(spec, device, keep)
         arr[k].outputs = buffers.outputs_struct()
-    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), 0)
+    if stack_entries is None:
+        stack_entries = launch_stack_entries([scene for scene, _, _ in jobs])
+    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), int(stack_entries))
     ws, ws_bytes, host = workspace.ensure(arr, len(jobs), cfg)
     _lib.check(_lib.load().ac_trace_batch(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,
                                           ctypes.c_void_p(host), _stream_ptr(stream)), "ac_trace_batch")
@@ -460,18 +482,22 @@ class TraceService:
     """
 
     def __init__(self, device: int = 0, *, capacity: int = 4096, blocks_per_sm: int = 2, block_size: int = 0,
-                 chunk_rays: int = 0, idle_timeout_s: float = 0.02) -> None:
+                 chunk_rays: int = 0, stack_entries: int = 0, idle_timeout_s: float = 0.02) -> None:
         self.device = require_cuda(device)
         cfg = _lib.ACServiceConfig(int(device), int(capacity), int(blocks_per_sm), int(block_size), int(chunk_rays),
-                                   0, int(idle_timeout_s * 1e9))
+                                   int(stack_entries), int(idle_timeout_s * 1e9))
         handle = ctypes.c_void_p()
         _lib.check(_lib.load().ac_service_create(ctypes.byref(cfg), ctypes.byref(handle)), "ac_service_create")
         self.handle = handle
         self._keep: dict[int, Any] = {}
         self._done = (ctypes.c_int64 * 4096)()
 
-    def submit(self, jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]]) -> list[int]:
-        """Append jobs; raises BackendError(AC_ERR_CAPACITY) when the ring cannot take them yet."""
+    def submit(self, jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], *,
+               stream: torch.cuda.Stream | None = None) -> list[int]:
+        """Append jobs; raises BackendError(AC_ERR_CAPACITY) when the ring cannot take them yet.
+
+        The jobs are traced only after the work queued on `stream` (default: the current stream) before the
+        call, such as the zero fill of freshly allocated output buffers."""
         if not jobs:
             return []
         arr = (_lib.ACJob * len(jobs))()
@@ -484,8 +510,10 @@ class TraceService:
             arr[k].outputs = buffers.outputs_struct()
             keep.append((scene, buffers))
         first = ctypes.c_int64()
-        _lib.check(_lib.load().ac_service_submit(self.handle, arr, len(jobs), ctypes.byref(first)),
-                   "ac_service_submit")
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        _lib.check(_lib.load().ac_service_submit(self.handle, arr, len(jobs), ctypes.byref(first),
+                                                 _stream_ptr(stream)), "ac_service_submit")
         seqs = list(range(first.value, first.value + len(jobs)))
         for seq in seqs:
             self._keep[seq] = keep
@@ -503,6 +531,12 @@ class TraceService:
         for seq in out:
             self._keep.pop(seq, None)
         return out
+
+    def job_state(self, seq: int) -> dict[str, int]:
+        """Progress of one of the last `capacity` submitted jobs (ac_service_inspect)."""
+        st = _lib.ACServiceJobState()
+        _lib.check(_lib.load().ac_service_inspect(self.handle, int(seq), ctypes.byref(st)), "ac_service_inspect")
+        return {k: int(getattr(st, k)) for k, _ in st._fields_ if k != "reserved"}
 
     def info(self) -> dict[str, int]:
         st = _lib.ACServiceStats()
@@ -551,7 +585,7 @@ class BatchTicket:
 
 
 def submit_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], workspace: BatchWorkspace, *,
-                 block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0,
+                 block_size: int = 0, grid_blocks: int = 0, chunk_rays: int = 0, stack_entries: int | None = None,
                  stream: torch.cuda.Stream | None = None) -> BatchTicket:
     """trace_batch through the queue entry points: the launch plus a ticket to poll (ac_batch_submit)."""
     if not jobs:
@@ -563,7 +597,9 @@ def submit_batch(jobs: Sequence[tuple[DeviceScene, TraceSpec, TraceBuffers]], wo
         arr[k].scene = scene.handle.value
         arr[k].params = params_struct(spec, device, keep)
         arr[k].outputs = buffers.outputs_struct()
-    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), 0)
+    if stack_entries is None:
+        stack_entries = launch_stack_entries([scene for scene, _, _ in jobs])
+    cfg = _lib.ACBatchConfig(int(block_size), int(chunk_rays), int(grid_blocks), int(stack_entries))
     ws, ws_bytes, host = workspace.ensure(arr, len(jobs), cfg)
     handle = ctypes.c_void_p()
     _lib.check(_lib.load().ac_batch_submit(arr, len(jobs), ctypes.byref(cfg), ctypes.c_void_p(ws), ws_bytes,

@@ -931,6 +931,7 @@ def run_mixed_batch(args) -> int:
     plan = renderer.plan(arrays, jobs, scene_options=options)
     launch = autotune.tune_launch([(plan.scenes[j.scene_index], j.spec) for j in plan.jobs], device=local)
     renderer.block_size, renderer.chunk_rays = launch.block_size, launch.chunk_rays
+    renderer.stack_entries = launch.stack_entries
     t_tune = time.perf_counter() - t0
     if not args.no_graph:
         renderer.capture(plan, split=True)
@@ -947,7 +948,8 @@ def run_mixed_batch(args) -> int:
         job_list = [(plan.scenes[j.scene_index], j.spec, b) for j, b in zip(plan.jobs, plan.buffers)]
         ws, sws = runtime.BatchWorkspace(device), runtime.SynthBatchWorkspace(device)
         torch.cuda.profiler.start()
-        runtime.trace_batch(job_list, ws, block_size=launch.block_size, chunk_rays=launch.chunk_rays)
+        runtime.trace_batch(job_list, ws, block_size=launch.block_size, chunk_rays=launch.chunk_rays,
+                            stack_entries=launch.stack_entries)
         runtime.synthesize_batch((plan.synth_jobs, len(plan.jobs), plan.synth_config), sws)
         torch.cuda.synchronize(device)
         torch.cuda.profiler.stop()
@@ -1002,7 +1004,8 @@ def run_mixed_batch(args) -> int:
     # end to end through the public API, host buffers: every step uploads the 256 scenes from host arrays,
     # lays out the jobs, traces + synthesises them (one launch each) and copies the band IRs to pinned host memory
     host_out = torch.empty(plan.ir_store.shape, dtype=plan.ir_store.dtype, pin_memory=True)
-    e2e_renderer = batching.RIRRenderer(local, block_size=launch.block_size, chunk_rays=launch.chunk_rays)
+    e2e_renderer = batching.RIRRenderer(local, block_size=launch.block_size, chunk_rays=launch.chunk_rays,
+                                        stack_entries=launch.stack_entries)
 
     def e2e_step():
         scenes_k = [runtime.DeviceScene(a, device=local, **o) for a, o in zip(arrays, options)]
@@ -1036,7 +1039,11 @@ def run_mixed_batch(args) -> int:
                    "graph": not args.no_graph, "rng": "philox", "parallelism": f"replicas x{world}",
                    "l2": "flushed between timed steps (256 MiB write)",
                    "traversal": {m: sum(1 for s in plan.scenes if s.traversal == m) for m in ("scan", "bvh", "hybrid")},
-                   "launch": {"block_size": launch.block_size, "chunk_rays": launch.chunk_rays}},
+                   "launch": {"block_size": launch.block_size, "chunk_rays": launch.chunk_rays,
+                              "stack_entries": launch.stack_entries,
+                              "stack_ms": {str(n): round(t, 3) for n, t in launch.stack_ms}},
+                   "stack_entries_by_scene": {str(n): sum(1 for o in options if o["stack_entries"] == n)
+                                              for n in sorted({o["stack_entries"] for o in options})}},
         "ray_bounces_per_step": rb, "ray_bounces_per_s": world * rb / (ms / 1000.0),
         "trace_launch_ms": trace_ms, "synthesis_ms": ms - trace_ms,
         "plain": {"rirs_per_s": plain_rirs_per_s, "jobs_timed": len(order), "seconds": plain_s,

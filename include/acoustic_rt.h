@@ -125,7 +125,8 @@ typedef struct ac_scene_info {
     int32_t bvh_depth;           /* float32 BVH: inner-node levels (0 in scan mode) */
     int64_t bvh_nodes;           /* float32 BVH: inner nodes (0 in scan mode) */
     int32_t bvh_width;           /* float32 BVH: children per inner node (0 in scan mode) */
-    int32_t bvh_stack_need;      /* float32 BVH: traversal stack entries a ray can need */
+    int32_t bvh_stack_need;      /* float32 BVH: traversal stack entries a ray can need, the sentinel
+                                    included (the least `stack_entries` a launch over it may use) */
 } ac_scene_info;
 
 /* One trace: rays from the listener, next-event estimation to the source.
@@ -170,7 +171,11 @@ typedef struct ac_trace_params {
      * visual_limit = 0: none. */
     int32_t visual_limit;
     int32_t visual_stride;
-    int32_t reserved;
+    /* Float32 BVH scenes: entries of each lane's traversal stack (shared
+     * memory, 1 KiB per entry per 256-thread block).  0: the library maximum
+     * (32); otherwise bvh_stack_need of the scene .. 32, else AC_ERR_INVALID.
+     * A schedule knob: results do not depend on it. */
+    int32_t stack_entries;
 } ac_trace_params;
 
 /* Outputs.  All pointers are DEVICE memory owned by the caller.  Energies
@@ -218,7 +223,8 @@ typedef struct ac_batch_config {
     int32_t block_size;          /* threads per block; 0: library default */
     int32_t chunk_rays;          /* rays per work item a warp takes from the queue; 0: default */
     int32_t grid_blocks;         /* persistent blocks; 0: SM count * occupancy */
-    int32_t reserved;
+    int32_t stack_entries;       /* traversal stack entries per lane (0: 32); at least every BVH scene's
+                                    bvh_stack_need, else AC_ERR_INVALID */
 } ac_batch_config;
 
 /* Band synthesis of J echograms (steam_rt.py:2205-2232, 3070-3083): per
@@ -337,7 +343,10 @@ int ac_batch_release(ac_batch_ticket_t ticket);
  * one bounce) and returns their sequence numbers first_seq ..
  * first_seq + num_jobs - 1; it returns once their descriptors are in device
  * memory, and starts a launch if none is running.  It zeroes the jobs'
- * outputs itself.  When the ring cannot take the jobs yet it fails with
+ * outputs itself, after the work queued on `stream` before the call (the
+ * caller's own initialisation of those buffers, say): the jobs are traced
+ * only once that work is done.  `stream` NULL: the legacy default stream.
+ * When the ring cannot take the jobs yet it fails with
  * AC_ERR_CAPACITY: poll and submit again.  ac_service_poll writes the
  * sequence numbers of jobs whose outputs (fixed-point sums, counters, float32
  * echogram and surface energy) are complete since the last poll; it never
@@ -358,7 +367,8 @@ typedef struct {
     int32_t blocks_per_sm;       /* persistent grid (0: 2, which leaves room for synthesis blocks beside it) */
     int32_t block_size;          /* 0: 256 */
     int32_t chunk_rays;          /* rays a warp takes at a time (0: 64) */
-    int32_t reserved;
+    int32_t stack_entries;       /* traversal stack entries per lane (0: 32); a job whose scene needs more
+                                    (bvh_stack_need) is refused at submit */
     int64_t idle_timeout_ns;     /* 0: 20 ms */
 } ac_service_config;
 typedef struct {
@@ -369,10 +379,26 @@ typedef struct {
     int32_t grid_blocks;
     int64_t capacity;
 } ac_service_stats;
+/* Progress of one submitted job, for monitoring (a job that stops moving is
+ * visible here): the counters are read from the device while launches run. */
+typedef struct {
+    int64_t seq;
+    int64_t chunks;              /* chunks of rays the job was split into */
+    int64_t chunks_taken;        /* taken by warps so far (may exceed `chunks`: late takers find none) */
+    int64_t rays;
+    int64_t rays_finished;       /* rays whose sums are complete */
+    int64_t done_seq;            /* the slot's done flag: == seq once the job's outputs are final */
+    int64_t low_water;           /* jobs below it have no chunks left */
+    int32_t in_flight;           /* 1: submitted and not yet reported done by ac_service_poll */
+    int32_t reserved;
+} ac_service_job_state;
 int ac_service_create(const ac_service_config *config, ac_service_t *out);
-int ac_service_submit(ac_service_t service, const ac_job *jobs, int32_t num_jobs, int64_t *first_seq);
+int ac_service_submit(ac_service_t service, const ac_job *jobs, int32_t num_jobs, int64_t *first_seq,
+                      void *stream);
 int ac_service_poll(ac_service_t service, int64_t *done_seqs, int32_t max_done, int32_t *num_done);
 int ac_service_info(ac_service_t service, ac_service_stats *stats);
+/* AC_ERR_INVALID unless `seq` is one of the last `capacity` jobs submitted. */
+int ac_service_inspect(ac_service_t service, int64_t seq, ac_service_job_state *state);
 int ac_service_destroy(ac_service_t service);
 
 /* Device workspace needed by ac_synthesize. */

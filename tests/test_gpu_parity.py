@@ -375,7 +375,7 @@ def test_fp32_bvh_traversal_equals_scan(rt, name):
         assert scene.traversal == (mode if mode != "hybrid" or has_boxes else "scan")
         if scene.traversal != "scan":
             assert 1 <= scene.bvh_depth <= 31 and scene.bvh_nodes >= 1
-            assert scene.bvh_width == width and 1 <= scene.bvh_stack_need <= 31
+            assert scene.bvh_width == width and 2 <= scene.bvh_stack_need <= 32
         buffers = rt.trace(scene, spec, record_rays=True)
         torch.cuda.synchronize()
         got[(mode, width)] = {"rays": buffers.ray_surfaces.cpu().numpy(),

@@ -47,11 +47,13 @@ def _alone(rt, scene, spec):
     return b
 
 
-def _wait_all(svc, seqs, limit_s=60.0):
-    done, t0 = set(), time.time()
+def _wait_all(svc, seqs, limit_s=60.0, done=None):
+    done, t0 = set() if done is None else done, time.time()
     while not set(seqs) <= done:
         done.update(svc.poll())
-        assert time.time() - t0 < limit_s, "service jobs did not finish"
+        if time.time() - t0 >= limit_s:
+            stuck = sorted(set(seqs) - done)[:4]
+            raise AssertionError(f"service jobs did not finish: {[svc.job_state(q) for q in stuck]}")
         time.sleep(0.001)
     return done
 
@@ -118,6 +120,57 @@ def test_a_full_ring_asks_the_caller_to_poll(rt):
         more = svc.submit(batch[:4])   # room again once the jobs are reported done
         _wait_all(svc, more)
         assert svc.info()["in_flight"] == 0
+    finally:
+        svc.close()
+        for sc in scenes:
+            sc.close()
+
+
+def test_the_ring_wraps_across_many_launches_and_every_job_equals_it_alone(rt):
+    """A 64-slot ring (32-job windows) wrapped several times by trickled submissions, so that launches
+    start and end while jobs wait and slots are rewritten; every job's sums equal the job traced alone and
+    its progress record ends complete."""
+    from acoustic_agent_b200 import _lib
+    scenes, jobs = _jobs(rt, rays=(1_500, 300, 4_000))
+    svc = rt.TraceService(0, capacity=64, idle_timeout_s=0.002)
+    dev = torch.device("cuda")
+    try:
+        submitted, done, keys = [], set(), {}
+        k = 0
+        for round_ in range(24):
+            batch = []
+            for _ in range(7 + round_ % 5):
+                sc, sp = jobs[k % len(jobs)]
+                sp = replace(sp, stream_key=5000 + k)
+                batch.append((sc, sp, rt.TraceBuffers.allocate(sc.num_surfaces, sp.num_bins, dev)))
+                k += 1
+            while True:
+                try:
+                    seqs = svc.submit(batch)
+                    break
+                except _lib.BackendError as exc:   # the ring is full: poll, then retry
+                    if exc.code != _lib.AC_ERR_CAPACITY:
+                        raise
+                    done.update(svc.poll())
+                    time.sleep(0.001)
+            for q, item in zip(seqs, batch):
+                keys[q] = item
+            submitted += seqs
+            done.update(svc.poll())
+            time.sleep(0.001 * (round_ % 4))
+        _wait_all(svc, submitted, done=done)
+        assert svc.info()["launches"] >= 4 and submitted[-1] >= 3 * 64
+        for q in submitted[-64:]:
+            st = svc.job_state(q)
+            assert st["done_seq"] == q and st["rays_finished"] == st["rays"] and st["in_flight"] == 0
+            assert st["chunks_taken"] >= st["chunks"]
+        torch.cuda.synchronize()
+        for q in submitted[::5]:
+            sc, sp, b = keys[q]
+            want = _alone(rt, sc, sp)
+            np.testing.assert_array_equal(b.echogram_fx.cpu().numpy(), want.echogram_fx.cpu().numpy())
+            np.testing.assert_array_equal(b.counters[:4].cpu().numpy(), want.counters[:4].cpu().numpy())
+            np.testing.assert_array_equal(b.echogram.cpu().numpy(), want.echogram.cpu().numpy())
     finally:
         svc.close()
         for sc in scenes:

@@ -69,6 +69,51 @@ def test_library_exports_every_declared_symbol():
     assert _lib.load().ac_abi_version() == 2
 
 
+# ctypes mirror -> C type name in the public header
+MIRRORS = {"ACBvh": "ac_bvh", "ACSceneDesc": "ac_scene_desc", "ACSceneInfo": "ac_scene_info",
+           "ACTraceParams": "ac_trace_params", "ACTraceOutputs": "ac_trace_outputs", "ACJob": "ac_job",
+           "ACBatchConfig": "ac_batch_config", "ACServiceConfig": "ac_service_config",
+           "ACServiceStats": "ac_service_stats", "ACServiceJobState": "ac_service_job_state", "ACSynthParams": "ac_synth_params", "ACSynthJob": "ac_synth_job",
+           "ACSynthBatchConfig": "ac_synth_batch_config", "ACFdnJob": "ac_fdn_job",
+           "ACLateTailJob": "ac_late_tail_job", "ACDirectQuery": "ac_direct_query",
+           "ACDirectResult": "ac_direct_result", "ACDirectTables": "ac_direct_tables"}
+
+
+def test_ctypes_mirrors_match_the_header_layout(tmp_path):
+    """Every field of every ctypes mirror sits at the header's offset, and the sizes agree (gcc, C11)."""
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc not found")
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "acoustic_rt.h"', "int main(void) {"]
+    expected = []
+    for mirror, ctype in MIRRORS.items():
+        cls = getattr(_lib, mirror)
+        lines.append(f'    printf("{ctype} sizeof %zu\\n", sizeof({ctype}));')
+        expected.append(f"{ctype} sizeof {ctypes.sizeof(cls)}")
+        for name, *_ in cls._fields_:
+            lines.append(f'    printf("{ctype} {name} %zu\\n", offsetof({ctype}, {name}));')
+            expected.append(f"{ctype} {name} {getattr(cls, name).offset}")
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(REPO / "include"), str(src), "-o", str(exe)], check=True,
+                   capture_output=True)
+    got = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    assert [g for g in got if g] == expected
+
+
+def test_stack_depth_candidates_start_at_the_need():
+    from acoustic_agent_b200 import autotune
+    assert autotune.stack_candidates(0) == [0]
+    assert autotune.stack_candidates(7) == [7, 8, 12, 16, 24, 32]
+    assert autotune.stack_candidates(16) == [16, 24, 32]
+    assert autotune.stack_candidates(32) == [32]
+    choice = autotune.SceneChoice("bvh", 1, 1.0, 2, 12, ((12, 1.0), (16, 1.1)))
+    assert choice.options()["stack_entries"] == 12
+
+
 def test_scene_create_rejects_bad_descriptions_without_touching_the_gpu():
     lib = _lib.load()
     handle = ctypes.c_void_p()
