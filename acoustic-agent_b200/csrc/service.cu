@@ -15,10 +15,10 @@
 //    finishes a job's last ray converts its fixed-point sums into the float32 echogram and writes the job's
 //    sequence number into the job's host-mapped done flag.
 //  * poll: the host reads the done flags of the jobs in flight.
-//  * every wait in the launch is bounded: a warp that finds no work for `idle_timeout_ns` leaves, and the
-//    launch ends when all have; the next submit or poll starts another.  A launch takes jobs below a window
-//    of half the ring beyond its first job and then ends, so a slot is rewritten only after every launch
-//    that could hold its old contents in L1 has ended.
+//  * every wait in the launch is bounded: once every warp of the launch has had nothing to trace for
+//    `idle_timeout_ns` the warps leave together and the launch ends; the next submit or poll starts
+//    another.  A launch takes jobs below a window of half the ring beyond its first job and then ends, so
+//    a slot is rewritten only after every launch that could hold its old contents in L1 has ended.
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -34,10 +34,12 @@
 namespace {
 
 constexpr int kMaxLaunches = 2;
+constexpr int kLaunchWords = 48;   // three counters, one 128-byte line each
 
 struct Launch {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    unsigned long long *words = nullptr;   // device: the launch's warp counts (FastTable::launch_words)
     bool alive = false;
     int64_t first = 0;          // lowest sequence number it may take
     int64_t window_end = 0;     // it takes jobs below this only
@@ -86,6 +88,7 @@ int service_fail_cleanup(ac_service_s *s, int code) {
     for (Launch &l : s->launches) {
         if (l.stream) cudaStreamDestroy(l.stream);
         if (l.done) cudaEventDestroy(l.done);
+        if (l.words) cudaFree(l.words);
     }
     delete s;
     return code;
@@ -134,6 +137,8 @@ int ensure_launch(ac_service_s *s) {
     t.window_end = slot->window_end;
     t.idle_ns = s->idle_ns;
     t.mask = s->capacity - 1;
+    t.launch_words = slot->words;
+    AC_CUDA_TRY(cudaMemsetAsync(slot->words, 0, kLaunchWords * sizeof(unsigned long long), slot->stream));
     ac::Job<float> unused;
     std::memset(&unused, 0, sizeof(unused));
     ac::FastScene none{};
@@ -222,7 +227,8 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     }
     for (Launch &l : s->launches) {
         if (cudaStreamCreateWithFlags(&l.stream, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&l.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMalloc(&l.words, kLaunchWords * sizeof(unsigned long long)) != cudaSuccess) {
             cudaGetLastError();
             ac::fail(AC_ERR_CUDA, "ac_service_create: stream set-up failed");
             return service_fail_cleanup(s, AC_ERR_CUDA);

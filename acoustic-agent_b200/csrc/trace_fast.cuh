@@ -137,6 +137,8 @@ struct FastTable {
     unsigned long long *low_water;       // device: jobs below it have no chunks left
     unsigned long long *published_copy;  // device: the published count as last read from the host
     unsigned long long *refresh_at;      // device: %globaltimer time at which the copy is read again
+    unsigned long long *launch_words;    // device, this launch's own: [0] warps alive, [16] warps waiting for
+                                         // work, [32] %globaltimer time at which a warp last began to wait
     int64_t window_first;                // this launch takes jobs from this sequence number
     int64_t window_end;                  // to below this one only
     int64_t idle_ns;                     // and ends once its warps found no work for this long
@@ -177,14 +179,22 @@ constexpr unsigned long long kServiceRetryNs = 4000;   // a warp with live lanes
 //  * kTakeNone (only when `may_wait` is false, i.e. some lanes of the warp still trace rays): nothing to
 //    take right now; the warp carries on with its live lanes and asks again later.  A warp never sleeps
 //    while it holds rays.
-//  * kTakeEnd: the launch should end for this warp -- it found no published job with chunks left for
-//    `idle_ns` while it had nothing to trace, or the launch's window of sequence numbers is used up.
+//  * kTakeEnd: the launch should end for this warp -- the whole launch has had nothing to trace for
+//    `idle_ns` (every warp alive is waiting, the latest for longer than that), or the launch's window of
+//    sequence numbers is used up.  Warps leave together, so a launch never shrinks to a few warps that
+//    happened to hold rays through a lull while the host, seeing it alive, starts no other.
 // Every wait is bounded: the idle deadline, and a poll cap.
 __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, int64_t &queue, int64_t &published,
                                             int64_t *seq_out, int64_t *chunk_out) {
+    unsigned long long *const alive = t.launch_words, *const waiting = t.launch_words + 16,
+                              *const last_wait = t.launch_words + 32;
     unsigned long long idle_from = 0;
     unsigned sleep_ns = 256;
-    bool rescanned = false;
+    bool rescanned = false, counted = false;   // counted: this warp is in the launch's waiting count
+    auto leave = [&](int result) {
+        if (counted) atomicAdd(waiting, ~0ull);   // -1
+        return result;
+    };
 #pragma unroll 1
     for (int polls = 0; polls < (1 << 22); ++polls) {
         if (queue < published && queue < t.window_end) {
@@ -196,7 +206,7 @@ __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, i
                 if (k < chunks) {
                     *seq_out = queue;
                     *chunk_out = k;
-                    return kTakeChunk;
+                    return leave(kTakeChunk);
                 }
             }
             // no chunks left here: raise the low-water mark past it if it points here, then move on
@@ -216,7 +226,7 @@ __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, i
                 continue;
             }
         }
-        if (queue >= t.window_end) return kTakeEnd;
+        if (queue >= t.window_end) return leave(kTakeEnd);
         const long long pub = service_published(t);
         if (pub > published) {
             published = pub;
@@ -224,14 +234,25 @@ __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, i
             continue;
         }
         if (!may_wait) return kTakeNone;
-        // nothing to trace: wait for the host to publish more, within the idle limit
+        // nothing to trace: wait for the host to publish more, until the whole launch has been idle for the
+        // idle limit
         const unsigned long long now = global_ns();
+        if (!counted) {
+            counted = true;
+            atomicAdd(waiting, 1ull);
+            atomicMax(last_wait, now);
+        }
         if (idle_from == 0) idle_from = now;
-        if (now - idle_from > static_cast<unsigned long long>(t.idle_ns)) return kTakeEnd;
+        const unsigned long long limit = static_cast<unsigned long long>(t.idle_ns);
+        if (now - idle_from > limit &&
+            *reinterpret_cast<volatile unsigned long long *>(waiting) >=
+                *reinterpret_cast<volatile unsigned long long *>(alive) &&
+            now - *reinterpret_cast<volatile unsigned long long *>(last_wait) > limit)
+            return leave(kTakeEnd);
         __nanosleep(sleep_ns);
         if (sleep_ns < 32768) sleep_ns <<= 1;
     }
-    return kTakeEnd;
+    return leave(kTakeEnd);
 }
 
 // Service launches, whole warp: `n` more rays of the job in `slot` have finished in this warp.  Every lane's
@@ -814,6 +835,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         const int64_t warp = static_cast<int64_t>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5);
         svc_published = pub;
         svc_queue = low;
+        if (lane_id == 0) atomicAdd(table.launch_words, 1ull);   // this warp is alive in the launch
         const int64_t last = min(static_cast<int64_t>(pub), table.window_end) - 1;
         if (last > low) {
             // start on the job that holds this warp's share of the published rays
@@ -868,7 +890,11 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     chunk = __shfl_sync(full, chunk, 0);
                     svc_queue = __shfl_sync(full, static_cast<long long>(svc_queue), 0);
                     svc_published = __shfl_sync(full, static_cast<long long>(svc_published), 0);
-                    if (got == kTakeEnd) { exhausted = true; break; }
+                    if (got == kTakeEnd) {
+                        if (lane_id == 0) atomicAdd(table.launch_words, ~0ull);   // takes no more work
+                        exhausted = true;
+                        break;
+                    }
                     if (got == kTakeNone) break;   // nothing now: trace the live lanes, ask again later
                     const int slot = static_cast<int>(seq & table.mask);
                     const ServiceSlot &sl = table.slots[slot];

@@ -203,10 +203,10 @@ class _StreamCache:
         size = sum(t.numel() * t.element_size() for t in value)
         with self.lock:
             self.misses += 1
-            while self.entries and self.bytes + size > self.limit:
-                _, old = self.entries.popitem(last=False)
-                self.bytes -= sum(t.numel() * t.element_size() for t in old)
-            if size <= self.limit:
+            if size <= self.limit:   # an entry that can never fit is returned uncached, evicting nothing
+                while self.entries and self.bytes + size > self.limit:
+                    _, old = self.entries.popitem(last=False)
+                    self.bytes -= sum(t.numel() * t.element_size() for t in old)
                 self.entries[key] = value
                 self.bytes += size
         return value

@@ -838,12 +838,16 @@ def single_rir_latency(workload, repeats: int = 5) -> dict:
     lst = np.asarray(workload.listeners[0], dtype=float)
     device = torch.device("cuda", 0)
     ws = runtime.SynthWorkspace(device)
-    trace_ms, synth_ms = [], []
+    trace_ms, synth_ms, kernel_ms, upload_ms, hits = [], [], [], [], []
     for k in range(repeats + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         field = backend.trace_energy_field(arrays, src, lst, cfg, workload.source_model, render_ambisonics=False)
         t1 = time.perf_counter()
+        if k:
+            kernel_ms.append(1e3 * field["kernel_time_s"])
+            upload_ms.append(1e3 * field["transfer_time_s"])
+            hits.append(field["device_input_cache"])
         echo = torch.as_tensor(field["echogram"][None], device=device)
         d = torch.tensor([field["direct_delay_s"]], dtype=torch.float64, device=device)
         params = runtime.synth_params(1, int(field["num_bins"]), cfg.rt_bin_duration_s, cfg.fs, cfg.c,
@@ -855,6 +859,8 @@ def single_rir_latency(workload, repeats: int = 5) -> dict:
             synth_ms.append(1e3 * (t2 - t1))
     tr, sy = float(np.median(trace_ms)), float(np.median(synth_ms))
     return {"trace_ms": tr, "synthesis_ms": sy, "total_ms": tr + sy, "synthesis_share": sy / (tr + sy),
+            "trace_kernel_ms": float(np.median(kernel_ms)), "transfer_ms": float(np.median(upload_ms)),
+            "device_input_cache": hits[-1],
             "note": "one channel: drop-in trace_energy_field (reference stream, on the device) + GPU band "
                     "synthesis, host arrays in and out, median of 5 after 1 warm-up"}
 
