@@ -114,7 +114,7 @@ class ACBatchConfig(ctypes.Structure):
 class ACServiceConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("capacity", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
                 ("block_size", ctypes.c_int32), ("chunk_rays", ctypes.c_int32), ("stack_entries", ctypes.c_int32),
-                ("idle_timeout_ns", ctypes.c_int64)]
+                ("idle_timeout_ns", ctypes.c_int64), ("reserve_blocks", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class ACServiceStats(ctypes.Structure):

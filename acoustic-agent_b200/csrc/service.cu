@@ -185,9 +185,11 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
     const int block = cfg->block_size > 0 ? cfg->block_size : 256;
     if (block % 32 != 0 || block > 256) return ac::fail(AC_ERR_INVALID, "block_size must be a multiple of 32 up to 256");
     if (cfg->chunk_rays < 0 || cfg->blocks_per_sm < 0 || cfg->blocks_per_sm > 8 || cfg->idle_timeout_ns < 0 ||
+        cfg->reserve_blocks < 0 ||
         cfg->stack_entries < 0 || cfg->stack_entries > ac::kBvhStack)
         return ac::fail(AC_ERR_INVALID,
-                        "ac_service_create: bad chunk_rays, blocks_per_sm, stack_entries or idle_timeout_ns");
+                        "ac_service_create: bad chunk_rays, blocks_per_sm, stack_entries, reserve_blocks or "
+                        "idle_timeout_ns");
     ac_service_s *s = new (std::nothrow) ac_service_s();
     if (!s) return ac::fail(AC_ERR_NOMEM, "out of host memory");
     s->device = cfg->device;
@@ -202,7 +204,11 @@ extern "C" int ac_service_create(const ac_service_config *cfg, ac_service_t *out
         return service_fail_cleanup(s, AC_ERR_CUDA);
     }
     const int per_sm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 2;
-    s->grid = per_sm * ac::device_sm_count(s->device);
+    s->grid = per_sm * ac::device_sm_count(s->device) - cfg->reserve_blocks;
+    if (s->grid < 1) {
+        ac::fail(AC_ERR_INVALID, "ac_service_create: reserve_blocks leaves no blocks");
+        return service_fail_cleanup(s, AC_ERR_INVALID);
+    }
     const size_t control_bytes = sizeof(ac::ServiceControl) + sizeof(long long) * static_cast<size_t>(capacity);
     if (cudaMalloc(&s->slots, sizeof(ac::ServiceSlot) * capacity) != cudaSuccess ||
         cudaMalloc(&s->state, sizeof(ac::ServiceSlotState) * capacity) != cudaSuccess ||

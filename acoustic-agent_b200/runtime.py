@@ -482,10 +482,11 @@ class TraceService:
     """
 
     def __init__(self, device: int = 0, *, capacity: int = 4096, blocks_per_sm: int = 2, block_size: int = 0,
-                 chunk_rays: int = 0, stack_entries: int = 0, idle_timeout_s: float = 0.02) -> None:
+                 chunk_rays: int = 0, stack_entries: int = 0, idle_timeout_s: float = 0.02,
+                 reserve_blocks: int = 0) -> None:
         self.device = require_cuda(device)
         cfg = _lib.ACServiceConfig(int(device), int(capacity), int(blocks_per_sm), int(block_size), int(chunk_rays),
-                                   int(stack_entries), int(idle_timeout_s * 1e9))
+                                   int(stack_entries), int(idle_timeout_s * 1e9), int(reserve_blocks), 0)
         handle = ctypes.c_void_p()
         _lib.check(_lib.load().ac_service_create(ctypes.byref(cfg), ctypes.byref(handle)), "ac_service_create")
         self.handle = handle

@@ -414,8 +414,12 @@ def main() -> int:
                         help="serving: kernel-level continuous batching or batch-level server")
     parser.add_argument("--slo", type=float, default=2.0,
                         help="serving (continuous): shed requests whose admitted work ahead exceeds this, seconds")
-    parser.add_argument("--capacity-rb", type=float, default=2.2e9,
+    parser.add_argument("--capacity-rb", type=float, default=2.6e9,
                         help="serving (continuous): ray-bounces/s assumed until measured while saturated")
+    parser.add_argument("--service-blocks-per-sm", type=int, default=3,
+                        help="serving (continuous): persistent trace blocks per SM")
+    parser.add_argument("--service-reserve-blocks", type=int, default=16,
+                        help="serving (continuous): blocks left out of the persistent grid, for the synthesis")
     parser.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     parser.add_argument("--policy", default="small_first", choices=("small_first", "fifo"),
                         help="serving: order in which waiting requests join a batch")
@@ -1180,7 +1184,9 @@ def run_serving(args) -> int:
     population = workloads.mixed_batch(1730, 64)
     rates = [float(r) for r in str(args.rates).split(",")] if args.rates else [args.rate]
     if args.server == "continuous":
-        server = serving.ContinuousServer(local, slo_s=args.slo, capacity_rb_per_s=args.capacity_rb)
+        server = serving.ContinuousServer(local, slo_s=args.slo, capacity_rb_per_s=args.capacity_rb,
+                                          blocks_per_sm=args.service_blocks_per_sm,
+                                          reserve_blocks=args.service_reserve_blocks)
     else:
         server = serving.Server(local, max_inflight=args.max_inflight, policy=args.policy,
                                 max_batch_rays=args.max_batch_rays, late_tail=args.late_tail,

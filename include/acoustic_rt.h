@@ -370,6 +370,9 @@ typedef struct {
     int32_t stack_entries;       /* traversal stack entries per lane (0: 32); a job whose scene needs more
                                     (bvh_stack_need) is refused at submit */
     int64_t idle_timeout_ns;     /* 0: 20 ms */
+    int32_t reserve_blocks;      /* grid = blocks_per_sm * SMs - reserve_blocks: the SMs left one block short
+                                    keep room for other kernels (band synthesis) beside the persistent launch */
+    int32_t reserved;
 } ac_service_config;
 typedef struct {
     int64_t submitted;           /* jobs submitted so far (next sequence number) */
