@@ -119,7 +119,8 @@ class ACServiceConfig(ctypes.Structure):
 
 class ACServiceStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_int64), ("in_flight", ctypes.c_int64), ("launches", ctypes.c_int64),
-                ("running_launches", ctypes.c_int32), ("grid_blocks", ctypes.c_int32), ("capacity", ctypes.c_int64)]
+                ("running_launches", ctypes.c_int32), ("grid_blocks", ctypes.c_int32), ("capacity", ctypes.c_int64),
+                ("warps_alive", ctypes.c_int64), ("warps_waiting", ctypes.c_int64)]
 
 
 class ACServiceJobState(ctypes.Structure):

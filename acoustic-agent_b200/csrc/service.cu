@@ -34,7 +34,7 @@
 namespace {
 
 constexpr int kMaxLaunches = 2;
-constexpr int kLaunchWords = 48;   // three counters, one 128-byte line each
+constexpr int kLaunchWords = 64;   // three counters and the closing flag, one 128-byte line each
 
 struct Launch {
     cudaStream_t stream = nullptr;
@@ -360,7 +360,17 @@ extern "C" int ac_service_info(ac_service_t s, ac_service_stats *stats) {
     stats->in_flight = static_cast<int64_t>(s->inflight.size());
     stats->launches = s->launches_started;
     int32_t alive = 0;
-    for (const Launch &l : s->launches) alive += l.alive ? 1 : 0;
+    stats->warps_alive = 0;
+    stats->warps_waiting = 0;
+    for (const Launch &l : s->launches) {
+        if (!l.alive) continue;
+        alive += 1;
+        unsigned long long words[kLaunchWords];
+        AC_CUDA_TRY(cudaMemcpyAsync(words, l.words, sizeof(words), cudaMemcpyDeviceToHost, s->copy_stream));
+        AC_CUDA_TRY(cudaStreamSynchronize(s->copy_stream));
+        stats->warps_alive += static_cast<int64_t>(words[0]);
+        stats->warps_waiting += static_cast<int64_t>(words[16]);
+    }
     stats->running_launches = alive;
     stats->capacity = s->capacity;
     stats->grid_blocks = s->grid;

@@ -138,7 +138,8 @@ struct FastTable {
     unsigned long long *published_copy;  // device: the published count as last read from the host
     unsigned long long *refresh_at;      // device: %globaltimer time at which the copy is read again
     unsigned long long *launch_words;    // device, this launch's own: [0] warps alive, [16] warps waiting for
-                                         // work, [32] %globaltimer time at which a warp last began to wait
+                                         // work, [32] %globaltimer time at which a warp last began to wait,
+                                         // [48] nonzero once the launch is closing
     int64_t window_first;                // this launch takes jobs from this sequence number
     int64_t window_end;                  // to below this one only
     int64_t idle_ns;                     // and ends once its warps found no work for this long
@@ -181,13 +182,16 @@ constexpr unsigned long long kServiceRetryNs = 4000;   // a warp with live lanes
 //    while it holds rays.
 //  * kTakeEnd: the launch should end for this warp -- the whole launch has had nothing to trace for
 //    `idle_ns` (every warp alive is waiting, the latest for longer than that), or the launch's window of
-//    sequence numbers is used up.  Warps leave together, so a launch never shrinks to a few warps that
-//    happened to hold rays through a lull while the host, seeing it alive, starts no other.
+//    sequence numbers is used up.  The first warp to find the launch idle marks it closing, and from then
+//    on no warp of it takes work, so the launch ends whole: it never shrinks to the few warps that happened
+//    to find a job arriving as the others left, while the host, seeing it alive, starts no other.  Jobs
+//    published meanwhile go to the next launch.
 // Every wait is bounded: the idle deadline, and a poll cap.
 __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, int64_t &queue, int64_t &published,
                                             int64_t *seq_out, int64_t *chunk_out) {
     unsigned long long *const alive = t.launch_words, *const waiting = t.launch_words + 16,
-                              *const last_wait = t.launch_words + 32;
+                              *const last_wait = t.launch_words + 32, *const closing = t.launch_words + 48;
+    if (*reinterpret_cast<volatile unsigned long long *>(closing)) return kTakeEnd;
     unsigned long long idle_from = 0;
     unsigned sleep_ns = 256;
     bool rescanned = false, counted = false;   // counted: this warp is in the launch's waiting count
@@ -227,6 +231,7 @@ __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, i
             }
         }
         if (queue >= t.window_end) return leave(kTakeEnd);
+        if (*reinterpret_cast<volatile unsigned long long *>(closing)) return leave(kTakeEnd);
         const long long pub = service_published(t);
         if (pub > published) {
             published = pub;
@@ -247,8 +252,10 @@ __device__ __forceinline__ int service_take(const FastTable &t, bool may_wait, i
         if (now - idle_from > limit &&
             *reinterpret_cast<volatile unsigned long long *>(waiting) >=
                 *reinterpret_cast<volatile unsigned long long *>(alive) &&
-            now - *reinterpret_cast<volatile unsigned long long *>(last_wait) > limit)
+            now - *reinterpret_cast<volatile unsigned long long *>(last_wait) > limit) {
+            atomicExch(closing, 1ull);   // the launch is idle: it ends whole
             return leave(kTakeEnd);
+        }
         __nanosleep(sleep_ns);
         if (sleep_ns < 32768) sleep_ns <<= 1;
     }

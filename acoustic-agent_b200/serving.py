@@ -508,8 +508,10 @@ class ContinuousServer:
 
     Admission: a request is admitted when its device footprint fits the HBM budget (resident scenes plus the
     outputs of requests in flight); one that could never fit is rejected.  With `slo_s`, a request is also
-    rejected at arrival when the traced work already admitted or waiting ahead of it would take longer than
-    `slo_s` at the service's throughput: overload is shed instead of queueing without bound.  The throughput
+    rejected at arrival when the traced work already admitted or waiting ahead of it, plus its own, would take
+    longer than `slo_s` at the service's throughput (never while nothing is ahead of it); work is estimated
+    from each scene's measured ray-bounces per ray: overload is shed instead of queueing without bound.  The
+    throughput
     is `capacity_rb_per_s` ray-bounces/s (about the served rate under overload) until the
     server has run saturated -- at least a quarter second of work ahead -- for a second; from then on, the
     rate measured while saturated (a rate measured while the device idles between requests would understate
@@ -537,6 +539,7 @@ class ContinuousServer:
         self.capacity_rb_per_s = float(capacity_rb_per_s)
         self.in_use = 0
         self.bounces_per_ray = 40.0      # running estimate of ray-bounces per ray, from finished jobs
+        self.scene_bounces: dict[str, float] = {}   # the same per scene (by workload name) once one finished
         self._sizer = Server.__new__(Server)   # footprint arithmetic shared with the batch server
         self._sizer.scenes, self._sizer.late_tail = self.scenes, False
 
@@ -551,8 +554,9 @@ class ContinuousServer:
             self.scenes.evict_idle(self.scenes.resident_bytes() + self.in_use + need - self.budget)
         return self.scenes.resident_bytes() + self.in_use + need <= self.budget
 
-    def _est_rb(self, specs: Sequence[runtime.TraceSpec]) -> float:
-        return sum(min(float(s.num_bounces), self.bounces_per_ray) * s.num_rays for s in specs)
+    def _est_rb(self, specs: Sequence[runtime.TraceSpec], scene: str | None = None) -> float:
+        per_ray = self.scene_bounces.get(scene, self.bounces_per_ray) if scene is not None else self.bounces_per_ray
+        return sum(min(float(s.num_bounces), per_ray) * s.num_rays for s in specs)
 
     def _admit(self, req: Request, specs: list[runtime.TraceSpec], need: int, now: float) -> _Live:
         scene = self.scenes.acquire(req.workload, specs[0])
@@ -563,7 +567,8 @@ class ContinuousServer:
             self.scenes.release(req.workload)
             raise
         self.in_use += need
-        return _Live(req, specs, scene, buffers, seqs, set(seqs), need, now, self._est_rb(specs))
+        return _Live(req, specs, scene, buffers, seqs, set(seqs), need, now,
+                     self._est_rb(specs, req.workload.name))
 
     def _synthesize(self, lives: list[_Live]) -> None:
         """Band IRs of requests whose traces are done: one ragged synthesis and one host copy per request."""
@@ -619,10 +624,14 @@ class ContinuousServer:
                     continue
                 if self.slo_s is not None:
                     rate = sat_rb / sat_s if sat_s >= 1.0 and sat_rb > 0 else self.capacity_rb_per_s
-                    wait = (outstanding_rb + sum(self._est_rb(w[1]) for w in waiting)) / rate
+                    # its latency is about the work ahead plus its own (the ring is served roughly in order);
+                    # a request is never shed while nothing is ahead of it
+                    ahead = outstanding_rb + sum(self._est_rb(w[1], w[0].workload.name) for w in waiting)
+                    wait = (ahead + self._est_rb(specs, req.workload.name)) / rate if ahead > 0 else 0.0
                     if wait > self.slo_s:
                         results.append(Result(req, [], 0, t, t, error=f"overloaded: about {wait:.2f} s of traced work "
-                                                                       f"ahead exceeds the {self.slo_s:g} s limit"))
+                                                                       f"(ahead of it and its own) exceeds the "
+                                                                       f"{self.slo_s:g} s limit"))
                         continue
                 waiting.append((req, specs, need))
             # admission in arrival order while memory allows; the ring may ask us to come back later
@@ -654,6 +663,9 @@ class ContinuousServer:
                     rb = sum(int(b.counters[2].item()) for b in live.buffers)
                     rays = sum(s.num_rays for s in live.specs)
                     self.bounces_per_ray = 0.8 * self.bounces_per_ray + 0.2 * rb / max(rays, 1)
+                    name = live.request.workload.name
+                    seen = self.scene_bounces.get(name)
+                    self.scene_bounces[name] = rb / max(rays, 1) if seen is None else 0.7 * seen + 0.3 * rb / max(rays, 1)
                     if saturated:
                         sat_rb += rb
                     outstanding_rb -= live.est_ray_bounces

@@ -381,6 +381,8 @@ typedef struct {
     int32_t running_launches;
     int32_t grid_blocks;
     int64_t capacity;
+    int64_t warps_alive;         /* warps of the running launches that may still take work */
+    int64_t warps_waiting;       /* of those, the ones waiting for work */
 } ac_service_stats;
 /* Progress of one submitted job, for monitoring (a job that stops moving is
  * visible here): the counters are read from the device while launches run. */
