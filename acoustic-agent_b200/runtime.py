@@ -428,6 +428,10 @@ class _StagedWorkspace:
         assert self.device_buffer is not None and self.host_buffer is not None
         return self.device_buffer.data_ptr(), self.device_buffer.numel(), self.host_buffer.data_ptr()
 
+    def idle(self) -> bool:
+        """True when the staging may be rewritten without waiting (its last launch has run)."""
+        return self._copied is None or self._copied.query()
+
     def launched(self, stream: torch.cuda.Stream | None) -> None:
         if torch.cuda.is_current_stream_capturing():
             return

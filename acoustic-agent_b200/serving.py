@@ -70,6 +70,7 @@ class Result:
     admitted_s: float
     done_s: float
     error: str | None = None            # set when the request was rejected (its band_irs are empty)
+    traced_s: float | None = None       # when its last job's trace was complete (continuous server)
 
     @property
     def latency_s(self) -> float:
@@ -96,6 +97,16 @@ class Report:
     def latency_ms(self, q: float) -> float:
         lat = np.array([r.latency_s for r in self.results if r.error is None]) * 1e3
         return float(np.percentile(lat, q)) if lat.size else float("nan")
+
+    def phase_ms(self, q: float) -> dict[str, float]:
+        """Percentile `q` of arrival -> admitted, admitted -> traced and traced -> band IRs on the host."""
+        served = [r for r in self.results if r.error is None and r.traced_s is not None]
+        if not served:
+            return {}
+        parts = {"queued": [r.admitted_s - r.request.arrival_s for r in served],
+                 "traced": [r.traced_s - r.admitted_s for r in served],
+                 "synthesized": [r.done_s - r.traced_s for r in served]}
+        return {k: float(np.percentile(np.array(v) * 1e3, q)) for k, v in parts.items()}
 
     def summary(self) -> dict[str, Any]:
         return {
@@ -489,6 +500,7 @@ class _Live:
     bytes: int
     admitted_s: float
     est_ray_bounces: float
+    predicted_s: float = 0.0            # admission to traced, as predicted when it was admitted
     irs: list[torch.Tensor] = field(default_factory=list)
     host: torch.Tensor | None = None
     done: torch.cuda.Event | None = None
@@ -510,8 +522,9 @@ class ContinuousServer:
     outputs of requests in flight); one that could never fit is rejected.  With `slo_s`, a request is also
     rejected at arrival when the traced work already admitted or waiting ahead of it, plus its own, would take
     longer than `slo_s` at the service's throughput (never while nothing is ahead of it); work is estimated
-    from each scene's measured ray-bounces per ray: overload is shed instead of queueing without bound.  The
-    throughput
+    from each scene's measured ray-bounces per ray, and the prediction is scaled by the running ratio of
+    measured to predicted times from admission to traced: overload is shed instead of queueing without
+    bound.  The throughput
     is `capacity_rb_per_s` ray-bounces/s (about the served rate under overload) until the
     server has run saturated -- at least a quarter second of work ahead -- for a second; from then on, the
     rate measured while saturated (a rate measured while the device idles between requests would understate
@@ -522,7 +535,7 @@ class ContinuousServer:
 
     def __init__(self, device: int = 0, *, hbm_budget: int | None = None, tune: bool = True,
                  slo_s: float | None = None, capacity_rb_per_s: float = 2.6e9, blocks_per_sm: int = 3,
-                 capacity: int = 4096, idle_timeout_s: float = 0.02, chunk_rays: int = 0,
+                 capacity: int = 16384, idle_timeout_s: float = 0.02, chunk_rays: int = 0,
                  reserve_blocks: int = 16) -> None:
         self.dev = runtime.require_cuda(device)
         if hbm_budget is None:
@@ -534,12 +547,18 @@ class ContinuousServer:
                                             chunk_rays=chunk_rays, idle_timeout_s=idle_timeout_s,
                                             reserve_blocks=reserve_blocks)
         self.synth_stream = torch.cuda.Stream(self.dev)
-        self.synth_ws = runtime.SynthBatchWorkspace(self.dev)
+        # synthesis workspaces in rotation: a workspace's staging is free once its last batch has run, and
+        # waiting for that on the host would stop admission and polling while synthesis queues for SM room
+        self.synth_pool: list[runtime.SynthBatchWorkspace] = []
         self.slo_s = slo_s
         self.capacity_rb_per_s = float(capacity_rb_per_s)
         self.in_use = 0
         self.bounces_per_ray = 40.0      # running estimate of ray-bounces per ray, from finished jobs
         self.scene_bounces: dict[str, float] = {}   # the same per scene (by workload name) once one finished
+        # measured / predicted time from admission to traced (running mean over requests whose prediction was
+        # at least a quarter second): corrects the work-over-rate prediction for what it leaves out (the
+        # sharing of the device with the synthesis, the order in which warps take jobs)
+        self.latency_scale = 1.0
         self._sizer = Server.__new__(Server)   # footprint arithmetic shared with the batch server
         self._sizer.scenes, self._sizer.late_tail = self.scenes, False
 
@@ -570,6 +589,15 @@ class ContinuousServer:
         return _Live(req, specs, scene, buffers, seqs, set(seqs), need, now,
                      self._est_rb(specs, req.workload.name))
 
+    def _synth_workspace(self, limit: int = 16) -> runtime.SynthBatchWorkspace:
+        for ws in self.synth_pool:
+            if ws.idle():
+                return ws
+        if len(self.synth_pool) < limit:
+            self.synth_pool.append(runtime.SynthBatchWorkspace(self.dev))
+            return self.synth_pool[-1]
+        return self.synth_pool[0]   # all busy: this one waits for its last batch
+
     def _synthesize(self, lives: list[_Live]) -> None:
         """Band IRs of requests whose traces are done: one ragged synthesis and one host copy per request."""
         synth = []
@@ -588,7 +616,7 @@ class ContinuousServer:
                                                   speed_of_sound=s.speed_of_sound))
                 live.host = torch.empty(store.shape, dtype=torch.float32, pin_memory=True)
                 live.keep = store    # type: ignore[attr-defined]
-            runtime.synthesize_batch(synth, self.synth_ws, stream=self.synth_stream)
+            runtime.synthesize_batch(synth, self._synth_workspace(), stream=self.synth_stream)
             for live in lives:
                 live.host.copy_(live.keep, non_blocking=True)   # type: ignore[attr-defined]
                 live.done = torch.cuda.Event()
@@ -612,6 +640,7 @@ class ContinuousServer:
         while pending or waiting or tracing or synthesizing:
             now = clock()
             saturated = outstanding_rb >= 0.25 * self.capacity_rb_per_s
+            rate = sat_rb / sat_s if sat_s >= 1.0 and sat_rb > 0 else self.capacity_rb_per_s
             # arrivals: reject what can never fit, or what the admitted work would make miss its SLO
             while pending and pending[0].arrival_s <= now:
                 req = pending.popleft()
@@ -623,11 +652,11 @@ class ContinuousServer:
                                                                    f"the budget is {self.budget}"))
                     continue
                 if self.slo_s is not None:
-                    rate = sat_rb / sat_s if sat_s >= 1.0 and sat_rb > 0 else self.capacity_rb_per_s
-                    # its latency is about the work ahead plus its own (the ring is served roughly in order);
-                    # a request is never shed while nothing is ahead of it
+                    # its latency is about the work ahead plus its own (the ring is served roughly in order),
+                    # scaled by the measured / predicted ratio; a request is never shed while nothing is ahead
                     ahead = outstanding_rb + sum(self._est_rb(w[1], w[0].workload.name) for w in waiting)
-                    wait = (ahead + self._est_rb(specs, req.workload.name)) / rate if ahead > 0 else 0.0
+                    own = self._est_rb(specs, req.workload.name)
+                    wait = self.latency_scale * (ahead + own) / rate if ahead > 0 else 0.0
                     if wait > self.slo_s:
                         results.append(Result(req, [], 0, t, t, error=f"overloaded: about {wait:.2f} s of traced work "
                                                                        f"(ahead of it and its own) exceeds the "
@@ -648,6 +677,7 @@ class ContinuousServer:
                 waiting.popleft()
                 for seq in live.seqs:
                     tracing[seq] = live
+                live.predicted_s = (outstanding_rb + live.est_ray_bounces) / rate
                 outstanding_rb += live.est_ray_bounces
                 live_now += 1
                 peak = max(peak, self.in_use + self.scenes.resident_bytes())
@@ -660,7 +690,7 @@ class ContinuousServer:
                     finished.append(live)
             if finished:
                 for live in finished:
-                    rb = sum(int(b.counters[2].item()) for b in live.buffers)
+                    rb = int(torch.stack([b.counters[2] for b in live.buffers]).sum().item())   # one host read
                     rays = sum(s.num_rays for s in live.specs)
                     self.bounces_per_ray = 0.8 * self.bounces_per_ray + 0.2 * rb / max(rays, 1)
                     name = live.request.workload.name
@@ -668,6 +698,11 @@ class ContinuousServer:
                     self.scene_bounces[name] = rb / max(rays, 1) if seen is None else 0.7 * seen + 0.3 * rb / max(rays, 1)
                     if saturated:
                         sat_rb += rb
+                    live.traced_s = time.perf_counter() - t0    # type: ignore[attr-defined]
+                    if live.predicted_s >= 0.25:
+                        measured = live.traced_s - live.admitted_s   # type: ignore[attr-defined]
+                        sample = min(4.0, max(0.5, measured / live.predicted_s))
+                        self.latency_scale = 0.9 * self.latency_scale + 0.1 * sample
                     outstanding_rb -= live.est_ray_bounces
                     live.ray_bounces = rb     # type: ignore[attr-defined]
                 self._synthesize(finished)
@@ -681,7 +716,8 @@ class ContinuousServer:
                         irs.append(host[off:off + ir.numel()].reshape(ir.shape).copy())
                         off += ir.numel()
                     results.append(Result(live.request, irs, live.ray_bounces,   # type: ignore[attr-defined]
-                                          live.admitted_s, time.perf_counter() - t0))
+                                          live.admitted_s, time.perf_counter() - t0,
+                                          traced_s=live.traced_s))   # type: ignore[attr-defined]
                     self.scenes.release(live.request.workload)
                     self.in_use -= live.bytes
                     live_now -= 1

@@ -1216,6 +1216,7 @@ def run_serving(args) -> int:
                     "rejected": s["rejected"], "offered_rirs_per_s": sum(r.num_rirs for r in requests) / args.duration,
                     "rirs_per_s": s["rirs_per_s"], "ray_bounces_per_s": s["ray_bounces_per_s"],
                     "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
+                    "p50_phase_ms": report.phase_ms(50), "p99_phase_ms": report.phase_ms(99),
                     "max_requests_on_gpu": s["max_inflight"], "launches_or_batches": s["batches"]})
     if hasattr(server, "close"):
         server.close()
