@@ -107,8 +107,14 @@ def parity(ours: np.ndarray, ref: np.ndarray, bin_dur: float) -> dict:
     def rel(x, y):
         x, y = np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64)
         with np.errstate(divide="ignore", invalid="ignore"):
-            r = np.where(y != 0.0, np.abs(x - y) / np.abs(y), np.where(x == y, 0.0, np.inf))
+            r = np.where(x == y, 0.0, np.where((y != 0.0) & np.isfinite(y), np.abs(x - y) / np.abs(y), np.inf))
         return float(np.max(r))
+
+    def c50_db_diff(x, y):
+        # equal values (a band with no late energy has +inf in both) differ by 0
+        with np.errstate(invalid="ignore"):
+            d = np.where(x == y, 0.0, np.abs(x - y))
+        return float(np.max(d))
 
     ca, cb = c50(a, bin_dur), c50(b, bin_dur)
     return {
@@ -116,6 +122,6 @@ def parity(ours: np.ndarray, ref: np.ndarray, bin_dur: float) -> dict:
         "t30_rel": rel(t30(a, bin_dur), t30(b, bin_dur)),
         "edt_rel": rel(edt(a, bin_dur), edt(b, bin_dur)),
         "c50_rel": rel(10.0 ** (ca / 10.0), 10.0 ** (cb / 10.0)),
-        "c50_db": float(np.max(np.abs(ca - cb))),
+        "c50_db": c50_db_diff(ca, cb),
         "band_energy_rel": rel(np.sum(a, axis=1), np.sum(b, axis=1)),
     }

@@ -219,3 +219,20 @@ def test_batch_queue_rejects_null_arguments_without_a_device():
     assert lib.ac_batch_wait(None) == _lib.AC_ERR_INVALID
     assert lib.ac_batch_release(None) == _lib.AC_OK
     assert lib.ac_batch_submit(None, 0, None, None, 0, None, None, None) == _lib.AC_ERR_INVALID
+
+
+def test_parity_metrics_treat_equal_infinite_c50_as_equal():
+    """A band with no energy after 50 ms has C50 = +inf in both echograms: no difference, not NaN."""
+    import warnings
+    from acoustic_agent_b200 import metrics
+    e = np.zeros((2, 100))
+    e[0, :3] = [1.0, 0.5, 0.25]           # band 0: all energy in the first 50 ms
+    e[1, :60] = np.exp(-np.arange(60) / 10.0)
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        same = metrics.parity(e, e, 0.01)
+    assert same["c50_db"] == 0.0 and same["c50_rel"] == 0.0 and same["edc_err_db_max"] == 0.0
+    late = e.copy()
+    late[0, 10] = 0.01                      # band 0 now has late energy: a finite C50 against +inf
+    assert metrics.parity(late, e, 0.01)["c50_db"] == np.inf
+    assert metrics.parity(late, e, 0.01)["c50_rel"] == np.inf
