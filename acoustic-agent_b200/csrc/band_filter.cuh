@@ -48,6 +48,7 @@ constexpr int kPrefetch = AC_SYNTH_PREFETCH;
 constexpr int kSkew = AC_SYNTH_SKEW;  // iterations between consecutive sections
 constexpr int kLag = kSkew * 3;  // section 3 runs kLag samples behind section 0
 static_assert(kSkew >= 3 && kLag + 2 <= kPrefetch, "the prefetch window must hold the lagged input");
+static_assert(kPrefetch >= 2, "section 0 reads its input two samples ahead");
 
 // Lane (unit, chain, stage): section `stage` works on sample it - kSkew*stage.
 // The float32 output it produces at iteration it is shuffled one lane up at
@@ -92,14 +93,17 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
     }
     // q[d]: the value the previous section produced at iteration it - 1 - d (received through the
     // shuffle issued one iteration after it was produced, so no shuffle result is used in the
-    // iteration that receives it); q[kSkew - 2] is this section's input at the next iteration.
-    float q[kSkew - 1];
+    // iteration that receives it); q[kSkew - 3] is this section's input two iterations ahead.
+    float q[kSkew - 2];
 #pragma unroll
-    for (int i = 0; i < kSkew - 1; ++i) q[i] = 0.0f;
+    for (int i = 0; i < kSkew - 2; ++i) q[i] = 0.0f;
     float y1f = 0.0f, y2f = 0.0f;   // this lane's float outputs of iterations it - 1 and it - 2
     float lower2 = 0.0f;            // the lower chain's output of iteration it - 2
-    // input part of the first sample (its input is ahead[0] for section 0 and +0.0 otherwise)
+    // input parts of the first two samples (their inputs are ahead[0], ahead[1] for section 0 and +0.0 for the
+    // later sections); each iteration then forms the input part two samples ahead, so that its dependent
+    // chain (conversion, products, sums) has a whole iteration to complete before the recursion needs it
     double v = sec.feed(is_first ? ahead[0] : 0.0);
+    double v_next = sec.feed(is_first ? ahead[1] : 0.0);
     for (int base = 0; base < iterations; base += kPrefetch) {
         double next[kPrefetch];
         float emitted[kPrefetch];   // this chunk's outputs, written after the chunk (off the recursion's path)
@@ -116,13 +120,14 @@ __device__ __forceinline__ void filter_units(const double *x, float *out_row, in
             const float sent = __shfl_up_sync(full, y1f, 1);
             const float lower = __shfl_down_sync(full, y1f, 4);
 #pragma unroll
-            for (int i = kSkew - 2; i > 0; --i) q[i] = q[i - 1];
+            for (int i = kSkew - 3; i > 0; --i) q[i] = q[i - 1];
             q[0] = sent;
-            // input part of the next iteration: section 0 reads the prefetched signal, later
-            // sections the value their predecessor produced kSkew - 1 iterations before it
-            const double in_next =
-                is_first ? (u + 1 < kPrefetch ? ahead[u + 1] : next[0]) : static_cast<double>(q[kSkew - 2]);
-            v = sec.feed(in_next);
+            // input part of iteration it + 2: section 0 reads the prefetched signal, later sections the
+            // value their predecessor produced at it + 2 - kSkew, received at it - 1 (q[kSkew - 3])
+            const double in_2 = is_first ? (u + 2 < kPrefetch ? ahead[u + 2] : next[u + 2 - kPrefetch])
+                                         : static_cast<double>(q[kSkew - 3]);
+            v = v_next;
+            v_next = sec.feed(in_2);
             // output of iteration it - 2; x[it - 2 - kLag] is still in registers from the prefetch
             const int k = u - 2 - kLag;
             const double x_n = k >= 0 ? ahead[k] : prev[k + kPrefetch];
