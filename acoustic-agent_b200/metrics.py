@@ -1,6 +1,6 @@
 """Room-acoustic decay metrics on six-band echograms.
 
-Used to judge a trace against the float64 oracle when ray-by-ray identity is
+Used to compare a trace with the float64 oracle when ray-by-ray identity is
 not expected (float32 arithmetic, or a different random stream):
 
 * EDC: Schroeder backward integral of bin energies, in dB re the total

@@ -299,7 +299,7 @@ def cpu_reference(workload, steps: int, warmup: int, *, channel: int = 0, rays: 
             times.append(time.perf_counter() - t0)
         stats = res
     per_rir = float(np.mean(times))
-    # Algorithmic bytes per ray-bounce in the reference's traversal order (survey 8(d) definition):
+    # Algorithmic bytes per ray-bounce in the reference's traversal order:
     # nodes 32 B, walls 32 B, polygons 16 B + 8 B per edge, boxes 48 B, one 32 B material row per bounce.
     q = stats["closest_queries"]
     walls, polys, boxes = stats["prims_tested"]
