@@ -825,12 +825,31 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     bool exhausted = false;
     const int64_t num_chunks = kSingle ? (single.num_rays + table.chunk_rays - 1) / table.chunk_rays : table.num_chunks;
     int queue = 0;                  // batched launches: the group queue this warp takes chunks from
-    int64_t svc_queue = 0, svc_published = 0;   // service launches: next job to take chunks from, jobs seen
-    int cur_slot = 0;                            // service launches: the job of the chunk being handed out
-    unsigned long long retry_at = 0;             // service launches, lane 0: next ask while lanes are live
-    int count_slot = -1;                         // service launches: the job whose finished rays the warp
-    unsigned long long count_n = 0;              //   is counting, and how many it has not added yet
-    int64_t pending_begin = 0, pending_end = 0;
+    // Service launches: the warp's job-ring state lives in shared memory and is read where it is used, so it
+    // holds no registers across the traversal (every lane stores the same values).
+    struct ServiceWarp {
+        long long queue, published;            // next job to take chunks from, jobs seen published
+        long long pending_begin, pending_end;  // the ray range of a chunk of another scene, taken but not started
+        unsigned long long retry_at;           // lane 0: next ask while lanes are live
+        unsigned long long count_n;            // finished rays of job count_slot not yet added to its count
+        int cur_slot;                          // the job of the chunk being handed out
+        int count_slot;
+    };
+    __shared__ ServiceWarp service_warps[kService ? 8 : 1];
+    volatile ServiceWarp &sw = service_warps[kService ? (threadIdx.x >> 5) : 0];
+    volatile long long &svc_queue = sw.queue;
+    volatile long long &svc_published = sw.published;
+    volatile int &cur_slot = sw.cur_slot;
+    volatile unsigned long long &retry_at = sw.retry_at;
+    volatile int &count_slot = sw.count_slot;
+    volatile unsigned long long &count_n = sw.count_n;
+    volatile long long &pending_begin = sw.pending_begin;
+    volatile long long &pending_end = sw.pending_end;
+    if (kService) {
+        svc_queue = 0; svc_published = 0; cur_slot = 0; retry_at = 0; count_slot = -1; count_n = 0;
+        pending_begin = 0; pending_end = 0;
+        __syncwarp();
+    }
     if (kService) {
         long long pub = 0;
         if (lane_id == 0)
@@ -886,17 +905,20 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     const bool live = __any_sync(full, has);
                     long long seq = -1, chunk = 0;
                     int got = kTakeNone;
+                    int64_t wq = svc_queue, wp = svc_published;
                     if (lane_id == 0 && (!live || global_ns() >= retry_at)) {   // live warps ask every few us
                         int64_t sq = 0, ck = 0;
-                        got = service_take(table, !live, svc_queue, svc_published, &sq, &ck);
+                        got = service_take(table, !live, wq, wp, &sq, &ck);
                         if (got == kTakeChunk) { seq = sq; chunk = ck; }
                         if (got == kTakeNone) retry_at = global_ns() + kServiceRetryNs;
                     }
                     got = __shfl_sync(full, got, 0);
                     seq = __shfl_sync(full, seq, 0);
                     chunk = __shfl_sync(full, chunk, 0);
-                    svc_queue = __shfl_sync(full, static_cast<long long>(svc_queue), 0);
-                    svc_published = __shfl_sync(full, static_cast<long long>(svc_published), 0);
+                    wq = __shfl_sync(full, static_cast<long long>(wq), 0);
+                    wp = __shfl_sync(full, static_cast<long long>(wp), 0);
+                    svc_queue = wq;
+                    svc_published = wp;
                     if (got == kTakeEnd) {
                         if (lane_id == 0) atomicAdd(table.launch_words, ~0ull);   // takes no more work
                         exhausted = true;
@@ -907,7 +929,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     const ServiceSlot &sl = table.slots[slot];
                     const int64_t cb = chunk * sl.chunk_rays;
                     const int64_t ce = min(cb + sl.chunk_rays, sl.job.num_rays);
-                    if (group >= 0 && sl.scene_id != table.slots[group].scene_id) {
+                    if (group >= 0 && sl.scene_id != table.slots[group].scene_id) {   // (group: a slot index)
                         if (!__any_sync(full, has)) {
                             group = slot; cur_slot = slot; next = cb; end = ce;   // idle warp: switch scenes now
                         } else {
@@ -1272,28 +1294,35 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             // The warp counts its finished rays per job and adds them to the job's count once it holds no
             // more of that job's rays (or a ray of another job finishes first): one fence per run of a job
             // through the warp instead of one per iteration in which a ray ends.
+            int cs = count_slot;
+            unsigned long long cn = count_n;
             unsigned rest = ending;
             while (rest) {
                 const int j = __shfl_sync(full, s.job, __ffs(rest) - 1);
                 const unsigned grp = __ballot_sync(full, finished && s.job == j);
                 rest &= ~grp;
-                if (j != count_slot) {
-                    if (count_n && service_count(table, count_slot, count_n, lane_id))
-                        service_finish(table, count_slot, lane_id);
-                    count_slot = j;
-                    count_n = 0;
+                if (j != cs) {
+                    if (cn && service_count(table, cs, cn, lane_id)) service_finish(table, cs, lane_id);
+                    cs = j;
+                    cn = 0;
                 }
-                count_n += static_cast<unsigned long long>(__popc(grp));
+                cn += static_cast<unsigned long long>(__popc(grp));
             }
-            if (count_n && !__any_sync(full, has && s.job == count_slot) && !(cur_slot == count_slot && next < end)) {
-                if (service_count(table, count_slot, count_n, lane_id)) service_finish(table, count_slot, lane_id);
-                count_slot = -1;
-                count_n = 0;
+            if (cn && !__any_sync(full, has && s.job == cs) && !(cur_slot == cs && next < end)) {
+                if (service_count(table, cs, cn, lane_id)) service_finish(table, cs, lane_id);
+                cs = -1;
+                cn = 0;
             }
+            __syncwarp();   // every lane has read the old values
+            count_slot = cs;
+            count_n = cn;
         }
     }
-    if (kService && count_n && service_count(table, count_slot, count_n, lane_id))
-        service_finish(table, count_slot, lane_id);
+    if (kService) {
+        const int cs = count_slot;
+        const unsigned long long cn = count_n;
+        if (cn && service_count(table, cs, cn, lane_id)) service_finish(table, cs, lane_id);
+    }
 }
 
 }  // namespace ac
