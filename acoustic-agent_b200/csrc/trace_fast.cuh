@@ -818,13 +818,20 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     const int lane_id = threadIdx.x & 31;
     const unsigned lanes_below = (1u << lane_id) - 1u;
 
-    // Warp-uniform work state.
-    int group = -1;
-    int64_t next = 0, end = 0;
-    int64_t pending = -1;           // chunk of another scene, taken but not started
-    bool exhausted = false;
+    // Warp-uniform work state, kept in shared memory between iterations: each iteration loads it into locals
+    // for the refill and stores it back before the rays are traced, so it holds no registers (nor spill
+    // slots) during the traversal.  Every lane stores the same values.
+    struct WarpWork {
+        long long next, end;   // rays next .. end - 1 of the current chunk are not handed out yet
+        long long pending;     // chunk of another scene, taken but not started (-1: none)
+        int group;             // the scene group (service launches: the slot) the warp's lanes trace
+        int queue;             // batched launches: the group queue this warp takes chunks from
+        int exhausted;
+    };
+    __shared__ WarpWork warp_work[8];
+    volatile WarpWork &ww = warp_work[threadIdx.x >> 5];
+    ww.next = 0; ww.end = 0; ww.pending = -1; ww.group = -1; ww.queue = 0; ww.exhausted = 0;
     const int64_t num_chunks = kSingle ? (single.num_rays + table.chunk_rays - 1) / table.chunk_rays : table.num_chunks;
-    int queue = 0;                  // batched launches: the group queue this warp takes chunks from
     // Service launches: the warp's job-ring state lives in shared memory and is read where it is used, so it
     // holds no registers across the traversal (every lane stores the same values).
     struct ServiceWarp {
@@ -888,7 +895,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             const int mid = (lo + hi + 1) >> 1;
             if (__ldg(table.group_ray_begin + mid) <= at) lo = mid; else hi = mid - 1;
         }
-        queue = lo;
+        ww.queue = lo;
     }
 
     FastLane s;
@@ -896,6 +903,14 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     s.job = 0;
 
     while (true) {
+        int group = ww.group, queue = ww.queue;
+        int64_t next = ww.next, end = ww.end, pending = ww.pending;
+        bool exhausted = ww.exhausted != 0;
+        auto save = [&]() {   // after every lane has read the old values
+            __syncwarp();
+            ww.group = group; ww.queue = queue; ww.next = next; ww.end = end; ww.pending = pending;
+            ww.exhausted = exhausted ? 1 : 0;
+        };
         // ---- refill lanes from the warp's range; take more chunks of the same scene as needed
         unsigned need = __ballot_sync(full, !has);
         while (need && pending < 0 && !exhausted) {
@@ -1042,13 +1057,16 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                     group = ch.group; next = ch.begin; end = ch.end;
                 }
                 pending = -1;
+                save();
                 continue;
             }
             if (exhausted || next >= end) {
                 if (exhausted) break;
+                save();
                 continue;
             }
         }
+        save();
 
         const FastScene &fs = kSingle ? single_fast : (kService ? table.slots[group].fast : table.groups[group].fast);
         const Job<float> &job = kSingle ? single : (kService ? table.slots[s.job].job : table.jobs[s.job]);
@@ -1308,7 +1326,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 }
                 cn += static_cast<unsigned long long>(__popc(grp));
             }
-            if (cn && !__any_sync(full, has && s.job == cs) && !(cur_slot == cs && next < end)) {
+            if (cn && !__any_sync(full, has && s.job == cs) && !(cur_slot == cs && ww.next < ww.end)) {
                 if (service_count(table, cs, cn, lane_id)) service_finish(table, cs, lane_id);
                 cs = -1;
                 cn = 0;
