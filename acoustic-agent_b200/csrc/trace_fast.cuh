@@ -788,18 +788,24 @@ __device__ __forceinline__ void diffuse_direction_f(float s0, float s1, float s2
 }
 
 
+// A lane's ray in registers; its band energies, counters and ray number, which only the shading and the
+// completion use, live in shared memory (LaneShared) so that they hold no registers during the traversal.
 struct FastLane {
     float o[3];
     float d[3];
     float d0[3];  // initial direction (ambisonic coefficients)
-    float acc[kBands];
     double path;
-    int64_t ray;
     int job;
     int bounce;
-    int queries;
-    int shadows;
     int vslot;    // visual-candidate slot, -1 for none
+};
+
+// Per-lane shared state, entry-major ([entry][256]) so that a warp's lanes hit 32 different banks.
+struct LaneShared {
+    float acc[kBands][kStackStride];     // band energies
+    int queries[kStackStride];           // closest-hit queries of the ray so far
+    int shadows[kStackStride];           // shadow queries
+    long long ray[kStackStride];         // ray number within its job
 };
 
 __device__ __forceinline__ int find_job_range(const int64_t *prefix, int lo, int hi, int64_t g) {
@@ -899,6 +905,11 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
     }
 
     FastLane s;
+    __shared__ LaneShared lane_shared;
+    volatile float *const lane_acc = &lane_shared.acc[0][threadIdx.x];          // [b * kStackStride]
+    volatile int &lane_queries = lane_shared.queries[threadIdx.x];
+    volatile int &lane_shadows = lane_shared.shadows[threadIdx.x];
+    volatile long long &lane_ray = lane_shared.ray[threadIdx.x];
     bool has = false;
     s.job = 0;
 
@@ -1019,10 +1030,10 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 }
                 const Job<float> &job = kSingle ? single : (kService ? table.slots[j].job : table.jobs[j]);
                 s.job = j;
-                s.ray = ri;
+                lane_ray = ri;
                 s.bounce = 0;
-                s.queries = 0;
-                s.shadows = 0;
+                lane_queries = 0;
+                lane_shadows = 0;
                 s.path = 0.0;
                 if (kVisual) {
                     s.vslot = visual_slot(job, ri);
@@ -1038,7 +1049,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 }
                 if (kAmb) { s.d0[0] = s.d[0]; s.d0[1] = s.d[1]; s.d0[2] = s.d[2]; }
 #pragma unroll
-                for (int b = 0; b < kBands; ++b) s.acc[b] = 1.0f;
+                for (int b = 0; b < kBands; ++b) lane_acc[b * kStackStride] = 1.0f;
                 has = true;
                 if (job.num_bounces <= 0) {   // the host refuses such jobs in service launches
                     atomicAdd(job.counters + 1, 1ull);
@@ -1105,7 +1116,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 from_walk = true;
             }
             if (has) {
-                s.queries += 1;
+                lane_queries += 1;
                 bool dead = surf < 0 || t <= job.listener_radius || s.path > job.max_path_length;
                 if (!dead && s.bounce > 0) {
                     if (sphere_before(s.o, s.d, job.lst, job.listener_radius, t)) dead = true;
@@ -1125,7 +1136,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                         n[2] = __ldg(job.scene.normals + 3 * surf + 2);
                         if (n[0] * s.d[0] + n[1] * s.d[1] + n[2] * s.d[2] > 0.0f) { n[0] = -n[0]; n[1] = -n[1]; n[2] = -n[2]; }
                     }
-                    if (job.ray_surfaces) job.ray_surfaces[s.ray * job.num_bounces + s.bounce] = surf;
+                    if (job.ray_surfaces) job.ray_surfaces[lane_ray * job.num_bounces + s.bounce] = surf;
                     hx = s.o[0] + t * s.d[0] + 1e-2f * n[0];
                     hy = s.o[1] + t * s.d[1] + 1e-2f * n[1];
                     hz = s.o[2] + t * s.d[2] + 1e-2f * n[2];
@@ -1169,7 +1180,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
             const float refl[kBands] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y};
             const float scat = m1.z;
             if (need_shadow) {
-                s.shadows += 1;
+                lane_shadows += 1;
                 if (!occluded) {
                     const float diffuse = static_cast<float>(1.0 / kPi) * scat * facing;
                     float half[3];
@@ -1208,7 +1219,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
 #endif
 #pragma unroll
                         for (int b = 0; b < kBands; ++b) {
-                            const float e = common * refl[b] * s.acc[b];
+                            const float e = common * refl[b] * lane_acc[b * kStackStride];
                             if (kVisual) energy_sum += e;
                             const long long qe = quantize(e, job.energy_scale);
 #if AC_WARP_DEPOSIT
@@ -1258,17 +1269,17 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 }
             }
 #pragma unroll
-            for (int b = 0; b < kBands; ++b) s.acc[b] *= refl[b];
+            for (int b = 0; b < kBands; ++b) lane_acc[b * kStackStride] *= refl[b];
             s.path += static_cast<double>(t);
             s.o[0] = hx; s.o[1] = hy; s.o[2] = hz;
             bool use_diffuse;
             int sample;
             if (!kPhilox) {
-                const size_t k = static_cast<size_t>(s.bounce) * job.num_rays + s.ray;
+                const size_t k = static_cast<size_t>(s.bounce) * job.num_rays + lane_ray;
                 use_diffuse = job.diffuse_random[k] < scat;
                 sample = use_diffuse ? job.diffuse_indices[k] : 0;
             } else {
-                const u32x4 rr = trace_draw(job.seed, job.stream_key, static_cast<uint32_t>(s.ray),
+                const u32x4 rr = trace_draw(job.seed, job.stream_key, static_cast<uint32_t>(lane_ray),
                                             static_cast<uint32_t>(s.bounce) + 1u);
                 use_diffuse = u01_53(rr.x, rr.y) < static_cast<double>(scat);
                 sample = static_cast<int>(below(rr.z, static_cast<uint32_t>(job.num_bank)));
@@ -1294,9 +1305,9 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
         const unsigned ending = __ballot_sync(full, finished);
         if (finished) {
             const unsigned grp = __match_any_sync(ending, static_cast<unsigned>(s.job));
-            const unsigned q_sum = __reduce_add_sync(grp, static_cast<unsigned>(s.queries));
-            const unsigned q_max = __reduce_max_sync(grp, static_cast<unsigned>(s.queries));
-            const unsigned sh_sum = __reduce_add_sync(grp, static_cast<unsigned>(s.shadows));
+            const unsigned q_sum = __reduce_add_sync(grp, static_cast<unsigned>(lane_queries));
+            const unsigned q_max = __reduce_max_sync(grp, static_cast<unsigned>(lane_queries));
+            const unsigned sh_sum = __reduce_add_sync(grp, static_cast<unsigned>(lane_shadows));
             const unsigned alive_sum = __reduce_add_sync(grp, alive_at_end ? 1u : 0u);
             if (lane_id == __ffs(grp) - 1) {
                 atomicMax(job.counters + 0, static_cast<unsigned long long>(q_max));
@@ -1305,7 +1316,7 @@ __global__ void __launch_bounds__(256, AC_FAST_MIN_BLOCKS) trace_fast_kernel(con
                 if (sh_sum) atomicAdd(job.counters + 3, static_cast<unsigned long long>(sh_sum));
             }
             if (job.ray_surfaces)
-                for (int b = s.bounce; b < job.num_bounces; ++b) job.ray_surfaces[s.ray * job.num_bounces + b] = -1;
+                for (int b = s.bounce; b < job.num_bounces; ++b) job.ray_surfaces[lane_ray * job.num_bounces + b] = -1;
             has = false;
         }
         if (kService) {
