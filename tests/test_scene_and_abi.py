@@ -221,6 +221,34 @@ def test_batch_queue_rejects_null_arguments_without_a_device():
     assert lib.ac_batch_submit(None, 0, None, None, 0, None, None, None) == _lib.AC_ERR_INVALID
 
 
+def test_service_config_and_arguments_are_checked_before_any_cuda_call():
+    """ac_service_create refuses bad configurations (ring size, launch shape, stack depth, reserved blocks)
+    and the other service entry points refuse null handles, all before touching a device."""
+    import ctypes
+    from acoustic_agent_b200 import _lib
+    lib = _lib.load()
+    handle = ctypes.c_void_p()
+    bad = [dict(capacity=100), dict(capacity=32), dict(block_size=48), dict(block_size=512), dict(blocks_per_sm=9),
+           dict(stack_entries=33), dict(stack_entries=-1), dict(reserve_blocks=-1), dict(idle_timeout_ns=-1),
+           dict(chunk_rays=-5)]
+    for fields in bad:
+        cfg = _lib.ACServiceConfig()
+        for k, v in fields.items():
+            setattr(cfg, k, v)
+        assert lib.ac_service_create(ctypes.byref(cfg), ctypes.byref(handle)) == _lib.AC_ERR_INVALID, fields
+        assert not handle.value
+    assert lib.ac_service_create(None, ctypes.byref(handle)) == _lib.AC_ERR_INVALID
+    first = ctypes.c_int64()
+    assert lib.ac_service_submit(None, None, 0, ctypes.byref(first), None) == _lib.AC_ERR_INVALID
+    n = ctypes.c_int32()
+    assert lib.ac_service_poll(None, None, 0, ctypes.byref(n)) == _lib.AC_ERR_INVALID
+    state = _lib.ACServiceJobState()
+    assert lib.ac_service_inspect(None, 0, ctypes.byref(state)) == _lib.AC_ERR_INVALID
+    stats = _lib.ACServiceStats()
+    assert lib.ac_service_info(None, ctypes.byref(stats)) == _lib.AC_ERR_INVALID
+    assert lib.ac_service_destroy(None) == _lib.AC_OK
+
+
 def test_parity_metrics_treat_equal_infinite_c50_as_equal():
     """A band with no energy after 50 ms has C50 = +inf in both echograms: no difference, not NaN."""
     import warnings
