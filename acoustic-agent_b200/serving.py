@@ -501,7 +501,10 @@ class _Live:
     admitted_s: float
     est_ray_bounces: float
     predicted_s: float = 0.0            # admission to traced, as predicted when it was admitted
+    traced_s: float | None = None       # when its last job's trace was complete
+    ray_bounces: int = 0
     irs: list[torch.Tensor] = field(default_factory=list)
+    keep: torch.Tensor | None = None    # the device store of its band IRs until the host copy is done
     host: torch.Tensor | None = None
     done: torch.cuda.Event | None = None
 
@@ -615,10 +618,10 @@ class ContinuousServer:
                                                   direct_delay=max(0.0, float(s.direct_delay)),
                                                   speed_of_sound=s.speed_of_sound))
                 live.host = torch.empty(store.shape, dtype=torch.float32, pin_memory=True)
-                live.keep = store    # type: ignore[attr-defined]
+                live.keep = store
             runtime.synthesize_batch(synth, self._synth_workspace(), stream=self.synth_stream)
             for live in lives:
-                live.host.copy_(live.keep, non_blocking=True)   # type: ignore[attr-defined]
+                live.host.copy_(live.keep, non_blocking=True)
                 live.done = torch.cuda.Event()
                 live.done.record(self.synth_stream)
 
@@ -698,13 +701,13 @@ class ContinuousServer:
                     self.scene_bounces[name] = rb / max(rays, 1) if seen is None else 0.7 * seen + 0.3 * rb / max(rays, 1)
                     if saturated:
                         sat_rb += rb
-                    live.traced_s = time.perf_counter() - t0    # type: ignore[attr-defined]
+                    live.traced_s = time.perf_counter() - t0
                     if live.predicted_s >= 0.25:
-                        measured = live.traced_s - live.admitted_s   # type: ignore[attr-defined]
+                        measured = live.traced_s - live.admitted_s
                         sample = min(4.0, max(0.5, measured / live.predicted_s))
                         self.latency_scale = 0.9 * self.latency_scale + 0.1 * sample
                     outstanding_rb -= live.est_ray_bounces
-                    live.ray_bounces = rb     # type: ignore[attr-defined]
+                    live.ray_bounces = rb
                 self._synthesize(finished)
                 synthesizing.extend(finished)
             for live in list(synthesizing):
@@ -715,9 +718,8 @@ class ContinuousServer:
                     for ir in live.irs:
                         irs.append(host[off:off + ir.numel()].reshape(ir.shape).copy())
                         off += ir.numel()
-                    results.append(Result(live.request, irs, live.ray_bounces,   # type: ignore[attr-defined]
-                                          live.admitted_s, time.perf_counter() - t0,
-                                          traced_s=live.traced_s))   # type: ignore[attr-defined]
+                    results.append(Result(live.request, irs, live.ray_bounces, live.admitted_s,
+                                          time.perf_counter() - t0, traced_s=live.traced_s))
                     self.scenes.release(live.request.workload)
                     self.in_use -= live.bytes
                     live_now -= 1
