@@ -249,6 +249,22 @@ def test_service_config_and_arguments_are_checked_before_any_cuda_call():
     assert lib.ac_service_destroy(None) == _lib.AC_OK
 
 
+def test_tune_cache_persists_stack_choices(tmp_path):
+    """Scene choices, the stack depth and its per-depth timings included, survive a JSON round trip."""
+    from acoustic_agent_b200 import autotune
+    path = tmp_path / "tune.json"
+    cache = autotune.TuneCache(path)
+    choice = autotune.SceneChoice("bvh", 1, 0.5, 2, 12, ((12, 0.5), (16, 0.52), (32, 0.55)))
+    cache.put("abc", choice)
+    again = autotune.TuneCache(path)
+    assert again.get("abc") == choice
+    assert again.get("abc").options() == {"traversal": "bvh", "bvh_leaf": 1, "bvh_width": 2, "stack_entries": 12}
+    import json                             # an entry written before the stack knob existed still loads
+    path.write_text(json.dumps({"old": {"traversal": "hybrid", "bvh_leaf": 1, "ms": 1.0, "bvh_width": 2}}))
+    old = autotune.TuneCache(path)
+    assert old.get("old").stack_entries == 0 and old.get("old").stack_ms == ()
+
+
 def test_parity_metrics_treat_equal_infinite_c50_as_equal():
     """A band with no energy after 50 ms has C50 = +inf in both echograms: no difference, not NaN."""
     import warnings
