@@ -265,6 +265,19 @@ def test_tune_cache_persists_stack_choices(tmp_path):
     assert old.get("old").stack_entries == 0 and old.get("old").stack_ms == ()
 
 
+def test_launch_stack_depth_is_the_largest_scene_choice():
+    """A launch over several scenes takes the largest of their tuned depths; a BVH scene without a choice
+    (0) leaves the launch at the library's maximum; scan-only scenes need no stack."""
+    from types import SimpleNamespace
+    from acoustic_agent_b200 import runtime
+    bvh = lambda entries: SimpleNamespace(bvh_nodes=9, stack_entries=entries)   # noqa: E731
+    scan = SimpleNamespace(bvh_nodes=0, stack_entries=0)
+    assert runtime.launch_stack_entries([bvh(8), bvh(14), scan]) == 14
+    assert runtime.launch_stack_entries([bvh(8), bvh(0)]) == 0
+    assert runtime.launch_stack_entries([scan, scan]) == 0
+    assert runtime.launch_stack_entries([]) == 0
+
+
 def test_parity_metrics_treat_equal_infinite_c50_as_equal():
     """A band with no energy after 50 ms has C50 = +inf in both echograms: no difference, not NaN."""
     import warnings
