@@ -33,6 +33,7 @@
 // returns the lowest visited surface with t = 1e30 (steam_rt.py:4501).
 #pragma once
 
+#include "common.h"
 #include "fast_bvh.h"
 #include "trace_kernel.cuh"
 
